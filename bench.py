@@ -1,0 +1,331 @@
+#!/usr/bin/env python3
+"""Benchmark: Metropolis site-updates/s of the B200 sampler at L=232, q=21,
+2^20 walkers (the reference-sized inference workload).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step is one runMCMC call: `nsteps` single-site proposals for every walker
+at the shared site list (the reference's kernel call, mcmcGPU.py:460-482,
+whose throughput MCMCbenchmark reports as MC steps per second, Mi3.py:706-715).
+Synthetic data: a ground-truth Potts model with the workload's shape (fields
+N(0,1), couplings N(0,0.05^2) plus 3L strong contacts, fieldless-even gauge)
+and walkers started from independent-site sequences.
+
+Under torchrun each rank samples its own 2^20 walkers on its own GPU with a
+disjoint RNG span (walkers are independent; no collective on the data path),
+so scaling is weak; the step time is the max over ranks.
+
+--impl reference times the reference's CPU generator
+(extras/mcmcCPUgenThreaded.c, built into oracle/_ref) on the host cores with
+all available threads.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L_, Q_, N_ = 232, 21, 1 << 20
+METRIC = "site-updates/s"
+WORKLOAD = "metropolis L=232 q=21 walkers=2^20 (plain native sampler)"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU legs
+def cpu_generator_rate(J, L, q, seconds, procs, seed=0):
+    """Run the reference's CPU generator (one walker per process, P
+    processes) for about `seconds`; returns (updates/s, sample description)."""
+    from oracle import oracle
+    exe = oracle.ref_cpu_binary()
+    kind = "reference"
+    if exe is None:
+        return None
+    alpha = "ABCDEFGHIJKLMNOPQRSTUVWXYZ"[:q]
+    rng = np.random.default_rng(seed)
+    start = "".join(alpha[k] for k in rng.integers(0, q, size=L))
+    with tempfile.TemporaryDirectory() as td:
+        jf = Path(td) / "J.dat"
+        np.asarray(J, dtype="<f4").tofile(jf)
+        # calibrate on one process
+        probe = 200_000
+        t0 = time.perf_counter()
+        subprocess.run([str(exe), str(jf), str(probe), "1", alpha, start], check=True, stdout=subprocess.DEVNULL)
+        per = (time.perf_counter() - t0) / probe
+        steps = max(1000, int(seconds / max(per, 1e-12)))
+        t0 = time.perf_counter()
+        ps = [subprocess.Popen([str(exe), str(jf), str(steps), "1", alpha, start], stdout=subprocess.DEVNULL)
+              for _ in range(procs)]
+        for p in ps:
+            p.wait()
+        wall = time.perf_counter() - t0
+    rate = procs * steps / wall
+    sample = (f"extras/mcmcCPUgenThreaded.c (oracle/_ref/mcmc_cpu), {procs} processes x {steps} "
+              f"single-site updates at L={L} q={q}, {wall:.1f} s wall")
+    return rate, sample, kind
+
+
+# ------------------------------------------------------------ GPU arm
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from mi3gpu_b200 import MCMCGPU, GPU_node, _lib
+    from mi3gpu_b200.potts import synthetic_ground_truth
+
+    rank, world, local = env_rank()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local if world > 1 else 0)
+
+    L, q, N = args.L, args.q, args.walkers
+    J = synthetic_ground_truth(L, q, seed=1001)
+    gpu = MCMCGPU((dev, rank), L, q, N, 512, None, 1024, args.seed + 1)
+    gpus = GPU_node([gpu])
+    span = np.uint64(2 ** 63) // np.uint64(world)
+    gpus._initMCMC_rng(args.nsteps, [np.uint64(rank) * span], span)
+    # independent-site start (uniform marginals), generated on the device
+    gpus.prepare_indep(np.full((L, q), 1.0 / q))
+    gpus.gen_indep('main')
+    gpus.setBuf('J', J)
+    gpus.wait()
+
+    s = gpu.stream
+    kernel_ms = []
+
+    def step():
+        gpu.runMCMC()
+
+    # warm-up
+    for _ in range(args.warmup):
+        step()
+    gpus.wait()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(dev.index) as clk:
+        e0.record(s)
+        for k in range(args.steps):
+            evs[k][0].record(s)
+            step()
+            evs[k][1].record(s)
+        e1.record(s)
+        torch.cuda.synchronize(dev)
+    gpu._check_status()
+    ms = e0.elapsed_time(e1)
+    kernel_ms = [a.elapsed_time(b) for a, b in evs]
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    updates = float(N) * args.nsteps * args.steps * world
+    value = updates / (ms_max / 1e3)
+
+    # ---- end to end through the public API: J from pinned host memory each
+    # step (setBuf), the sampler call, and the packed sequences read back.
+    Jh = J.copy()
+    e2e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    ee0 = torch.cuda.Event(enable_timing=True)
+    ee1 = torch.cuda.Event(enable_timing=True)
+    ee0.record(s)
+    for _ in range(e2e_steps):
+        gpus.setBuf('J', Jh)
+        gpus.runMCMC()
+        fut = gpu.getBuf('seq main')
+        fut.event.synchronize()
+    ee1.record(s)
+    torch.cuda.synchronize(dev)
+    e2e_ms = ee0.elapsed_time(ee1)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = float(N) * args.nsteps * e2e_steps * world / (float(te.item()) / 1e3)
+    h2d = J.nbytes
+    d2h = gpu.SWORDS * N * 4
+
+    # ---- roofline of the sampler kernel
+    per_launch_ms = statistics.mean(kernel_ms)
+    upd_launch = float(N) * args.nsteps
+    hbm_bytes_per_update = 4 * ((L - 1) // 4 + 1)          # sequence words per update
+    onchip_bytes_per_update = 8 * (L - 1) + hbm_bytes_per_update  # 2 couplings per site + sequence words
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = upd_launch * hbm_bytes_per_update / (per_launch_ms / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "metropolis_L232_q21.md"
+    if tf.exists():
+        for line in tf.read_text().splitlines():
+            if line.startswith("dram_bytes_per_full_launch:"):
+                try:
+                    traffic = float(line.split(":")[1])
+                except ValueError:
+                    pass
+    # shared-memory load roofline: 148 SMs x 128 B/clk at the sampled clock
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    smem_peak = 148 * 128 * sm_mhz * 1e6 / 1e9
+    onchip = upd_launch * onchip_bytes_per_update / (per_launch_ms / 1e3) / 1e9
+
+    out = None
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (ground-truth Potts model of the workload's shape; independent-site start)",
+            "config": {"workload": WORKLOAD, "L": L, "q": q, "walkers_per_gpu": N, "nsteps_per_call": args.nsteps,
+                       "parallelism": f"walkers x{world} (independent RNG spans)",
+                       "l2": "inputs larger than L2 (sequence buffer 243 MB); couplings stay L2-resident by design"},
+            "e2e": {"value": e2e_value, "unit": "site-updates/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                    "path": "GPU_node.setBuf('J') + runMCMC() + MCMCGPU.getBuf('seq main') (pinned, packed words)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": traffic,
+                         "kernel": "k_metropolis",
+                         "algorithmic_bytes_per_update": hbm_bytes_per_update,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if pk.exists() else "fallback"},
+            "roofline_onchip": {"bound": "smem", "achieved": onchip, "peak": smem_peak, "unit": "GB/s",
+                                "frac": onchip / smem_peak, "bytes_per_update": onchip_bytes_per_update,
+                                "peak_basis": "148 SM x 128 B/clk x sampled SM clock"},
+            "kernel_ms_per_launch": per_launch_ms,
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+        }
+    return out, J
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nsteps", type=int, default=2048, help="MC steps per sampler call")
+    ap.add_argument("--L", type=int, default=L_)
+    ap.add_argument("--q", type=int, default=Q_)
+    ap.add_argument("--walkers", type=int, default=N_)
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    rank, world, _ = env_rank()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from mi3gpu_b200.potts import synthetic_ground_truth
+        J = synthetic_ground_truth(args.L, args.q, seed=1001)
+        procs = os.cpu_count() or 1
+        vals, sample, kind = [], "", "reference"
+        for k in range(args.warmup + args.steps):
+            r = cpu_generator_rate(J, args.L, args.q, max(1.0, args.cpu_seconds / 4), procs, seed=k)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference CPU generator not built (oracle/_ref)"}))
+                return
+            if k >= args.warmup:
+                vals.append(r[0])
+                sample, kind = r[1], r[2]
+        v = statistics.mean(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "site-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "L": args.L, "q": args.q},
+            "cpu_baseline": {"value": v, "unit": "site-updates/s", "cores": procs, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    out, J = run_gpu(args)
+    if rank == 0:
+        if not args.no_cpu:
+            r = cpu_generator_rate(J, args.L, args.q, args.cpu_seconds, os.cpu_count() or 1)
+            if r is not None:
+                out["cpu_baseline"] = {"value": r[0], "unit": "site-updates/s", "cores": os.cpu_count() or 1,
+                                       "kind": r[2], "sample": r[1]}
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,187 @@
+/*
+ * mi3b200.h -- C ABI of libmi3b200, the B200 (sm_100a) implementation of
+ * Mi3-GPU's inference inner loop (Metropolis sweeps, Potts energies,
+ * bimarginal counts, Zwanzig-reweighted quasi-Newton coupling update).
+ *
+ * Conventions
+ *   - Every pointer argument is a DEVICE pointer owned by the caller (for
+ *     example a PyTorch CUDA tensor), unless the comment says otherwise.
+ *   - Every call is asynchronous on the caller's stream (`stream` is a
+ *     cudaStream_t passed as void*; NULL means the legacy default stream).
+ *   - Every call returns 0 on success and a negative MI3_ERR_* code on a
+ *     rejected argument or a launch failure; mi3_last_error() then returns a
+ *     thread-local message.  No C++ exception crosses this boundary.
+ *   - Array layouts are the reference's (mi3gpu/mcmcGPU.py:173-184):
+ *       J, dJ, bi, bi target : (nPairs, q*q) float32, pair order (i<j) row
+ *                              major, residue index q*a+b
+ *       bicount              : (nPairs, q*q) uint32
+ *       seq                  : (SWORDS, buflen) uint32, SWORDS=(L-1)/4+1,
+ *                              byte k of word w = site 4w+k, walker-minor
+ *       rngstates            : (N, 4) uint32 = {x.s0, x.s1, c.s0, c.s1}, the
+ *                              memory image of mwc64xvec2_state_t ('<2u8')
+ *       E, weights, Bs       : (N,) float32
+ *   - The one layout that differs is the unpacked coupling table used by the
+ *     sampler ("Jrows"): L rows of L blocks of q*q floats, each row padded to
+ *     mi3_jrows_stride(L, q) floats, diagonal blocks zero.  The reference's
+ *     (L*L, q*q) Junpacked is the same table without the row padding.
+ *
+ * Each entry point names the reference interface it replaces as
+ * file:line in the reference tree (mi3gpu/...).
+ */
+#ifndef MI3B200_H
+#define MI3B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MI3_OK 0
+#define MI3_ERR_ARG (-1)       /* bad size, null pointer, unsupported shape   */
+#define MI3_ERR_CUDA (-2)      /* CUDA runtime / launch error                 */
+#define MI3_ERR_ALIGN (-3)     /* pointer not aligned as required             */
+#define MI3_ERR_WORKSPACE (-4) /* workspace too small                         */
+
+/* Status word values written by the sampler kernel (int32 in device memory). */
+#define MI3_STATUS_OK 0
+#define MI3_STATUS_TIMEOUT_FULL 1  /* consumer gave up waiting for a J chunk   */
+#define MI3_STATUS_TIMEOUT_EMPTY 2 /* producer gave up waiting for a free slot */
+#define MI3_STATUS_BAD_INPUT 3     /* a site index >= L in position_list       */
+
+/* Thread-local message for the last failed call on this host thread. */
+const char *mi3_last_error(void);
+/* ABI version of this library. */
+int mi3_abi_version(void);
+
+/* ---------------------------------------------------------------- sampler */
+
+/* initRNG2 (mcmc.cl:349-356) as launched by MCMCGPU._initMCMC_RNG
+ * (mcmcGPU.py:410-445): walker g, lane v gets the MWC64X stream at distance
+ * rng_offset + (2g+v)*walker_span. */
+int mi3_init_rng(uint32_t *rngstates, uint32_t nwalkers, uint64_t rng_offset,
+                 uint64_t walker_span, void *stream);
+
+/* Floats per row of the unpacked coupling table (see Conventions). */
+uint64_t mi3_jrows_stride(uint32_t L, uint32_t q);
+
+/* unpackfV (mcmc.cl:42-65) as launched by MCMCGPU.unpackJ
+ * (mcmcGPU.py:393-408), into the padded Jrows layout (diagonal zeroed).
+ * Jrows must hold L*mi3_jrows_stride(L,q) floats, 16-byte aligned. */
+int mi3_unpack_j(const float *J, float *Jrows, uint32_t L, uint32_t q, void *stream);
+
+/* metropolis + DeltaEnergy (mcmc.cl:360-458) as launched by MCMCGPU.runMCMC
+ * (mcmcGPU.py:460-482): nsteps single-site proposals per walker at the
+ * shared sites position_list[position_offset + i] (each < L; residues in
+ * seqmem must be < q -- the results are undefined otherwise, but no access
+ * leaves the caller's buffers).  betas may be NULL (then
+ * every walker uses `beta`, the reference's -DBETA macro; with betas given it
+ * is the -DTEMPERING build).  nseqs must be a multiple of 128.  *status
+ * (int32, device) receives MI3_STATUS_* if an internal bounded wait gave up;
+ * the caller zeroes it. */
+int mi3_metropolis(const float *Jrows, uint32_t *rngstates, uint32_t position_offset,
+                   const uint32_t *position_list, uint32_t nsteps, const float *betas,
+                   float beta, uint32_t *seqmem, uint32_t nseqs, uint32_t L, uint32_t q,
+                   int32_t *status, void *stream);
+
+/* gen_indep (mcmc.cl:170-244) as launched by MCMCGPU.gen_indep
+ * (mcmcGPU.py:380-390); cprob is (L, q-1) cumulative probabilities
+ * (MCMCGPU.prepare_indep, mcmcGPU.py:375-378). */
+int mi3_gen_indep(uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t *rngstates,
+                  const float *cprob, uint32_t L, uint32_t q, void *stream);
+
+/* --------------------------------------------------------------- energies */
+
+/* Bytes of workspace mi3_energies needs for nseq sequences. */
+size_t mi3_energies_workspace(uint32_t nseq);
+
+/* getEnergies (mcmc.cl:249-345) as launched by MCMCGPU.calcEnergies
+ * (mcmcGPU.py:536-553): E[n] = sum_{i<j} J[pair(i,j)][q*s_i+s_j] for the
+ * first nseq sequences of a buffer of row length buflen.  Accumulated in
+ * double and fixed point (deterministic), rounded once to float.  The
+ * workspace (device, >= mi3_energies_workspace(nseq) bytes, 8-byte aligned)
+ * is clobbered. */
+int mi3_energies(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
+                 float *energies, uint32_t L, uint32_t q, void *workspace, size_t ws_bytes,
+                 void *stream);
+
+/* ------------------------------------------------------------ bimarginals */
+
+/* countBivariate (mcmc.cl:462-516) as launched by MCMCGPU.calcBicounts
+ * (mcmcGPU.py:501-518): exact uint32 pair histograms. */
+int mi3_bicounts(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t *bicount,
+                 uint32_t L, uint32_t q, void *stream);
+
+/* bicounts_to_bimarg (mcmc.cl:518-528), MCMCGPU.bicounts_to_bimarg
+ * (mcmcGPU.py:520-534). */
+int mi3_bicounts_to_bimarg(const uint32_t *bicount, float *bimarg, uint32_t nseq, uint32_t L,
+                           uint32_t q, void *stream);
+
+/* weightedMarg (mcmc.cl:646-718), MCMCGPU.weightedMarg (mcmcGPU.py:634-661):
+ * unnormalised bi[pair][q*a+b] = sum_n w_n [s_i=a][s_j=b].  Reads the seq
+ * main layout directly (no transposed copy needed). */
+int mi3_weighted_marg(const float *weights, const uint32_t *seqmem, uint32_t buflen,
+                      uint32_t nseq, float *bimarg, uint32_t L, uint32_t q, void *stream);
+
+/* renormalize_bimarg (mcmc.cl:753-759), MCMCGPU.renormalize_bimarg
+ * (mcmcGPU.py:663-668), same summation tree as the reference. */
+int mi3_renormalize_bimarg(float *bimarg, uint32_t L, uint32_t q, void *stream);
+
+/* unpackseqs1T (mcmc.cl:124-168), MCMCGPU.repackseqs_T (mcmcGPU.py:356-373):
+ * (SWORDS, buf4len) words -> (L, buf1len) words, 4 walkers per word. */
+int mi3_repack_seqs_T(const uint32_t *seq4, uint32_t buf4len, uint32_t *seqL, uint32_t buf1len,
+                      uint32_t L, void *stream);
+
+/* ------------------------------------------------------ quasi-Newton step */
+
+/* updatedJ (mcmc.cl:829-843), MCMCGPU.updateJ (mcmcGPU.py:704-718):
+ * Jo = Ji - gamma*(bi_target - bi)/(bi + pc).  Ji may equal Jo. */
+int mi3_update_j(const float *bi_target, const float *bi, float gamma, float pc, const float *Ji,
+                 float *Jo, uint32_t L, uint32_t q, void *stream);
+
+/* reg_l1z (mcmc.cl:845-872), MCMCGPU.reg_l1z (mcmcGPU.py:720-731). */
+int mi3_reg_l1z(const float *bi, float gamma, float pc, float lJ, const float *J, float *dJ,
+                uint32_t L, uint32_t q, void *stream);
+
+/* reg_l2z (mcmc.cl:874-902), MCMCGPU.reg_l2z (mcmcGPU.py:733-745). */
+int mi3_reg_l2z(const float *bi, float gamma, float pc, float lJ, const float *J, float *dJ,
+                uint32_t L, uint32_t q, void *stream);
+
+/* minFloats (mcmc.cl:558-584), MCMCGPU.min_buf (mcmcGPU.py:555-567):
+ * *out = min(0, min(data)) (the reference's accumulator starts at 0). */
+int mi3_min_floats(const float *data, uint32_t len, float *out, void *stream);
+
+/* dE_to_weights (mcmc.cl:624-633), MCMCGPU.dE_to_weights (mcmcGPU.py:591-610):
+ * w = exp(-dE + ref_E). */
+int mi3_dE_to_weights(float ref_E, const float *dE, float *weights, uint32_t n, void *stream);
+
+/* fixed_beta_weights (mcmc.cl:635-644), MCMCGPU.fixed_beta_weights
+ * (mcmcGPU.py:613-632): w = exp((beta-1)*(E - ref_E)). */
+int mi3_fixed_beta_weights(float beta, float ref_E, const float *E, float *weights, uint32_t n,
+                           void *stream);
+
+/* Bytes of workspace mi3_weight_stats / mi3_weights_fused need. */
+size_t mi3_weight_stats_workspace(uint32_t n);
+
+/* weight_stats (mcmc.cl:586-622), MCMCGPU.weight_statistics
+ * (mcmcGPU.py:569-589): out2 = {sum w, sum w^2} as float; out2_f64 (may be
+ * NULL) receives the same sums in double.  Deterministic. */
+int mi3_weight_stats(const float *weights, uint32_t n, float *out2, double *out2_f64,
+                     void *workspace, size_t ws_bytes, void *stream);
+
+/* One pass of the Newton step's per-sequence work (NewtonSteps.py:226-231):
+ * weights = exp(-dE + ref_E), *minout = min(0, min dE), stats = {sum w,
+ * sum w^2} (float and double). */
+int mi3_weights_fused(float ref_E, const float *dE, float *weights, uint32_t n, float *minout,
+                      float *out2, double *out2_f64, void *workspace, size_t ws_bytes,
+                      void *stream);
+
+/* addFloatBufs (mcmc.cl:720-727), MCMCGPU.addFloatBuf (mcmcGPU.py:670-685). */
+int mi3_add_float_bufs(float *dst, const float *src, uint32_t n, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MI3B200_H */

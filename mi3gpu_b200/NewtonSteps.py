@@ -1,0 +1,335 @@
+"""Host quasi-Newton / MCMC driver: the reference's NewtonSteps module
+(mi3gpu/NewtonSteps.py) over the B200 device group.
+
+The control flow follows the reference function by function -- iterNewton
+(:159-268), runMCMC (:385-486), MCMCstep (:610-687), newtonMCMC (:689-767),
+NewtonSteps (:595-608), singleNewton (:109-124) -- and drives a GPU_node
+(node_manager.py) of MCMCGPU devices.  Differences from the reference:
+
+  * Neff comes from the FP64 weight sums ('weightstats64'), not from the
+    float32 sums the reference's weight_stats kernel produces.
+  * Output files are written only when param.outdir is set.
+  * Parallel tempering (runMCMC_tempered) is not provided; it does not run
+    in the reference either (undefined readGPUbufs / markSeqs / split).
+"""
+import time
+
+import numpy as np
+from scipy.stats import spearmanr
+
+from .potts import bimarg_stats, fieldlessGaugeEven, indepF, printsome
+
+
+class Param(dict):
+    """Attribute-style parameter dict (the reference's attrdict, Mi3.py:68-75)."""
+
+    def __getattr__(self, attr):
+        if attr.startswith('_'):
+            raise AttributeError(attr)
+        return self.get(attr)
+
+    def __setattr__(self, k, v):
+        self[k] = v
+
+
+def getNeff(w):
+    """Effective sample size (sum w)^2 / sum w^2 (NewtonSteps.py:126-130)."""
+    w = np.asarray(w, dtype=np.float64)
+    return (np.sum(w) ** 2) / np.sum(w ** 2)
+
+
+def printstats(name, jstep, bimarg_target, bimarg_model, couplings, energies, e_rho):
+    ferr, ssr, maxd = bimarg_stats(bimarg_target, bimarg_model)
+    ferr, maxd = ferr * 100, maxd * 100
+    C = bimarg_model - indepF(bimarg_model)
+    X = np.sum(couplings * C, axis=1)
+    Co = bimarg_target - indepF(bimarg_target)
+    Xo = np.sum(couplings * Co, axis=1)
+    X = f"{np.sum(X): 6.1f} ({np.sum(Xo): 6.1f})"
+    rhostr = '(none)'
+    if e_rho is not None:
+        rho = [r[0] for r in e_rho]
+        rhostr = np.array2string(np.array(rho), precision=2, floatmode='fixed', suppress_small=True)[1:-1]
+    lowE, meanE, stdE = np.min(energies), np.mean(energies), np.std(energies)
+    return (f"{name} {jstep: 6d} Error: SSR:{ssr:6.3f}   rel%:{ferr:5.2f}   max%:{maxd:5.2f}   X:{X}\n"
+            f"{name} bimarg: {printsome(bimarg_model)} ...\n"
+            f"{name}      J: {printsome(couplings)} ...\n"
+            f"{name} min(E) = {lowE:.4f}     mean(E) = {meanE:.4f}     std(E) = {stdE:.4f}\n"
+            f"{name} E Autocorr vs time: {rhostr}")
+
+
+def singleNewton(bimarg, gamma, param, gpus):
+    """One J update from the given bimarg (NewtonSteps.py:109-124).  As in the
+    reference, the update is applied to 'dJ' and the unchanged 'J' is read
+    back, so this is a no-op on J."""
+    pc = param.pcdamping
+    gpus.setBuf('bi', bimarg)
+    gpus.updateJ(gamma, pc)
+    return gpus.head_gpu.getBuf('J')[0].read()
+
+
+def iterNewton(param, bimarg_model, gpus, log, fused=False):
+    """Zwanzig-reweighted quasi-Newton steps until Neff < fracNeff*N
+    (NewtonSteps.py:159-268).  Returns (steps, trialJ, predicted bimarg).
+
+    fused=True replaces min_buf + dE_to_weights + weight_statistics by the
+    single-pass weights_fused kernel (same values)."""
+    bimarg_target = param.bimarg
+    gamma = param.gamma0
+    newtonSteps = param.newtonSteps
+    pc = param.pcdamping
+    Nfrac = param.fracNeff
+    N = param.nwalkers
+
+    log("")
+    log(f"Perturbation optimization for up to {newtonSteps} steps:")
+    if param.reg:
+        log(f"Using regularization {param.reg} ({param.regarg})")
+    s = time.time()
+
+    seqbuf, wbufname, ebufname, etmpname = 'main', 'weights', 'E main', 'E tmp'
+    if param.distribute_jstep not in (None, 'all'):
+        raise NotImplementedError("distribute_jstep other than 'all' needs the large sequence buffers")
+
+    gpus.calcEnergies(seqbuf)
+    gpus.calcBicounts(seqbuf)
+    gpus.bicounts_to_bimarg(seqbuf)
+    gpus.merge_bimarg()
+    gpus.fillBuf('dJ', 0)
+
+    N0 = N
+    ref_dE = 0.0
+    if param.beta is not None:
+        E = gpus.readBufs(ebufname)
+        beta_mod = [(-(param.beta - 1) * x).astype('<f4') for x in E]
+        dEB = np.concatenate(beta_mod)
+        ref_dE = np.min(dEB)
+        N0 = getNeff(np.exp(-(dEB - ref_dE)))
+        gpus.setBuf(etmpname, beta_mod)
+        log(f"Temperature reweight decreases Neff from {N} to {N0}")
+
+    lastNeff = 2 * N0
+    i = 0
+    for i in range(newtonSteps):
+        gpus.updateJ(gamma, pc)
+        if param.reg is not None:
+            gpus.reg(param.reg, (gamma, pc,) + tuple(param.regarg))
+        gpus.calcEnergies(seqbuf, 'dJ')
+        if param.beta is not None:
+            gpus.addFloatBuf(ebufname, etmpname)
+
+        if fused:
+            gpus.weights_fused(ref_dE, seqbuf)
+        else:
+            gpus.min_buf(ebufname)
+        mindE_fut = gpus.getBuf('minout')
+        if not fused:
+            gpus.dE_to_weights(seqbuf, ref_dE)  # ref_dE comes from the previous step
+            gpus.weight_statistics(seqbuf)
+        w_fut = gpus.getBuf('weightstats64')
+
+        gpus.weightedMarg(seqbuf)
+        gpus.merge_bimarg()
+
+        wsum, wsum2 = (np.sum(x) for x in zip(*(w.read() for w in w_fut)))
+        Neff = wsum ** 2 / wsum2
+        if i % 64 == 0 or abs(lastNeff - Neff) / N0 > 0.05 or Neff < Nfrac * N0:
+            log(f"J-step {i: 5d}   Neff: {Neff:.1f}   ({Neff / N0 * 100:.1f}% of {N0})")
+            lastNeff = Neff
+        if Neff < Nfrac * N0:
+            log(f"Ending coupling updates because Neff/N < {Nfrac:.2f}")
+            break
+        ref_dE = np.min([x.read()[()] for x in mindE_fut])
+
+    log(f"Performed {i} coupling update steps")
+
+    bi, J, dJ = gpus.head_gpu.readBufs(['bi', 'J', 'dJ'])
+    bimarg_model, trialJ = bi[0], J[0] + dJ[0]
+    weights = gpus.collect(wbufname)
+    gpus.setBuf('J', trialJ)
+    log(f"Predicted statistics after perturbing J: SSR {bimarg_stats(bimarg_target, bimarg_model)[1]:.4f}")
+
+    Neff = np.sum(weights)
+    if not np.isfinite(Neff) or Neff == 0:
+        raise Exception("Error: Divergence. Decrease gamma or increase pc-damping")
+    log(f"Total Newton-step running time: {time.time() - s:.1f} s")
+    gpus.logProfile()
+    return i, trialJ, bimarg_model
+
+
+def track_main_bufs(param, gpus, savedir=None, step=None):
+    gpus.calcBicounts('main')
+    gpus.calcEnergies('main')
+    bicounts, energies = gpus.collect(['bicount', 'E main'])
+    bimarg_model = bicounts.astype('f4') / np.float32(np.sum(bicounts[0, :]))
+    if savedir is not None:
+        if 'bim' in (param.tracked or ''):
+            np.save(savedir / f'bimarg_{step}', bimarg_model)
+        if 'E' in (param.tracked or ''):
+            np.save(savedir / f'energies_{step}', energies)
+    return energies, bimarg_model
+
+
+def runMCMC(gpus, couplings, runName, param, log):
+    """Equilibrate the walkers at `couplings` and measure their bimarginals
+    (NewtonSteps.py:385-486)."""
+    nloop = param.equiltime
+    trackequil = param.trackequil or 0
+    outdir = param.outdir
+    gpus.setBuf('J', couplings)
+
+    if nloop == 'auto':
+        equil_dir = None
+        if trackequil != 0 and outdir is not None:
+            equil_dir = outdir / runName / 'equilibration'
+            equil_dir.mkdir(parents=True, exist_ok=True)
+        loops = 8
+        for _ in range(loops):
+            gpus.runMCMC()
+        step = loops
+        equil_e = []
+        while True:
+            for _ in range(loops):
+                gpus.runMCMC()
+            step += loops
+            energies, _ = track_main_bufs(param, gpus, equil_dir, step)
+            equil_e.append(energies)
+            rstr = f"Step {step} <E>={np.mean(energies):.2f}. "
+            if len(equil_e) >= 3:
+                r1, p1 = spearmanr(equil_e[-1], equil_e[-2])
+                r2, p2 = spearmanr(equil_e[-1], equil_e[-3])
+                fmt = "({:.3f}, {:.2g}) ".format
+                rstr += f"r={fmt(r1, p1)} prev:{fmt(r2, p2)}"
+                if p1 > 0.02 and p2 > 0.02 and step >= (param.min_equil or 64):
+                    log(rstr + "Equilibrated.")
+                    break
+            if step >= (param.max_equil or 32768):
+                log(rstr + "Reached Max Steps. Stopping")
+                break
+            log(rstr + "Continuing.")
+            loops = loops * 2
+        e_rho = [spearmanr(ei, equil_e[-1]) for ei in equil_e]
+    elif trackequil == 0:
+        for _ in range(int(nloop)):
+            gpus.runMCMC()
+        step = int(nloop)
+        e_rho = None
+    else:
+        equil_dir = None
+        if outdir is not None:
+            equil_dir = outdir / runName / 'equilibration'
+            equil_dir.mkdir(parents=True, exist_ok=True)
+        equil_e = []
+        for j in range(int(nloop) // trackequil):
+            for _ in range(trackequil):
+                gpus.runMCMC()
+            energies, _ = track_main_bufs(param, gpus, equil_dir, j * trackequil)
+            equil_e.append(energies)
+        step = int(nloop)
+        e_rho = [spearmanr(ei, equil_e[-1]) for ei in equil_e]
+
+    if param.beta is None:
+        gpus.calcBicounts('main')
+        gpus.calcEnergies('main')
+        bicount, es = gpus.collect(['bicount', 'E main'])
+        bimarg_model = (bicount / np.sum(bicount[0, :])).astype('f4')
+    else:
+        log("Reweighting to account for modified temperature.")
+        gpus.calcEnergies('main')
+        es = gpus.collect('E main')
+        gpus.fixed_beta_weights(np.min(es), 'main')
+        gpus.weightedMarg('main')
+        bimarg_model = gpus.collect('bi')
+        bimarg_model /= np.sum(bimarg_model, axis=1, keepdims=True)
+        bicount = None
+    gpus.logProfile()
+    return bimarg_model, bicount, es, e_rho, None, step
+
+
+def NewtonSteps(runName, param, bimarg_model, gpus, log):
+    outdir = param.outdir
+    if param.newtonSteps != 1:
+        Jsteps, newJ, bimarg_p = iterNewton(param, bimarg_model, gpus, log, fused=bool(param.fused))
+        if outdir is not None:
+            np.save(outdir / runName / 'predictedBimarg', bimarg_p)
+            np.save(outdir / runName / 'perturbedJ', newJ)
+    else:
+        log("Performing single newton update step")
+        newJ = singleNewton(bimarg_model, param.gamma0, param, gpus)
+        Jsteps = 1
+    return Jsteps, newJ
+
+
+def MCMCstep(runName, Jstep, couplings, param, gpus, log):
+    """One round: re-gauge J, equilibrate, report, Newton-update
+    (NewtonSteps.py:610-687)."""
+    outdir = param.outdir
+    L, q = param.L, param.q
+    bimarg_target = param.bimarg
+
+    log("")
+    log(f"Gradient Descent step {runName}")
+    couplings = fieldlessGaugeEven(np.zeros((L, q)), couplings)[1].astype('<f4')
+    if outdir is not None:
+        rundir = outdir / runName
+        rundir.mkdir(parents=True, exist_ok=True)
+        np.save(rundir / 'J', couplings)
+        (rundir / 'newtonsteps').write_text(str(param.newtonSteps))
+        (rundir / 'jstep').write_text(str(Jstep))
+
+    start_time = time.time()
+    (bimarg_model, bicount, sampledenergies, e_rho, ptinfo,
+     equilsteps) = runMCMC(gpus, couplings, runName, param, log)
+    dt = time.time() - start_time
+    MC_s = equilsteps * param.nsteps * np.float64(gpus.nwalkers) / dt
+    log(f"Total MCMC running time: {dt:.1f} s    ({MC_s:.3g} MC/s)")
+
+    seqs = gpus.collect('seq main')
+    log(printstats(runName, Jstep, bimarg_target, bimarg_model, couplings, sampledenergies, e_rho))
+    if outdir is not None:
+        np.save(outdir / runName / 'seqs', seqs)
+
+    ns_delta = param.newton_delta or 32
+    ssr = np.sum((bimarg_target - bimarg_model) ** 2)
+    if param.last_ssr is not None:
+        if ssr > (param.last_ssr + param.min_ssr) / 2:
+            param.newtonSteps = max(ns_delta, param.newtonSteps - int(1.5 * ns_delta))
+            log(f"SSR increased over min. Decreasing newtonsteps to {param.newtonSteps}")
+    param.last_ssr = ssr
+    param.min_ssr = min(ssr, param.min_ssr if param.min_ssr is not None else np.inf)
+    param.history = (param.history or []) + [dict(run=runName, ssr=float(ssr), mcmc_s=dt, mc_per_s=MC_s)]
+
+    Jsteps, newJ = NewtonSteps(runName, param, bimarg_model, gpus, log)
+    param.newtonSteps = min(2048, Jsteps + ns_delta)
+    log(f"Increasing newtonsteps to {param.newtonSteps}")
+    return Jstep + Jsteps, seqs, sampledenergies, newJ
+
+
+def newtonMCMC(param, gpus, start_run, Jstep, log):
+    """Round loop (NewtonSteps.py:689-767) for the reseed strategies that
+    need no file input: 'independent', 'single_indep', 'single_best',
+    'single_random', 'none'."""
+    J = param.couplings
+    gpus.setBuf('bi target', param.bimarg)
+    param.max_newtonSteps = param.newtonSteps
+    param.min_ssr = np.inf
+    seqs, es = None, None
+    rng = np.random.RandomState(param.rngseed)
+    for i in range(start_run, param.mcmcsteps):
+        runname = f'run_{i:02d}'
+        seed = None
+        if param.seedseq is not None:
+            seed, param.seedseq = param.seedseq, None
+        elif param.reseed == 'single_indep':
+            f = param.unimarg
+            seed = np.array([rng.choice(param.q, p=f[k] / f[k].sum()) for k in range(param.L)], dtype='<u1')
+        elif param.reseed == 'single_random' and seqs is not None:
+            seed = seqs[rng.randint(0, seqs.shape[0])]
+        elif param.reseed == 'single_best' and seqs is not None:
+            seed = seqs[np.argmin(es)]
+        if seed is not None:
+            gpus.fillSeqs(seed)
+        elif param.reseed == 'independent':
+            gpus.gen_indep('main')
+        Jstep, seqs, es, J = MCMCstep(runname, Jstep, J, param, gpus, log)
+    return J

@@ -1,0 +1,81 @@
+"""ctypes binding of libmi3b200.so (the C ABI declared in include/mi3b200.h).
+
+The library is loaded from the package directory.  There is no fallback:
+if the shared library is missing or fails to load, every call raises.
+"""
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libmi3b200.so"
+
+c = ctypes
+_vp, _u32, _u64, _f32, _i32 = c.c_void_p, c.c_uint32, c.c_uint64, c.c_float, c.c_int32
+
+# name -> (restype, argtypes); mirrors include/mi3b200.h
+SIGNATURES = {
+    "mi3_last_error": (c.c_char_p, []),
+    "mi3_abi_version": (c.c_int, []),
+    "mi3_init_rng": (c.c_int, [_vp, _u32, _u64, _u64, _vp]),
+    "mi3_jrows_stride": (_u64, [_u32, _u32]),
+    "mi3_unpack_j": (c.c_int, [_vp, _vp, _u32, _u32, _vp]),
+    "mi3_metropolis": (c.c_int, [_vp, _vp, _u32, _vp, _u32, _vp, _f32, _vp, _u32, _u32, _u32, _vp, _vp]),
+    "mi3_gen_indep": (c.c_int, [_vp, _u32, _u32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_energies_workspace": (c.c_size_t, [_u32]),
+    "mi3_energies": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),
+    "mi3_bicounts": (c.c_int, [_vp, _u32, _u32, _vp, _u32, _u32, _vp]),
+    "mi3_bicounts_to_bimarg": (c.c_int, [_vp, _vp, _u32, _u32, _u32, _vp]),
+    "mi3_weighted_marg": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp]),
+    "mi3_renormalize_bimarg": (c.c_int, [_vp, _u32, _u32, _vp]),
+    "mi3_repack_seqs_T": (c.c_int, [_vp, _u32, _vp, _u32, _u32, _vp]),
+    "mi3_update_j": (c.c_int, [_vp, _vp, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_l1z": (c.c_int, [_vp, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_l2z": (c.c_int, [_vp, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_min_floats": (c.c_int, [_vp, _u32, _vp, _vp]),
+    "mi3_dE_to_weights": (c.c_int, [_f32, _vp, _vp, _u32, _vp]),
+    "mi3_fixed_beta_weights": (c.c_int, [_f32, _f32, _vp, _vp, _u32, _vp]),
+    "mi3_weight_stats_workspace": (c.c_size_t, [_u32]),
+    "mi3_weight_stats": (c.c_int, [_vp, _u32, _vp, _vp, _vp, c.c_size_t, _vp]),
+    "mi3_weights_fused": (c.c_int, [_f32, _vp, _vp, _u32, _vp, _vp, _vp, _vp, c.c_size_t, _vp]),
+    "mi3_add_float_bufs": (c.c_int, [_vp, _vp, _u32, _vp]),
+}
+
+
+class Mi3Error(RuntimeError):
+    """A libmi3b200 call returned an error code."""
+
+    def __init__(self, name, code, msg):
+        super().__init__(f"{name} failed ({code}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load():
+    """Load the shared library (raises if it is missing or incomplete)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"libmi3b200.so not built at {LIB_PATH}; run python -m mi3gpu_b200.build")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def call(name, *args):
+    """Call an int-returning entry point; raise Mi3Error on a negative code."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != 0:
+        msg = lib.mi3_last_error().decode(errors="replace")
+        raise Mi3Error(name, rc, msg)
+    return rc
+
+
+def query(name, *args):
+    """Call a value-returning entry point (sizes, strides)."""
+    return getattr(load(), name)(*args)

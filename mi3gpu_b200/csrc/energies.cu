@@ -1,0 +1,121 @@
+// energies.cu -- Potts energies E(s) = sum_{i<j} J_ij(s_i, s_j).
+//
+// Slice-tiled (tiling.cuh): a CTA holds the couplings of one block pair in
+// shared memory and streams a chunk of sequences through it; each thread
+// sums its sequence's B*B gathered couplings in double and adds the slice
+// total to a per-sequence 64-bit fixed-point accumulator (scale 2^40) with an
+// integer atomic.  Integer addition is associative, so the result does not
+// depend on CTA order: energies are deterministic, and accurate to ~1e-12
+// absolute before the final rounding to float.  The reference sums each
+// sequence serially with Kahan compensation in float (getEnergiesf,
+// mcmc.cl:249-336); this result is at least as accurate.
+#include "tiling.cuh"
+
+namespace mi3 {
+
+constexpr double FIX_SCALE = 1099511627776.0;  // 2^40
+constexpr double FIX_INV = 1.0 / 1099511627776.0;
+
+template <int B>
+__global__ void __launch_bounds__(512) k_energies(const float *__restrict__ J,
+                                                  const uint32_t *__restrict__ seq, uint32_t buflen,
+                                                  uint32_t nseq, unsigned long long *acc, uint32_t L,
+                                                  uint32_t q, SliceGeom g) {
+    extern __shared__ __align__(16) float js[];  // [B*B][q*q]
+    const uint32_t qq = q * q;
+    const uint32_t s = blockIdx.x % g.nslices;
+    const uint32_t chunk = blockIdx.x / g.nslices;
+    uint32_t bi, bj;
+    slice_coords(s, g.nb, bi, bj);
+    const uint32_t i0 = bi * B, j0 = bj * B;
+
+    // Stage the slice's couplings: for each i, pairs (i, jlo..jhi-1) are
+    // contiguous in the packed table.
+    for (int ii = 0; ii < B; ++ii) {
+        uint32_t i = i0 + ii;
+        if (i + 1 >= L) break;
+        uint32_t jlo = max(j0, i + 1), jhi = min(j0 + B, L);
+        if (jlo >= jhi) continue;
+        const float *src = J + pair_index(i, jlo, L) * qq;
+        float *dst = js + ((size_t)ii * B + (jlo - j0)) * qq;
+        uint32_t cnt = (jhi - jlo) * qq;
+        for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) dst[k] = __ldg(&src[k]);
+    }
+    __syncthreads();
+
+    const uint32_t swords = (L - 1) / 4 + 1;
+    const uint32_t nbeg = chunk * g.chunk;
+    const uint32_t nend = min(nseq, nbeg + g.chunk);
+    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += blockDim.x) {
+        uint32_t wI[B / 4], wJ[B / 4];
+        load_block_words<B>(seq, buflen, n, bi, swords, wI);
+        load_block_words<B>(seq, buflen, n, bj, swords, wJ);
+        double e = 0.0;
+#pragma unroll
+        for (int ii = 0; ii < B; ++ii) {
+            uint32_t i = i0 + ii;
+            if (i >= L) break;
+            uint32_t siq = block_byte<B>(wI, ii, q - 1) * q;
+            const float *row = js + (size_t)ii * B * qq + siq;
+#pragma unroll
+            for (int jj = 0; jj < B; ++jj) {
+                uint32_t j = j0 + jj;
+                if (j < L && j > i) e += (double)row[(size_t)jj * qq + block_byte<B>(wJ, jj, q - 1)];
+            }
+        }
+        long long v = __double2ll_rn(e * FIX_SCALE);
+        atomicAdd(&acc[n], (unsigned long long)v);
+    }
+}
+
+__global__ void k_energies_final(const unsigned long long *__restrict__ acc, float *E, uint32_t n) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) E[k] = (float)((double)(long long)acc[k] * FIX_INV);
+}
+
+template <int B>
+static int launch_energies(const float *J, const uint32_t *seq, uint32_t buflen, uint32_t nseq,
+                           unsigned long long *acc, uint32_t L, uint32_t q, cudaStream_t st) {
+    SliceGeom g = make_geom(L, B, nseq, 148 * 8, 2048);
+    size_t smem = (size_t)B * B * q * q * 4;
+    cudaFuncSetAttribute(k_energies<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    uint64_t nblk = (uint64_t)g.nslices * g.nchunks;
+    if (nblk > 0x7fffffffull) return fail(MI3_ERR_ARG, "mi3_energies: grid too large");
+    k_energies<B><<<(uint32_t)nblk, 512, smem, st>>>(J, seq, buflen, nseq, acc, L, q, g);
+    return check_launch("mi3_energies");
+}
+
+}  // namespace mi3
+
+using namespace mi3;
+
+extern "C" size_t mi3_energies_workspace(uint32_t nseq) { return (size_t)nseq * 8; }
+
+extern "C" int mi3_energies(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
+                            float *energies, uint32_t L, uint32_t q, void *workspace,
+                            size_t ws_bytes, void *stream) {
+    if (!J || !seqmem || !energies || !workspace)
+        return fail(MI3_ERR_ARG, "mi3_energies: null pointer");
+    if (L < 2 || q < 1 || q > 255 || nseq > buflen)
+        return fail(MI3_ERR_ARG, "mi3_energies: bad L/q/nseq");
+    if (nseq == 0) return MI3_OK;
+    if (ws_bytes < mi3_energies_workspace(nseq))
+        return fail(MI3_ERR_WORKSPACE, "mi3_energies: workspace too small");
+    if (!aligned(workspace, 8)) return fail(MI3_ERR_ALIGN, "mi3_energies: workspace alignment");
+    cudaStream_t st = as_stream(stream);
+    auto *acc = reinterpret_cast<unsigned long long *>(workspace);
+    if (cudaMemsetAsync(acc, 0, (size_t)nseq * 8, st) != cudaSuccess)
+        return check_launch("mi3_energies: memset");
+    uint32_t B = pick_block(q, 116 * 1024);
+    int rc;
+    switch (B) {
+        case 32: rc = launch_energies<32>(J, seqmem, buflen, nseq, acc, L, q, st); break;
+        case 16: rc = launch_energies<16>(J, seqmem, buflen, nseq, acc, L, q, st); break;
+        case 8: rc = launch_energies<8>(J, seqmem, buflen, nseq, acc, L, q, st); break;
+        case 4: rc = launch_energies<4>(J, seqmem, buflen, nseq, acc, L, q, st); break;
+        default: return fail(MI3_ERR_ARG, "mi3_energies: q too large");
+    }
+    if (rc) return rc;
+    k_energies_final<<<(nseq + 255) / 256, 256, 0, st>>>(acc, energies, nseq);
+    return check_launch("mi3_energies: final");
+}

@@ -1,0 +1,291 @@
+// mcmc.cu -- coupling unpacking and the Metropolis sampler.
+//
+// Sampler design (B200): one walker per consumer thread, NW walkers per CTA.
+// Each walker's packed sequence lives in shared memory for the whole launch
+// (loaded once, stored once), so HBM sees the sequences twice per launch
+// instead of once per step.  All walkers of the launch share the site
+// sequence (position_list), so every CTA needs the same coupling row
+// Jrows[pos] (L blocks of q*q floats) at every step.  One producer warp
+// streams that row through an S-stage shared-memory ring with 1-D bulk
+// copies (cp.async.bulk, completion on mbarriers); the row stays hot in L2
+// (the whole unpacked table is < L2 at L=232, q=21).  Consumers gather the
+// two entries J[pos][m][mut][s_m] and J[pos][m][cur][s_m] per site m from the
+// staged chunk and accumulate dE in site order, as DeltaEnergy does
+// (mcmc.cl:360-413).
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace mi3 {
+
+// ----------------------------------------------------------------- unpack J
+// Jrows[i][j][a][b] = J_ij(a,b) for i<j, J_ji(b,a) for i>j, 0 on the diagonal
+// and in the row padding (unpackfV, mcmc.cl:42-65).
+__global__ void k_unpack_j(const float *__restrict__ J, float *__restrict__ Jrows, uint32_t L,
+                           uint32_t q, uint64_t stride) {
+    uint32_t i = blockIdx.y;
+    uint32_t qq = q * q;
+    const uint64_t row_len = stride;
+    float *row = Jrows + (uint64_t)i * stride;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < row_len;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t j = (uint32_t)(k / qq);
+        uint32_t li = (uint32_t)(k - (uint64_t)j * qq);
+        float v = 0.0f;
+        if (j < L && j != i) {
+            if (i < j) {
+                uint64_t n = (uint64_t)i * (2 * L - i - 1) / 2 + (j - i - 1);
+                v = J[n * qq + li];
+            } else {
+                uint64_t n = (uint64_t)j * (2 * L - j - 1) / 2 + (i - j - 1);
+                v = J[n * qq + q * (li % q) + li / q];
+            }
+        }
+        row[k] = v;
+    }
+}
+
+// ---------------------------------------------------------------- sampler
+struct MetroParams {
+    const float *Jrows;
+    uint64_t stride;  // floats per row
+    uint4 *rng;
+    const uint32_t *poslist;
+    uint32_t pos_off;
+    uint32_t nsteps;
+    const float *betas;
+    float beta;
+    uint32_t *seq;
+    uint32_t nseqs;
+    uint32_t L, q;
+    uint32_t M;        // sites per chunk (multiple of 4)
+    uint32_t nchunks;  // ceil(L / M)
+    uint32_t stages;
+    uint32_t stage_floats;  // floats per stage buffer (multiple of 32)
+    int32_t *status;
+};
+
+// Shared memory: [full mbarriers S][empty mbarriers S][abort flag] (pad 128)
+//                [stage buffers S * stage_floats][pad STAGE_PAD][seq words SWORDS * NW]
+// The pad absorbs gathers with an out-of-range residue byte (< 256 floats).
+constexpr uint32_t STAGE_PAD = 256;
+__global__ void __launch_bounds__(544, 1) k_metropolis(const MetroParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const uint32_t NW = blockDim.x - 32;  // consumer threads = walkers
+    const uint32_t S = p.stages;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + S;
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + S);
+    float *stage = reinterpret_cast<float *>(smem + 128 * ((16 * S + 4 + 127) / 128));
+    uint32_t *seq_s = reinterpret_cast<uint32_t *>(stage + (size_t)S * p.stage_floats + STAGE_PAD);
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t warp = tid >> 5, lane = tid & 31;
+    const uint32_t qq = p.q * p.q;
+    const uint32_t sw = (p.L - 1) / 4 + 1;
+
+    if (tid == 0) {
+        for (uint32_t s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NW / 32);
+        }
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    if (warp == NW / 32) {
+        // ---------------------------------------------------- producer warp
+        if (lane == 0) {
+            uint32_t k = 0;
+            bool ok = true;
+            for (uint32_t i = 0; i < p.nsteps && ok; ++i) {
+                uint32_t pos = __ldg(&p.poslist[p.pos_off + i]);
+                if (pos >= p.L) pos = 0;  // invalid site: consumers report it
+                const float *row = p.Jrows + (uint64_t)pos * p.stride;
+                for (uint32_t c = 0; c < p.nchunks; ++c, ++k) {
+                    uint32_t s = k % S;
+                    if (k >= S) {
+                        uint32_t ph = ((k / S) - 1) & 1;
+                        if (!mbar_wait_bounded(&empty[s], ph, abort_flag, WAIT_LIMIT_NS)) {
+                            if (!*abort_flag) report(p.status, ST_TIMEOUT_EMPTY);
+                            *abort_flag = 1;
+                            ok = false;
+                            break;
+                        }
+                    }
+                    uint32_t m0 = c * p.M;
+                    uint32_t nm = min(p.M, p.L - m0);
+                    uint32_t bytes = (nm * qq * 4 + 15) & ~15u;
+                    mbar_arrive_expect_tx(&full[s], bytes);
+                    bulk_g2s(stage + (size_t)s * p.stage_floats, row + (uint64_t)m0 * qq, bytes,
+                             &full[s]);
+                }
+            }
+            // Drain: every copy issued must land before the CTA may exit.
+            uint32_t first = k > S ? k - S : 0;
+            for (uint32_t kk = first; kk < k; ++kk)
+                mbar_wait_bounded(&full[kk % S], (kk / S) & 1, nullptr, WAIT_LIMIT_NS);
+        }
+        return;
+    }
+
+    // -------------------------------------------------------- consumers
+    const uint32_t g = blockIdx.x * NW + tid;
+    for (uint32_t w = 0; w < sw; ++w) seq_s[w * NW + tid] = p.seq[(size_t)w * p.nseqs + g];
+    uint4 s4 = p.rng[g];
+    Rng2 rng{s4.x, s4.y, s4.z, s4.w};
+    const float B = p.betas ? p.betas[g] : p.beta;
+    // seq_s is private per thread (column tid), no barrier needed.
+
+    uint32_t k = 0;
+    bool ok = true;
+    for (uint32_t i = 0; i < p.nsteps && ok; ++i) {
+        uint32_t pos = __ldg(&p.poslist[p.pos_off + i]);
+        if (pos >= p.L) {
+            report(p.status, ST_BAD_INPUT);
+            pos = 0;
+        }
+        uint32_t r0, r1;
+        rng_next2(rng, r0, r1);
+        uint32_t mut = r0 % p.q;
+        uint32_t wpos = seq_s[(pos >> 2) * NW + tid];
+        // residues are < q for valid input; the clamp keeps an invalid one
+        // inside the stage buffer (an out-of-range s_m lands in the pad).
+        uint32_t cur = min(getbyte(wpos, pos & 3), p.q - 1);
+        uint32_t mq = mut * p.q, cq = cur * p.q;
+        float dE = 0.0f;
+        for (uint32_t c = 0; c < p.nchunks; ++c, ++k) {
+            uint32_t s = k % S;
+            if (!mbar_wait_bounded(&full[s], (k / S) & 1, abort_flag, WAIT_LIMIT_NS)) {
+                if (!*abort_flag) report(p.status, ST_TIMEOUT_FULL);
+                *abort_flag = 1;
+                ok = false;
+                break;
+            }
+            const float *Jc = stage + (size_t)s * p.stage_floats;
+            uint32_t m0 = c * p.M;
+            uint32_t nm = min(p.M, p.L - m0);
+            uint32_t nfull = nm >> 2;
+            const uint32_t *sq = seq_s + (m0 >> 2) * NW + tid;
+#pragma unroll 2
+            for (uint32_t w = 0; w < nfull; ++w) {
+                uint32_t word = sq[w * NW];
+                const float *Jm = Jc + w * 4 * qq;
+#pragma unroll
+                for (uint32_t b = 0; b < 4; ++b) {
+                    uint32_t sm = getbyte(word, b);
+                    dE += Jm[b * qq + mq + sm] - Jm[b * qq + cq + sm];
+                }
+            }
+            uint32_t rem = nm & 3;
+            if (rem) {
+                uint32_t word = sq[nfull * NW];
+                const float *Jm = Jc + nfull * 4 * qq;
+                for (uint32_t b = 0; b < rem; ++b) {
+                    uint32_t sm = getbyte(word, b);
+                    dE += Jm[b * qq + mq + sm] - Jm[b * qq + cq + sm];
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        }
+        if (!ok) break;
+        float x = -B * dE;
+        if (accept_exp(x, uniform_map(r1))) seq_s[(pos >> 2) * NW + tid] = setbyte(wpos, pos & 3, mut);
+    }
+    for (uint32_t w = 0; w < sw; ++w) p.seq[(size_t)w * p.nseqs + g] = seq_s[w * NW + tid];
+    p.rng[g] = make_uint4(rng.x0, rng.x1, rng.c0, rng.c1);
+}
+
+struct MetroConfig {
+    uint32_t NW, M, nchunks, stages, stage_floats;
+    size_t smem;
+};
+
+static size_t metro_smem(uint32_t NW, uint32_t S, uint32_t stage_floats, uint32_t sw) {
+    size_t head = 128 * ((16 * S + 4 + 127) / 128);
+    return head + (size_t)S * stage_floats * 4 + STAGE_PAD * 4 + (size_t)sw * NW * 4;
+}
+
+static bool pick_metro_config(uint32_t L, uint32_t q, uint32_t nseqs, MetroConfig &cfg) {
+    const size_t SMEM_MAX = 227 * 1024;
+    const uint32_t qq = q * q;
+    const uint32_t sw = (L - 1) / 4 + 1;
+    const uint32_t Lr = (L + 3) & ~3u;
+    // sites per chunk: ~24 KB stages, multiple of 4, at most the (rounded) row
+    uint32_t M = (24 * 1024) / (qq * 4);
+    M = std::max<uint32_t>(4, M & ~3u);
+    M = std::min(M, Lr);
+    uint32_t cands[3] = {512, 256, 128};
+    for (uint32_t NW : cands) {
+        if (nseqs % NW) continue;
+        // prefer enough CTAs to fill the SMs when walkers are few
+        if (NW > 128 && nseqs / NW < 148) continue;
+        for (uint32_t S = 4; S >= 2; --S) {
+            for (uint32_t m = M; m >= 4; m -= 4) {
+                uint32_t stage_floats = ((m * qq) + 31) & ~31u;
+                size_t sm = metro_smem(NW, S, stage_floats, sw);
+                if (sm <= SMEM_MAX) {
+                    cfg = MetroConfig{NW, m, (L + m - 1) / m, S, stage_floats, sm};
+                    return true;
+                }
+            }
+        }
+    }
+    return false;
+}
+
+}  // namespace mi3
+
+using namespace mi3;
+
+extern "C" int mi3_unpack_j(const float *J, float *Jrows, uint32_t L, uint32_t q, void *stream) {
+    if (!J || !Jrows) return fail(MI3_ERR_ARG, "mi3_unpack_j: null pointer");
+    if (L < 2 || q < 1 || q > 255) return fail(MI3_ERR_ARG, "mi3_unpack_j: bad L/q");
+    if (!aligned(Jrows, 16)) return fail(MI3_ERR_ALIGN, "mi3_unpack_j: Jrows not 16B aligned");
+    uint64_t stride = jrow_stride(L, q);
+    uint32_t tb = 256;
+    uint32_t gx = (uint32_t)std::min<uint64_t>((stride + tb - 1) / tb, 1024);
+    dim3 grid(gx, L);
+    k_unpack_j<<<grid, tb, 0, as_stream(stream)>>>(J, Jrows, L, q, stride);
+    return check_launch("mi3_unpack_j");
+}
+
+extern "C" int mi3_metropolis(const float *Jrows, uint32_t *rngstates, uint32_t position_offset,
+                              const uint32_t *position_list, uint32_t nsteps, const float *betas,
+                              float beta, uint32_t *seqmem, uint32_t nseqs, uint32_t L, uint32_t q,
+                              int32_t *status, void *stream) {
+    if (!Jrows || !rngstates || !position_list || !seqmem || !status)
+        return fail(MI3_ERR_ARG, "mi3_metropolis: null pointer");
+    if (L < 2 || q < 2 || q > 255) return fail(MI3_ERR_ARG, "mi3_metropolis: bad L/q");
+    if (nseqs == 0 || nseqs % 128)
+        return fail(MI3_ERR_ARG, "mi3_metropolis: nseqs must be a positive multiple of 128");
+    if (!aligned(Jrows, 16) || !aligned(rngstates, 16))
+        return fail(MI3_ERR_ALIGN, "mi3_metropolis: Jrows/rngstates must be 16B aligned");
+    if (nsteps == 0) return MI3_OK;
+    MetroConfig cfg;
+    if (!pick_metro_config(L, q, nseqs, cfg))
+        return fail(MI3_ERR_ARG, "mi3_metropolis: L/q too large for the shared-memory plan");
+    cudaFuncSetAttribute(k_metropolis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
+    MetroParams p;
+    p.Jrows = Jrows;
+    p.stride = jrow_stride(L, q);
+    p.rng = reinterpret_cast<uint4 *>(rngstates);
+    p.poslist = position_list;
+    p.pos_off = position_offset;
+    p.nsteps = nsteps;
+    p.betas = betas;
+    p.beta = beta;
+    p.seq = seqmem;
+    p.nseqs = nseqs;
+    p.L = L;
+    p.q = q;
+    p.M = cfg.M;
+    p.nchunks = cfg.nchunks;
+    p.stages = cfg.stages;
+    p.stage_floats = cfg.stage_floats;
+    p.status = status;
+    k_metropolis<<<nseqs / cfg.NW, cfg.NW + 32, cfg.smem, as_stream(stream)>>>(p);
+    return check_launch("mi3_metropolis");
+}

@@ -1,0 +1,341 @@
+// newton.cu -- the quasi-Newton coupling update and the Zwanzig reweighting
+// statistics (NewtonSteps.iterNewton, NewtonSteps.py:159-268).
+//
+//   mi3_update_j         updatedJ           (mcmc.cl:829-843)
+//   mi3_reg_l1z / l2z    reg_l1z / reg_l2z  (mcmc.cl:845-902, zeroGauge :764-822)
+//   mi3_min_floats       minFloats          (mcmc.cl:558-584)
+//   mi3_dE_to_weights    dE_to_weights      (mcmc.cl:624-633)
+//   mi3_fixed_beta_weights                  (mcmc.cl:635-644)
+//   mi3_weight_stats     weight_stats       (mcmc.cl:586-622), in double
+//   mi3_weights_fused    dE -> (weights, min dE, sums) in one pass
+//   mi3_add_float_bufs   addFloatBufs       (mcmc.cl:720-727)
+//
+// Reductions over walkers run as a fixed grid of CTAs that write partials to
+// a workspace; the last CTA to finish (ticket counter) combines them in a
+// fixed order, so sums are deterministic.
+#include "common.cuh"
+
+namespace mi3 {
+
+__global__ void k_update_j(const float *__restrict__ bt, const float *__restrict__ bi, float gamma,
+                           float pc, const float *Ji, float *Jo, uint64_t n) {
+    uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) Jo[k] = Ji[k] - gamma * (bt[k] - bi[k]) / (bi[k] + pc);
+}
+
+__device__ __forceinline__ float ocl_sign(float x) {
+    if (x > 0.0f) return 1.0f;
+    if (x < 0.0f) return -1.0f;
+    if (x != x) return 0.0f;
+    return x;
+}
+
+// Odd-aware tree over the q columns of each row of the q*q scratch block
+// (the row loops of zeroGauge, mcmc.cl:772-781).  One warp.
+__device__ __forceinline__ void rows_tree(float *sc, uint32_t q, uint32_t lane) {
+    const uint32_t qq = q * q;
+    uint32_t m = q;
+    while (m > 1) {
+        uint32_t odd = m & 1;
+        m = (m + 1) >> 1;
+        for (uint32_t li = lane; li < qq; li += 32)
+            if (li % q < m - odd) sc[li] = sc[li] + sc[li + m];
+        __syncwarp();
+    }
+}
+
+// reg_l1z (L2=false) / reg_l2z (L2=true): one warp per pair block.
+template <bool L2>
+__global__ void k_reg_lz(const float *__restrict__ bi, float gamma, float pc, float lJ,
+                         const float *__restrict__ J, float *dJ, uint64_t npairs, uint32_t q) {
+    extern __shared__ float sm[];
+    const uint32_t qq = q * q;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    float *sc = sm + warp * (qq + 2 * q + 2);  // [q*q scratch][hi q][hj q]
+    float *hi = sc + qq;
+    float *hj = hi + q;
+    const float fq = (float)q;
+    for (uint64_t p = (uint64_t)blockIdx.x * wpb + warp; p < npairs; p += (uint64_t)gridDim.x * wpb) {
+        const float *Jb = J + p * qq;
+        float *dJb = dJ + p * qq;
+        // row sums
+        for (uint32_t li = lane; li < qq; li += 32) sc[li] = Jb[li] + dJb[li];
+        __syncwarp();
+        rows_tree(sc, q, lane);
+        for (uint32_t a = lane; a < q; a += 32) hi[a] = sc[q * a] / fq;
+        __syncwarp();
+        // column sums (transpose into scratch)
+        for (uint32_t li = lane; li < qq; li += 32) sc[q * (li % q) + li / q] = Jb[li] + dJb[li];
+        __syncwarp();
+        rows_tree(sc, q, lane);
+        for (uint32_t b = lane; b < q; b += 32) hj[b] = sc[q * b] / fq;
+        __syncwarp();
+        // total of the column sums
+        uint32_t m = q;
+        while (m > 1) {
+            uint32_t odd = m & 1;
+            m = (m + 1) >> 1;
+            for (uint32_t li = lane; li < m - odd; li += 32) sc[q * li] = sc[q * li] + sc[q * (li + m)];
+            __syncwarp();
+        }
+        float mean = sc[0] / fq / fq;
+        __syncwarp();
+        for (uint32_t a = lane; a < q; a += 32) {
+            hi[a] = hi[a] - mean;
+            hj[a] = hj[a] - mean;
+        }
+        __syncwarp();
+        for (uint32_t li = lane; li < qq; li += 32) {
+            float Jp = dJb[li];
+            float Jt0 = Jb[li] + Jp;
+            float J0 = Jt0 - (hi[li / q] + hj[li % q]) - mean;
+            float R;
+            if (L2) R = -lJ * J0 * gamma / (bi[p * qq + li] + pc);
+            else R = -lJ * ocl_sign(J0) * gamma / (bi[p * qq + li] + pc);
+            if (ocl_sign(J0) != ocl_sign(J0 + R)) Jp = Jp - J0;
+            else Jp = Jp + R;
+            dJb[li] = Jp;
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------ reductions
+// Workspace: [ticket counter (uint32, padded to 16 B)][partials: NBLK x 4 doubles]
+constexpr uint32_t RED_BLOCKS = 296;
+constexpr uint32_t RED_THREADS = 512;
+
+enum RedMode : uint32_t { RM_WEIGHTS = 1, RM_MIN = 2, RM_STATS = 4 };
+
+struct RedOut {
+    float *weights;   // RM_WEIGHTS: output
+    float *minout;    // RM_MIN
+    float *stats;     // RM_STATS: {sum, sum2} float
+    double *stats64;  // RM_STATS: {sum, sum2} double (nullable)
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// in = dE when RM_WEIGHTS (weights computed as exp(-dE + ref)), else weights.
+__global__ void __launch_bounds__(RED_THREADS) k_reduce(const float *__restrict__ in, uint32_t n,
+                                                        float ref, uint32_t mode, RedOut o,
+                                                        unsigned char *ws) {
+    unsigned int *ticket = reinterpret_cast<unsigned int *>(ws);
+    double *part = reinterpret_cast<double *>(ws + 16);
+    __shared__ double s_sum[RED_THREADS / 32], s_sum2[RED_THREADS / 32];
+    __shared__ float s_min[RED_THREADS / 32];
+    __shared__ bool s_last;
+    double a = 0.0, b = 0.0;
+    float mn = 0.0f;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        float v = in[k];
+        if (mode & RM_MIN) mn = fminf(v, mn);
+        if (mode & RM_WEIGHTS) {
+            v = expf(-v + ref);
+            o.weights[k] = v;
+        }
+        if (mode & RM_STATS) {
+            double dv = (double)v;
+            a += dv;
+            b += dv * dv;
+        }
+    }
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    mn = warp_min(mn);
+    if (lane == 0) {
+        s_sum[warp] = a;
+        s_sum2[warp] = b;
+        s_min[warp] = mn;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0.0, tb = 0.0;
+        float tm = 0.0f;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+            ta += s_sum[w];
+            tb += s_sum2[w];
+            tm = fminf(tm, s_min[w]);
+        }
+        part[4 * blockIdx.x + 0] = ta;
+        part[4 * blockIdx.x + 1] = tb;
+        part[4 * blockIdx.x + 2] = (double)tm;
+        __threadfence();
+        unsigned int t = atomicAdd(ticket, 1u);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        volatile double *vp = part;
+        double ta = 0.0, tb = 0.0, tm = 0.0;
+        for (uint32_t k = 0; k < gridDim.x; ++k) {
+            ta += vp[4 * k + 0];
+            tb += vp[4 * k + 1];
+            tm = fmin(tm, vp[4 * k + 2]);
+        }
+        if (mode & RM_STATS) {
+            o.stats[0] = (float)ta;
+            o.stats[1] = (float)tb;
+            if (o.stats64) {
+                o.stats64[0] = ta;
+                o.stats64[1] = tb;
+            }
+        }
+        if (mode & RM_MIN) *o.minout = (float)tm;
+        *ticket = 0u;  // ready for the next call
+    }
+}
+
+// min(0, min data): per-CTA minimum, then an integer atomicMax on the bit
+// pattern -- for non-positive floats a larger magnitude is a larger unsigned
+// pattern, so the result is exact and order independent.
+__global__ void __launch_bounds__(RED_THREADS) k_min(const float *__restrict__ in, uint32_t n,
+                                                     unsigned int *out) {
+    __shared__ float s_min[RED_THREADS / 32];
+    float mn = 0.0f;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        mn = fminf(in[k], mn);
+    mn = warp_min(mn);
+    if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = mn;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float tm = 0.0f;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) tm = fminf(tm, s_min[w]);
+        if (tm < 0.0f) atomicMax(out, __float_as_uint(tm));
+    }
+}
+
+__global__ void k_dE_to_weights(float ref, const float *__restrict__ dE, float *w, uint32_t n) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) w[k] = expf(-dE[k] + ref);
+}
+
+__global__ void k_fixed_beta(float beta, float ref, const float *__restrict__ E, float *w, uint32_t n) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) w[k] = expf((beta - 1.0f) * (E[k] - ref));
+}
+
+__global__ void k_add(float *dst, const float *__restrict__ src, uint32_t n) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] += src[k];
+}
+
+static size_t red_ws_bytes() { return 16 + (size_t)RED_BLOCKS * 4 * sizeof(double); }
+
+static int launch_reduce(const float *in, uint32_t n, float ref, uint32_t mode, RedOut o, void *ws,
+                         size_t ws_bytes, cudaStream_t st, const char *what) {
+    if (ws_bytes < red_ws_bytes()) return fail(MI3_ERR_WORKSPACE, std::string(what) + ": workspace too small");
+    if (!aligned(ws, 16)) return fail(MI3_ERR_ALIGN, std::string(what) + ": workspace alignment");
+    uint32_t blocks = std::min<uint32_t>(RED_BLOCKS, std::max<uint32_t>(1, (n + RED_THREADS - 1) / RED_THREADS));
+    if (cudaMemsetAsync(ws, 0, 16, st) != cudaSuccess) return check_launch(what);
+    k_reduce<<<blocks, RED_THREADS, 0, st>>>(in, n, ref, mode, o, reinterpret_cast<unsigned char *>(ws));
+    return check_launch(what);
+}
+
+}  // namespace mi3
+
+using namespace mi3;
+
+extern "C" int mi3_update_j(const float *bi_target, const float *bi, float gamma, float pc, const float *Ji,
+                            float *Jo, uint32_t L, uint32_t q, void *stream) {
+    if (!bi_target || !bi || !Ji || !Jo) return fail(MI3_ERR_ARG, "mi3_update_j: null pointer");
+    if (L < 2 || q < 1) return fail(MI3_ERR_ARG, "mi3_update_j: bad L/q");
+    uint64_t n = npairs_of(L) * q * q;
+    k_update_j<<<(uint32_t)((n + 255) / 256), 256, 0, as_stream(stream)>>>(bi_target, bi, gamma, pc, Ji, Jo, n);
+    return check_launch("mi3_update_j");
+}
+
+static int reg_lz(bool l2, const float *bi, float gamma, float pc, float lJ, const float *J, float *dJ,
+                  uint32_t L, uint32_t q, void *stream) {
+    const char *name = l2 ? "mi3_reg_l2z" : "mi3_reg_l1z";
+    if (!bi || !J || !dJ) return fail(MI3_ERR_ARG, std::string(name) + ": null pointer");
+    if (L < 2 || q < 1 || q * q > 4096) return fail(MI3_ERR_ARG, std::string(name) + ": bad L/q");
+    uint64_t np = npairs_of(L);
+    uint32_t tb = 256;
+    size_t smem = (size_t)(tb / 32) * (q * q + 2 * q + 2) * 4;
+    uint32_t grid = (uint32_t)std::min<uint64_t>((np + 7) / 8, 148 * 16);
+    if (smem > 48 * 1024) {
+        if (l2) cudaFuncSetAttribute(k_reg_lz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        else cudaFuncSetAttribute(k_reg_lz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    if (l2) k_reg_lz<true><<<grid, tb, smem, as_stream(stream)>>>(bi, gamma, pc, lJ, J, dJ, np, q);
+    else k_reg_lz<false><<<grid, tb, smem, as_stream(stream)>>>(bi, gamma, pc, lJ, J, dJ, np, q);
+    return check_launch(name);
+}
+
+extern "C" int mi3_reg_l1z(const float *bi, float gamma, float pc, float lJ, const float *J, float *dJ,
+                           uint32_t L, uint32_t q, void *stream) {
+    return reg_lz(false, bi, gamma, pc, lJ, J, dJ, L, q, stream);
+}
+
+extern "C" int mi3_reg_l2z(const float *bi, float gamma, float pc, float lJ, const float *J, float *dJ,
+                           uint32_t L, uint32_t q, void *stream) {
+    return reg_lz(true, bi, gamma, pc, lJ, J, dJ, L, q, stream);
+}
+
+extern "C" size_t mi3_weight_stats_workspace(uint32_t n) {
+    (void)n;
+    return red_ws_bytes();
+}
+
+extern "C" int mi3_min_floats(const float *data, uint32_t len, float *out, void *stream) {
+    if (!data || !out) return fail(MI3_ERR_ARG, "mi3_min_floats: null pointer");
+    cudaStream_t st = as_stream(stream);
+    if (cudaMemsetAsync(out, 0, sizeof(float), st) != cudaSuccess) return check_launch("mi3_min_floats: memset");
+    if (len == 0) return MI3_OK;
+    uint32_t blocks = std::min<uint32_t>(RED_BLOCKS, (len + RED_THREADS - 1) / RED_THREADS);
+    k_min<<<blocks, RED_THREADS, 0, st>>>(data, len, reinterpret_cast<unsigned int *>(out));
+    return check_launch("mi3_min_floats");
+}
+
+extern "C" int mi3_dE_to_weights(float ref_E, const float *dE, float *weights, uint32_t n, void *stream) {
+    if (!dE || !weights) return fail(MI3_ERR_ARG, "mi3_dE_to_weights: null pointer");
+    if (n == 0) return MI3_OK;
+    k_dE_to_weights<<<(n + 255) / 256, 256, 0, as_stream(stream)>>>(ref_E, dE, weights, n);
+    return check_launch("mi3_dE_to_weights");
+}
+
+extern "C" int mi3_fixed_beta_weights(float beta, float ref_E, const float *E, float *weights, uint32_t n,
+                                      void *stream) {
+    if (!E || !weights) return fail(MI3_ERR_ARG, "mi3_fixed_beta_weights: null pointer");
+    if (n == 0) return MI3_OK;
+    k_fixed_beta<<<(n + 255) / 256, 256, 0, as_stream(stream)>>>(beta, ref_E, E, weights, n);
+    return check_launch("mi3_fixed_beta_weights");
+}
+
+extern "C" int mi3_weight_stats(const float *weights, uint32_t n, float *out2, double *out2_f64,
+                                void *workspace, size_t ws_bytes, void *stream) {
+    if (!weights || !out2 || !workspace) return fail(MI3_ERR_ARG, "mi3_weight_stats: null pointer");
+    RedOut o{nullptr, nullptr, out2, out2_f64};
+    return launch_reduce(weights, n, 0.0f, RM_STATS, o, workspace, ws_bytes, as_stream(stream),
+                         "mi3_weight_stats");
+}
+
+extern "C" int mi3_weights_fused(float ref_E, const float *dE, float *weights, uint32_t n, float *minout,
+                                 float *out2, double *out2_f64, void *workspace, size_t ws_bytes,
+                                 void *stream) {
+    if (!dE || !weights || !minout || !out2 || !workspace)
+        return fail(MI3_ERR_ARG, "mi3_weights_fused: null pointer");
+    RedOut o{weights, minout, out2, out2_f64};
+    return launch_reduce(dE, n, ref_E, RM_WEIGHTS | RM_MIN | RM_STATS, o, workspace, ws_bytes,
+                         as_stream(stream), "mi3_weights_fused");
+}
+
+extern "C" int mi3_add_float_bufs(float *dst, const float *src, uint32_t n, void *stream) {
+    if (!dst || !src) return fail(MI3_ERR_ARG, "mi3_add_float_bufs: null pointer");
+    if (n == 0) return MI3_OK;
+    k_add<<<(n + 255) / 256, 256, 0, as_stream(stream)>>>(dst, src, n);
+    return check_launch("mi3_add_float_bufs");
+}

@@ -1,0 +1,700 @@
+"""Per-device runtime: the B200 counterpart of the reference's MCMCGPU class.
+
+This mirrors mi3gpu/mcmcGPU.py:110-1018 -- same constructor arguments,
+method names, buffer names, dtypes and shapes -- so the host algorithm
+(NewtonSteps.iterNewton / runMCMC, node_manager.GPU_node) drives it
+unchanged.  Device buffers are PyTorch CUDA tensors used purely as memory;
+all arithmetic runs in libmi3b200 (hand-written sm_100a CUDA) through the C
+ABI in include/mi3b200.h.  There is no CPU fallback: without a CUDA device
+or without the built library every method raises.
+
+Ordering: the reference chains OpenCL events on an out-of-order queue so
+that each command waits for the previous one (mcmcGPU.py:76-81, 211-222).
+Here every MCMCGPU owns one CUDA stream and issues everything on it, which
+gives the same order.  `wait_for` arguments are accepted for signature
+compatibility; commands are always ordered after the previous command.
+"""
+import collections
+import time
+from pathlib import Path
+
+import numpy as np
+from numpy.random import RandomState
+import torch
+
+from . import _lib
+
+rng_buf_mul = 1024  # position-list blocks of 1024*nsteps (mcmcGPU.py:30)
+
+
+def _full_shape(buftype, bufshape):
+    """numpy shape of an array of `bufshape` elements of `buftype` (a
+    subarray dtype such as '<2u8' adds its own axes)."""
+    dt = np.dtype(buftype)
+    sub = dt.subdtype[1] if dt.subdtype is not None else ()
+    return tuple(bufshape) + tuple(sub)
+
+
+def _base_dtype(buftype):
+    dt = np.dtype(buftype)
+    return dt.subdtype[0] if dt.subdtype is not None else dt
+
+
+def _spec_to_torch(buftype, bufshape, pad=0):
+    """(numpy dtype string, shape) -> (torch dtype, flat element count).
+
+    uint32 buffers are held as int32 tensors (same bits); '<2u8' (the MWC64X
+    vec2 state, 16 bytes per walker) as two int64 per walker."""
+    dt = np.dtype(buftype)
+    if dt.subdtype is not None:
+        base, sub = dt.subdtype
+        n = int(np.prod(bufshape)) * int(np.prod(sub))
+        dt = base
+    else:
+        n = int(np.prod(bufshape))
+    n += int(pad or 0)
+    tmap = {np.dtype('<f4'): torch.float32, np.dtype('<u4'): torch.int32, np.dtype('<i4'): torch.int32,
+            np.dtype('<u8'): torch.int64, np.dtype('<f8'): torch.float64, np.dtype('<u1'): torch.uint8}
+    return tmap[dt], n
+
+
+class FutureBuf:
+    """Result of getBuf: read() blocks until the device->host copy is done
+    (mcmcGPU.py:95-108)."""
+
+    def __init__(self, buffer, event, postprocess=None, owner=None):
+        self.buffer = buffer
+        self.event = event
+        self.postfunc = postprocess
+        self.owner = owner
+        self.shape = buffer.shape
+        self.dtype = buffer.dtype
+
+    def read(self):
+        self.event.synchronize()
+        if self.owner is not None:
+            self.owner._check_status()
+        if self.postfunc is not None:
+            return self.postfunc(self.buffer)
+        return self.buffer
+
+
+class MCMCGPU:
+    def __init__(self, gpuinfo, L, q, nseq, wgsize, outdir, vsize, seed, profile=False, beta=None):
+        if nseq % 512 != 0:
+            raise ValueError("nwalkers/ngpus must be a multiple of 512")
+
+        self.L = L
+        self.q = q
+        self.nPairs = L * (L - 1) // 2
+        self.events = collections.deque()
+        self.SWORDS = ((L - 1) // 4 + 1)
+        self.SBYTES = (4 * self.SWORDS)
+        self.nseq = {'main': nseq}
+        self.nwalkers = nseq
+        self.beta = 1.0 if beta is None else float(beta)
+
+        device, gpunum = gpuinfo[0], gpuinfo[1]
+        if isinstance(device, int):
+            device = torch.device('cuda', device)
+        if not isinstance(device, torch.device):
+            device = torch.device(device)
+        if device.type != 'cuda' or not torch.cuda.is_available():
+            raise RuntimeError("MCMCGPU needs a CUDA device (no CPU fallback)")
+        _lib.load()
+        self.device = device
+        self.gpunum = gpunum
+
+        self.wgsize = wgsize
+        self.nhist, self.histws = histogram_heuristic(q)
+        if nseq % wgsize != 0:
+            raise Exception("nseq per GPU must be a multiple of wgsize")
+        if wgsize < q * q:
+            raise Exception("wgsize cannot be less than q*q")
+
+        self.logfn = None
+        if outdir is not None:
+            self.logfn = Path(outdir) / 'gpu-{}.log'.format(gpunum)
+            with open(self.logfn, "wt") as f:
+                printDevice(f.write, device)
+
+        self.rngstate = RandomState(seed)
+        self.stream = torch.cuda.Stream(device=device)
+        self.profile = profile
+        self._t0evt = None
+        self._pending_host = collections.deque()
+
+        self.initted = []
+        self.bufs = {}
+        self.buf_spec = {}
+        self.seqbufs = {}
+        self.Ebufs = {}
+        self.largebufs = []
+
+        nPairs, SWORDS = self.nPairs, self.SWORDS
+        self._setupBuffer('J', '<f4', (nPairs, q * q))
+        self._setupBuffer('Junpacked', '<f4', (L * L, q * q))
+        self._setupBuffer('bi', '<f4', (nPairs, q * q))
+        self._setupBuffer('bicount', '<u4', (nPairs, q * q))
+        self._setupBuffer('seq main', '<u4', (SWORDS, self.nseq['main']))
+        self._setupBuffer('seqL main', '<u4', (L, self.nseq['main'] // 4))
+        self._setupBuffer('cprob', '<f4', (L, (q - 1)))
+        self._setupBuffer('E main', '<f4', (self.nseq['main'],))
+        self._setupBuffer('minout', '<f4', (1,))
+        # library-side state: sampler status word and reduction/energy workspaces
+        self._setupBuffer('status', '<i4', (1,))
+        self._setupWorkspace('ws energies', _lib.query('mi3_energies_workspace', nseq))
+        self._setupWorkspace('ws reduce', _lib.query('mi3_weight_stats_workspace', nseq))
+        self.fillBuf('status', 0)
+        self.unpackedJ = False
+        self.repackedSeqT = {'main': False}
+        self.lastevt = None
+
+    # ------------------------------------------------------------ plumbing
+    def log(self, msg):
+        if self.logfn is None:
+            return
+        with open(self.logfn, "at") as f:
+            print("{: 10.3f}".format(time.process_time()), msg, file=f)
+
+    def _ptr(self, name):
+        return self.bufs[name].data_ptr()
+
+    @property
+    def _s(self):
+        return self.stream.cuda_stream
+
+    def _begin(self):
+        if not self.profile:
+            return None
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        if self._t0evt is None:
+            self._t0evt = e
+        return e
+
+    def logevt(self, name, start=None, nbytes=None):
+        """Record a command (profiling events when profile=True)."""
+        evt = None
+        if self.profile:
+            evt = torch.cuda.Event(enable_timing=True)
+            evt.record(self.stream)
+            self.events.append((start, evt, name, nbytes))
+        self.lastevt = evt
+        return evt
+
+    def _evtlist(self, evts):
+        if evts is None:
+            return []
+        if isinstance(evts, (list, tuple)):
+            return list(evts)
+        return [evts]
+
+    def logProfile(self):
+        """Write 'EVT name start end bytes' lines (ns, relative to the first
+        profiled command) for completed commands (mcmcGPU.py:224-237)."""
+        if not self.profile:
+            return
+        out = []
+        while self.events and self.events[0][1].query():
+            start, end, name, nbytes = self.events.popleft()
+            t0 = self._t0evt
+            s = t0.elapsed_time(start) * 1e6 if start is not None else 0.0
+            e = t0.elapsed_time(end) * 1e6
+            out.append("EVT {} {:.0f} {:.0f} {}".format(name, s, e, nbytes if nbytes else ''))
+        if self.logfn is not None and out:
+            with open(self.logfn, "at") as f:
+                f.write("\n".join(out) + "\n")
+        return out
+
+    def _setupBuffer(self, bufname, buftype, bufshape, pad=None):
+        tdt, n = _spec_to_torch(buftype, bufshape, pad)
+        if bufname == 'Junpacked':
+            # padded row layout of the sampler (include/mi3b200.h)
+            n = self.L * int(_lib.query('mi3_jrows_stride', self.L, self.q))
+        with torch.cuda.device(self.device):
+            buf = torch.empty(max(n, 1), dtype=tdt, device=self.device)
+        self.bufs[bufname] = buf
+        self.buf_spec[bufname] = (buftype, bufshape)
+        names = bufname.split()
+        if len(names) > 1:
+            bufs = {'seq': self.seqbufs, 'E': self.Ebufs}
+            if names[0] in bufs:
+                bufs[names[0]][names[1]] = buf
+
+    def _setupWorkspace(self, name, nbytes):
+        with torch.cuda.device(self.device):
+            self.bufs[name] = torch.zeros(max(int(nbytes), 16) // 8 + 2, dtype=torch.int64, device=self.device)
+
+    def _wsbytes(self, name):
+        b = self.bufs[name]
+        return b.numel() * b.element_size()
+
+    def require(self, *reqs):
+        for r in reqs:
+            if r not in self.initted:
+                raise Exception("{} not initialized".format(r))
+
+    def _initcomponent(self, cmp):
+        if cmp in self.initted:
+            raise Exception("Already initialized {}".format(cmp))
+        self.initted.append(cmp)
+
+    def _check_status(self):
+        st = int(self.bufs['status'].cpu()[0])
+        if st != 0:
+            raise RuntimeError("libmi3b200 sampler reported status {} (a bounded wait gave up)".format(st))
+
+    # ------------------------------------------------------------ set-up
+    def initMCMC(self, nsteps, rng_offset, rng_span):
+        self._initcomponent('MCMC')
+        self.nsteps = nsteps
+        self._setupBuffer('rngstates', '<2u8', (self.nseq['main'],))
+        self._setupBuffer('Bs', '<f4', (self.nseq['main'],))
+        self._setupBuffer('randpos', '<u4', (self.nsteps * rng_buf_mul,))
+        self.randpos_offset = rng_buf_mul * self.nsteps
+        self.setBuf('Bs', np.ones(self.nseq['main'], dtype='<f4'))
+        self._initMCMC_RNG(rng_offset, rng_span)
+        self.nsteps = int(nsteps)
+
+    def initLargeBufs(self, nseq_large):
+        raise NotImplementedError("large sequence buffers (distribute_jstep head_gpu/head_node) are not "
+                                  "part of the single-device path")
+
+    def initSubseq(self):
+        raise NotImplementedError("subsequence mode is not part of the single-device path")
+
+    def initJstep(self):
+        self._initcomponent('Jstep')
+        nPairs, q = self.nPairs, self.q
+        self._setupBuffer('dJ', '<f4', (nPairs, q * q))
+        self._setupBuffer('bi target', '<f4', (nPairs, q * q))
+        self._setupBuffer('Creg', '<f4', (nPairs, q * q))
+        self._setupBuffer('Xlambdas', '<f4', (nPairs,))
+        self._setupBuffer('weights', '<f4', (self.nseq['main'],))
+        self._setupBuffer('weightstats', '<f4', (2,))
+        self._setupBuffer('weightstats64', '<f8', (2,))
+        self._setupBuffer('E tmp', '<f4', (self.nseq['main'],))
+
+    # ------------------------------------------------------------ layouts
+    def packSeqs_4(self, seqs):
+        """(N, L) u1 -> (SWORDS, N) u4, 4 sites per word (mcmcGPU.py:333-347)."""
+        if seqs.dtype != np.dtype('<u1'):
+            raise Exception("seqs must have u1 dtype")
+        bseqs = np.zeros((seqs.shape[0], self.SBYTES), dtype='<u1', order='C')
+        bseqs[:, :self.L] = seqs
+        return np.ascontiguousarray(bseqs.view(np.uint32).T)
+
+    def unpackSeqs_4(self, mem):
+        """reverses packSeqs_4 (mcmcGPU.py:349-354)"""
+        mem = np.asarray(mem).view(np.uint32).reshape(self.SWORDS, -1)
+        bseqs = np.ascontiguousarray(mem.T).view(np.uint8)
+        return bseqs[:, :self.L].copy()
+
+    def repackseqs_T(self, bufname, wait_for=None):
+        nseq = self.nseq[bufname]
+        s = self._begin()
+        _lib.call('mi3_repack_seqs_T', self._ptr('seq ' + bufname), nseq, self._ptr('seqL ' + bufname),
+                  nseq // 4, self.L, self._s)
+        self.repackedSeqT[bufname] = True
+        return self.logevt('repackseqs_T', s)
+
+    def prepare_indep(self, unimarg, wait_for=None):
+        cprob = np.cumsum(unimarg, axis=1)
+        cprob = (cprob[:, :-1] / cprob[:, -1, None]).astype('<f4')
+        return self.setBuf('cprob', cprob)
+
+    def gen_indep(self, bufname, wait_for=None):
+        self.require('MCMC')
+        nseq = self.nseq[bufname]
+        s = self._begin()
+        _lib.call('mi3_gen_indep', self._ptr('seq ' + bufname), nseq, nseq, self._ptr('rngstates'),
+                  self._ptr('cprob'), self.L, self.q, self._s)
+        self.repackedSeqT[bufname] = False
+        return self.logevt('gen_indep', s)
+
+    def unpackJ(self, wait_for=None):
+        if self.unpackedJ:
+            return wait_for
+        s = self._begin()
+        _lib.call('mi3_unpack_j', self._ptr('J'), self._ptr('Junpacked'), self.L, self.q, self._s)
+        self.unpackedJ = True
+        return self.logevt('unpackJ', s)
+
+    # ------------------------------------------------------------ sampler
+    def _initMCMC_RNG(self, rng_offset, rng_span, wait_for=None):
+        self.require('MCMC')
+        rng_offset = np.uint64(rng_offset)
+        nwalkers = np.uint64(self.nseq['main'])
+        v2 = np.uint64(2)
+        walker_span = np.uint64(rng_span) // (v2 * nwalkers)
+        assert walker_span * v2 * nwalkers <= np.uint64(rng_span)
+        self.log("RNG offset: {}  walker-span: {}  nwalkers {}".format(rng_offset, walker_span, nwalkers))
+        s = self._begin()
+        _lib.call('mi3_init_rng', self._ptr('rngstates'), int(nwalkers), int(rng_offset), int(walker_span),
+                  self._s)
+        return self.logevt('initMCMC_RNG', s)
+
+    def updateRngPos(self, wait_evt=None):
+        """Shared site list, refilled from the host MT19937 stream every
+        1024 calls (mcmcGPU.py:447-458)."""
+        self.randpos_offset = self.randpos_offset + self.nsteps
+        rng_evt = None
+        bufsize = rng_buf_mul * self.nsteps
+        if self.randpos_offset >= bufsize:
+            rng = self.rngstate.randint(0, self.L, size=bufsize).astype('u4')
+            rng_evt = self.setBuf('randpos', rng)
+            self.randpos_offset = 0
+        return np.uint32(self.randpos_offset), rng_evt
+
+    def runMCMC(self, wait_for=None):
+        """Performs a single round of mcmc sampling (nsteps MC steps)"""
+        self.require('MCMC')
+        self.unpackJ()
+        rngoffset, _ = self.updateRngPos()
+        self.repackedSeqT['main'] = False
+        s = self._begin()
+        betas = self._ptr('Bs') if getattr(self, 'tempering', False) else None
+        _lib.call('mi3_metropolis', self._ptr('Junpacked'), self._ptr('rngstates'), int(rngoffset),
+                  self._ptr('randpos'), self.nsteps, betas, self.beta, self._ptr('seq main'),
+                  self.nseq['main'], self.L, self.q, self._ptr('status'), self._s)
+        return self.logevt('mcmc', s)
+
+    # ------------------------------------------------------------ statistics
+    def calcBicounts(self, seqbufname, wait_for=None):
+        nseq = self.nseq[seqbufname]
+        s = self._begin()
+        _lib.call('mi3_bicounts', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, self._ptr('bicount'),
+                  self.L, self.q, self._s)
+        return self.logevt('calcBicounts', s)
+
+    def bicounts_to_bimarg(self, seqbufname='main', wait_for=None):
+        nseq = self.nseq[seqbufname]
+        s = self._begin()
+        _lib.call('mi3_bicounts_to_bimarg', self._ptr('bicount'), self._ptr('bi'), nseq, self.L, self.q,
+                  self._s)
+        return self.logevt('bicounts_to_bimarg', s)
+
+    def calcEnergies(self, seqbufname, Jbufname='J', wait_for=None):
+        nseq = self.nseq[seqbufname]
+        s = self._begin()
+        _lib.call('mi3_energies', self._ptr(Jbufname), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
+                  self.Ebufs[seqbufname].data_ptr(), self.L, self.q, self._ptr('ws energies'),
+                  self._wsbytes('ws energies'), self._s)
+        return self.logevt('getEnergies', s)
+
+    def min_buf(self, buf, wait_for=None):
+        self.require('Jstep')
+        buflen = int(np.prod(self.buf_spec[buf][1]))
+        s = self._begin()
+        _lib.call('mi3_min_floats', self._ptr(buf), buflen, self._ptr('minout'), self._s)
+        return self.logevt('min_buf', s)
+
+    def weight_statistics(self, buf='main', wait_for=None):
+        self.require('Jstep')
+        nseq = self.nseq[buf]
+        s = self._begin()
+        _lib.call('mi3_weight_stats', self._ptr('weights'), nseq, self._ptr('weightstats'),
+                  self._ptr('weightstats64'), self._ptr('ws reduce'), self._wsbytes('ws reduce'), self._s)
+        return self.logevt('weight_statistics', s)
+
+    def dE_to_weights(self, buf='main', offset=0., wait_for=None):
+        self.require('Jstep')
+        nseq = self.nseq[buf]
+        s = self._begin()
+        _lib.call('mi3_dE_to_weights', float(offset), self._ptr('E main'), self._ptr('weights'), nseq, self._s)
+        return self.logevt('dE_to_weights', s)
+
+    def weights_fused(self, offset=0., buf='main'):
+        """dE -> weights, minout = min(0, min dE), weightstats in one pass
+        (same results as min_buf + dE_to_weights + weight_statistics)."""
+        self.require('Jstep')
+        nseq = self.nseq[buf]
+        s = self._begin()
+        _lib.call('mi3_weights_fused', float(offset), self._ptr('E main'), self._ptr('weights'), nseq,
+                  self._ptr('minout'), self._ptr('weightstats'), self._ptr('weightstats64'),
+                  self._ptr('ws reduce'), self._wsbytes('ws reduce'), self._s)
+        return self.logevt('weights_fused', s)
+
+    def fixed_beta_weights(self, ref_E, seqbufname='main', wait_for=None):
+        self.require('Jstep')
+        nseq = self.nseq[seqbufname]
+        s = self._begin()
+        _lib.call('mi3_fixed_beta_weights', float(self.beta), float(ref_E), self.Ebufs[seqbufname].data_ptr(),
+                  self._ptr('weights'), nseq, self._s)
+        return self.logevt('fixed_beta_weights', s)
+
+    def weightedMarg(self, seqbufname='main', wait_for=None):
+        self.require('Jstep')
+        nseq = self.nseq[seqbufname]
+        s = self._begin()
+        _lib.call('mi3_weighted_marg', self._ptr('weights'), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
+                  self._ptr('bi'), self.L, self.q, self._s)
+        return self.logevt('weightedMarg', s)
+
+    def renormalize_bimarg(self, wait_for=None):
+        s = self._begin()
+        _lib.call('mi3_renormalize_bimarg', self._ptr('bi'), self.L, self.q, self._s)
+        return self.logevt('renormalize_bimarg', s)
+
+    def addFloatBuf(self, dstname, srcname, wait_for=None):
+        dst, src = self.bufs[dstname], self.bufs[srcname]
+        if dst.numel() != src.numel():
+            raise Exception('Tried to add bufs of different sizes')
+        buflen = int(np.prod(self.buf_spec[dstname][1]))
+        s = self._begin()
+        _lib.call('mi3_add_float_bufs', dst.data_ptr(), src.data_ptr(), buflen, self._s)
+        return self.logevt('addbuf', s)
+
+    def addBiBuffer(self, bufname, otherbuf, wait_for=None):
+        selfbuf = self.bufs[bufname]
+        if selfbuf.numel() != otherbuf.numel():
+            raise Exception('Tried to add bufs of different sizes')
+        if otherbuf.device != self.device:
+            with torch.cuda.stream(self.stream):
+                otherbuf = otherbuf.to(self.device, non_blocking=False)
+        s = self._begin()
+        _lib.call('mi3_add_float_bufs', selfbuf.data_ptr(), otherbuf.data_ptr(), self.nPairs * self.q * self.q,
+                  self._s)
+        return self.logevt('addbibuf', s)
+
+    # ------------------------------------------------------------ Newton step
+    def updateJ(self, gamma, pc, Jbuf='dJ', wait_for=None):
+        self.require('Jstep')
+        s = self._begin()
+        p = self._ptr(Jbuf)
+        _lib.call('mi3_update_j', self._ptr('bi target'), self._ptr('bi'), float(gamma), float(pc), p, p,
+                  self.L, self.q, self._s)
+        self.unpackedJ = False
+        return self.logevt('updateJ', s)
+
+    def reg_l1z(self, gamma, pc, lJ, wait_for=None):
+        self.require('Jstep')
+        s = self._begin()
+        _lib.call('mi3_reg_l1z', self._ptr('bi'), float(gamma), float(pc), float(lJ), self._ptr('J'),
+                  self._ptr('dJ'), self.L, self.q, self._s)
+        self.unpackedJ = None
+        return self.logevt('reg_l1z', s)
+
+    def reg_l2z(self, gamma, pc, lJ, wait_for=None):
+        self.require('Jstep')
+        s = self._begin()
+        _lib.call('mi3_reg_l2z', self._ptr('bi'), float(gamma), float(pc), float(lJ), self._ptr('J'),
+                  self._ptr('dJ'), self.L, self.q, self._s)
+        self.unpackedJ = None
+        return self.logevt('reg_l2z', s)
+
+    def _reg_not_built(self, name):
+        raise NotImplementedError("regularizer {} is not built yet (only l1z and l2z)".format(name))
+
+    def reg_SCADJ(self, *a, **k):
+        self._reg_not_built('SCADJ')
+
+    def reg_Xij(self, *a, **k):
+        self._reg_not_built('Xij')
+
+    def reg_X(self, *a, **k):
+        self._reg_not_built('X')
+
+    def reg_SCADX(self, *a, **k):
+        self._reg_not_built('SCADX')
+
+    def reg_expX(self, *a, **k):
+        self._reg_not_built('expX')
+
+    def reg_ddE(self, *a, **k):
+        self._reg_not_built('ddE')
+
+    def reg_SCADddE(self, *a, **k):
+        self._reg_not_built('SCADddE')
+
+    # ------------------------------------------------------------ host I/O
+    def getBuf(self, bufname, truncateLarge=True, wait_for=None):
+        """Copy a device buffer to host; returns a FutureBuf
+        (mcmcGPU.py:845-867)."""
+        buftype, bufshape = self.buf_spec[bufname]
+        dev = self.bufs[bufname]
+        host = torch.empty(dev.shape, dtype=dev.dtype, pin_memory=True)
+        s = self._begin()
+        with torch.cuda.stream(self.stream):
+            host.copy_(dev, non_blocking=True)
+        evt = torch.cuda.Event()
+        evt.record(self.stream)
+        self.logevt('getBuf', s, host.numel() * host.element_size())
+        L, q = self.L, self.q
+
+        if bufname == 'Junpacked':
+            stride = int(_lib.query('mi3_jrows_stride', L, q))
+
+            def post(b):
+                a = b.numpy().reshape(L, stride)[:, :L * q * q]
+                return a.reshape(L * L, q * q).copy()
+            return FutureBuf(host, evt, post, self)
+
+        shape = _full_shape(buftype, bufshape)
+
+        def post(b):
+            a = b.numpy().view(_base_dtype(buftype))
+            a = a[:int(np.prod(shape))].reshape(shape)
+            if bufname.split()[0] == 'seq':
+                return self.unpackSeqs_4(a)
+            return a.copy()
+        return FutureBuf(host, evt, post, self)
+
+    def setBuf(self, bufname, buf, wait_for=None):
+        """Host (numpy) or device (tensor) -> device buffer, with the
+        reference's dtype/shape checks (mcmcGPU.py:869-907)."""
+        dev = self.bufs[bufname]
+        if isinstance(buf, torch.Tensor):
+            s = self._begin()
+            with torch.cuda.stream(self.stream):
+                src = buf.reshape(-1).view(dev.dtype) if buf.dtype != dev.dtype else buf.reshape(-1)
+                dev[:src.numel()].copy_(src, non_blocking=True)
+            evt = self.logevt('setBuf', s, src.numel() * src.element_size())
+            if bufname.split()[0] == 'J':
+                self.unpackedJ = None
+            return evt
+
+        if bufname.split()[0] == 'seq':
+            buf = self.packSeqs_4(np.asarray(buf))
+
+        buftype, bufshape = self.buf_spec[bufname]
+        if not isinstance(buf, np.ndarray):
+            buf = np.array(buf, dtype=buftype)
+        if np.dtype(buftype) != buf.dtype:
+            raise ValueError("Buffer dtype mismatch.Expected {}, got {}".format(np.dtype(buftype), buf.dtype))
+        if _full_shape(buftype, bufshape) != buf.shape and not (bufshape == (1,) or buf.size == 1):
+            raise ValueError("Buffer size mismatch. Expected {}, got {}".format(bufshape, buf.shape))
+
+        raw = np.ascontiguousarray(buf).reshape(-1).view(np.uint8)
+        host = self._staging_for(bufname, raw.size)
+        host.numpy()[:] = raw
+        s = self._begin()
+        with torch.cuda.stream(self.stream):
+            dev.view(torch.uint8)[:raw.size].copy_(host, non_blocking=True)
+        evt = torch.cuda.Event()
+        evt.record(self.stream)
+        self._staging[bufname][1] = evt
+        self.logevt('setBuf', s, raw.size)
+        if bufname.split()[0] == 'J':
+            self.unpackedJ = None
+        if bufname.split()[0] == 'seq':
+            self.repackedSeqT[bufname.split()[1]] = False
+        return evt
+
+    def _staging_for(self, bufname, nbytes):
+        """Pinned host staging buffer reused per device buffer; waits for the
+        previous copy out of it before handing it back."""
+        st = getattr(self, '_staging', None)
+        if st is None:
+            st = self._staging = {}
+        ent = st.get(bufname)
+        if ent is not None and ent[0].numel() >= nbytes:
+            if ent[1] is not None:
+                ent[1].synchronize()
+            return ent[0][:nbytes]
+        host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        st[bufname] = [host, None]
+        return host
+
+    def fillBuf(self, bufname, val, wait_for=None):
+        dev = self.bufs[bufname]
+        with torch.cuda.stream(self.stream):
+            if dev.dtype in (torch.float32, torch.float64):
+                dev.fill_(float(val))
+            else:
+                dev.fill_(int(val))
+        self.logevt('fill_buffer')
+
+    def fillSeqs(self, startseq, seqbufname='main', wait_for=None):
+        nseq = self.nseq[seqbufname]
+        self.setBuf('seq ' + seqbufname, np.tile(np.asarray(startseq, dtype='<u1'), (nseq, 1)))
+
+    def storeSeqs(self, seqs=None, wait_for=None):
+        raise NotImplementedError("large sequence buffers are not part of the single-device path")
+
+    def wait(self):
+        self.stream.synchronize()
+        while self._pending_host:
+            self._pending_host.popleft()
+        self._check_status()
+
+
+################################################################################
+
+def printDevice(log, d):
+    p = torch.cuda.get_device_properties(d)
+    log("  Device '{}':\n".format(p.name))
+    log("    Compute capability: {}.{}\n".format(p.major, p.minor))
+    log("    Multiprocessors: {}\n".format(p.multi_processor_count))
+    log("    Global Mem Size: {}\n".format(p.total_memory))
+
+
+def unpackJ_CPU(couplings):
+    """(nPairs, q*q) -> (L*L, q*q) with the transposed mirror
+    (mcmcGPU.py:1022-1034)."""
+    from .potts import getLq
+    L, q = getLq(couplings)
+    full = np.zeros((L * L, q * q), dtype='<f4')
+    n = 0
+    for i in range(L - 1):
+        for j in range(i + 1, L):
+            c = couplings[n, :]
+            full[L * i + j, :] = c
+            full[L * j + i, :] = c.reshape((q, q)).T.flatten()
+            n += 1
+    return full
+
+
+def setup_GPU_context(param, log):
+    """Select the CUDA devices to use (mcmcGPU.py:1038-1100 counterpart).
+    param.gpuspec: None (all visible devices) or a comma separated list of
+    device indices.  No run-time compilation: the kernels are prebuilt."""
+    if not torch.cuda.is_available():
+        raise Exception("Error: No GPUs found")
+    _lib.load()
+    if param.get('gpuspec') is not None:
+        devs = [int(x.split(':')[-1]) for x in str(param['gpuspec']).split(',')]
+    else:
+        devs = list(range(torch.cuda.device_count()))
+    log("Using CUDA devices {}".format(devs))
+    return devs
+
+
+def initGPU(devnum, device, nwalkers, param, log):
+    """(mcmcGPU.py:1102-1119 counterpart)"""
+    wgsize = param.get('wgsize', 512)
+    if wgsize not in [1 << n for n in range(32)]:
+        raise Exception("wgsize must be a power of two")
+    return MCMCGPU((device, devnum), param['L'], param['q'], nwalkers, wgsize, param.get('outdir'), 1024,
+                   param.get('rngseed', 0), profile=param.get('profile', False), beta=param.get('beta'))
+
+
+def wgsize_heuristic(q, wgsize='auto'):
+    if wgsize == 'auto':
+        wgsize = 256
+        while wgsize < q * q:
+            wgsize *= 2
+        return wgsize
+    wgsize = int(wgsize)
+    if wgsize < q * q:
+        raise Exception("Must have wgsize >= q*q, but got {} < {}".format(wgsize, q * q))
+    return wgsize
+
+
+def histogram_heuristic(q):
+    """(NHIST, HISTWS) of the reference (mcmcGPU.py:1135-1163); kept for
+    interface parity -- the B200 kernels pick their own tiling."""
+    nhist = 4096 // (q * q)
+    if nhist == 0:
+        raise Exception("alphabet size too large to make histogram on gpu")
+    nhist = 2 ** int(np.log2(nhist))
+    if q <= 12:
+        hist_ws = 512
+    elif q <= 16:
+        hist_ws = 256
+    else:
+        hist_ws = 128
+    if nhist > hist_ws:
+        nhist = hist_ws
+    return nhist, hist_ws

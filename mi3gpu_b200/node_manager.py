@@ -1,0 +1,226 @@
+"""Device-group facade: the reference's GPU_node (mi3gpu/node_manager.py:44-312).
+
+The host algorithm talks to a GPU_node, which fans each call out to its
+MCMCGPU devices and merges results.  The hot path of this library runs on one
+device; with one device merge_bimarg is the renormalisation, exactly as in the
+reference (node_manager.py:283-287).  Several devices in one process are
+still accepted (walkers split across them, bimarginals summed on device 0),
+for completeness rather than speed.
+"""
+import numpy as np
+
+
+def sumarr(arrlist):
+    tot = arrlist[0].copy()
+    for a in arrlist[1:]:
+        np.add(tot, a, tot)
+    return tot
+
+
+def meanarr(arrlist):
+    return sumarr(arrlist) / len(arrlist)
+
+
+def skip_single(f):
+    def skipper(x):
+        if len(x) == 1:
+            return x[0]
+        return f(x)
+    return skipper
+
+
+class GPU_node:
+    def __init__(self, gpus):
+        self.gpus = gpus
+        self.head_node = self
+
+    @property
+    def head_gpu(self):
+        return type(self)([self.gpus[0]])
+
+    @property
+    def nwalkers(self):
+        return sum(g.nwalkers for g in self.gpus)
+
+    @property
+    def nseq(self):
+        return {'main': sum(g.nseq['main'] for g in self.gpus)}
+
+    @property
+    def ngpus(self):
+        return len(self.gpus)
+
+    @property
+    def gpu_list(self):
+        return ["({}) {}".format(g.gpunum, g.device) for g in self.gpus]
+
+    def initMCMC(self, nsteps):
+        # the MWC64X period 2^63 split evenly across devices (node_manager.py:73-81)
+        rng_span = np.uint64(2 ** 63) // np.uint64(self.ngpus)
+        rng_offsets = [np.uint64(i) * rng_span for i in range(self.ngpus)]
+        self._initMCMC_rng(nsteps, rng_offsets, rng_span)
+
+    def _initMCMC_rng(self, nsteps, rng_offsets, rng_span):
+        for gpu, offset in zip(self.gpus, rng_offsets):
+            gpu.initMCMC(nsteps, offset, rng_span)
+
+    def initJstep(self):
+        for gpu in self.gpus:
+            gpu.initJstep()
+
+    def logProfile(self):
+        for gpu in self.gpus:
+            gpu.logProfile()
+
+    def prepare_indep(self, unimarg):
+        for gpu in self.gpus:
+            gpu.prepare_indep(unimarg)
+
+    def gen_indep(self, bufname):
+        for gpu in self.gpus:
+            gpu.gen_indep(bufname)
+
+    def runMCMC(self):
+        for gpu in self.gpus:
+            gpu.runMCMC()
+
+    def calcEnergies(self, seqbufname, Jbufname='J'):
+        for gpu in self.gpus:
+            gpu.calcEnergies(seqbufname, Jbufname)
+
+    def calcBicounts(self, seqbufname):
+        for gpu in self.gpus:
+            gpu.calcBicounts(seqbufname)
+
+    def bicounts_to_bimarg(self, seqbufname='main'):
+        for gpu in self.gpus:
+            gpu.bicounts_to_bimarg(seqbufname)
+
+    def updateJ(self, gamma, pc, Jbuf='dJ'):
+        for gpu in self.gpus:
+            gpu.updateJ(gamma, pc, Jbuf)
+
+    def reg(self, name, param):
+        meth = 'reg_{}'.format(name)
+        for gpu in self.gpus:
+            getattr(gpu, meth)(*param)
+
+    def min_buf(self, buf):
+        for gpu in self.gpus:
+            gpu.min_buf(buf)
+
+    def weight_statistics(self, buf='main'):
+        for gpu in self.gpus:
+            gpu.weight_statistics(buf)
+
+    def dE_to_weights(self, offset=0., buf='main'):
+        # argument order as in the reference facade (node_manager.py:148-150)
+        for gpu in self.gpus:
+            gpu.dE_to_weights(offset, buf)
+
+    def weights_fused(self, offset=0., buf='main'):
+        for gpu in self.gpus:
+            gpu.weights_fused(offset, buf)
+
+    def fixed_beta_weights(self, ref_E, seqbufname='main'):
+        for gpu in self.gpus:
+            gpu.fixed_beta_weights(ref_E, seqbufname)
+
+    def weightedMarg(self, seqbufname):
+        for gpu in self.gpus:
+            gpu.weightedMarg(seqbufname)
+
+    def addFloatBuf(self, dstname, srcname):
+        for gpu in self.gpus:
+            gpu.addFloatBuf(dstname, srcname)
+
+    def renormalize_bimarg(self):
+        for gpu in self.gpus:
+            gpu.renormalize_bimarg()
+
+    def getBuf(self, bufname):
+        return [gpu.getBuf(bufname) for gpu in self.gpus]
+
+    def readBufs(self, bufnames):
+        if isinstance(bufnames, str):
+            return [buf.read() for buf in self.getBuf(bufnames)]
+        futures = [self.getBuf(bn) for bn in bufnames]
+        return [[fut.read() for fut in buff] for buff in futures]
+
+    groupfunc = {
+        'weights': skip_single(np.concatenate),
+        'E': skip_single(np.concatenate),
+        'Bs': skip_single(np.concatenate),
+        'bicount': skip_single(sumarr),
+        'bi': skip_single(meanarr),
+        'seq': skip_single(np.concatenate)}
+
+    def collect(self, bufs):
+        if isinstance(bufs, str):
+            func = self.groupfunc.get(bufs.split()[0], lambda x: x)
+            return func(self.readBufs(bufs))
+        ret = []
+        for bufname, arrs in zip(bufs, self.readBufs(bufs)):
+            func = self.groupfunc.get(bufname.split()[0], lambda x: x)
+            ret.append(func(arrs))
+        return ret
+
+    def setBuf(self, bufname, dat):
+        if isinstance(dat, list):
+            for gpu, buf in zip(self.gpus, dat):
+                gpu.setBuf(bufname, buf)
+        else:
+            for gpu in self.gpus:
+                gpu.setBuf(bufname, dat)
+
+    def fillBuf(self, bufname, val):
+        for gpu in self.gpus:
+            gpu.fillBuf(bufname, val)
+
+    def setSeqs(self, bufname, seqs, log=None):
+        if isinstance(seqs, np.ndarray) or len(seqs) == 1:
+            if not isinstance(seqs, np.ndarray):
+                seqs = seqs[0]
+            nbuf = self.nseq[bufname]
+            if seqs.shape[0] != nbuf:
+                raise Exception("Expected {} total sequences, got {}".format(nbuf, seqs.shape[0]))
+            seqs = np.split(seqs, self.ngpus)
+        elif len(seqs) != self.ngpus:
+            raise Exception("Expected {} sequence bufs, got {}".format(self.ngpus, len(seqs)))
+        if log:
+            log("Transferring {} seqs to gpu's {} seq buffer...".format(str([len(s) for s in seqs]), bufname))
+        for gpu, seq in zip(self.gpus, seqs):
+            gpu.setBuf('seq ' + bufname, seq)
+
+    def fillSeqs(self, seq):
+        for gpu in self.gpus:
+            gpu.fillSeqs(seq)
+
+    def reduce_node_bimarg(self):
+        """Pairwise tree sum of 'bi' onto device 0 (node_manager.py:254-281)."""
+        self.wait()
+        rgpus = self.gpus
+        while len(rgpus) > 1:
+            h = (len(rgpus) - 1) // 2 + 1
+            for even, odd in zip(rgpus[:h], rgpus[h:]):
+                even.addBiBuffer('bi', odd.bufs['bi'])
+            for even in rgpus[:h]:
+                even.wait()
+            rgpus = rgpus[:h]
+
+    def merge_bimarg(self):
+        if len(self.gpus) == 1:
+            # other code expects merge_bimarg to do renormalization
+            self.gpus[0].renormalize_bimarg()
+            return
+        self.reduce_node_bimarg()
+        self.gpus[0].renormalize_bimarg()
+        self.wait()
+        bibuf = self.gpus[0].bufs['bi']
+        for g in self.gpus[1:]:
+            g.setBuf('bi', bibuf.to(g.device))
+        self.wait()
+
+    def wait(self):
+        for g in self.gpus:
+            g.wait()

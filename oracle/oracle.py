@@ -1,0 +1,286 @@
+"""numpy front end of the CPU oracle (oracle/mi3_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+the CPU legs of bench.py as the checker (or the timed CPU port).  The
+library in mi3gpu_b200 never imports it.
+
+Each function restates one kernel of the reference's mi3gpu/mcmc.cl (or a
+host routine of mi3gpu/mcmcGPU.py) -- the C file cites the lines -- and
+takes/returns arrays in the reference's layouts.
+"""
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_LIB = HERE / "_build" / "libmi3oracle.so"
+_REF_RNG = HERE / "_ref" / "libmwc64x_ref.so"
+_REF_CPU = HERE / "_ref" / "mcmc_cpu"
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_c = ctypes
+
+
+def _build():
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not _LIB.exists():
+            _build()
+        L = ctypes.CDLL(str(_LIB))
+        sig = {
+            "mi3o_init_rng": [_u32p, _c.c_uint32, _c.c_uint64, _c.c_uint64],
+            "mi3o_vec2_next": [_u32p, _c.POINTER(_c.c_uint32), _c.POINTER(_c.c_uint32)],
+            "mi3o_mwc_skip": [_c.POINTER(_c.c_uint32), _c.POINTER(_c.c_uint32), _c.c_uint64],
+            "mi3o_accept": [_c.c_float, _c.c_float],
+            "mi3o_unpack_j": [_f32p, _f32p, _c.c_uint32, _c.c_uint32, _c.c_uint64],
+            "mi3o_metropolis": [_f32p, _c.c_uint64, _u32p, _c.c_uint32, _u32p, _c.c_uint32,
+                                _c.c_void_p, _c.c_float, _u32p, _c.c_uint32, _c.c_uint32,
+                                _c.c_uint32, _c.c_uint32, _c.c_uint32],
+            "mi3o_energies_kahan": [_f32p, _u32p, _c.c_uint32, _c.c_uint32, _f32p, _c.c_uint32, _c.c_uint32],
+            "mi3o_energies_f64": [_f32p, _u32p, _c.c_uint32, _c.c_uint32, _f64p, _c.c_uint32, _c.c_uint32],
+            "mi3o_count_bivariate": [_u32p, _c.c_uint32, _c.c_uint32, _u32p, _c.c_uint32, _c.c_uint32],
+            "mi3o_bicounts_to_bimarg": [_u32p, _f32p, _c.c_uint32, _c.c_uint64],
+            "mi3o_min_floats": [_f32p, _c.c_uint32],
+            "mi3o_weight_stats": [_f32p, _c.c_uint32, _f32p],
+            "mi3o_weight_stats_f64": [_f32p, _c.c_uint32, _f64p],
+            "mi3o_dE_to_weights": [_c.c_float, _f32p, _f32p, _c.c_uint32],
+            "mi3o_fixed_beta_weights": [_c.c_float, _c.c_float, _f32p, _f32p, _c.c_uint32],
+            "mi3o_weighted_marg_f64": [_f32p, _u32p, _c.c_uint32, _c.c_uint32, _f64p, _c.c_uint32, _c.c_uint32],
+            "mi3o_renormalize_bimarg": [_f32p, _c.c_uint64, _c.c_uint32],
+            "mi3o_zero_gauge_block": [_f32p, _f32p, _c.c_uint32],
+            "mi3o_updatedJ": [_f32p, _f32p, _c.c_float, _c.c_float, _f32p, _f32p, _c.c_uint64],
+            "mi3o_reg_lz": [_f32p, _c.c_float, _c.c_float, _c.c_float, _f32p, _f32p, _c.c_uint64,
+                            _c.c_uint32, _c.c_int],
+            "mi3o_gen_indep": [_u32p, _c.c_uint32, _c.c_uint32, _u32p, _f32p, _c.c_uint32, _c.c_uint32],
+            "mi3o_repack_seqs_T": [_u32p, _c.c_uint32, _u8p, _c.c_uint32, _c.c_uint32],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+        L.mi3o_accept.restype = _c.c_int
+        L.mi3o_min_floats.restype = _c.c_float
+        _lib = L
+    return _lib
+
+
+def ref_rng_lib():
+    """The reference's own mwc64x .cl sources compiled as C++ (oracle/_ref),
+    or None when they were not built (no reference tree)."""
+    if not _REF_RNG.exists():
+        try:
+            _build()
+        except Exception:
+            return None
+    if not _REF_RNG.exists():
+        return None
+    L = ctypes.CDLL(str(_REF_RNG))
+    L.ref_init_rng2.argtypes = [_u32p, _c.c_uint32, _c.c_uint64, _c.c_uint64]
+    L.ref_vec2_stream.argtypes = [_u32p, _c.c_uint32, _u32p]
+    L.ref_vec2_skip.argtypes = [_u32p, _c.c_uint64]
+    L.ref_scalar_seed.argtypes = [_c.c_uint64, _c.c_uint64, _c.c_uint64, _u32p]
+    L.ref_scalar_stream.argtypes = [_u32p, _c.c_uint32, _u32p]
+    L.ref_scalar_skip.argtypes = [_u32p, _c.c_uint64]
+    return L
+
+
+def ref_cpu_binary():
+    """Path of the reference's CPU generator built here, or None."""
+    if not _REF_CPU.exists():
+        try:
+            _build()
+        except Exception:
+            return None
+    return _REF_CPU if _REF_CPU.exists() else None
+
+
+# --------------------------------------------------------------- layouts
+def swords(L):
+    return (L - 1) // 4 + 1
+
+
+def pack_seqs(seqs):
+    """MCMCGPU.packSeqs_4 (mcmcGPU.py:333-347): (N, L) u1 -> (SWORDS, N) u4."""
+    seqs = np.asarray(seqs, dtype=np.uint8)
+    N, L = seqs.shape
+    sb = np.zeros((N, 4 * swords(L)), dtype=np.uint8)
+    sb[:, :L] = seqs
+    return np.ascontiguousarray(sb.view("<u4").T)
+
+
+def unpack_seqs(mem, L):
+    """MCMCGPU.unpackSeqs_4 (mcmcGPU.py:349-354)."""
+    mem = np.asarray(mem, dtype=np.uint32)
+    b = np.ascontiguousarray(mem.T).view(np.uint8)
+    return b[:, :L].copy()
+
+
+def jrow_stride(L, q):
+    n = L * q * q
+    return (n + 3) & ~3
+
+
+def npairs(L):
+    return L * (L - 1) // 2
+
+
+# ------------------------------------------------------------- kernels
+def init_rng(n, offset, span):
+    st = np.zeros(4 * n, np.uint32)
+    lib().mi3o_init_rng(st, n, int(offset), int(span))
+    return st.reshape(n, 4)
+
+
+def rng_stream(state, count):
+    """count vec2 draws from one walker state (modified in place)."""
+    s = np.ascontiguousarray(state, dtype=np.uint32).copy()
+    out = np.zeros((count, 2), np.uint32)
+    r0, r1 = _c.c_uint32(), _c.c_uint32()
+    for k in range(count):
+        lib().mi3o_vec2_next(s, _c.byref(r0), _c.byref(r1))
+        out[k] = (r0.value, r1.value)
+    state[:] = s
+    return out
+
+
+def unpack_j(J, L, q):
+    J = np.ascontiguousarray(J, dtype=np.float32)
+    stride = jrow_stride(L, q)
+    Ju = np.zeros(L * stride, np.float32)
+    lib().mi3o_unpack_j(J, Ju, L, q, stride)
+    return Ju.reshape(L, stride)
+
+
+def metropolis(J, rngstates, position_list, position_offset, nsteps, seqmem, L, q,
+               betas=None, beta=1.0, walkers=None):
+    """Runs the sampler in place on (rngstates (N,4) u4, seqmem (SWORDS,N) u4)."""
+    Ju = unpack_j(J, L, q)
+    N = seqmem.shape[1]
+    g0, g1 = (0, N) if walkers is None else walkers
+    assert rngstates.flags.c_contiguous and seqmem.flags.c_contiguous
+    bp = None
+    if betas is not None:
+        betas = np.ascontiguousarray(betas, dtype=np.float32)
+        bp = betas.ctypes.data
+    lib().mi3o_metropolis(Ju.reshape(-1), jrow_stride(L, q), rngstates.reshape(-1),
+                          int(position_offset), np.ascontiguousarray(position_list, np.uint32),
+                          int(nsteps), bp, float(beta), seqmem.reshape(-1), N, L, q, g0, g1)
+
+
+def energies_kahan(J, seqmem, L, q, nseq=None):
+    buflen = seqmem.shape[1]
+    nseq = buflen if nseq is None else nseq
+    E = np.zeros(nseq, np.float32)
+    lib().mi3o_energies_kahan(np.ascontiguousarray(J, np.float32), np.ascontiguousarray(seqmem).reshape(-1),
+                              buflen, nseq, E, L, q)
+    return E
+
+
+def energies_f64(J, seqmem, L, q, nseq=None):
+    buflen = seqmem.shape[1]
+    nseq = buflen if nseq is None else nseq
+    E = np.zeros(nseq, np.float64)
+    lib().mi3o_energies_f64(np.ascontiguousarray(J, np.float32), np.ascontiguousarray(seqmem).reshape(-1),
+                            buflen, nseq, E, L, q)
+    return E
+
+
+def bicounts(seqmem, L, q, nseq=None):
+    buflen = seqmem.shape[1]
+    nseq = buflen if nseq is None else nseq
+    out = np.zeros((npairs(L), q * q), np.uint32)
+    lib().mi3o_count_bivariate(np.ascontiguousarray(seqmem).reshape(-1), buflen, nseq, out.reshape(-1), L, q)
+    return out
+
+
+def bicounts_to_bimarg(c, nseq):
+    c = np.ascontiguousarray(c, np.uint32)
+    out = np.zeros(c.shape, np.float32)
+    lib().mi3o_bicounts_to_bimarg(c.reshape(-1), out.reshape(-1), nseq, c.size)
+    return out
+
+
+def min_floats(x):
+    return float(lib().mi3o_min_floats(np.ascontiguousarray(x, np.float32), len(x)))
+
+
+def weight_stats(w):
+    out = np.zeros(2, np.float32)
+    lib().mi3o_weight_stats(np.ascontiguousarray(w, np.float32), len(w), out)
+    return out
+
+
+def weight_stats_f64(w):
+    out = np.zeros(2, np.float64)
+    lib().mi3o_weight_stats_f64(np.ascontiguousarray(w, np.float32), len(w), out)
+    return out
+
+
+def dE_to_weights(ref, dE):
+    dE = np.ascontiguousarray(dE, np.float32)
+    w = np.zeros_like(dE)
+    lib().mi3o_dE_to_weights(float(ref), dE, w, len(dE))
+    return w
+
+
+def fixed_beta_weights(beta, ref, E):
+    E = np.ascontiguousarray(E, np.float32)
+    w = np.zeros_like(E)
+    lib().mi3o_fixed_beta_weights(float(beta), float(ref), E, w, len(E))
+    return w
+
+
+def weighted_marg_f64(w, seqmem, L, q, nseq=None):
+    buflen = seqmem.shape[1]
+    nseq = buflen if nseq is None else nseq
+    out = np.zeros((npairs(L), q * q), np.float64)
+    lib().mi3o_weighted_marg_f64(np.ascontiguousarray(w, np.float32), np.ascontiguousarray(seqmem).reshape(-1),
+                                 buflen, nseq, out.reshape(-1), L, q)
+    return out
+
+
+def renormalize_bimarg(bi, q):
+    bi = np.ascontiguousarray(bi, np.float32).copy()
+    lib().mi3o_renormalize_bimarg(bi.reshape(-1), bi.shape[0], q)
+    return bi
+
+
+def updatedJ(bt, bi, gamma, pc, Ji):
+    Jo = np.zeros_like(np.asarray(Ji, np.float32))
+    lib().mi3o_updatedJ(np.ascontiguousarray(bt, np.float32).reshape(-1),
+                        np.ascontiguousarray(bi, np.float32).reshape(-1), float(gamma), float(pc),
+                        np.ascontiguousarray(Ji, np.float32).reshape(-1), Jo.reshape(-1), Jo.size)
+    return Jo
+
+
+def reg_lz(bi, gamma, pc, lJ, J, dJ, q, l2):
+    dJ = np.ascontiguousarray(dJ, np.float32).copy()
+    lib().mi3o_reg_lz(np.ascontiguousarray(bi, np.float32).reshape(-1), float(gamma), float(pc), float(lJ),
+                      np.ascontiguousarray(J, np.float32).reshape(-1), dJ.reshape(-1), dJ.shape[0], q,
+                      1 if l2 else 0)
+    return dJ
+
+
+def gen_indep(seqmem, rngstates, cprob, L, q, nseq=None):
+    buflen = seqmem.shape[1]
+    nseq = buflen if nseq is None else nseq
+    lib().mi3o_gen_indep(seqmem.reshape(-1), buflen, nseq, rngstates.reshape(-1),
+                         np.ascontiguousarray(cprob, np.float32).reshape(-1), L, q)
+
+
+def repack_seqs_T(seqmem, L):
+    buf4len = seqmem.shape[1]
+    out = np.zeros((L, buf4len), np.uint8)
+    lib().mi3o_repack_seqs_T(np.ascontiguousarray(seqmem).reshape(-1), buf4len, out.reshape(-1), buf4len, L)
+    return out.view("<u4")

@@ -1,0 +1,81 @@
+"""The C ABI without a GPU: the library loads, exports every entry point
+declared in include/mi3b200.h with the ctypes signature the host binds, and
+rejects bad arguments with error codes before touching the device."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from mi3gpu_b200 import _lib
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    src = (ROOT / "include" / "mi3b200.h").read_text()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return re.findall(r"^\s*(?:const\s+)?[a-z0-9_]+\s*\*?\s*(mi3_[a-z0-9_A-Z]+)\s*\(", src, flags=re.M)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert len(names) >= 24
+    assert "mi3_metropolis" in names and "mi3_energies" in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    assert set(declared_functions()) == set(_lib.SIGNATURES)
+
+
+def test_abi_version_and_sizes():
+    lib = _lib.load()
+    assert lib.mi3_abi_version() == 1
+    assert lib.mi3_jrows_stride(232, 21) == 232 * 441  # already a multiple of 4
+    assert lib.mi3_jrows_stride(93, 21) % 4 == 0 and lib.mi3_jrows_stride(93, 21) >= 93 * 441
+    assert lib.mi3_energies_workspace(1 << 20) == 8 << 20
+    assert lib.mi3_weight_stats_workspace(1000) >= 16
+
+
+@pytest.mark.parametrize("name,args", [
+    ("mi3_metropolis", (None, None, 0, None, 10, None, 1.0, None, 512, 10, 4, None, None)),
+    ("mi3_energies", (None, None, 10, 10, None, 10, 4, None, 0, None)),
+    ("mi3_bicounts", (None, 10, 10, None, 10, 4, None)),
+    ("mi3_weighted_marg", (None, None, 10, 10, None, 10, 4, None)),
+    ("mi3_update_j", (None, None, 0.1, 0.1, None, None, 10, 4, None)),
+    ("mi3_reg_l1z", (None, 0.1, 0.1, 0.1, None, None, 10, 4, None)),
+    ("mi3_init_rng", (None, 10, 0, 1, None)),
+    ("mi3_unpack_j", (None, None, 10, 4, None)),
+    ("mi3_gen_indep", (None, 10, 10, None, None, 10, 4, None)),
+])
+def test_null_pointers_rejected(name, args):
+    with pytest.raises(_lib.Mi3Error) as e:
+        _lib.call(name, *args)
+    assert e.value.code == -1
+    assert name in str(e.value)
+
+
+def test_bad_shapes_rejected():
+    # non-null dummy addresses; validation must fail before any launch
+    p = 4096
+    with pytest.raises(_lib.Mi3Error) as e:
+        _lib.call("mi3_metropolis", p, p, 0, p, 10, None, 1.0, p, 500, 10, 4, p, None)   # nseqs % 128
+    assert e.value.code == -1
+    with pytest.raises(_lib.Mi3Error) as e:
+        _lib.call("mi3_metropolis", p + 4, p, 0, p, 10, None, 1.0, p, 512, 10, 4, p, None)  # Jrows misaligned
+    assert e.value.code == -3
+    with pytest.raises(_lib.Mi3Error) as e:
+        _lib.call("mi3_energies", p, p, 10, 20, p, 10, 4, p, 1 << 20, None)  # nseq > buflen
+    assert e.value.code == -1
+    with pytest.raises(_lib.Mi3Error) as e:
+        _lib.call("mi3_energies", p, p, 100, 100, p, 10, 4, p, 8, None)  # workspace too small
+    assert e.value.code == -4
+    with pytest.raises(_lib.Mi3Error) as e:
+        _lib.call("mi3_metropolis", p, p, 0, p, 10, None, 1.0, p, 512, 10, 300, p, None)  # q > 255
+    assert e.value.code == -1

@@ -1,0 +1,295 @@
+"""GPU parity: every kernel of libmi3b200, called through the C ABI, against
+the CPU oracle (itself pinned to the reference in test_oracle.py).
+
+Integer/byte/index results are bit-exact; floating-point tolerances are
+stated per test."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from mi3gpu_b200 import _lib
+from tests._util import dev, host, empty, stream, random_model
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(10, 5, 512), (48, 4, 1024), (37, 21, 512), (93, 4, 512), (64, 8, 640)]
+
+
+def _seqs(L, q, N, seed):
+    return np.random.default_rng(seed).integers(0, q, size=(N, L)).astype("<u1")
+
+
+@pytest.mark.parametrize("n,off,span", [(4096, 0, 2 ** 63 // (2 * 4096)),
+                                        (1024, 2 ** 62 + 12345, 987654321987),
+                                        (512, 3 * (2 ** 61), 2 ** 40)])
+def test_init_rng_bitexact(cuda, n, off, span):
+    st = empty((n, 4), np.uint32)
+    _lib.call("mi3_init_rng", st.data_ptr(), n, off, span, stream())
+    np.testing.assert_array_equal(host(st, np.uint32), oracle.init_rng(n, off, span))
+
+
+def test_init_rng_matches_reference_golden(cuda, golden):
+    for tag in "ab":
+        st = empty((64, 4), np.uint32)
+        _lib.call("mi3_init_rng", st.data_ptr(), 64, int(golden[f"rng_{tag}_offset"]),
+                  int(golden[f"rng_{tag}_span"]), stream())
+        np.testing.assert_array_equal(host(st, np.uint32), golden[f"rng_{tag}_states"])
+
+
+@pytest.mark.parametrize("L,q,N", SHAPES)
+def test_unpack_j_bitexact(cuda, L, q, N):
+    J = random_model(L, q, 1)
+    stride = int(_lib.query("mi3_jrows_stride", L, q))
+    Ju = empty((L, stride), np.float32)
+    Ju.fill_(7.0)
+    _lib.call("mi3_unpack_j", dev(J).data_ptr(), Ju.data_ptr(), L, q, stream())
+    np.testing.assert_array_equal(host(Ju), oracle.unpack_j(J, L, q))
+
+
+@pytest.mark.parametrize("L,q,N", SHAPES)
+@pytest.mark.parametrize("nsteps", [1, 37, 300])
+def test_metropolis_trajectory_bitexact(cuda, L, q, N, nsteps):
+    """Same walkers, same RNG streams, same site list: identical sequences and
+    RNG states after nsteps proposals."""
+    J = random_model(L, q, 2, sigma=0.5)
+    seqs = _seqs(L, q, N, 3)
+    mem = oracle.pack_seqs(seqs)
+    st = oracle.init_rng(N, 0, 2 ** 63 // (2 * N))
+    pos = np.random.RandomState(11).randint(0, L, size=nsteps + 13).astype("<u4")
+    off = 13 if nsteps < 100 else 0
+    stride = int(_lib.query("mi3_jrows_stride", L, q))
+    Ju = empty((L, stride), np.float32)
+    dJ, dmem, dst, dpos = dev(J), dev(mem), dev(st), dev(pos)
+    status = empty((1,), np.int32)
+    _lib.call("mi3_unpack_j", dJ.data_ptr(), Ju.data_ptr(), L, q, stream())
+    _lib.call("mi3_metropolis", Ju.data_ptr(), dst.data_ptr(), off, dpos.data_ptr(), nsteps, None, 1.0,
+              dmem.data_ptr(), N, L, q, status.data_ptr(), stream())
+    g_mem, g_st = host(dmem, np.uint32), host(dst, np.uint32)
+    assert int(host(status)[0]) == 0
+    o_mem, o_st = mem.copy(), st.copy()
+    oracle.metropolis(J, o_st, pos, off, nsteps, o_mem, L, q)
+    np.testing.assert_array_equal(g_st, o_st)
+    np.testing.assert_array_equal(g_mem, o_mem)
+    assert (g_mem != mem).any()  # something was accepted
+
+
+def test_metropolis_betas(cuda):
+    L, q, N, nsteps = 20, 6, 512, 64
+    J = random_model(L, q, 4, sigma=0.6)
+    seqs = _seqs(L, q, N, 5)
+    mem = oracle.pack_seqs(seqs)
+    st = oracle.init_rng(N, 77, 10 ** 9)
+    pos = np.random.RandomState(1).randint(0, L, size=nsteps).astype("<u4")
+    betas = np.linspace(0.2, 2.0, N).astype("<f4")
+    stride = int(_lib.query("mi3_jrows_stride", L, q))
+    Ju = empty((L, stride), np.float32)
+    dmem, dst = dev(mem), dev(st)
+    status = empty((1,), np.int32)
+    _lib.call("mi3_unpack_j", dev(J).data_ptr(), Ju.data_ptr(), L, q, stream())
+    _lib.call("mi3_metropolis", Ju.data_ptr(), dst.data_ptr(), 0, dev(pos).data_ptr(), nsteps,
+              dev(betas).data_ptr(), 1.0, dmem.data_ptr(), N, L, q, status.data_ptr(), stream())
+    oracle.metropolis(J, st, pos, 0, nsteps, mem, L, q, betas=betas)
+    np.testing.assert_array_equal(host(dmem, np.uint32), mem)
+    np.testing.assert_array_equal(host(dst, np.uint32), st)
+
+
+@pytest.mark.parametrize("L,q,N", SHAPES + [(232, 21, 512)])
+def test_energies_vs_fp64(cuda, L, q, N):
+    """|E - E_fp64| <= 1e-5 * max(1, |E_fp64|) (the bar); measured error is
+    the float rounding of an exact-to-1e-12 sum."""
+    J = random_model(L, q, 6)
+    seqs = _seqs(L, q, N, 7)
+    mem = oracle.pack_seqs(seqs)
+    E = empty((N,), np.float32)
+    ws = empty((int(_lib.query("mi3_energies_workspace", N)) // 8 + 1,), np.int64)
+    _lib.call("mi3_energies", dev(J).data_ptr(), dev(mem).data_ptr(), N, N, E.data_ptr(), L, q, ws.data_ptr(),
+              ws.numel() * 8, stream())
+    e = host(E)
+    e64 = oracle.energies_f64(J, mem, L, q)
+    err = np.abs(e - e64) / np.maximum(1.0, np.abs(e64))
+    assert err.max() <= 1e-5
+    # deterministic: a second call gives identical bits
+    E2 = empty((N,), np.float32)
+    _lib.call("mi3_energies", dev(J).data_ptr(), dev(mem).data_ptr(), N, N, E2.data_ptr(), L, q, ws.data_ptr(),
+              ws.numel() * 8, stream())
+    np.testing.assert_array_equal(host(E2), e)
+
+
+def test_energies_golden(cuda, golden):
+    for tag in "ABC":
+        J, seqs = golden[f"m{tag}_J"], golden[f"m{tag}_seqs"]
+        N, L = seqs.shape
+        q = int(round(np.sqrt(J.shape[1])))
+        E = empty((N,), np.float32)
+        ws = empty((N + 1,), np.int64)
+        _lib.call("mi3_energies", dev(J).data_ptr(), dev(oracle.pack_seqs(seqs)).data_ptr(), N, N, E.data_ptr(),
+                  L, q, ws.data_ptr(), ws.numel() * 8, stream())
+        e64 = golden[f"m{tag}_E64"]
+        assert (np.abs(host(E) - e64) / np.maximum(1.0, np.abs(e64))).max() <= 1e-5
+
+
+@pytest.mark.parametrize("L,q,N", SHAPES + [(232, 21, 1024)])
+def test_bicounts_bitexact(cuda, L, q, N):
+    seqs = _seqs(L, q, N, 8)
+    mem = oracle.pack_seqs(seqs)
+    out = empty((L * (L - 1) // 2, q * q), np.uint32)
+    _lib.call("mi3_bicounts", dev(mem).data_ptr(), N, N, out.data_ptr(), L, q, stream())
+    np.testing.assert_array_equal(host(out, np.uint32), oracle.bicounts(mem, L, q))
+
+
+def test_bicounts_golden(cuda, golden):
+    for tag in "ABC":
+        J, seqs = golden[f"m{tag}_J"], golden[f"m{tag}_seqs"]
+        N, L = seqs.shape
+        q = int(round(np.sqrt(J.shape[1])))
+        out = empty((L * (L - 1) // 2, q * q), np.uint32)
+        _lib.call("mi3_bicounts", dev(oracle.pack_seqs(seqs)).data_ptr(), N, N, out.data_ptr(), L, q, stream())
+        np.testing.assert_array_equal(host(out, np.uint32), golden[f"m{tag}_bicounts"])
+
+
+def test_bicounts_partial_buffer(cuda):
+    """nseq < buflen: only the first nseq columns are counted."""
+    L, q, N = 30, 7, 1024
+    seqs = _seqs(L, q, N, 9)
+    mem = oracle.pack_seqs(seqs)
+    out = empty((L * (L - 1) // 2, q * q), np.uint32)
+    _lib.call("mi3_bicounts", dev(mem).data_ptr(), N, 700, out.data_ptr(), L, q, stream())
+    np.testing.assert_array_equal(host(out, np.uint32), oracle.bicounts(mem, L, q, nseq=700))
+
+
+@pytest.mark.parametrize("L,q,N", SHAPES)
+def test_weighted_marg(cuda, L, q, N):
+    """float accumulation vs double oracle: rtol 1e-5 of each pair's total."""
+    seqs = _seqs(L, q, N, 10)
+    mem = oracle.pack_seqs(seqs)
+    w = np.random.default_rng(11).uniform(0.01, 3.0, size=N).astype("<f4")
+    out = empty((L * (L - 1) // 2, q * q), np.float32)
+    _lib.call("mi3_weighted_marg", dev(w).data_ptr(), dev(mem).data_ptr(), N, N, out.data_ptr(), L, q, stream())
+    ref = oracle.weighted_marg_f64(w, mem, L, q)
+    tot = ref.sum(axis=1, keepdims=True)
+    assert (np.abs(host(out) - ref) / tot).max() < 1e-5
+
+
+def test_weighted_marg_golden(cuda, golden):
+    for tag in "ABC":
+        J, seqs, w = golden[f"m{tag}_J"], golden[f"m{tag}_seqs"], golden[f"m{tag}_w"]
+        N, L = seqs.shape
+        q = int(round(np.sqrt(J.shape[1])))
+        out = empty((L * (L - 1) // 2, q * q), np.float32)
+        _lib.call("mi3_weighted_marg", dev(w).data_ptr(), dev(oracle.pack_seqs(seqs)).data_ptr(), N, N,
+                  out.data_ptr(), L, q, stream())
+        ref = golden[f"m{tag}_wcounts"]
+        assert (np.abs(host(out) - ref) / ref.sum(axis=1, keepdims=True)).max() < 1e-5
+
+
+@pytest.mark.parametrize("q", [2, 4, 5, 8, 21])
+def test_renormalize_bitexact(cuda, q):
+    L = 17
+    bi = np.random.default_rng(q).uniform(0, 1, size=(L * (L - 1) // 2, q * q)).astype("<f4")
+    d = dev(bi)
+    _lib.call("mi3_renormalize_bimarg", d.data_ptr(), L, q, stream())
+    np.testing.assert_array_equal(host(d), oracle.renormalize_bimarg(bi, q))
+
+
+def test_bicounts_to_bimarg(cuda):
+    L, q = 12, 5
+    c = np.random.default_rng(1).integers(0, 1000, size=(66, 25)).astype("<u4")
+    out = empty((66, 25), np.float32)
+    _lib.call("mi3_bicounts_to_bimarg", dev(c).data_ptr(), out.data_ptr(), 4096, L, q, stream())
+    np.testing.assert_array_equal(host(out), oracle.bicounts_to_bimarg(c, 4096))
+
+
+def test_update_j_bitexact(cuda):
+    L, q = 40, 21
+    rng = np.random.default_rng(12)
+    n = (L * (L - 1) // 2, q * q)
+    bt, bi = rng.uniform(0, 0.2, size=n).astype("<f4"), rng.uniform(0, 0.2, size=n).astype("<f4")
+    Ji = rng.normal(0, 0.1, size=n).astype("<f4")
+    d = dev(Ji)
+    _lib.call("mi3_update_j", dev(bt).data_ptr(), dev(bi).data_ptr(), 4e-4, 1e-3, d.data_ptr(), d.data_ptr(),
+              L, q, stream())
+    np.testing.assert_array_equal(host(d), oracle.updatedJ(bt, bi, 4e-4, 1e-3, Ji))
+
+
+@pytest.mark.parametrize("l2", [False, True])
+@pytest.mark.parametrize("q", [2, 3, 4, 8, 21])
+def test_reg_lz_bitexact(cuda, l2, q):
+    L = 15
+    rng = np.random.default_rng(13 + q)
+    n = (L * (L - 1) // 2, q * q)
+    bi = rng.uniform(0, 0.2, size=n).astype("<f4")
+    J = rng.normal(0, 0.05, size=n).astype("<f4")
+    dJ = rng.normal(0, 0.01, size=n).astype("<f4")
+    d = dev(dJ)
+    name = "mi3_reg_l2z" if l2 else "mi3_reg_l1z"
+    _lib.call(name, dev(bi).data_ptr(), 4e-4, 1e-3, 2e-2, dev(J).data_ptr(), d.data_ptr(), L, q, stream())
+    np.testing.assert_array_equal(host(d), oracle.reg_lz(bi, 4e-4, 1e-3, 2e-2, J, dJ, q, l2))
+
+
+@pytest.mark.parametrize("n", [1, 1000, 262144, 1 << 20])
+def test_min_weights_stats(cuda, n):
+    rng = np.random.default_rng(n)
+    dE = rng.normal(0, 2, size=n).astype("<f4")
+    out = empty((1,), np.float32)
+    _lib.call("mi3_min_floats", dev(dE).data_ptr(), n, out.data_ptr(), stream())
+    assert host(out)[0] == oracle.min_floats(dE)
+    w = empty((n,), np.float32)
+    _lib.call("mi3_dE_to_weights", np.float32(-0.7), dev(dE).data_ptr(), w.data_ptr(), n, stream())
+    wo = oracle.dE_to_weights(-0.7, dE)
+    np.testing.assert_allclose(host(w), wo, rtol=3e-7)  # expf: 2 ulp
+    ws = empty((int(_lib.query("mi3_weight_stats_workspace", n)) // 8 + 1,), np.int64)
+    s2, s64 = empty((2,), np.float32), empty((2,), np.float64)
+    _lib.call("mi3_weight_stats", w.data_ptr(), n, s2.data_ptr(), s64.data_ptr(), ws.data_ptr(), ws.numel() * 8,
+              stream())
+    ref64 = oracle.weight_stats_f64(host(w))
+    np.testing.assert_allclose(host(s64), ref64, rtol=1e-12)
+    np.testing.assert_allclose(host(s2), ref64, rtol=1e-6)
+    # fused pass gives the same three results
+    w2, mn = empty((n,), np.float32), empty((1,), np.float32)
+    f2, f64 = empty((2,), np.float32), empty((2,), np.float64)
+    _lib.call("mi3_weights_fused", np.float32(-0.7), dev(dE).data_ptr(), w2.data_ptr(), n, mn.data_ptr(),
+              f2.data_ptr(), f64.data_ptr(), ws.data_ptr(), ws.numel() * 8, stream())
+    np.testing.assert_array_equal(host(w2), host(w))
+    assert host(mn)[0] == oracle.min_floats(dE)
+    np.testing.assert_array_equal(host(f64), host(s64))
+
+
+def test_fixed_beta_and_add(cuda):
+    n = 5000
+    rng = np.random.default_rng(14)
+    E = rng.normal(0, 5, size=n).astype("<f4")
+    w = empty((n,), np.float32)
+    _lib.call("mi3_fixed_beta_weights", np.float32(0.8), np.float32(-3.0), dev(E).data_ptr(), w.data_ptr(), n,
+              stream())
+    np.testing.assert_allclose(host(w), oracle.fixed_beta_weights(0.8, -3.0, E), rtol=3e-7)
+    a, b = dev(E), dev(E * 2)
+    _lib.call("mi3_add_float_bufs", a.data_ptr(), b.data_ptr(), n, stream())
+    np.testing.assert_array_equal(host(a), E + E * 2)
+
+
+@pytest.mark.parametrize("L,q", [(10, 5), (48, 4), (37, 21), (9, 2)])
+def test_gen_indep_bitexact(cuda, L, q):
+    N = 1024
+    rng = np.random.default_rng(L * q)
+    f = rng.uniform(0.1, 1, size=(L, q))
+    f /= f.sum(axis=1, keepdims=True)
+    cprob = np.cumsum(f, axis=1)
+    cprob = (cprob[:, :-1] / cprob[:, -1, None]).astype("<f4")
+    st = oracle.init_rng(N, 5, 10 ** 12)
+    mem = np.zeros((oracle.swords(L), N), np.uint32)
+    dmem, dst = dev(mem), dev(st)
+    _lib.call("mi3_gen_indep", dmem.data_ptr(), N, N, dst.data_ptr(), dev(cprob).data_ptr(), L, q, stream())
+    oracle.gen_indep(mem, st, cprob, L, q)
+    np.testing.assert_array_equal(host(dmem, np.uint32), mem)
+    np.testing.assert_array_equal(host(dst, np.uint32), st)
+
+
+@pytest.mark.parametrize("L", [5, 48, 93])
+def test_repack_T_bitexact(cuda, L):
+    N = 1024
+    seqs = _seqs(L, 21, N, L)
+    mem = oracle.pack_seqs(seqs)
+    out = empty((L, N // 4), np.uint32)
+    _lib.call("mi3_repack_seqs_T", dev(mem).data_ptr(), N, out.data_ptr(), N // 4, L, stream())
+    np.testing.assert_array_equal(host(out, np.uint32), oracle.repack_seqs_T(mem, L))
+    np.testing.assert_array_equal(host(out, np.uint32).view(np.uint8), seqs.T)

@@ -1,0 +1,198 @@
+"""The CPU oracle pinned against the reference's own code (golden vectors
+from tests/golden/make_golden.py) and against invariants of the reference's
+RNG test bench (mwc64x/test/test_mwc64xvec2.cl)."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_init_rng_matches_reference_source(golden, tag):
+    st = oracle.init_rng(64, int(golden[f"rng_{tag}_offset"]), int(golden[f"rng_{tag}_span"]))
+    np.testing.assert_array_equal(st, golden[f"rng_{tag}_states"])
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_rng_draws_match_reference_source(golden, tag):
+    st = golden[f"rng_{tag}_states"]
+    for k, g in enumerate((0, 1, 63)):
+        s = st[g].copy()
+        d = oracle.rng_stream(s, 32)
+        np.testing.assert_array_equal(d, golden[f"rng_{tag}_draws"][k])
+
+
+@pytest.mark.parametrize("dist", [0, 1, 17, 4095, 2 ** 40 + 3])
+def test_rng_skip_matches_reference_source(golden, dist):
+    import ctypes
+    s = golden["rng_skip_base"].copy()
+    lib = oracle.lib()
+    for lane in (0, 1):
+        x = ctypes.c_uint32(int(s[lane]))
+        c = ctypes.c_uint32(int(s[2 + lane]))
+        lib.mi3o_mwc_skip(ctypes.byref(x), ctypes.byref(c), dist)
+        s[lane], s[2 + lane] = x.value, c.value
+    np.testing.assert_array_equal(s, golden[f"rng_skip_{dist}"])
+
+
+def test_rng_skip_equals_stepping():
+    """Skip(d) == d calls of NextUint2 (test_mwc64xvec2.cl:1-20)."""
+    import ctypes
+    base = np.array([7, 11, 13, 17], np.uint32)
+    lib = oracle.lib()
+    for dist in (0, 1, 2, 5, 100, 1000):
+        stepped = base.copy()
+        oracle.rng_stream(stepped, dist)
+        s = base.copy()
+        for lane in (0, 1):
+            x, c = ctypes.c_uint32(int(s[lane])), ctypes.c_uint32(int(s[2 + lane]))
+            lib.mi3o_mwc_skip(ctypes.byref(x), ctypes.byref(c), dist)
+            s[lane], s[2 + lane] = x.value, c.value
+        np.testing.assert_array_equal(s, stepped)
+
+
+def test_rng_streams_partition():
+    """Walker g's stream starts where walker g-1's span ends: streams seeded
+    with span S equal one stream stepped S draws (dump_samples invariant,
+    mwc64x/test/makefile:45-64)."""
+    span = 40
+    st = oracle.init_rng(3, 0, span)
+    # lane v of walker g starts at distance (2g+v)*span: lane 0 of walker 0
+    # stepped 2*span draws reaches lane 0 of walker 1.
+    s = st[0].copy()
+    d = oracle.rng_stream(s, 2 * span)
+    assert s[0] == st[1][0] and s[2] == st[1][2]
+    assert d.shape == (2 * span, 2)
+
+
+@pytest.mark.parametrize("tag", ["A", "B", "C"])
+def test_energies_match_E_potts(golden, tag):
+    J, seqs = golden[f"m{tag}_J"], golden[f"m{tag}_seqs"]
+    N, L = seqs.shape
+    q = int(round(np.sqrt(J.shape[1])))
+    mem = oracle.pack_seqs(seqs)
+    e64 = oracle.energies_f64(J, mem, L, q)
+    np.testing.assert_allclose(e64, golden[f"m{tag}_E64"], rtol=0, atol=1e-9)
+    ek = oracle.energies_kahan(J, mem, L, q)
+    scale = np.maximum(1.0, np.abs(golden[f"m{tag}_E64"]))
+    assert np.max(np.abs(ek - golden[f"m{tag}_E64"]) / scale) < 1e-5
+
+
+@pytest.mark.parametrize("tag", ["A", "B", "C"])
+def test_bicounts_match_getMarginals(golden, tag):
+    J, seqs = golden[f"m{tag}_J"], golden[f"m{tag}_seqs"]
+    N, L = seqs.shape
+    q = int(round(np.sqrt(J.shape[1])))
+    c = oracle.bicounts(oracle.pack_seqs(seqs), L, q)
+    np.testing.assert_array_equal(c, golden[f"m{tag}_bicounts"])
+
+
+@pytest.mark.parametrize("tag", ["A", "B", "C"])
+def test_weighted_marg_matches_getMarginals(golden, tag):
+    J, seqs, w = golden[f"m{tag}_J"], golden[f"m{tag}_seqs"], golden[f"m{tag}_w"]
+    N, L = seqs.shape
+    q = int(round(np.sqrt(J.shape[1])))
+    c = oracle.weighted_marg_f64(w, oracle.pack_seqs(seqs), L, q)
+    np.testing.assert_allclose(c, golden[f"m{tag}_wcounts"], rtol=1e-12, atol=1e-12)
+
+
+def test_pack_roundtrip(golden):
+    seqs = golden["mA_seqs"]
+    mem = oracle.pack_seqs(seqs)
+    assert mem.shape == (oracle.swords(seqs.shape[1]), seqs.shape[0])
+    np.testing.assert_array_equal(oracle.unpack_seqs(mem, seqs.shape[1]), seqs)
+
+
+def test_unpack_j_layout(golden):
+    J = golden["mA_J"]
+    L, q = 10, 5
+    Ju = oracle.unpack_j(J, L, q)
+    stride = oracle.jrow_stride(L, q)
+    assert Ju.shape == (L, stride) and stride % 4 == 0
+    n = 0
+    for i in range(L - 1):
+        for j in range(i + 1, L):
+            blk = J[n].reshape(q, q)
+            np.testing.assert_array_equal(Ju[i, j * q * q:(j + 1) * q * q].reshape(q, q), blk)
+            np.testing.assert_array_equal(Ju[j, i * q * q:(i + 1) * q * q].reshape(q, q), blk.T)
+            n += 1
+    for i in range(L):
+        assert not Ju[i, i * q * q:(i + 1) * q * q].any()
+
+
+def test_accept_rule():
+    lib = oracle.lib()
+    assert lib.mi3o_accept(0.0, 0.999999) == 1
+    assert lib.mi3o_accept(-1.0, 0.5) == 0        # e^-1 = 0.37 < 0.5
+    assert lib.mi3o_accept(-1.0, 0.367879) == 1
+    assert lib.mi3o_accept(-1.0, 0.3679) == 0
+    assert lib.mi3o_accept(-200.0, 0.0) == 0      # underflows to 0, not > 0
+    assert lib.mi3o_accept(-50.0, 0.0) == 1
+
+
+def test_metropolis_single_walker_by_hand():
+    """Oracle sampler vs a direct Python restatement of DeltaEnergy +
+    accept (mcmc.cl:360-458) for a few walkers and steps."""
+    rng = np.random.default_rng(5)
+    L, q, N = 7, 3, 4
+    J = rng.normal(0, 0.7, size=(L * (L - 1) // 2, q * q)).astype("<f4")
+    seqs = rng.integers(0, q, size=(N, L)).astype("<u1")
+    st = oracle.init_rng(N, 0, 1000)
+    pos = rng.integers(0, L, size=50).astype("<u4")
+    mem = oracle.pack_seqs(seqs)
+    st_o = st.copy()
+    oracle.metropolis(J, st_o, pos, 0, 50, mem, L, q)
+    out = oracle.unpack_seqs(mem, L)
+    Ju = oracle.unpack_j(J, L, q)
+    for g in range(N):
+        s = seqs[g].copy()
+        state = st[g].copy()
+        for i in range(50):
+            p = int(pos[i])
+            r = oracle.rng_stream(state, 1)[0]
+            mut = int(r[0]) % q
+            cur = int(s[p])
+            dE = np.float32(0)
+            for m in range(L):
+                if m == p:
+                    continue
+                a = Ju[p, m * q * q + q * mut + s[m]]
+                b = Ju[p, m * q * q + q * cur + s[m]]
+                dE = np.float32(dE + np.float32(a - b))
+            u = np.float32((int(r[1]) >> 8) * 2.0 ** -24)
+            x = np.float32(-dE)
+            acc = True if x >= 0 else np.float32(np.exp(np.float64(x))) > u
+            if acc:
+                s[p] = mut
+        np.testing.assert_array_equal(out[g], s)
+        np.testing.assert_array_equal(st_o[g], state)
+
+
+def test_renormalize_and_tree_sums():
+    rng = np.random.default_rng(3)
+    bi = rng.uniform(0, 1, size=(20, 21 * 21)).astype("<f4")
+    r = oracle.renormalize_bimarg(bi, 21)
+    np.testing.assert_allclose(r.sum(axis=1), 1.0, rtol=1e-5)
+
+
+def test_zero_gauge_block_properties():
+    rng = np.random.default_rng(4)
+    for q in (2, 3, 4, 5, 21):
+        Jb = rng.normal(size=q * q).astype("<f4")
+        J0 = np.zeros_like(Jb)
+        oracle.lib().mi3o_zero_gauge_block(Jb, J0, q)
+        M = J0.reshape(q, q).astype(np.float64)
+        assert np.abs(M.sum(axis=0)).max() < 1e-5 and np.abs(M.sum(axis=1)).max() < 1e-5
+
+
+def test_min_weights_stats():
+    rng = np.random.default_rng(6)
+    x = rng.normal(0, 3, size=5000).astype("<f4")
+    assert oracle.min_floats(x) == np.float32(min(0.0, x.min()))
+    assert oracle.min_floats(np.abs(x)) == 0.0
+    w = oracle.dE_to_weights(-1.5, x)
+    arg = (-x + np.float32(-1.5)).astype(np.float64)  # the float argument of exp
+    np.testing.assert_allclose(w, np.exp(arg), rtol=2.5e-7)
+    s = oracle.weight_stats(w)
+    s64 = oracle.weight_stats_f64(w)
+    np.testing.assert_allclose(s, s64, rtol=1e-5)
