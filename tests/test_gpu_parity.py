@@ -8,7 +8,25 @@ import pytest
 
 from oracle import oracle
 from mi3gpu_b200 import _lib
-from tests._util import dev, host, empty, stream, random_model
+from tests._util import dev as _dev, host, empty, stream, random_model
+
+_alive = []
+
+
+def dev(a):
+    """Device copy kept alive until the test module ends (a temporary
+    passed as data_ptr() could be freed and reused before the launch)."""
+    t = _dev(a)
+    _alive.append(t)
+    return t
+
+
+@pytest.fixture(autouse=True)
+def _release():
+    yield
+    import torch
+    torch.cuda.synchronize()
+    _alive.clear()
 
 pytestmark = pytest.mark.gpu
 
