@@ -244,6 +244,8 @@ def run_gpu(args):
     smem_peak = 148 * 128 * sm_mhz * 1e6 / 1e9
     onchip = upd_launch * onchip_bytes_per_update / (per_launch_ms / 1e3) / 1e9
 
+    newton = run_newton(args, gpu, gpus, dev, world) if args.newton_steps > 0 else None
+
     out = None
     if rank == 0:
         out = {
@@ -266,10 +268,100 @@ def run_gpu(args):
                                 "frac": onchip / smem_peak, "bytes_per_update": onchip_bytes_per_update,
                                 "peak_basis": "148 SM x 128 B/clk x sampled SM clock"},
             "kernel_ms_per_launch": per_launch_ms,
+            "newton": newton,
             "gpu_launches": args.steps,
             "clocks": clocks,
         }
     return out, J
+
+
+def run_newton(args, gpu, gpus, dev, world):
+    """Time the Zwanzig-reweighted quasi-Newton step on the sampled walkers
+    (the body of NewtonSteps.iterNewton, NewtonSteps.py:217-246): updateJ,
+    reg l1z, energies of dJ, weights/min/stats, weighted bimarginals,
+    renormalisation, and the per-step host read of the weight sums."""
+    import torch
+    from mi3gpu_b200.potts import mutation_pc
+    L, q, N = args.L, args.q, args.walkers
+    s = gpu.stream
+    gpu.initJstep()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    # counts of the current walkers (timed separately: bimarginal-count GB/s)
+    c0, c1 = ev(), ev()
+    gpus.calcBicounts('main')
+    c0.record(s)
+    for _ in range(3):
+        gpus.calcBicounts('main')
+    c1.record(s)
+    bicount = gpus.collect('bicount')
+    count_ms = c0.elapsed_time(c1) / 3
+    f = bicount.astype(np.float64) / N
+    rng = np.random.default_rng(7)
+    f = f * np.exp(rng.normal(0, 0.2, size=f.shape))
+    f /= f.sum(axis=1, keepdims=True)
+    target = mutation_pc(f, 1 << 16).astype('<f4')
+    gpus.setBuf('bi target', target)
+    gamma, pc, lJ = 4e-4, 1e-3, 2e-4
+    gpus.calcEnergies('main')
+    gpus.calcBicounts('main')
+    gpus.bicounts_to_bimarg('main')
+    gpus.merge_bimarg()
+    gpus.fillBuf('dJ', 0)
+    ref_dE = 0.0
+    names = ["updateJ+reg", "energies", "weights", "weightedMarg", "renorm"]
+    per = {k: 0.0 for k in names}
+    nsteps = args.newton_steps
+
+    def one(instrument):
+        nonlocal ref_dE
+        evs = [ev() for _ in range(6)] if instrument else None
+        if instrument:
+            evs[0].record(s)
+        gpus.updateJ(gamma, pc)
+        gpus.reg('l1z', (gamma, pc, lJ))
+        if instrument:
+            evs[1].record(s)
+        gpus.calcEnergies('main', 'dJ')
+        if instrument:
+            evs[2].record(s)
+        gpus.weights_fused(ref_dE, 'main')
+        mfut = gpus.getBuf('minout')
+        wfut = gpus.getBuf('weightstats64')
+        if instrument:
+            evs[3].record(s)
+        gpus.weightedMarg('main')
+        if instrument:
+            evs[4].record(s)
+        gpus.merge_bimarg()
+        if instrument:
+            evs[5].record(s)
+        w = wfut[0].read()
+        ref_dE = float(mfut[0].read()[0])
+        if instrument:
+            evs[5].synchronize()
+            for k in range(5):
+                per[names[k]] += evs[k].elapsed_time(evs[k + 1])
+        return w[0] ** 2 / w[1]
+
+    for _ in range(3):
+        one(False)
+    torch.cuda.synchronize(dev)
+    t0, t1 = ev(), ev()
+    w0 = time.perf_counter()
+    t0.record(s)
+    for _ in range(nsteps):
+        neff = one(False)
+    t1.record(s)
+    torch.cuda.synchronize(dev)
+    wall = (time.perf_counter() - w0) * 1e3 / nsteps
+    dev_ms = t0.elapsed_time(t1) / nsteps
+    for _ in range(2):
+        one(True)
+    per = {k: v / 2 for k, v in per.items()}
+    return {"steps": nsteps, "ms_per_newton_step": dev_ms, "wall_ms_per_newton_step": wall,
+            "kernel_ms": per, "neff_frac_after": float(neff) / N,
+            "bicounts_ms": count_ms, "bicounts_GBps": N * L / (count_ms / 1e3) / 1e9,
+            "note": "body of iterNewton with reg l1z, fused weights pass, FP64 Neff"}
 
 
 def main():
@@ -285,6 +377,7 @@ def main():
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--newton-steps", type=int, default=10, help="quasi-Newton steps to time (0: skip)")
     args = ap.parse_args()
     rank, world, _ = env_rank()
 
