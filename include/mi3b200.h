@@ -106,6 +106,25 @@ int mi3_energies(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32
                  float *energies, uint32_t L, uint32_t q, void *workspace, size_t ws_bytes,
                  void *stream);
 
+/* Capacity of mi3_energies_noalloc, in sequences. */
+#define MI3_ENERGIES_NOALLOC_MAX_SEQ (1u << 20)
+
+/* mi3_energies without a workspace argument, for callers that cannot
+ * allocate device memory (for example code running during CUDA graph
+ * capture, hosts whose device memory belongs to a pool they do not manage,
+ * or language bindings without a device allocator).  No counterpart in the
+ * reference: it is an addition of this library.  The accumulators live in
+ * an array inside the library: 8 MiB on every GPU where the library's
+ * kernels are loaded, held until the process exits.  nseq above
+ * MI3_ENERGIES_NOALLOC_MAX_SEQ is rejected with MI3_ERR_ARG.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress)
+ * with that device current; make that first call before any stream capture.
+ * The call allocates nothing.  All calls share the one array, so calls whose
+ * executions overlap on the GPU (other streams, other threads) race and
+ * must be serialised by the caller.  Results equal mi3_energies. */
+int mi3_energies_noalloc(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
+                         float *energies, uint32_t L, uint32_t q, void *stream);
+
 /* ------------------------------------------------------------ bimarginals */
 
 /* countBivariate (mcmc.cl:462-516) as launched by MCMCGPU.calcBicounts

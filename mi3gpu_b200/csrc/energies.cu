@@ -9,6 +9,8 @@
 // absolute before the final rounding to float.  The reference sums each
 // sequence serially with Kahan compensation in float (getEnergiesf,
 // mcmc.cl:249-336); this result is at least as accurate.
+#include <mutex>
+
 #include "tiling.cuh"
 
 namespace mi3 {
@@ -118,4 +120,74 @@ extern "C" int mi3_energies(const float *J, const uint32_t *seqmem, uint32_t buf
     if (rc) return rc;
     k_energies_final<<<(nseq + 255) / 256, 256, 0, st>>>(acc, energies, nseq);
     return check_launch("mi3_energies: final");
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers cannot allocate device memory at the
+// point where they need energies: code running while a CUDA graph is being
+// captured, hosts that hand the whole GPU to a pool they do not control, or
+// foreign-language front ends that have no binding for a device allocator.
+// For them the 64-bit accumulators live in a fixed array inside this library
+// instead of a caller-provided workspace.  Capacity: MI3_ENERGIES_NOALLOC_MAX_SEQ
+// sequences (8 bytes each, 8 MiB); every GPU on which the library's kernels are
+// loaded holds the array until the process exits.
+namespace mi3 {
+
+static __device__ __align__(256) unsigned long long g_energies_noalloc_acc[MI3_ENERGIES_NOALLOC_MAX_SEQ];
+
+// Device address of the array, looked up once per device.  The name of the
+// array in host code is only a host-side handle, so it must not be passed to
+// a kernel; cudaGetSymbolAddress gives the real device address for the device
+// that is current when it runs.
+static std::mutex g_noalloc_mutex;
+static unsigned long long *g_noalloc_ptr[256] = {nullptr};
+
+static int noalloc_scratch(unsigned long long **out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 256)
+        return fail(MI3_ERR_CUDA, std::string("mi3_energies_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_energies_noalloc_acc);
+        if (e != cudaSuccess || p == nullptr)
+            return fail(MI3_ERR_CUDA,
+                        std::string("mi3_energies_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<unsigned long long *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return MI3_OK;
+}
+
+}  // namespace mi3
+
+extern "C" int mi3_energies_noalloc(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
+                                    float *energies, uint32_t L, uint32_t q, void *stream) {
+    if (!J || !seqmem || !energies) return fail(MI3_ERR_ARG, "mi3_energies_noalloc: null pointer");
+    if (L < 2 || q < 1 || q > 255 || nseq > buflen)
+        return fail(MI3_ERR_ARG, "mi3_energies_noalloc: bad L/q/nseq");
+    if (nseq > MI3_ENERGIES_NOALLOC_MAX_SEQ)
+        return fail(MI3_ERR_ARG, "mi3_energies_noalloc: nseq " + std::to_string(nseq) +
+                                     " exceeds the built-in scratch capacity of " +
+                                     std::to_string((unsigned)MI3_ENERGIES_NOALLOC_MAX_SEQ) +
+                                     " sequences; use mi3_energies with a workspace");
+    if (nseq == 0) return MI3_OK;
+    unsigned long long *acc = nullptr;
+    int rc = noalloc_scratch(&acc);
+    if (rc) return rc;
+    cudaStream_t st = as_stream(stream);
+    // the accumulators keep the previous call's sums: clear the part used
+    if (cudaMemsetAsync(acc, 0, (size_t)nseq * 8, st) != cudaSuccess)
+        return check_launch("mi3_energies_noalloc: memset");
+    switch (pick_block(q, 116 * 1024)) {
+        case 32: rc = launch_energies<32>(J, seqmem, buflen, nseq, acc, L, q, st); break;
+        case 16: rc = launch_energies<16>(J, seqmem, buflen, nseq, acc, L, q, st); break;
+        case 8: rc = launch_energies<8>(J, seqmem, buflen, nseq, acc, L, q, st); break;
+        case 4: rc = launch_energies<4>(J, seqmem, buflen, nseq, acc, L, q, st); break;
+        default: return fail(MI3_ERR_ARG, "mi3_energies_noalloc: q too large");
+    }
+    if (rc) return rc;
+    k_energies_final<<<(nseq + 255) / 256, 256, 0, st>>>(acc, energies, nseq);
+    return check_launch("mi3_energies_noalloc: final");
 }
