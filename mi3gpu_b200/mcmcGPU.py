@@ -548,6 +548,8 @@ class MCMCGPU:
         if isinstance(buf, torch.Tensor):
             s = self._begin()
             with torch.cuda.stream(self.stream):
+                if buf.device != self.device:
+                    buf = buf.to(self.device)
                 src = buf.reshape(-1).view(dev.dtype) if buf.dtype != dev.dtype else buf.reshape(-1)
                 dev[:src.numel()].copy_(src, non_blocking=True)
             evt = self.logevt('setBuf', s, src.numel() * src.element_size())

@@ -218,7 +218,7 @@ class GPU_node:
         self.wait()
         bibuf = self.gpus[0].bufs['bi']
         for g in self.gpus[1:]:
-            g.setBuf('bi', bibuf.to(g.device))
+            g.setBuf('bi', bibuf)  # device-to-device (peer) copy
         self.wait()
 
     def wait(self):

@@ -1,0 +1,127 @@
+"""A CPU stand-in for MCMCGPU used only to test the host logic (GPU_node,
+NewtonSteps) without a GPU.  Every method computes with the CPU oracle, so
+it also documents what each device call must do."""
+import numpy as np
+
+from oracle import oracle
+from mi3gpu_b200.mcmcGPU import rng_buf_mul
+
+
+class _Fut:
+    def __init__(self, v):
+        self.v = v
+
+    def read(self):
+        return self.v
+
+
+class FakeMCMCGPU:
+    def __init__(self, L, q, nseq, seed, gpunum=0):
+        self.L, self.q, self.nseq, self.nwalkers = L, q, {'main': nseq}, nseq
+        self.nPairs = L * (L - 1) // 2
+        self.gpunum = gpunum
+        self.rngstate = np.random.RandomState(seed)
+        self.device = 'cpu'
+        self.bufs = {'J': np.zeros((self.nPairs, q * q), '<f4'), 'bi': np.zeros((self.nPairs, q * q), '<f4'),
+                     'bicount': np.zeros((self.nPairs, q * q), '<u4'),
+                     'seq main': np.zeros((oracle.swords(L), nseq), '<u4'), 'E main': np.zeros(nseq, '<f4'),
+                     'minout': np.zeros(1, '<f4'), 'cprob': np.zeros((L, q - 1), '<f4')}
+        self.calls = []
+
+    def initMCMC(self, nsteps, rng_offset, rng_span):
+        self.nsteps = int(nsteps)
+        ws = int(rng_span) // (2 * self.nwalkers)
+        self.rng_offset, self.walker_span = int(rng_offset), ws
+        self.bufs['rngstates'] = oracle.init_rng(self.nwalkers, int(rng_offset), ws)
+        self.bufs['randpos'] = np.zeros(self.nsteps * rng_buf_mul, '<u4')
+        self.randpos_offset = rng_buf_mul * self.nsteps
+
+    def initJstep(self):
+        z = lambda: np.zeros((self.nPairs, self.q * self.q), '<f4')
+        self.bufs.update({'dJ': z(), 'bi target': z(), 'weights': np.zeros(self.nwalkers, '<f4'),
+                          'weightstats': np.zeros(2, '<f4'), 'weightstats64': np.zeros(2, '<f8'),
+                          'E tmp': np.zeros(self.nwalkers, '<f4')})
+
+    def updateRngPos(self):
+        self.randpos_offset += self.nsteps
+        if self.randpos_offset >= rng_buf_mul * self.nsteps:
+            self.bufs['randpos'] = self.rngstate.randint(0, self.L, size=rng_buf_mul * self.nsteps).astype('u4')
+            self.randpos_offset = 0
+        return self.randpos_offset
+
+    def runMCMC(self):
+        off = self.updateRngPos()
+        oracle.metropolis(self.bufs['J'], self.bufs['rngstates'], self.bufs['randpos'], off, self.nsteps,
+                          self.bufs['seq main'], self.L, self.q)
+        self.calls.append('runMCMC')
+
+    def calcEnergies(self, seqbufname, Jbufname='J'):
+        self.bufs['E main'] = oracle.energies_f64(self.bufs[Jbufname], self.bufs['seq main'], self.L,
+                                                  self.q).astype('<f4')
+
+    def calcBicounts(self, seqbufname):
+        self.bufs['bicount'] = oracle.bicounts(self.bufs['seq main'], self.L, self.q)
+
+    def bicounts_to_bimarg(self, seqbufname='main'):
+        self.bufs['bi'] = oracle.bicounts_to_bimarg(self.bufs['bicount'], self.nwalkers)
+
+    def updateJ(self, gamma, pc, Jbuf='dJ'):
+        self.bufs[Jbuf] = oracle.updatedJ(self.bufs['bi target'], self.bufs['bi'], gamma, pc, self.bufs[Jbuf])
+
+    def reg_l1z(self, gamma, pc, lJ):
+        self.bufs['dJ'] = oracle.reg_lz(self.bufs['bi'], gamma, pc, lJ, self.bufs['J'], self.bufs['dJ'], self.q, False)
+
+    def min_buf(self, buf):
+        self.bufs['minout'][0] = oracle.min_floats(self.bufs[buf])
+
+    def dE_to_weights(self, buf='main', offset=0.):
+        self.bufs['weights'] = oracle.dE_to_weights(offset, self.bufs['E main'])
+
+    def weight_statistics(self, buf='main'):
+        self.bufs['weightstats'] = oracle.weight_stats(self.bufs['weights'])
+        self.bufs['weightstats64'] = oracle.weight_stats_f64(self.bufs['weights'])
+
+    def weights_fused(self, offset=0., buf='main'):
+        self.min_buf('E main')
+        self.dE_to_weights(buf, offset)
+        self.weight_statistics(buf)
+
+    def weightedMarg(self, seqbufname='main'):
+        self.bufs['bi'] = oracle.weighted_marg_f64(self.bufs['weights'], self.bufs['seq main'], self.L,
+                                                   self.q).astype('<f4')
+
+    def renormalize_bimarg(self):
+        self.bufs['bi'] = oracle.renormalize_bimarg(self.bufs['bi'], self.q)
+
+    def prepare_indep(self, unimarg):
+        c = np.cumsum(unimarg, axis=1)
+        self.bufs['cprob'] = (c[:, :-1] / c[:, -1, None]).astype('<f4')
+
+    def gen_indep(self, bufname):
+        oracle.gen_indep(self.bufs['seq main'], self.bufs['rngstates'], self.bufs['cprob'], self.L, self.q)
+
+    def getBuf(self, name):
+        v = self.bufs[name]
+        if name.startswith('seq'):
+            return _Fut(oracle.unpack_seqs(v, self.L))
+        return _Fut(np.array(v, copy=True))
+
+    def setBuf(self, name, v):
+        if name.startswith('seq'):
+            v = oracle.pack_seqs(v)
+        self.bufs[name] = np.array(v, copy=True)
+
+    def fillBuf(self, name, val):
+        self.bufs[name][...] = val
+
+    def fillSeqs(self, seq):
+        self.setBuf('seq main', np.tile(np.asarray(seq, '<u1'), (self.nwalkers, 1)))
+
+    def addBiBuffer(self, name, other):
+        self.bufs[name] = self.bufs[name] + other
+
+    def logProfile(self):
+        pass
+
+    def wait(self):
+        pass

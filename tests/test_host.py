@@ -1,0 +1,147 @@
+"""Host-side logic without a GPU: sequence packing, the shared site list,
+GPU_node fan-out/merge and the NewtonSteps loop, driven over a CPU fake
+device (tests/fake_device.py)."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from mi3gpu_b200 import GPU_node, NewtonSteps, potts
+from mi3gpu_b200.mcmcGPU import MCMCGPU, histogram_heuristic, wgsize_heuristic
+from tests.fake_device import FakeMCMCGPU
+
+
+def test_pack_unpack_match_oracle():
+    rng = np.random.default_rng(0)
+    for L in (1, 3, 4, 5, 48, 93):
+        seqs = rng.integers(0, 21, size=(64, L)).astype('<u1')
+        g = MCMCGPU.__new__(MCMCGPU)
+        g.L, g.SWORDS, g.SBYTES = L, (L - 1) // 4 + 1, 4 * ((L - 1) // 4 + 1)
+        mem = g.packSeqs_4(seqs)
+        np.testing.assert_array_equal(mem, oracle.pack_seqs(seqs))
+        np.testing.assert_array_equal(g.unpackSeqs_4(mem), seqs)
+
+
+def test_heuristics_match_reference_values():
+    assert histogram_heuristic(4) == (256, 512)
+    assert histogram_heuristic(8) == (64, 512)
+    assert histogram_heuristic(21) == (8, 128)
+    assert wgsize_heuristic(21) == 512 and wgsize_heuristic(4) == 256
+
+
+def test_position_list_refill_schedule():
+    """A new block of 1024*nsteps sites is drawn on the first call and every
+    1024 calls; all devices draw the same sequence (mcmcGPU.py:447-458)."""
+    a = FakeMCMCGPU(10, 3, 512, seed=7)
+    b = FakeMCMCGPU(10, 3, 512, seed=7)
+    a.initMCMC(4, 0, 2 ** 62)
+    b.initMCMC(4, 2 ** 62, 2 ** 62)
+    offs = [a.updateRngPos() for _ in range(2050)]
+    assert offs[0] == 0 and offs[1] == 4 and offs[1023] == 4092 and offs[1024] == 0
+    for _ in range(2050):
+        b.updateRngPos()
+    np.testing.assert_array_equal(a.bufs['randpos'], b.bufs['randpos'])
+    ref = np.random.RandomState(7)
+    blocks = [ref.randint(0, 10, size=4096) for _ in range(3)]
+    np.testing.assert_array_equal(a.bufs['randpos'], blocks[2])
+
+
+def test_gpu_node_rng_spans_disjoint():
+    gpus = GPU_node([FakeMCMCGPU(6, 3, 512, seed=1, gpunum=k) for k in range(3)])
+    gpus.initMCMC(8)
+    spans = []
+    for g in gpus.gpus:
+        for w in range(g.nwalkers):
+            for v in range(2):
+                start = g.rng_offset + (2 * w + v) * g.walker_span
+                spans.append((start, start + g.walker_span))
+    spans.sort()
+    assert all(a[1] <= b[0] for a, b in zip(spans, spans[1:]))
+    assert spans[-1][1] <= 2 ** 63
+
+
+def test_merge_bimarg_multi_device_equals_pooled():
+    rng = np.random.default_rng(2)
+    L, q = 9, 4
+    seqs = rng.integers(0, q, size=(3 * 512, L)).astype('<u1')
+    gpus = GPU_node([FakeMCMCGPU(L, q, 512, seed=1, gpunum=k) for k in range(3)])
+    gpus.setSeqs('main', seqs)
+    w = rng.uniform(0.5, 1.5, size=3 * 512).astype('<f4')
+    for k, g in enumerate(gpus.gpus):
+        g.initJstep()
+        g.bufs['weights'] = w[512 * k:512 * (k + 1)]
+    gpus.weightedMarg('main')
+    gpus.merge_bimarg()
+    pooled = oracle.weighted_marg_f64(w, oracle.pack_seqs(seqs), L, q)
+    pooled /= pooled.sum(axis=1, keepdims=True)
+    for g in gpus.gpus:
+        np.testing.assert_allclose(g.bufs['bi'], pooled, rtol=2e-6)
+    gpus.calcBicounts('main')
+    np.testing.assert_array_equal(gpus.collect('bicount'), oracle.bicounts(oracle.pack_seqs(seqs), L, q))
+
+
+def _param(L, q, N, target, J, newtonSteps=20):
+    p = NewtonSteps.Param()
+    p.update(dict(bimarg=target, gamma0=4e-3, newtonSteps=newtonSteps, pcdamping=1e-2, fracNeff=0.9,
+                  nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all', L=L, q=q,
+                  couplings=J, nsteps=4 * L, equiltime=4, trackequil=0, outdir=None, mcmcsteps=2,
+                  newton_delta=8, reseed='independent', rngseed=3))
+    return p
+
+
+def test_iterNewton_over_fake_device_moves_toward_target():
+    L, q, N = 8, 3, 1024
+    rng = np.random.default_rng(4)
+    J = potts.synthetic_ground_truth(L, q, seed=5, contact_sigma=0.4)
+    g = FakeMCMCGPU(L, q, N, seed=2)
+    gpus = GPU_node([g])
+    gpus.initMCMC(4 * L)
+    gpus.initJstep()
+    gpus.setSeqs('main', rng.integers(0, q, size=(N, L)).astype('<u1'))
+    gpus.setBuf('J', J)
+    gpus.calcBicounts('main')
+    f0 = gpus.collect('bicount') / N
+    target = potts.mutation_pc(np.clip(f0 * np.exp(rng.normal(0, 0.3, f0.shape)), 1e-6, None)
+                               / np.sum(f0, axis=1, keepdims=True), N).astype('<f4')
+    target /= target.sum(axis=1, keepdims=True)
+    gpus.setBuf('bi target', target)
+    logs = []
+    p = _param(L, q, N, target, J)
+    steps, trialJ, bim = NewtonSteps.iterNewton(p, f0, gpus, logs.append)
+    assert steps >= 1
+    # predicted bimarginals are closer to the target than the start
+    assert potts.bimarg_stats(target, bim)[1] < potts.bimarg_stats(target, f0.astype('<f4'))[1]
+    np.testing.assert_allclose(trialJ, g.bufs['J'], rtol=0, atol=0)
+    # fused weights path gives the same result
+    g2 = FakeMCMCGPU(L, q, N, seed=2)
+    gpus2 = GPU_node([g2])
+    gpus2.initMCMC(4 * L)
+    gpus2.initJstep()
+    g2.bufs['seq main'] = g.bufs['seq main'].copy()
+    gpus2.setBuf('J', J)
+    gpus2.setBuf('bi target', target)
+    s2, J2, b2 = NewtonSteps.iterNewton(_param(L, q, N, target, J), f0, gpus2, lambda *a: None, fused=True)
+    assert s2 == steps
+    np.testing.assert_array_equal(J2, trialJ)
+
+
+def test_newtonMCMC_rounds_over_fake_device():
+    L, q, N = 6, 3, 512
+    J0 = np.zeros((L * (L - 1) // 2, q * q), '<f4')
+    truth = potts.synthetic_ground_truth(L, q, seed=9, contact_sigma=0.5)
+    g = FakeMCMCGPU(L, q, N, seed=4)
+    gpus = GPU_node([g])
+    gpus.initMCMC(4 * L)
+    gpus.initJstep()
+    gpus.setBuf('J', truth)
+    gpus.setSeqs('main', np.zeros((N, L), '<u1'))
+    for _ in range(30):
+        gpus.runMCMC()
+    gpus.calcBicounts('main')
+    target = potts.mutation_pc(gpus.collect('bicount') / N, N).astype('<f4')
+    p = _param(L, q, N, target, J0, newtonSteps=16)
+    p.unimarg = potts.getUnimarg(target)
+    gpus.prepare_indep(p.unimarg)
+    logs = []
+    J = NewtonSteps.newtonMCMC(p, gpus, 0, 0, logs.append)
+    assert J.shape == J0.shape and np.isfinite(J).all() and np.abs(J).max() > 0
+    assert len(p.history) == 2 and all(np.isfinite(h['ssr']) for h in p.history)
