@@ -137,11 +137,19 @@ int mi3_bicounts(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_
 int mi3_bicounts_to_bimarg(const uint32_t *bicount, float *bimarg, uint32_t nseq, uint32_t L,
                            uint32_t q, void *stream);
 
+/* Bytes of workspace mi3_weighted_marg needs. */
+size_t mi3_weighted_marg_workspace(uint32_t L, uint32_t q);
+
 /* weightedMarg (mcmc.cl:646-718), MCMCGPU.weightedMarg (mcmcGPU.py:634-661):
- * unnormalised bi[pair][q*a+b] = sum_n w_n [s_i=a][s_j=b].  Reads the seq
- * main layout directly (no transposed copy needed). */
+ * unnormalised bi[pair][q*a+b] = sum_n w_n [s_i=a][s_j=b] for weights >= 0.
+ * Reads the seq main layout directly (no transposed copy needed).  Sums are
+ * accumulated as integers in fixed point (each weight rounded to 2^-s,
+ * s >= 16 - log2(max w)), so the result is deterministic.  The workspace
+ * (>= mi3_weighted_marg_workspace(L,q) bytes, 256-byte aligned) is
+ * clobbered. */
 int mi3_weighted_marg(const float *weights, const uint32_t *seqmem, uint32_t buflen,
-                      uint32_t nseq, float *bimarg, uint32_t L, uint32_t q, void *stream);
+                      uint32_t nseq, float *bimarg, uint32_t L, uint32_t q, void *workspace,
+                      size_t ws_bytes, void *stream);
 
 /* renormalize_bimarg (mcmc.cl:753-759), MCMCGPU.renormalize_bimarg
  * (mcmcGPU.py:663-668), same summation tree as the reference. */

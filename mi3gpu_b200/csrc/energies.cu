@@ -48,25 +48,33 @@ __global__ void __launch_bounds__(512) k_energies(const float *__restrict__ J,
     const uint32_t swords = (L - 1) / 4 + 1;
     const uint32_t nbeg = chunk * g.chunk;
     const uint32_t nend = min(nseq, nbeg + g.chunk);
-    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += blockDim.x) {
-        uint32_t wI[B / 4], wJ[B / 4];
+    // two sequences per thread: two independent gather/add chains in flight
+    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += 2 * blockDim.x) {
+        const uint32_t n2 = n + blockDim.x;
+        const bool two = n2 < nend;
+        uint32_t wI[B / 4], wJ[B / 4], vI[B / 4], vJ[B / 4];
         load_block_words<B>(seq, buflen, n, bi, swords, wI);
         load_block_words<B>(seq, buflen, n, bj, swords, wJ);
-        double e = 0.0;
+        load_block_words<B>(seq, buflen, two ? n2 : n, bi, swords, vI);
+        load_block_words<B>(seq, buflen, two ? n2 : n, bj, swords, vJ);
+        double e1 = 0.0, e2 = 0.0;
 #pragma unroll
         for (int ii = 0; ii < B; ++ii) {
             uint32_t i = i0 + ii;
             if (i >= L) break;
-            uint32_t siq = block_byte<B>(wI, ii, q - 1) * q;
-            const float *row = js + (size_t)ii * B * qq + siq;
+            const float *row1 = js + (size_t)ii * B * qq + block_byte<B>(wI, ii, q - 1) * q;
+            const float *row2 = js + (size_t)ii * B * qq + block_byte<B>(vI, ii, q - 1) * q;
 #pragma unroll
             for (int jj = 0; jj < B; ++jj) {
                 uint32_t j = j0 + jj;
-                if (j < L && j > i) e += (double)row[(size_t)jj * qq + block_byte<B>(wJ, jj, q - 1)];
+                if (j < L && j > i) {
+                    e1 += (double)row1[(size_t)jj * qq + block_byte<B>(wJ, jj, q - 1)];
+                    e2 += (double)row2[(size_t)jj * qq + block_byte<B>(vJ, jj, q - 1)];
+                }
             }
         }
-        long long v = __double2ll_rn(e * FIX_SCALE);
-        atomicAdd(&acc[n], (unsigned long long)v);
+        atomicAdd(&acc[n], (unsigned long long)__double2ll_rn(e1 * FIX_SCALE));
+        if (two) atomicAdd(&acc[n2], (unsigned long long)__double2ll_rn(e2 * FIX_SCALE));
     }
 }
 

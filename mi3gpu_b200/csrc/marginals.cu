@@ -1,7 +1,7 @@
 // marginals.cu -- pair histograms of the walkers' sequences.
 //
 //   mi3_bicounts        exact uint32 counts (countBivariate, mcmc.cl:462-516)
-//   mi3_weighted_marg   float weighted sums (weightedMarg, mcmc.cl:646-718)
+//   mi3_weighted_marg   weighted sums (weightedMarg, mcmc.cl:646-718), fixed point
 //   mi3_bicounts_to_bimarg, mi3_renormalize_bimarg, mi3_repack_seqs_T
 //
 // The histogram kernels use the slice tiling of tiling.cuh: a CTA keeps the
@@ -13,37 +13,27 @@
 
 namespace mi3 {
 
-template <int B, typename T>
-__device__ __forceinline__ void hist_flush(const T *h, T *out, uint32_t L, uint32_t q,
-                                           uint32_t i0, uint32_t j0, bool accumulate) {
-    const uint32_t qq = q * q;
-    for (int ii = 0; ii < B; ++ii) {
-        uint32_t i = i0 + ii;
-        if (i + 1 >= L) break;
-        uint32_t jlo = max(j0, i + 1), jhi = min(j0 + B, L);
-        if (jlo >= jhi) continue;
-        T *dst = out + pair_index(i, jlo, L) * qq;
-        const T *src = h + ((size_t)ii * B + (jlo - j0)) * qq;
-        uint32_t cnt = (jhi - jlo) * qq;
-        for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
-            T v = src[k];
-            if (accumulate) {
-                if (v != T(0)) atomicAdd(&dst[k], v);
-            } else {
-                dst[k] = v;
-            }
-        }
-    }
+// Pair histograms over a chunk of sequences, two sequences per thread (two
+// independent atomic streams in flight).  WEIGHTED=false: +1 per sequence
+// (exact counts, flushed as u32).  WEIGHTED=true: +round(w * 2^s) per
+// sequence in u32 fixed point; s is chosen from the largest weight so a CTA's
+// bin cannot overflow, and the CTA flushes into a u64 accumulator with
+// integer atomics -- the sums are exact integers, so the result does not
+// depend on the order of the atomics (deterministic).
+__device__ __forceinline__ int fixed_shift(float wmax, uint32_t chunk) {
+    if (!(wmax > 0.0f)) return 40;
+    double lim = 4294967295.0 / ((double)chunk * (double)wmax);
+    int s = (int)floor(log2(lim));
+    return min(s, 40);
 }
 
-// WEIGHTED=false: uint32 counts.  WEIGHTED=true: float sums of weights[n].
 template <int B, bool WEIGHTED>
 __global__ void __launch_bounds__(512) k_pairhist(const uint32_t *__restrict__ seq, uint32_t buflen,
                                                   uint32_t nseq, const float *__restrict__ weights,
-                                                  void *out, uint32_t L, uint32_t q, SliceGeom g) {
-    using T = typename std::conditional<WEIGHTED, float, uint32_t>::type;
+                                                  const unsigned int *__restrict__ wmax_bits, void *out,
+                                                  uint32_t L, uint32_t q, SliceGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *h = reinterpret_cast<T *>(smem_raw);  // [B*B][q*q]
+    uint32_t *h = reinterpret_cast<uint32_t *>(smem_raw);  // [B*B][q*q]
     const uint32_t qq = q * q;
     const uint32_t s = blockIdx.x % g.nslices;
     const uint32_t chunk = blockIdx.x / g.nslices;
@@ -51,60 +41,126 @@ __global__ void __launch_bounds__(512) k_pairhist(const uint32_t *__restrict__ s
     slice_coords(s, g.nb, bi, bj);
     const uint32_t i0 = bi * B, j0 = bj * B;
     const uint32_t nh = B * B * qq;
-    for (uint32_t k = threadIdx.x; k < nh; k += blockDim.x) h[k] = T(0);
+    for (uint32_t k = threadIdx.x; k < nh; k += blockDim.x) h[k] = 0u;
+    float scale = 1.0f;
+    if constexpr (WEIGHTED) scale = ldexpf(1.0f, fixed_shift(__uint_as_float(*wmax_bits), g.chunk));
     __syncthreads();
 
     const uint32_t swords = (L - 1) / 4 + 1;
     const uint32_t nbeg = chunk * g.chunk;
     const uint32_t nend = min(nseq, nbeg + g.chunk);
-    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += blockDim.x) {
-        uint32_t wI[B / 4], wJ[B / 4];
+    const uint32_t stride = 2 * blockDim.x;
+    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += stride) {
+        const uint32_t n2 = n + blockDim.x;
+        const bool two = n2 < nend;
+        uint32_t wI[B / 4], wJ[B / 4], vI[B / 4], vJ[B / 4];
         load_block_words<B>(seq, buflen, n, bi, swords, wI);
         load_block_words<B>(seq, buflen, n, bj, swords, wJ);
-        T inc;
-        if constexpr (WEIGHTED) inc = __ldg(&weights[n]);
-        else inc = 1u;
+        load_block_words<B>(seq, buflen, two ? n2 : n, bi, swords, vI);
+        load_block_words<B>(seq, buflen, two ? n2 : n, bj, swords, vJ);
+        uint32_t inc1 = 1u, inc2 = two ? 1u : 0u;
+        if constexpr (WEIGHTED) {
+            inc1 = __float2uint_rn(__ldg(&weights[n]) * scale);
+            inc2 = two ? __float2uint_rn(__ldg(&weights[n2]) * scale) : 0u;
+        }
 #pragma unroll
         for (int ii = 0; ii < B; ++ii) {
             uint32_t i = i0 + ii;
             if (i >= L) break;
-            T *row = h + (size_t)ii * B * qq + block_byte<B>(wI, ii, q - 1) * q;
+            uint32_t *row1 = h + (size_t)ii * B * qq + block_byte<B>(wI, ii, q - 1) * q;
+            uint32_t *row2 = h + (size_t)ii * B * qq + block_byte<B>(vI, ii, q - 1) * q;
 #pragma unroll
             for (int jj = 0; jj < B; ++jj) {
                 uint32_t j = j0 + jj;
-                if (j < L && j > i) atomicAdd(&row[(size_t)jj * qq + block_byte<B>(wJ, jj, q - 1)], inc);
+                if (j < L && j > i) {
+                    atomicAdd(&row1[(size_t)jj * qq + block_byte<B>(wJ, jj, q - 1)], inc1);
+                    if (two) atomicAdd(&row2[(size_t)jj * qq + block_byte<B>(vJ, jj, q - 1)], inc2);
+                }
             }
         }
     }
     __syncthreads();
-    hist_flush<B, T>(h, reinterpret_cast<T *>(out), L, q, i0, j0, g.nchunks > 1);
+    // flush the slice's valid pairs
+    for (int ii = 0; ii < B; ++ii) {
+        uint32_t i = i0 + ii;
+        if (i + 1 >= L) break;
+        uint32_t jlo = max(j0, i + 1), jhi = min(j0 + B, L);
+        if (jlo >= jhi) continue;
+        const uint64_t dst0 = pair_index(i, jlo, L) * qq;
+        const uint32_t *src = h + ((size_t)ii * B + (jlo - j0)) * qq;
+        uint32_t cnt = (jhi - jlo) * qq;
+        for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
+            uint32_t v = src[k];
+            if constexpr (WEIGHTED) {
+                if (v) atomicAdd(reinterpret_cast<unsigned long long *>(out) + dst0 + k, (unsigned long long)v);
+            } else if (g.nchunks > 1) {
+                if (v) atomicAdd(reinterpret_cast<uint32_t *>(out) + dst0 + k, v);
+            } else {
+                reinterpret_cast<uint32_t *>(out)[dst0 + k] = v;
+            }
+        }
+    }
 }
+
+// Largest weight (weights are >= 0, so the float order is the bit order).
+__global__ void k_wmax(const float *__restrict__ w, uint32_t n, unsigned int *out) {
+    float m = 0.0f;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        m = fmaxf(m, w[k]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(out, __float_as_uint(m));
+}
+
+// Fixed-point accumulators -> float weighted bimarginals.
+__global__ void k_fixed_to_float(const unsigned long long *__restrict__ acc, const unsigned int *wmax_bits,
+                                 uint32_t chunk, float *out, uint64_t n) {
+    uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int s = fixed_shift(__uint_as_float(*wmax_bits), chunk);
+    out[k] = (float)ldexp((double)acc[k], -s);
+}
+
+constexpr uint32_t WMARG_CHUNK = 65536;  // sequences per CTA (fixed-point headroom)
 
 template <int B, bool WEIGHTED>
 static int launch_pairhist(const uint32_t *seq, uint32_t buflen, uint32_t nseq, const float *w,
-                           void *out, uint32_t L, uint32_t q, cudaStream_t st, bool split) {
-    SliceGeom g = make_geom(L, B, nseq, split ? 148 * 8 : 1, split ? 2048 : nseq);
+                           unsigned char *ws, void *out, uint32_t L, uint32_t q, cudaStream_t st) {
+    SliceGeom g = make_geom(L, B, nseq, 148 * 8, 2048);
+    if (WEIGHTED && g.chunk > WMARG_CHUNK) {
+        g.chunk = WMARG_CHUNK;
+        g.nchunks = (nseq + g.chunk - 1) / g.chunk;
+    }
     size_t smem = (size_t)B * B * q * q * 4;
-    cudaFuncSetAttribute(k_pairhist<B, WEIGHTED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    cudaFuncSetAttribute(k_pairhist<B, WEIGHTED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     uint64_t nblk = (uint64_t)g.nslices * g.nchunks;
     if (nblk > 0x7fffffffull) return fail(MI3_ERR_ARG, "pair histogram: grid too large");
-    if (g.nchunks > 1) {
-        size_t bytes = (size_t)npairs_of(L) * q * q * 4;
-        if (cudaMemsetAsync(out, 0, bytes, st) != cudaSuccess) return check_launch("pair histogram: memset");
+    const uint64_t nbins = npairs_of(L) * q * q;
+    unsigned int *wmax = nullptr;
+    void *dst = out;
+    if (WEIGHTED) {
+        wmax = reinterpret_cast<unsigned int *>(ws);
+        dst = ws + 256;
+        if (cudaMemsetAsync(ws, 0, 256 + nbins * 8, st) != cudaSuccess) return check_launch("weighted marg: memset");
+        k_wmax<<<296, 512, 0, st>>>(w, nseq, wmax);
+    } else if (g.nchunks > 1) {
+        if (cudaMemsetAsync(out, 0, nbins * 4, st) != cudaSuccess) return check_launch("bicounts: memset");
     }
-    k_pairhist<B, WEIGHTED><<<(uint32_t)nblk, 512, smem, st>>>(seq, buflen, nseq, w, out, L, q, g);
+    k_pairhist<B, WEIGHTED><<<(uint32_t)nblk, 512, smem, st>>>(seq, buflen, nseq, w, wmax, dst, L, q, g);
+    if (WEIGHTED)
+        k_fixed_to_float<<<(uint32_t)((nbins + 255) / 256), 256, 0, st>>>(
+            reinterpret_cast<const unsigned long long *>(dst), wmax, g.chunk, reinterpret_cast<float *>(out), nbins);
     return check_launch(WEIGHTED ? "mi3_weighted_marg" : "mi3_bicounts");
 }
 
 template <bool WEIGHTED>
 static int dispatch_pairhist(const uint32_t *seq, uint32_t buflen, uint32_t nseq, const float *w,
-                             void *out, uint32_t L, uint32_t q, cudaStream_t st, bool split) {
+                             unsigned char *ws, void *out, uint32_t L, uint32_t q, cudaStream_t st) {
     switch (pick_block(q, 116 * 1024)) {
-        case 32: return launch_pairhist<32, WEIGHTED>(seq, buflen, nseq, w, out, L, q, st, split);
-        case 16: return launch_pairhist<16, WEIGHTED>(seq, buflen, nseq, w, out, L, q, st, split);
-        case 8: return launch_pairhist<8, WEIGHTED>(seq, buflen, nseq, w, out, L, q, st, split);
-        case 4: return launch_pairhist<4, WEIGHTED>(seq, buflen, nseq, w, out, L, q, st, split);
+        case 32: return launch_pairhist<32, WEIGHTED>(seq, buflen, nseq, w, ws, out, L, q, st);
+        case 16: return launch_pairhist<16, WEIGHTED>(seq, buflen, nseq, w, ws, out, L, q, st);
+        case 8: return launch_pairhist<8, WEIGHTED>(seq, buflen, nseq, w, ws, out, L, q, st);
+        case 4: return launch_pairhist<4, WEIGHTED>(seq, buflen, nseq, w, ws, out, L, q, st);
         default: return fail(MI3_ERR_ARG, "pair histogram: q too large");
     }
 }
@@ -168,19 +224,28 @@ extern "C" int mi3_bicounts(const uint32_t *seqmem, uint32_t buflen, uint32_t ns
         cudaMemsetAsync(bicount, 0, (size_t)npairs_of(L) * q * q * 4, as_stream(stream));
         return check_launch("mi3_bicounts: memset");
     }
-    return dispatch_pairhist<false>(seqmem, buflen, nseq, nullptr, bicount, L, q, as_stream(stream), true);
+    return dispatch_pairhist<false>(seqmem, buflen, nseq, nullptr, nullptr, bicount, L, q, as_stream(stream));
+}
+
+extern "C" size_t mi3_weighted_marg_workspace(uint32_t L, uint32_t q) {
+    return 256 + (size_t)npairs_of(L) * q * q * 8;
 }
 
 extern "C" int mi3_weighted_marg(const float *weights, const uint32_t *seqmem, uint32_t buflen,
-                                 uint32_t nseq, float *bimarg, uint32_t L, uint32_t q, void *stream) {
-    if (!weights || !seqmem || !bimarg) return fail(MI3_ERR_ARG, "mi3_weighted_marg: null pointer");
+                                 uint32_t nseq, float *bimarg, uint32_t L, uint32_t q, void *workspace,
+                                 size_t ws_bytes, void *stream) {
+    if (!weights || !seqmem || !bimarg || !workspace) return fail(MI3_ERR_ARG, "mi3_weighted_marg: null pointer");
     if (L < 2 || q < 1 || q > 255 || nseq > buflen)
         return fail(MI3_ERR_ARG, "mi3_weighted_marg: bad L/q/nseq");
     if (nseq == 0) {
         cudaMemsetAsync(bimarg, 0, (size_t)npairs_of(L) * q * q * 4, as_stream(stream));
         return check_launch("mi3_weighted_marg: memset");
     }
-    return dispatch_pairhist<true>(seqmem, buflen, nseq, weights, bimarg, L, q, as_stream(stream), false);
+    if (ws_bytes < mi3_weighted_marg_workspace(L, q))
+        return fail(MI3_ERR_WORKSPACE, "mi3_weighted_marg: workspace too small");
+    if (!aligned(workspace, 256)) return fail(MI3_ERR_ALIGN, "mi3_weighted_marg: workspace must be 256B aligned");
+    return dispatch_pairhist<true>(seqmem, buflen, nseq, weights, reinterpret_cast<unsigned char *>(workspace),
+                                   bimarg, L, q, as_stream(stream));
 }
 
 extern "C" int mi3_bicounts_to_bimarg(const uint32_t *bicount, float *bimarg, uint32_t nseq, uint32_t L,

@@ -145,6 +145,7 @@ class MCMCGPU:
         self._setupBuffer('status', '<i4', (1,))
         self._setupWorkspace('ws energies', _lib.query('mi3_energies_workspace', nseq))
         self._setupWorkspace('ws reduce', _lib.query('mi3_weight_stats_workspace', nseq))
+        self._setupWorkspace('ws wmarg', _lib.query('mi3_weighted_marg_workspace', L, q))
         self.fillBuf('status', 0)
         self.unpackedJ = False
         self.repackedSeqT = {'main': False}
@@ -429,7 +430,7 @@ class MCMCGPU:
         nseq = self.nseq[seqbufname]
         s = self._begin()
         _lib.call('mi3_weighted_marg', self._ptr('weights'), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
-                  self._ptr('bi'), self.L, self.q, self._s)
+                  self._ptr('bi'), self.L, self.q, self._ptr('ws wmarg'), self._wsbytes('ws wmarg'), self._s)
         return self.logevt('weightedMarg', s)
 
     def renormalize_bimarg(self, wait_for=None):

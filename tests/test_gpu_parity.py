@@ -33,6 +33,10 @@ pytestmark = pytest.mark.gpu
 SHAPES = [(10, 5, 512), (48, 4, 1024), (37, 21, 512), (93, 4, 512), (64, 8, 640)]
 
 
+def _wmarg_ws(L, q):
+    return empty((int(_lib.query("mi3_weighted_marg_workspace", L, q)) // 8 + 1,), np.int64)
+
+
 def _seqs(L, q, N, seed):
     return np.random.default_rng(seed).integers(0, q, size=(N, L)).astype("<u1")
 
@@ -182,10 +186,35 @@ def test_weighted_marg(cuda, L, q, N):
     mem = oracle.pack_seqs(seqs)
     w = np.random.default_rng(11).uniform(0.01, 3.0, size=N).astype("<f4")
     out = empty((L * (L - 1) // 2, q * q), np.float32)
-    _lib.call("mi3_weighted_marg", dev(w).data_ptr(), dev(mem).data_ptr(), N, N, out.data_ptr(), L, q, stream())
+    ws = _wmarg_ws(L, q)
+    dw, dm = dev(w), dev(mem)
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, ws.data_ptr(),
+              ws.numel() * 8, stream())
     ref = oracle.weighted_marg_f64(w, mem, L, q)
     tot = ref.sum(axis=1, keepdims=True)
-    assert (np.abs(host(out) - ref) / tot).max() < 1e-5
+    got = host(out)
+    assert (np.abs(got - ref) / tot).max() < 1e-5
+    # integer (fixed-point) accumulation: a second call gives identical bits
+    out2 = empty((L * (L - 1) // 2, q * q), np.float32)
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out2.data_ptr(), L, q, ws.data_ptr(),
+              ws.numel() * 8, stream())
+    np.testing.assert_array_equal(host(out2), got)
+
+
+def test_weighted_marg_c1_shape_and_wide_weights(cuda):
+    """L=232 q=21; weights spanning 6 decades (fixed-point shift adapts to
+    the largest weight): still within 1e-5 of each pair's total."""
+    L, q, N = 232, 21, 2048
+    seqs = _seqs(L, q, N, 21)
+    mem = oracle.pack_seqs(seqs)
+    w = np.exp(np.random.default_rng(22).uniform(-14, 0, size=N)).astype("<f4")
+    out = empty((L * (L - 1) // 2, q * q), np.float32)
+    ws = _wmarg_ws(L, q)
+    dw, dm = dev(w), dev(mem)
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, ws.data_ptr(),
+              ws.numel() * 8, stream())
+    ref = oracle.weighted_marg_f64(w, mem, L, q)
+    assert (np.abs(host(out) - ref) / ref.sum(axis=1, keepdims=True)).max() < 1e-5
 
 
 def test_weighted_marg_golden(cuda, golden):
@@ -194,8 +223,9 @@ def test_weighted_marg_golden(cuda, golden):
         N, L = seqs.shape
         q = int(round(np.sqrt(J.shape[1])))
         out = empty((L * (L - 1) // 2, q * q), np.float32)
+        ws = _wmarg_ws(L, q)
         _lib.call("mi3_weighted_marg", dev(w).data_ptr(), dev(oracle.pack_seqs(seqs)).data_ptr(), N, N,
-                  out.data_ptr(), L, q, stream())
+                  out.data_ptr(), L, q, ws.data_ptr(), ws.numel() * 8, stream())
         ref = golden[f"m{tag}_wcounts"]
         assert (np.abs(host(out) - ref) / ref.sum(axis=1, keepdims=True)).max() < 1e-5
 
