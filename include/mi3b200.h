@@ -175,6 +175,32 @@ int mi3_reg_l1z(const float *bi, float gamma, float pc, float lJ, const float *J
 int mi3_reg_l2z(const float *bi, float gamma, float pc, float lJ, const float *J, float *dJ,
                 uint32_t L, uint32_t q, void *stream);
 
+/* The other regularizers, each one kernel of mcmc.cl applied per q*q pair
+ * block to dJ (in place), with J the current couplings and bi the current
+ * bimarginals; 2 <= q <= 32.  Host wrappers in mcmcGPU.py:747-843. */
+/* reg_SCADJ (mcmc.cl:904-934): SCAD penalty on the zero-gauge J+dJ. */
+int mi3_reg_scadj(const float *bi, float gamma, float pc, float lJ, float a, const float *J, float *dJ,
+                  uint32_t L, uint32_t q, void *stream);
+/* reg_X (mcmc.cl:1005-1030): penalty on X_ij = sum (J+dJ) C_ij. */
+int mi3_reg_x(const float *bi, float lX, float gamma, float pc, const float *J, float *dJ, uint32_t L,
+              uint32_t q, void *stream);
+/* reg_Xij (mcmc.cl:975-1003): as reg_X with one lambda per pair
+ * (lambdas: nPairs floats, the 'Xlambdas' buffer). */
+int mi3_reg_xij(const float *bi, const float *lambdas, float gamma, float pc, const float *J, float *dJ,
+                uint32_t L, uint32_t q, void *stream);
+/* reg_SCADX (mcmc.cl:1078-1121). */
+int mi3_reg_scadx(const float *bi, float gamma, float pc, float s, float r, float a, const float *J,
+                  float *dJ, uint32_t L, uint32_t q, void *stream);
+/* reg_expX (mcmc.cl:1123-1150). */
+int mi3_reg_expx(const float *bi, float gamma, float pc, float lam, const float *J, float *dJ, uint32_t L,
+                 uint32_t q, void *stream);
+/* reg_ddE (mcmc.cl:1152-1188). */
+int mi3_reg_dde(const float *bi, float gamma, float pc, float lambda, const float *J, float *dJ,
+                uint32_t L, uint32_t q, void *stream);
+/* reg_SCADddE (mcmc.cl:1192-1243). */
+int mi3_reg_scaddde(const float *bi, float gamma, float pc, float lambda, float r, const float *J,
+                    float *dJ, uint32_t L, uint32_t q, void *stream);
+
 /* minFloats (mcmc.cl:558-584), MCMCGPU.min_buf (mcmcGPU.py:555-567):
  * *out = min(0, min(data)) (the reference's accumulator starts at 0). */
 int mi3_min_floats(const float *data, uint32_t len, float *out, void *stream);

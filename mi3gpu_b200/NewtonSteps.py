@@ -299,7 +299,10 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
     param.min_ssr = min(ssr, param.min_ssr if param.min_ssr is not None else np.inf)
     param.history = (param.history or []) + [dict(run=runName, ssr=float(ssr), mcmc_s=dt, mc_per_s=MC_s)]
 
+    t_newton = time.time()
     Jsteps, newJ = NewtonSteps(runName, param, bimarg_model, gpus, log)
+    param.history[-1].update(newton_s=time.time() - t_newton, newton_steps=int(Jsteps),
+                             round_s=time.time() - start_time)
     param.newtonSteps = min(2048, Jsteps + ns_delta)
     log(f"Increasing newtonsteps to {param.newtonSteps}")
     return Jstep + Jsteps, seqs, sampledenergies, newJ

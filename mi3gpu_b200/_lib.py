@@ -32,6 +32,13 @@ SIGNATURES = {
     "mi3_update_j": (c.c_int, [_vp, _vp, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
     "mi3_reg_l1z": (c.c_int, [_vp, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
     "mi3_reg_l2z": (c.c_int, [_vp, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_scadj": (c.c_int, [_vp, _f32, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_x": (c.c_int, [_vp, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_xij": (c.c_int, [_vp, _vp, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_scadx": (c.c_int, [_vp, _f32, _f32, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_expx": (c.c_int, [_vp, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_dde": (c.c_int, [_vp, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
+    "mi3_reg_scaddde": (c.c_int, [_vp, _f32, _f32, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
     "mi3_min_floats": (c.c_int, [_vp, _u32, _vp, _vp]),
     "mi3_dE_to_weights": (c.c_int, [_f32, _vp, _vp, _u32, _vp]),
     "mi3_fixed_beta_weights": (c.c_int, [_f32, _f32, _vp, _vp, _u32, _vp]),

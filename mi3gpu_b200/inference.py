@@ -1,0 +1,76 @@
+"""End-to-end quasi-Newton inference on one device (the reference's
+`Mi3.py infer` loop reduced to the hot path: NewtonSteps.newtonMCMC with
+fixed-length equilibration and independent-site reseeding).
+
+    from mi3gpu_b200.inference import make_target, infer
+    target, truth = make_target(L, q, n_msa=2**16, seed=1001)
+    history = infer(target, L, q, nwalkers=2**20, rounds=5)
+
+`make_target` builds the synthetic benchmark problem: a ground-truth Potts
+model (potts.synthetic_ground_truth), an "MSA" of n_msa sequences sampled
+from it with the device sampler, and the target bimarginals = their counts
+with the Jeffreys mutation pseudocount (the reference rejects f = 0,
+Mi3.py:1032-1033).
+"""
+import time
+
+import numpy as np
+
+from . import potts
+from .mcmcGPU import MCMCGPU
+from .node_manager import GPU_node
+from . import NewtonSteps
+
+
+def sample_msa(J, L, q, n, sweeps, seed, device=0, nsteps=None):
+    """n sequences sampled from the Potts model J by `sweeps` sweeps of the
+    plain sampler from independent uniform starts."""
+    nsteps = nsteps or 8 * L
+    g = MCMCGPU((device, 0), L, q, n, 512, None, 1024, seed)
+    gpus = GPU_node([g])
+    gpus.initMCMC(nsteps)
+    gpus.prepare_indep(np.full((L, q), 1.0 / q))
+    gpus.gen_indep('main')
+    gpus.setBuf('J', J)
+    calls = max(1, (sweeps * L + nsteps - 1) // nsteps)
+    for _ in range(calls):
+        gpus.runMCMC()
+    gpus.calcBicounts('main')
+    counts = gpus.collect('bicount')
+    seqs = gpus.collect('seq main')
+    return counts, seqs
+
+
+def make_target(L, q, n_msa, seed, sweeps=None, contact_sigma=0.5, device=0):
+    truth = potts.synthetic_ground_truth(L, q, seed=seed, contact_sigma=contact_sigma)
+    sweeps = sweeps or max(256, 4 * L)
+    counts, _ = sample_msa(truth, L, q, n_msa, sweeps, seed + 1, device=device)
+    f = counts.astype(np.float64) / n_msa
+    target = potts.mutation_pc(f, n_msa, 'jeffreys').astype('<f4')
+    return target, truth
+
+
+def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e-4, damping=1e-3,
+          reg=('l1z', (2e-4,)), seed=1234, device=0, log=print, fused=True, outdir=None):
+    """Run `rounds` quasi-Newton iterations from the independent model;
+    returns the per-round history (SSR, wall seconds of MCMC and Newton
+    phases) as recorded by NewtonSteps.MCMCstep."""
+    unimarg = potts.getUnimarg(target)
+    J0 = potts.independent_couplings(unimarg)
+    nsteps = 8 * L
+    p = NewtonSteps.Param()
+    p.update(dict(bimarg=target, gamma0=gamma, newtonSteps=newtonsteps, pcdamping=damping, fracNeff=0.9,
+                  nwalkers=nwalkers, reg=reg[0] if reg else None, regarg=reg[1] if reg else None, beta=None,
+                  distribute_jstep='all', L=L, q=q, couplings=J0, nsteps=nsteps,
+                  equiltime=max(1, sweeps * L // nsteps), trackequil=0, outdir=outdir, mcmcsteps=rounds,
+                  newton_delta=32, reseed='independent', rngseed=seed + 1, unimarg=unimarg, fused=fused))
+    g = MCMCGPU((device, 0), L, q, nwalkers, 512, outdir, 1024, seed + 1)
+    gpus = GPU_node([g])
+    gpus.initMCMC(nsteps)
+    gpus.initJstep()
+    gpus.prepare_indep(unimarg)
+    t0 = time.time()
+    J = NewtonSteps.newtonMCMC(p, gpus, 0, 0, log)
+    total = time.time() - t0
+    hist = p.history or []
+    return dict(history=hist, total_s=total, J=J, expected_ssr=float(np.sum(target * (1 - target)) / nwalkers))

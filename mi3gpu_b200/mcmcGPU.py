@@ -485,29 +485,46 @@ class MCMCGPU:
         self.unpackedJ = None
         return self.logevt('reg_l2z', s)
 
-    def _reg_not_built(self, name):
-        raise NotImplementedError("regularizer {} is not built yet (only l1z and l2z)".format(name))
+    def _reg(self, entry, name, *args, lambdas=False):
+        self.require('Jstep')
+        s = self._begin()
+        head = [self._ptr('bi')] + ([self._ptr('Xlambdas')] if lambdas else [])
+        _lib.call(entry, *head, *[float(a) for a in args], self._ptr('J'), self._ptr('dJ'), self.L, self.q,
+                  self._s)
+        self.unpackedJ = None
+        return self.logevt(name, s)
 
-    def reg_SCADJ(self, *a, **k):
-        self._reg_not_built('SCADJ')
+    def reg_SCADJ(self, gamma, pc, r, a, wait_for=None):
+        """SCAD penalty on the zero-gauge couplings (mcmcGPU.py:747-759)."""
+        return self._reg('mi3_reg_scadj', 'reg_SCADJ', gamma, pc, r, a)
 
-    def reg_Xij(self, *a, **k):
-        self._reg_not_built('Xij')
+    def reg_Xij(self, gamma, pc, wait_for=None):
+        """X penalty with one lambda per pair from the 'Xlambdas' buffer, the
+        semantics of the reg_Xij kernel (mcmc.cl:975-1003; the reference's
+        host wrappers for X and Xij call each other's kernels,
+        mcmcGPU.py:761-787)."""
+        return self._reg('mi3_reg_xij', 'reg_Xij', gamma, pc, lambdas=True)
 
-    def reg_X(self, *a, **k):
-        self._reg_not_built('X')
+    def reg_X(self, gamma, pc, lX, wait_for=None):
+        """X penalty with one global lambda (reg_X kernel, mcmc.cl:1005-1030)."""
+        self.require('Jstep')
+        s = self._begin()
+        _lib.call('mi3_reg_x', self._ptr('bi'), float(lX), float(gamma), float(pc), self._ptr('J'),
+                  self._ptr('dJ'), self.L, self.q, self._s)
+        self.unpackedJ = None
+        return self.logevt('reg_X', s)
 
-    def reg_SCADX(self, *a, **k):
-        self._reg_not_built('SCADX')
+    def reg_SCADX(self, gamma, pc, s, r, a, wait_for=None):
+        return self._reg('mi3_reg_scadx', 'reg_SCADX', gamma, pc, s, r, a)
 
-    def reg_expX(self, *a, **k):
-        self._reg_not_built('expX')
+    def reg_expX(self, gamma, pc, lam, wait_for=None):
+        return self._reg('mi3_reg_expx', 'reg_expX', gamma, pc, lam)
 
-    def reg_ddE(self, *a, **k):
-        self._reg_not_built('ddE')
+    def reg_ddE(self, gamma, pc, lam, wait_for=None):
+        return self._reg('mi3_reg_dde', 'reg_ddE', gamma, pc, lam)
 
-    def reg_SCADddE(self, *a, **k):
-        self._reg_not_built('SCADddE')
+    def reg_SCADddE(self, gamma, pc, lam, r, wait_for=None):
+        return self._reg('mi3_reg_scaddde', 'reg_SCADddE', gamma, pc, lam, r)
 
     # ------------------------------------------------------------ host I/O
     def getBuf(self, bufname, truncateLarge=True, wait_for=None):
@@ -515,11 +532,12 @@ class MCMCGPU:
         (mcmcGPU.py:845-867)."""
         buftype, bufshape = self.buf_spec[bufname]
         dev = self.bufs[bufname]
-        host = torch.empty(dev.shape, dtype=dev.dtype, pin_memory=True)
+        host = self._readback_buffer(bufname, dev)
         s = self._begin()
         with torch.cuda.stream(self.stream):
             host.copy_(dev, non_blocking=True)
-        evt = torch.cuda.Event()
+        evt = getattr(self, '_ring_pending', None) or torch.cuda.Event()
+        self._ring_pending = None
         evt.record(self.stream)
         self.logevt('getBuf', s, host.numel() * host.element_size())
         L, q = self.L, self.q
@@ -584,6 +602,31 @@ class MCMCGPU:
         if bufname.split()[0] == 'seq':
             self.repackedSeqT[bufname.split()[1]] = False
         return evt
+
+    def _readback_buffer(self, bufname, dev):
+        """Pinned host buffer for a device->host read.  Small buffers (the
+        per-step scalars of the Newton loop) come from a ring of 4 per name, so
+        a loop does not pin fresh memory every step; a FutureBuf older than 4
+        reads of the same name must have been read before it is reused."""
+        nbytes = dev.numel() * dev.element_size()
+        if nbytes > (1 << 20):
+            return torch.empty(dev.shape, dtype=dev.dtype, pin_memory=True)
+        rings = getattr(self, '_rings', None)
+        if rings is None:
+            rings = self._rings = {}
+        ring = rings.get(bufname)
+        if ring is None:
+            ring = rings[bufname] = [[torch.empty(dev.shape, dtype=dev.dtype, pin_memory=True), None]
+                                     for _ in range(4)] + [0]
+        k = ring[4]
+        ring[4] = (k + 1) % 4
+        ent = ring[k]
+        if ent[1] is not None:
+            ent[1].synchronize()
+        evt = torch.cuda.Event()
+        ent[1] = evt
+        self._ring_pending = evt
+        return ent[0]
 
     def _staging_for(self, bufname, nbytes):
         """Pinned host staging buffer reused per device buffer; waits for the

@@ -422,3 +422,129 @@ void mi3o_repack_seqs_T(const uint32_t *seq4, uint32_t buf4len, uint8_t *seqL,
         for (uint32_t n = 0; n < buf4len; n++)
             seqL[(uint64_t)i*buf1len_bytes + n] = (uint8_t)getbyte(seq4[(i/4)*buf4len + n], i%4);
 }
+
+/* ---------------------------------------------------------------------------
+ * Remaining regularizers (mcmc.cl:904-1243), one q*q block per pair, with
+ * the reference's reduction trees and operation order.
+ */
+
+/* odd-aware tree over the q columns of each row of a q*q scratch block */
+static void rows_tree(float *sc, uint32_t q) {
+    uint32_t m = q, qq = q*q;
+    while (m > 1) {
+        uint32_t odd = m % 2;
+        m = (m + 1) >> 1;
+        for (uint32_t li = 0; li < qq; li++) if (li % q < m - odd) sc[li] = sc[li] + sc[li + m];
+    }
+}
+
+/* getUnimarg (mcmc.cl:936-973): row sums fi[a], column sums fj[b] */
+static void get_unimarg(const float *fij, float *fi, float *fj, uint32_t q) {
+    float sc[1024];
+    uint32_t qq = q*q;
+    for (uint32_t li = 0; li < qq; li++) sc[li] = fij[li];
+    rows_tree(sc, q);
+    for (uint32_t a = 0; a < q; a++) fi[a] = sc[q*a];
+    for (uint32_t li = 0; li < qq; li++) sc[q*(li % q) + li/q] = fij[li];
+    rows_tree(sc, q);
+    for (uint32_t b = 0; b < q; b++) fj[b] = sc[q*b];
+}
+
+/* getXijab (mcmc.cl:1051-1067) for element li */
+static float get_xijab(const float *Jt, const float *fi, const float *fj, uint32_t li, uint32_t q) {
+    uint32_t c = li / q, d = li % q;
+    float x = 0.0f;
+    for (uint32_t a = 0; a < q; a++)
+        for (uint32_t b = 0; b < q; b++)
+            x += Jt[a*q + b]*(fi[a] - (float)(a == c))*(fj[b] - (float)(b == d));
+    return x;
+}
+
+/* kind: 0 SCADJ(p0=lJ, p1=a), 1 X(p0=lX), 2 Xij(lambdas), 3 SCADX(p0=s, p1=r, p2=a),
+ *       4 expX(p0=lam), 5 ddE(p0=lambda), 6 SCADddE(p0=lambda, p1=r) */
+void mi3o_reg_other(int kind, const float *bi, const float *lambdas, float gamma, float pc,
+                    float p0, float p1, float p2, const float *J, float *dJ, uint64_t npairs,
+                    uint32_t q) {
+    uint32_t qq = q*q;
+    float Jt[1024], Jp[1024], fij[1024], C[1024], J0[1024], sc[1024], fi[32], fj[32], out[1024];
+    for (uint64_t p = 0; p < npairs; p++) {
+        for (uint32_t li = 0; li < qq; li++) {
+            Jp[li] = dJ[p*qq + li];
+            Jt[li] = J[p*qq + li] + Jp[li];
+            fij[li] = bi[p*qq + li];
+        }
+        if (kind == 0) {                                   /* reg_SCADJ :904-934 */
+            float lJ = p0, a = p1;
+            zero_gauge_block(Jt, J0, q);
+            for (uint32_t li = 0; li < qq; li++) {
+                float j0 = J0[li], R = 0.0f;
+                if (fabsf(j0) < lJ) R = fminf(lJ, fabsf(j0)/gamma);
+                else if (fabsf(j0) < a*lJ) R = (a*lJ - fabsf(j0))/(a - 1.0f);
+                R *= gamma*ocl_sign(j0)/(fij[li] + pc);
+                out[li] = Jp[li] - R;
+            }
+        } else if (kind <= 4) {                            /* X-based :975-1150 */
+            get_unimarg(fij, fi, fj, q);
+            for (uint32_t li = 0; li < qq; li++) C[li] = fij[li] - fi[li/q]*fj[li%q];
+            for (uint32_t li = 0; li < qq; li++) sc[li] = Jt[li]*C[li];
+            float X = sumqq(sc, qq);
+            float Xnorm = 0.0f;
+            if (kind != 4) {
+                for (uint32_t li = 0; li < qq; li++) sc[li] = C[li]*C[li]/(fij[li] + pc);
+                Xnorm = sumqq(sc, qq);
+            }
+            for (uint32_t li = 0; li < qq; li++) {
+                float c = C[li], f = fij[li];
+                if (kind == 1) {                           /* reg_X :1005-1030 */
+                    float lX = fminf(p0, fabsf(X)/(Xnorm*gamma));
+                    out[li] = Jp[li] - gamma*lX*c*ocl_sign(X)/(f + pc);
+                } else if (kind == 2) {                    /* reg_Xij :975-1003 */
+                    float lX = fminf(lambdas[p], fabsf(X)/(Xnorm*gamma));
+                    float R = lX*c*ocl_sign(X);
+                    out[li] = Jp[li] - gamma*R/(f + pc);
+                } else if (kind == 3) {                    /* reg_SCADX :1078-1121 */
+                    float s = p0, r = p1, a = p2;
+                    float xab = get_xijab(Jt, fi, fj, li, q);
+                    float R = 0.0f;
+                    if (fabsf(X) < r) {
+                        r = fminf(r, fabsf(X)/(Xnorm*gamma*s));
+                        R = r*ocl_sign(X);
+                    } else if (fabsf(X) < a*r) {
+                        R = (a*r*ocl_sign(X) - X)/(a - 1.0f);
+                    }
+                    R *= gamma*s*(c + f*(X - xab))/(f + pc);
+                    out[li] = Jp[li] - R;
+                } else {                                   /* reg_expX :1123-1150 */
+                    float xab = get_xijab(Jt, fi, fj, li, q);
+                    float R = ocl_sign(X)*expf(-fabsf(X)/p0)*(c + f*(X - xab));
+                    out[li] = Jp[li] - gamma*R/(f + pc);
+                }
+            }
+        } else {                                           /* ddE :1152-1243 */
+            float lambda = p0, r = p1;
+            for (uint32_t li = 0; li < qq; li++) {
+                uint32_t a = li / q, b = li % q;
+                float dR = 0.0f;
+                for (uint32_t g = 1; g < q; g++) {
+                    float jr = Jt[q*a + b] - Jt[q*((a + g) % q) + b];
+                    for (uint32_t d = 1; d < q; d++) {
+                        float jc = -Jt[q*a + (b + d) % q] + Jt[q*((a + g) % q) + (b + d) % q];
+                        float dde = jr + jc;
+                        if (kind == 5) {
+                            dR += ocl_sign(dde);
+                        } else {
+                            float R = 0.0f, absD = fabsf(dde);
+                            if (absD < r) R = 1.0f;
+                            else if (absD < 4.0f*r) R = (4.0f*r - absD)/(4.0f*r - r);
+                            dR += lambda*ocl_sign(dde)*R;
+                        }
+                    }
+                }
+                dR = dR / (float)((q - 1)*(q - 1));
+                if (kind == 5) out[li] = Jp[li] - lambda*dR*gamma/(fij[li] + pc);
+                else out[li] = Jp[li] - gamma*dR/(fij[li] + pc);
+            }
+        }
+        for (uint32_t li = 0; li < qq; li++) dJ[p*qq + li] = out[li];
+    }
+}

@@ -63,6 +63,8 @@ def lib():
             "mi3o_updatedJ": [_f32p, _f32p, _c.c_float, _c.c_float, _f32p, _f32p, _c.c_uint64],
             "mi3o_reg_lz": [_f32p, _c.c_float, _c.c_float, _c.c_float, _f32p, _f32p, _c.c_uint64,
                             _c.c_uint32, _c.c_int],
+            "mi3o_reg_other": [_c.c_int, _f32p, _c.c_void_p, _c.c_float, _c.c_float, _c.c_float, _c.c_float,
+                               _c.c_float, _f32p, _f32p, _c.c_uint64, _c.c_uint32],
             "mi3o_gen_indep": [_u32p, _c.c_uint32, _c.c_uint32, _u32p, _f32p, _c.c_uint32, _c.c_uint32],
             "mi3o_repack_seqs_T": [_u32p, _c.c_uint32, _u8p, _c.c_uint32, _c.c_uint32],
         }
@@ -269,6 +271,26 @@ def reg_lz(bi, gamma, pc, lJ, J, dJ, q, l2):
     lib().mi3o_reg_lz(np.ascontiguousarray(bi, np.float32).reshape(-1), float(gamma), float(pc), float(lJ),
                       np.ascontiguousarray(J, np.float32).reshape(-1), dJ.reshape(-1), dJ.shape[0], q,
                       1 if l2 else 0)
+    return dJ
+
+
+REG_KINDS = {"SCADJ": 0, "X": 1, "Xij": 2, "SCADX": 3, "expX": 4, "ddE": 5, "SCADddE": 6}
+
+
+def reg_other(kind, bi, gamma, pc, params, J, dJ, q, lambdas=None):
+    """reg_SCADJ / X / Xij / SCADX / expX / ddE / SCADddE (mcmc.cl:904-1243)
+    applied to a copy of dJ; params are the kernel's extra float arguments
+    in order (SCADJ: lJ, a; X: lX; SCADX: s, r, a; expX: lam; ddE: lambda;
+    SCADddE: lambda, r)."""
+    dJ = np.ascontiguousarray(dJ, np.float32).copy()
+    p = list(params) + [0.0] * (3 - len(params))
+    lp = None
+    if lambdas is not None:
+        lambdas = np.ascontiguousarray(lambdas, np.float32)
+        lp = lambdas.ctypes.data
+    lib().mi3o_reg_other(REG_KINDS[kind], np.ascontiguousarray(bi, np.float32).reshape(-1), lp, float(gamma),
+                         float(pc), float(p[0]), float(p[1]), float(p[2]),
+                         np.ascontiguousarray(J, np.float32).reshape(-1), dJ.reshape(-1), dJ.shape[0], q)
     return dJ
 
 

@@ -341,3 +341,36 @@ def test_repack_T_bitexact(cuda, L):
     _lib.call("mi3_repack_seqs_T", dev(mem).data_ptr(), N, out.data_ptr(), N // 4, L, stream())
     np.testing.assert_array_equal(host(out, np.uint32), oracle.repack_seqs_T(mem, L))
     np.testing.assert_array_equal(host(out, np.uint32).view(np.uint8), seqs.T)
+
+
+REG_CASES = [("SCADJ", "mi3_reg_scadj", (0.02, 4.0)), ("X", "mi3_reg_x", (0.05,)), ("Xij", "mi3_reg_xij", ()),
+             ("SCADX", "mi3_reg_scadx", (2.0, 0.05, 4.0)), ("expX", "mi3_reg_expx", (0.3,)),
+             ("ddE", "mi3_reg_dde", (0.01,)), ("SCADddE", "mi3_reg_scaddde", (0.01, 0.02))]
+
+
+@pytest.mark.parametrize("kind,entry,params", REG_CASES)
+@pytest.mark.parametrize("q", [2, 4, 5, 21])
+def test_reg_other_vs_oracle(cuda, kind, entry, params, q):
+    """Bit-exact for every regularizer but expX (expf: 2 ulp -> rtol 1e-6)."""
+    L = 9
+    rng = np.random.default_rng(40 + q)
+    n = (L * (L - 1) // 2, q * q)
+    bi = rng.dirichlet(np.ones(q * q), size=n[0]).astype("<f4")
+    J = rng.normal(0, 0.1, size=n).astype("<f4")
+    dJ = rng.normal(0, 0.02, size=n).astype("<f4")
+    lam = rng.uniform(0.01, 0.2, size=n[0]).astype("<f4")
+    gamma, pc = 4e-3, 1e-2
+    d = dev(dJ)
+    head = [dev(bi).data_ptr()] + ([dev(lam).data_ptr()] if kind == "Xij" else [])
+    if kind == "X":
+        args = head + [np.float32(params[0]), gamma, pc]
+    else:
+        args = head + [gamma, pc] + list(params)
+    _lib.call(entry, *args, dev(J).data_ptr(), d.data_ptr(), L, q, stream())
+    ref = oracle.reg_other(kind, bi, gamma, pc, params, J, dJ, q, lambdas=lam if kind == "Xij" else None)
+    got = host(d)
+    assert not np.array_equal(ref, dJ)  # the penalty did something
+    if kind == "expX":
+        np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-9)
+    else:
+        np.testing.assert_array_equal(got, ref)

@@ -1,0 +1,99 @@
+"""The MCMCGPU runtime (the reference's per-device class) on the GPU against
+the same calls on the CPU fake device (tests/fake_device.py, built on the
+oracle): same seeds, same position lists, same results."""
+import numpy as np
+import pytest
+
+from mi3gpu_b200 import GPU_node, MCMCGPU, NewtonSteps, potts
+from tests.fake_device import FakeMCMCGPU
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(L, q, N, seed=11):
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, seed)
+    f = FakeMCMCGPU(L, q, N, seed)
+    return GPU_node([g]), GPU_node([f]), g, f
+
+
+def test_runtime_sampling_matches_fake_device(cuda):
+    L, q, N = 30, 6, 1024
+    gpus, fakes, g, f = _pair(L, q, N)
+    rng = np.random.default_rng(1)
+    J = potts.synthetic_ground_truth(L, q, seed=3, contact_sigma=0.4)
+    seqs = rng.integers(0, q, size=(N, L)).astype('<u1')
+    for node in (gpus, fakes):
+        node.initMCMC(2 * L)
+        node.initJstep()
+        node.setSeqs('main', seqs)
+        node.setBuf('J', J)
+        for _ in range(3):
+            node.runMCMC()
+    np.testing.assert_array_equal(gpus.collect('seq main'), fakes.collect('seq main'))
+    np.testing.assert_array_equal(g.getBuf('rngstates').read().view(np.uint32).reshape(N, 4),
+                                  f.bufs['rngstates'])
+    for node in (gpus, fakes):
+        node.calcEnergies('main')
+        node.calcBicounts('main')
+    np.testing.assert_array_equal(gpus.collect('bicount'), fakes.collect('bicount'))
+    e, ef = gpus.collect('E main'), fakes.collect('E main')
+    assert (np.abs(e - ef) / np.maximum(1, np.abs(ef))).max() <= 1e-5
+    Ju = g.getBuf('Junpacked').read()
+    assert Ju.shape == (L * L, q * q)
+    from mi3gpu_b200.mcmcGPU import unpackJ_CPU
+    full = unpackJ_CPU(J)
+    off = ~np.eye(L, dtype=bool).reshape(-1)
+    np.testing.assert_array_equal(Ju[off], full[off])
+
+
+def test_runtime_gen_indep_and_newton(cuda):
+    L, q, N = 24, 4, 2048
+    gpus, fakes, g, f = _pair(L, q, N, seed=5)
+    truth = potts.synthetic_ground_truth(L, q, seed=7, contact_sigma=0.5)
+    uni = np.random.default_rng(2).dirichlet(np.ones(q), size=L)
+    for node in (gpus, fakes):
+        node.initMCMC(4 * L)
+        node.initJstep()
+        node.prepare_indep(uni)
+        node.gen_indep('main')
+    np.testing.assert_array_equal(gpus.collect('seq main'), fakes.collect('seq main'))
+    for node in (gpus, fakes):
+        node.setBuf('J', truth)
+        for _ in range(4):
+            node.runMCMC()
+    np.testing.assert_array_equal(gpus.collect('seq main'), fakes.collect('seq main'))
+    gpus.calcBicounts('main')
+    f0 = gpus.collect('bicount') / N
+    target = potts.mutation_pc(f0 * np.exp(np.random.default_rng(3).normal(0, 0.2, f0.shape)), N).astype('<f4')
+    target /= target.sum(axis=1, keepdims=True)
+    res = []
+    for node in (gpus, fakes):
+        node.setBuf('bi target', target)
+        p = NewtonSteps.Param(bimarg=target, gamma0=4e-3, newtonSteps=12, pcdamping=1e-2, fracNeff=0.5,
+                              nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all')
+        res.append(NewtonSteps.iterNewton(p, f0, node, lambda *a: None))
+    (s1, J1, b1), (s2, J2, b2) = res
+    assert s1 == s2 == 11
+    # float32 energies of dJ (device: exact sum rounded once; fake: double)
+    # feed exp(): trajectories agree to float precision
+    np.testing.assert_allclose(J1, J2, rtol=1e-4, atol=1e-6)
+    np.testing.assert_allclose(b1, b2, rtol=1e-4, atol=1e-6)
+
+
+def test_runtime_regularizers_dispatch(cuda):
+    L, q, N = 9, 4, 512
+    gpus, fakes, g, f = _pair(L, q, N)
+    gpus.initMCMC(L)
+    gpus.initJstep()
+    rng = np.random.default_rng(4)
+    n = (L * (L - 1) // 2, q * q)
+    gpus.setBuf('bi', rng.dirichlet(np.ones(q * q), size=n[0]).astype('<f4'))
+    gpus.setBuf('J', rng.normal(0, 0.1, size=n).astype('<f4'))
+    gpus.setBuf('Xlambdas', np.full(n[0], 0.05, '<f4'))
+    for name, args in [('l1z', (0.01,)), ('l2z', (0.01,)), ('SCADJ', (0.02, 4.0)), ('X', (0.05,)), ('Xij', ()),
+                       ('SCADX', (2.0, 0.05, 4.0)), ('expX', (0.3,)), ('ddE', (0.01,)), ('SCADddE', (0.01, 0.02))]:
+        gpus.setBuf('dJ', rng.normal(0, 0.02, size=n).astype('<f4'))
+        before = gpus.collect('dJ')[0] if isinstance(gpus.collect('dJ'), list) else gpus.collect('dJ')
+        gpus.reg(name, (4e-3, 1e-2) + args)
+        after = gpus.collect('dJ')
+        assert np.isfinite(after).all() and not np.array_equal(after, before), name
