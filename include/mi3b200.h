@@ -132,6 +132,14 @@ int mi3_energies_noalloc(const float *J, const uint32_t *seqmem, uint32_t buflen
 int mi3_bicounts(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t *bicount,
                  uint32_t L, uint32_t q, void *stream);
 
+/* countBivariate (mcmc.cl:462-516) on the tensor cores: the same exact
+ * uint32 counts as mi3_bicounts, computed as FP8 one-hot GEMMs X^T X with
+ * tcgen05 MMAs (FP32 accumulation, exact below 2^24 per chunk).  4 <= q <= 32.
+ * *status (int32, device, zeroed by the caller) receives
+ * MI3_STATUS_TIMEOUT_FULL if a bounded wait for the tensor cores gave up. */
+int mi3_bicounts_tc(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t *bicount,
+                    uint32_t L, uint32_t q, int32_t *status, void *stream);
+
 /* bicounts_to_bimarg (mcmc.cl:518-528), MCMCGPU.bicounts_to_bimarg
  * (mcmcGPU.py:520-534). */
 int mi3_bicounts_to_bimarg(const uint32_t *bicount, float *bimarg, uint32_t nseq, uint32_t L,

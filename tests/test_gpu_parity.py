@@ -374,3 +374,38 @@ def test_reg_other_vs_oracle(cuda, kind, entry, params, q):
         np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-9)
     else:
         np.testing.assert_array_equal(got, ref)
+
+
+@pytest.mark.parametrize("L,q,N", [(10, 5, 512), (48, 4, 16384), (37, 21, 1000), (93, 4, 3000), (64, 8, 640),
+                                   (232, 21, 4096), (50, 32, 300), (13, 7, 130)])
+def test_bicounts_tensorcore_bitexact(cuda, L, q, N):
+    """FP8 one-hot GEMM counts on tcgen05 equal the integer histogram exactly."""
+    seqs = _seqs(L, q, N, 50 + q)
+    mem = oracle.pack_seqs(seqs)
+    out = empty((L * (L - 1) // 2, q * q), np.uint32)
+    out.fill_(-1)
+    status = empty((1,), np.int32)
+    dm = dev(mem)
+    _lib.call("mi3_bicounts_tc", dm.data_ptr(), N, N, out.data_ptr(), L, q, status.data_ptr(), stream())
+    assert int(host(status)[0]) == 0
+    np.testing.assert_array_equal(host(out, np.uint32), oracle.bicounts(mem, L, q))
+
+
+def test_bicounts_tensorcore_golden_and_partial(cuda, golden):
+    for tag in "ABC":
+        J, seqs = golden[f"m{tag}_J"], golden[f"m{tag}_seqs"]
+        N, L = seqs.shape
+        q = int(round(np.sqrt(J.shape[1])))
+        out = empty((L * (L - 1) // 2, q * q), np.uint32)
+        status = empty((1,), np.int32)
+        dm = dev(oracle.pack_seqs(seqs))
+        _lib.call("mi3_bicounts_tc", dm.data_ptr(), N, N, out.data_ptr(), L, q, status.data_ptr(), stream())
+        np.testing.assert_array_equal(host(out, np.uint32), golden[f"m{tag}_bicounts"])
+    # nseq < buflen: only the first nseq sequences
+    L, q, N = 30, 6, 1024
+    mem = oracle.pack_seqs(_seqs(L, q, N, 3))
+    out = empty((L * (L - 1) // 2, q * q), np.uint32)
+    status = empty((1,), np.int32)
+    dm = dev(mem)
+    _lib.call("mi3_bicounts_tc", dm.data_ptr(), N, 777, out.data_ptr(), L, q, status.data_ptr(), stream())
+    np.testing.assert_array_equal(host(out, np.uint32), oracle.bicounts(mem, L, q, nseq=777))
