@@ -364,6 +364,72 @@ def run_newton(args, gpu, gpus, dev, world):
             "note": "body of iterNewton with reg l1z, fused weights pass, FP64 Neff"}
 
 
+def time_call(fn, reps, stream):
+    import torch
+    for _ in range(2):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_kernels(args):
+    """Per-kernel times of the pair kernels at the benchmark shapes: plain
+    shared-memory counts vs tcgen05 FP8 one-hot GEMM counts, energies and
+    weighted bimarginals; tensor figures use 2*N*nPairs*q^2 flops."""
+    import torch
+    from mi3gpu_b200 import _lib
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    fp8_peak = 2 * peaks.get("bf16_tflops", 1590.0)
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream(dev)
+    s = st.cuda_stream
+    rows = []
+    for (L, q, N) in [(232, 21, 1 << 20), (99, 4, 1 << 18), (48, 4, 16384), (512, 21, 1 << 19), (128, 8, 1 << 18)]:
+        g = torch.Generator(device=dev)
+        g.manual_seed(L * q)
+        sw = (L - 1) // 4 + 1
+        seqb = torch.randint(0, q, (sw * 4, N), device=dev, dtype=torch.uint8, generator=g)
+        if L % 4:
+            seqb[L:] = 0
+        seq = seqb.view(sw, 4, N).permute(0, 2, 1).contiguous().view(torch.int32).view(sw, N)
+        npairs = L * (L - 1) // 2
+        out = torch.empty(npairs * q * q, dtype=torch.int32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        J = torch.randn(npairs * q * q, device=dev) * 0.05
+        E = torch.empty(N, device=dev)
+        ws = torch.zeros(N + 2, dtype=torch.int64, device=dev)
+        w = torch.rand(N, device=dev) + 0.5
+        wws = torch.zeros(int(_lib.query("mi3_weighted_marg_workspace", L, q)) // 8 + 2, dtype=torch.int64, device=dev)
+        bi = torch.empty(npairs * q * q, device=dev)
+        reps = 5 if N * npairs > 1e10 else 20
+        t_plain = time_call(lambda: _lib.call("mi3_bicounts", seq.data_ptr(), N, N, out.data_ptr(), L, q, s), reps, st)
+        ref = out.clone()
+        t_tc = None
+        if 4 <= q <= 32:
+            t_tc = time_call(lambda: _lib.call("mi3_bicounts_tc", seq.data_ptr(), N, N, out.data_ptr(), L, q,
+                                               status.data_ptr(), s), reps, st)
+            assert torch.equal(out, ref) and int(status.item()) == 0, "tensor-core counts differ"
+        t_e = time_call(lambda: _lib.call("mi3_energies", J.data_ptr(), seq.data_ptr(), N, N, E.data_ptr(), L, q,
+                                          ws.data_ptr(), ws.numel() * 8, s), reps, st)
+        t_w = time_call(lambda: _lib.call("mi3_weighted_marg", w.data_ptr(), seq.data_ptr(), N, N, bi.data_ptr(), L, q,
+                                          wws.data_ptr(), wws.numel() * 8, s), reps, st)
+        flops = 2.0 * N * npairs * q * q
+        r = {"L": L, "q": q, "N": N, "counts_smem_ms": t_plain, "counts_tc_ms": t_tc, "energies_ms": t_e,
+             "weighted_ms": t_w, "counts_GBps_smem": N * L / t_plain / 1e6}
+        if t_tc:
+            r.update(counts_GBps_tc=N * L / t_tc / 1e6, tc_tflops=flops / t_tc / 1e9,
+                     tc_frac_of_fp8=flops / t_tc / 1e9 / fp8_peak)
+        rows.append(r)
+        del seqb, seq, out, J, E, ws, w, wws, bi
+    print(json.dumps({"mode": "kernels", "fp8_peak_tflops": fp8_peak,
+                      "fp8_peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (of measured)", "rows": rows}))
+
+
 def run_inference(args):
     """Quasi-Newton inference at the workload's shape: seconds per iteration
     (MCMC round of 128 sweeps + Newton steps until Neff < 0.9 N) and the SSR
@@ -399,7 +465,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--newton-steps", type=int, default=10, help="quasi-Newton steps to time (0: skip)")
-    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference"],
+    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels"],
                     help="inference: run full quasi-Newton rounds and report s/iter and SSR")
     ap.add_argument("--rounds", type=int, default=4, help="inference rounds (--mode inference)")
     ap.add_argument("--msa", type=int, default=1 << 16, help="synthetic MSA size (--mode inference)")
@@ -434,6 +500,9 @@ def main():
 
     if args.mode == "inference":
         run_inference(args)
+        return
+    if args.mode == "kernels":
+        run_kernels(args)
         return
     out, J = run_gpu(args)
     if rank == 0:

@@ -362,11 +362,22 @@ class MCMCGPU:
         return self.logevt('mcmc', s)
 
     # ------------------------------------------------------------ statistics
-    def calcBicounts(self, seqbufname, wait_for=None):
+    # alphabet sizes for which the tcgen05 one-hot GEMM counts beat the
+    # shared-memory histogram (measured on B200: 8x at q=4, 2.3x at q=8,
+    # 3x slower at q=21); both give identical integers.
+    TENSOR_COUNT_Q = range(4, 13)
+
+    def calcBicounts(self, seqbufname, wait_for=None, tensor=None):
         nseq = self.nseq[seqbufname]
+        if tensor is None:
+            tensor = self.q in self.TENSOR_COUNT_Q
         s = self._begin()
-        _lib.call('mi3_bicounts', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, self._ptr('bicount'),
-                  self.L, self.q, self._s)
+        if tensor:
+            _lib.call('mi3_bicounts_tc', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, self._ptr('bicount'),
+                      self.L, self.q, self._ptr('status'), self._s)
+        else:
+            _lib.call('mi3_bicounts', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, self._ptr('bicount'),
+                      self.L, self.q, self._s)
         return self.logevt('calcBicounts', s)
 
     def bicounts_to_bimarg(self, seqbufname='main', wait_for=None):
