@@ -238,6 +238,58 @@ int mi3_weights_fused(float ref_E, const float *dE, float *weights, uint32_t n, 
                       float *out2, double *out2_f64, void *workspace, size_t ws_bytes,
                       void *stream);
 
+/* ------------------------------------------------ learned proposal (MADE)
+ * No counterpart in the reference: a masked autoregressive network over
+ * L sites x q residues (two hidden layers of H units) trained on sampled
+ * sequences and used as an independence Metropolis-Hastings proposal.
+ * Layouts: W1T [Lq][H], b1 [H], W2 [H][H], b2 [H], W3 [Lq][H], b3 [Lq];
+ * masked entries are zero and stay zero.  Sequences in the seq layout. */
+
+/* Teacher-forced forward of sequences n0..n0+B-1: h1 = b1 + sum_i W1T[s_i],
+ * a1 = relu(h1), h2 = a1 W2^T + b2, a2 = relu(h2), logits = a2 W3^T + b3;
+ * logq (nullable) = sum_i log softmax(logits_i)[s_i]. */
+int mi3_made_forward(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+                     uint32_t q, uint32_t H, const float *W1T, const float *b1, const float *W2,
+                     const float *b2, const float *W3, const float *b3, float *h1, float *a1, float *h2,
+                     float *a2, float *logits, float *logq, void *stream);
+
+/* Gradients of the batch-mean negative log-likelihood (masked), from the
+ * forward's activations; dlogits, X (B x Lq), dh1, dh2 (B x H) are scratch;
+ * loss_per_seq (nullable) receives log q per sequence. */
+int mi3_made_backward(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+                      uint32_t q, uint32_t H, const float *W2, const float *W3, const float *h1,
+                      const float *a1, const float *h2, const float *a2, const float *logits,
+                      float *dlogits, float *X, float *dh1, float *dh2, float *gW1T, float *gb1,
+                      float *gW2, float *gb2, float *gW3, float *gb3, const float *mW1T,
+                      const float *mW2, const float *mW3, float *loss_per_seq, void *stream);
+
+/* Adam step (bias-corrected, step >= 1) on n parameters p with gradient g
+ * and moments m, v; refreshes the bf16-rounded float copy pc and the bf16
+ * copy ph (nullable); entries with mask 0 (mask nullable) stay 0. */
+int mi3_made_adam(float *p, float *pc, void *ph_bf16, const float *g, float *m, float *v,
+                  const float *mask, uint64_t n, float lr, float beta1, float beta2, float eps,
+                  uint32_t step, void *stream);
+
+/* pc = bf16-rounded p (as float), ph = the bf16 values (nullable). */
+int mi3_made_round_bf16(const float *p, float *pc, void *ph_bf16, uint64_t n, void *stream);
+
+/* Autoregressive sampling of nseq sequences into seq (given = 0), or log q
+ * of the sequences in seq (given = 1); hidden-2 units grouped by MADE degree
+ * (deg2_start [L+1], deg2_units [H]); one forward pass per sequence.
+ * q <= 32, H <= 1024.  Weights in bf16. */
+int mi3_made_sample(uint32_t L, uint32_t q, uint32_t H, const void *W1T_bf16, const float *b1,
+                    const void *W2_bf16, const float *b2, const void *W3_bf16, const float *b3,
+                    const int32_t *deg2_start, const int32_t *deg2_units, uint32_t *seq,
+                    uint32_t buflen, uint32_t nseq, float *logq, uint64_t seed, int32_t given,
+                    void *stream);
+
+/* Independence Metropolis-Hastings: walker n takes proposal n with
+ * probability min(1, exp(-(Ep-E)) exp(logq - logq_prop)); accepted walkers
+ * copy sequence, energy and log q; *naccept (uint64) += acceptances. */
+int mi3_mh_independence(uint32_t *seq, const uint32_t *prop, uint32_t buflen, uint32_t nseq,
+                        uint32_t L, float *E, const float *Ep, float *logq, const float *logq_prop,
+                        uint64_t seed, unsigned long long *naccept, void *stream);
+
 /* addFloatBufs (mcmc.cl:720-727), MCMCGPU.addFloatBuf (mcmcGPU.py:670-685). */
 int mi3_add_float_bufs(float *dst, const float *src, uint32_t n, void *stream);
 

@@ -47,6 +47,12 @@ SIGNATURES = {
     "mi3_weight_stats": (c.c_int, [_vp, _u32, _vp, _vp, _vp, c.c_size_t, _vp]),
     "mi3_weights_fused": (c.c_int, [_f32, _vp, _vp, _u32, _vp, _vp, _vp, _vp, c.c_size_t, _vp]),
     "mi3_add_float_bufs": (c.c_int, [_vp, _vp, _u32, _vp]),
+    "mi3_made_forward": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _u32, _u32] + [_vp] * 12 + [_vp]),
+    "mi3_made_backward": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _u32, _u32] + [_vp] * 21 + [_vp]),
+    "mi3_made_adam": (c.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _u64, _f32, _f32, _f32, _f32, _u32, _vp]),
+    "mi3_made_round_bf16": (c.c_int, [_vp, _vp, _vp, _u64, _vp]),
+    "mi3_made_sample": (c.c_int, [_u32, _u32, _u32] + [_vp] * 8 + [_vp, _u32, _u32, _vp, _u64, c.c_int32, _vp]),
+    "mi3_mh_independence": (c.c_int, [_vp, _vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp, _u64, _vp, _vp]),
 }
 
 
