@@ -430,6 +430,80 @@ def run_kernels(args):
                       "fp8_peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (of measured)", "rows": rows}))
 
 
+def energy_autocorr(Es):
+    """Energy autocorrelation across walkers, rho(t) = corr(E_0, E_t), and
+    tau_int = 1 + 2 sum_t rho(t) summed until rho first drops below 0.05."""
+    E = np.asarray(Es, dtype=np.float64)  # (T, N)
+    E0 = E[0] - E[0].mean()
+    rho = [float(np.mean(E0 * (e - e.mean())) / (E0.std() * e.std() + 1e-300)) for e in E]
+    tau = 1.0
+    for r in rho[1:]:
+        if r < 0.05:
+            break
+        tau += 2 * r
+    return rho, tau
+
+
+def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, epochs=16, every=4):
+    """Learned independence proposal at L=99, q=4 with strong contacts
+    (sigma 0.8): train the MADE on 2^18 equilibrated walkers, then track
+    the energy autocorrelation over `track` sampler calls of one sweep each,
+    plain vs. with one proposal step every `every` sweeps."""
+    import torch
+    from mi3gpu_b200 import MCMCGPU, GPU_node
+    from mi3gpu_b200.potts import synthetic_ground_truth
+    from mi3gpu_b200.learned import MadeProposal, LearnedSampler
+    J = synthetic_ground_truth(L, q, seed=1003, contact_sigma=0.8)
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, args.seed + 1)
+    gpus = GPU_node([g])
+    gpus.initMCMC(L)  # one sweep per sampler call
+    gpus.prepare_indep(np.full((L, q), 1.0 / q))
+    gpus.gen_indep('main')
+    gpus.setBuf('J', J)
+    t0 = time.time()
+    for _ in range(equil_sweeps):
+        g.runMCMC()
+    gpus.wait()
+    t_equil = time.time() - t0
+    made = MadeProposal(L, q, H=H, device=0, seed=3, lr=1e-3)
+    t0 = time.time()
+    hist = made.train(g.bufs['seq main'], N, epochs=epochs, batch=4096)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    start = g.bufs['seq main'].clone()
+    start_rng = g.bufs['rngstates'].clone()
+    res = {}
+    for mode in ("plain", "learned"):
+        g.bufs['seq main'].copy_(start)
+        g.bufs['rngstates'].copy_(start_rng)
+        ls = LearnedSampler(g, made, every=every, min_accept=0.005, seed=7)
+        Es, rates = [], []
+        gpus.calcEnergies('main')
+        Es.append(gpus.collect('E main').copy())
+        torch.cuda.synchronize()
+        t_run = 0.0
+        for k in range(track):
+            t1 = time.time()
+            g.runMCMC()
+            if mode == "learned" and ls.enabled and (k + 1) % every == 0:
+                rates.append(ls.propose())
+            gpus.wait()
+            t_run += time.time() - t1
+            gpus.calcEnergies('main')
+            Es.append(gpus.collect('E main').copy())
+        rho, tau = energy_autocorr(Es)
+        res[mode] = {"tau_int_sweeps": tau, "rho": [round(r, 4) for r in rho[:17]],
+                     "s_per_sweep": t_run / track, "tau_int_s": tau * t_run / track,
+                     "accept": rates, "mean_E": float(np.mean(Es[-1]))}
+    gain = res["plain"]["tau_int_sweeps"] / res["learned"]["tau_int_sweeps"]
+    print(json.dumps({"mode": "learned", "config": {"L": L, "q": q, "walkers": N, "H": H, "contact_sigma": 0.8,
+                                                    "equil_sweeps": equil_sweeps, "every": every,
+                                                    "train_epochs": epochs},
+                      "train_nll": hist, "t_equil_s": t_equil, "t_train_s": t_train, "results": res,
+                      "tau_gain_per_sweep": gain,
+                      "tau_gain_per_second": res["plain"]["tau_int_s"] / res["learned"]["tau_int_s"]}))
+
+
 def run_inference(args):
     """Quasi-Newton inference at the workload's shape: seconds per iteration
     (MCMC round of 128 sweeps + Newton steps until Neff < 0.9 N) and the SSR
@@ -465,7 +539,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--newton-steps", type=int, default=10, help="quasi-Newton steps to time (0: skip)")
-    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels"],
+    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned"],
                     help="inference: run full quasi-Newton rounds and report s/iter and SSR")
     ap.add_argument("--rounds", type=int, default=4, help="inference rounds (--mode inference)")
     ap.add_argument("--msa", type=int, default=1 << 16, help="synthetic MSA size (--mode inference)")
@@ -503,6 +577,9 @@ def main():
         return
     if args.mode == "kernels":
         run_kernels(args)
+        return
+    if args.mode == "learned":
+        run_learned(args)
         return
     out, J = run_gpu(args)
     if rank == 0:

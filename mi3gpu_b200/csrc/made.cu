@@ -202,7 +202,8 @@ __device__ __forceinline__ float hash_uniform(uint64_t seed, uint64_t n, uint64_
     return (float)(z >> 40) * 0x1.0p-24f;
 }
 
-constexpr int SAMP_S = 32;  // sequences per CTA
+constexpr int SAMP_S = 32;  // sequences per CTA (one per lane)
+constexpr int NWARP = 8;    // warps per CTA (256 threads)
 
 // Autoregressive sampling in MADE degree order.  Hidden-1 unit k with degree
 // m1 depends on sites < m1, hidden-2 unit k' with degree m2 on hidden-1 units
@@ -221,50 +222,91 @@ __global__ void __launch_bounds__(256) k_made_sample(int L, int q, int H, const 
                                                      uint32_t buflen, uint32_t nseq, float *logq, uint64_t seed,
                                                      int given) {
     extern __shared__ float sm[];
-    float *h1 = sm;                      // [S][H] hidden-1 pre-activations
-    float *h2 = h1 + SAMP_S * H;         // [S][H] hidden-2 activations (0 until evaluated)
-    float *lg = h2 + SAMP_S * H;         // [S][32] logits of the current site
-    uint32_t *res = reinterpret_cast<uint32_t *>(lg + SAMP_S * 32);  // [S] residue just chosen
+    // rows padded to H+1 floats: lane s of a warp reads row s, and a stride
+    // of H+1 puts the 32 lanes in 32 different banks
+    const int HP = H + 1;
+    float *h1 = sm;                      // [S][H+1] hidden-1 pre-activations
+    float *h2 = h1 + SAMP_S * HP;        // [S][H+1] hidden-2 activations (0 until evaluated)
+    float *lg = h2 + SAMP_S * HP;        // [S][33] logits of the current site
+    uint32_t *res = reinterpret_cast<uint32_t *>(lg + SAMP_S * 33);  // [S] residue just chosen
     float *lq = reinterpret_cast<float *>(res + SAMP_S);             // [S] log q accumulator
+    float *red = lq + SAMP_S;                                        // [8 warps][4][S] partial sums
     const int tid = threadIdx.x, nthr = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int KC = (H + NWARP - 1) / NWARP;
     const uint32_t nbase = blockIdx.x * SAMP_S;
 
     for (int e = tid; e < SAMP_S * H; e += nthr) {
-        h1[e] = b1[e % H];
-        h2[e] = 0.0f;
+        const int s = e / H, k = e % H;
+        h1[s * HP + k] = b1[k];
+        h2[s * HP + k] = 0.0f;
     }
     if (tid < SAMP_S) lq[tid] = 0.0f;
     __syncthreads();
 
     for (int i = 0; i < L; ++i) {
-        // (a) hidden-2 units of degree i (all their hidden-1 inputs are final)
+        // (a) hidden-2 units of degree i (all their hidden-1 inputs are final).
+        // Warp w sums inputs k in [w*KC, (w+1)*KC) for sequence s = lane, four
+        // units at a time; the 8 partial sums are then added in warp order.
         const int u0 = deg2_start[i], u1 = deg2_start[i + 1];
-        const int nu = u1 - u0;
-        for (int e = tid; e < nu * SAMP_S; e += nthr) {
-            const int u = deg2_units[u0 + e / SAMP_S];
-            const int s = e % SAMP_S;
-            const __nv_bfloat16 *w = W2 + (size_t)u * H;
-            const float *x = h1 + s * H;
-            float acc = b2[u];
-            for (int k = 0; k < H; ++k) acc = fmaf(__bfloat162float(w[k]), fmaxf(x[k], 0.0f), acc);
-            h2[s * H + u] = fmaxf(acc, 0.0f);
+        for (int ug = u0; ug < u1; ug += 4) {
+            const int nu = min(4, u1 - ug);
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            const float *x = h1 + lane * HP;
+            const int kb = warp * KC, ke = min(H, kb + KC);
+            int uu[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) uu[j] = deg2_units[ug + min(j, nu - 1)];
+            for (int k = kb; k < ke; ++k) {
+                const float xv = fmaxf(x[k], 0.0f);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[j] = fmaf(__bfloat162float(W2[(size_t)uu[j] * H + k]), xv, acc[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) red[(warp * 4 + j) * SAMP_S + lane] = acc[j];
+            __syncthreads();
+            if (tid < 4 * SAMP_S) {
+                const int j = tid / SAMP_S, sq = tid % SAMP_S;
+                if (j < nu) {
+                    float v = b2[uu[j]];
+                    for (int w = 0; w < NWARP; ++w) v += red[(w * 4 + j) * SAMP_S + sq];
+                    h2[sq * HP + uu[j]] = fmaxf(v, 0.0f);
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        // (b) logits of site i
-        for (int e = tid; e < q * SAMP_S; e += nthr) {
-            const int a = e / SAMP_S, s = e % SAMP_S;
-            const __nv_bfloat16 *w = W3 + (size_t)(i * q + a) * H;
-            const float *x = h2 + s * H;
-            float acc = b3[i * q + a];
-            for (int k = 0; k < H; ++k) acc = fmaf(__bfloat162float(w[k]), x[k], acc);
-            lg[s * 32 + a] = acc;
+        // (b) logits of site i, four residues at a time, same split
+        for (int ag = 0; ag < q; ag += 4) {
+            const int na = min(4, q - ag);
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            const float *x = h2 + lane * HP;
+            const int kb = warp * KC, ke = min(H, kb + KC);
+            for (int k = kb; k < ke; ++k) {
+                const float xv = x[k];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int a = ag + min(j, na - 1);
+                    acc[j] = fmaf(__bfloat162float(W3[(size_t)(i * q + a) * H + k]), xv, acc[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) red[(warp * 4 + j) * SAMP_S + lane] = acc[j];
+            __syncthreads();
+            if (tid < 4 * SAMP_S) {
+                const int j = tid / SAMP_S, sq = tid % SAMP_S;
+                if (j < na) {
+                    float v = b3[i * q + ag + j];
+                    for (int w = 0; w < NWARP; ++w) v += red[(w * 4 + j) * SAMP_S + sq];
+                    lg[sq * 33 + ag + j] = v;
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
         // (c) draw (or read) residue i, accumulate log q
         if (tid < SAMP_S) {
             const int s = tid;
             const uint32_t n = nbase + s;
-            const float *o = lg + s * 32;
+            const float *o = lg + s * 33;
             float mx = o[0];
             for (int a = 1; a < q; ++a) mx = fmaxf(mx, o[a]);
             float se = 0.0f;
@@ -298,7 +340,7 @@ __global__ void __launch_bounds__(256) k_made_sample(int L, int q, int H, const 
         // (d) add the chosen residue's column to every hidden-1 unit
         for (int e = tid; e < SAMP_S * H; e += nthr) {
             const int s = e / H, k = e % H;
-            h1[e] += __bfloat162float(W1T[(size_t)(i * q + res[s]) * H + k]);
+            h1[s * HP + k] += __bfloat162float(W1T[(size_t)(i * q + res[s]) * H + k]);
         }
         __syncthreads();
     }
@@ -421,7 +463,7 @@ extern "C" int mi3_made_sample(uint32_t L, uint32_t q, uint32_t H, const void *W
     if (L < 2 || q < 2 || q > 32 || H == 0 || H > 1024 || nseq > buflen)
         return fail(MI3_ERR_ARG, "mi3_made_sample: bad sizes (q <= 32, H <= 1024)");
     if (nseq == 0) return MI3_OK;
-    size_t smem = (size_t)(2 * SAMP_S * H + SAMP_S * 32 + 2 * SAMP_S) * 4;
+    size_t smem = (size_t)(2 * SAMP_S * (H + 1) + SAMP_S * 33 + 2 * SAMP_S + NWARP * 4 * SAMP_S) * 4;
     if (smem > 227 * 1024) return fail(MI3_ERR_ARG, "mi3_made_sample: H too large");
     cudaFuncSetAttribute(k_made_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_made_sample<<<(nseq + SAMP_S - 1) / SAMP_S, 256, smem, as_stream(stream)>>>(

@@ -179,3 +179,43 @@ def test_independence_mh_leaves_boltzmann_invariant(cuda):
     rates = ls.sweeps(60)
     assert min(rates) > 0.02
     assert _zscores(gpus.collect('seq main'), p, L, q).max() < 5.0
+
+
+def test_trained_proposal_decorrelates_faster_per_sweep(cuda):
+    """What the trained network gains: on a strongly coupled model the energy
+    autocorrelation after the same number of sweeps is lower when proposal
+    steps (network trained on the equilibrated walkers) are interleaved."""
+    L, q, N, H = 40, 4, 1 << 15, 128
+    J = potts.synthetic_ground_truth(L, q, seed=12, contact_sigma=0.9)
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 6)
+    gpus = GPU_node([g])
+    gpus.initMCMC(L)
+    gpus.prepare_indep(np.full((L, q), 1.0 / q))
+    gpus.gen_indep('main')
+    gpus.setBuf('J', J)
+    for _ in range(400):
+        g.runMCMC()
+    made = MadeProposal(L, q, H=H, device=0, seed=3, lr=3e-3)
+    hist = made.train(g.bufs['seq main'], N, epochs=20, batch=2048)
+    assert hist[-1] < hist[0]
+    start, start_rng = g.bufs['seq main'].clone(), g.bufs['rngstates'].clone()
+
+    def rho_after(with_proposals, sweeps=16):
+        g.bufs['seq main'].copy_(start)
+        g.bufs['rngstates'].copy_(start_rng)
+        gpus.calcEnergies('main')
+        E0 = gpus.collect('E main').astype(np.float64).copy()
+        ls = LearnedSampler(g, made, every=2, min_accept=0.0, seed=9)
+        rates = []
+        for k in range(sweeps):
+            g.runMCMC()
+            if with_proposals and (k + 1) % 2 == 0:
+                rates.append(ls.propose())
+        gpus.calcEnergies('main')
+        E1 = gpus.collect('E main').astype(np.float64)
+        return np.corrcoef(E0, E1)[0, 1], rates
+
+    rho_plain, _ = rho_after(False)
+    rho_learned, rates = rho_after(True)
+    assert np.mean(rates) > 0.05
+    assert rho_learned < rho_plain - 0.05, (rho_plain, rho_learned, np.mean(rates))
