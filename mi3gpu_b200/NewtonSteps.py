@@ -332,7 +332,13 @@ def newtonMCMC(param, gpus, start_run, Jstep, log):
             seed = seqs[np.argmin(es)]
         if seed is not None:
             gpus.fillSeqs(seed)
-        elif param.reseed == 'independent':
+        elif param.reseed == 'independent' or (param.reseed == 'none' and i == start_run and param.init_indep):
+            # 'none' keeps the walkers from round to round; they start from
+            # independent-site sequences when init_indep is set
             gpus.gen_indep('main')
+        equil = param.equiltime
+        if i == start_run and param.equiltime_first is not None:
+            param.equiltime = param.equiltime_first
         Jstep, seqs, es, J = MCMCstep(runname, Jstep, J, param, gpus, log)
+        param.equiltime = equil
     return J

@@ -51,10 +51,17 @@ def make_target(L, q, n_msa, seed, sweeps=None, contact_sigma=0.5, device=0):
 
 
 def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e-4, damping=1e-3,
-          reg=('l1z', (2e-4,)), seed=1234, device=0, log=print, fused=True, outdir=None):
+          reg=('l1z', (2e-4,)), seed=1234, device=0, log=print, fused=True, outdir=None, reseed='independent',
+          sweeps_first=None):
     """Run `rounds` quasi-Newton iterations from the independent model;
     returns the per-round history (SSR, wall seconds of MCMC and Newton
-    phases) as recorded by NewtonSteps.MCMCstep."""
+    phases) as recorded by NewtonSteps.MCMCstep.
+
+    reseed='independent' restarts every walker from independent-site
+    sequences each round (`sweeps` sweeps of equilibration); reseed='none'
+    keeps the walkers from the previous round, so after a first round of
+    `sweeps_first` sweeps each round only re-equilibrates to the slightly
+    changed couplings."""
     unimarg = potts.getUnimarg(target)
     J0 = potts.independent_couplings(unimarg)
     nsteps = 8 * L
@@ -63,7 +70,8 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
                   nwalkers=nwalkers, reg=reg[0] if reg else None, regarg=reg[1] if reg else None, beta=None,
                   distribute_jstep='all', L=L, q=q, couplings=J0, nsteps=nsteps,
                   equiltime=max(1, sweeps * L // nsteps), trackequil=0, outdir=outdir, mcmcsteps=rounds,
-                  newton_delta=32, reseed='independent', rngseed=seed + 1, unimarg=unimarg, fused=fused))
+                  newton_delta=32, reseed=reseed, rngseed=seed + 1, unimarg=unimarg, fused=fused, init_indep=True,
+                  equiltime_first=None if sweeps_first is None else max(1, sweeps_first * L // nsteps)))
     g = MCMCGPU((device, 0), L, q, nwalkers, 512, outdir, 1024, seed + 1)
     gpus = GPU_node([g])
     gpus.initMCMC(nsteps)
