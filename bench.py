@@ -302,6 +302,7 @@ def run_newton(args, gpu, gpus, dev, world):
     target = mutation_pc(f, 1 << 16).astype('<f4')
     gpus.setBuf('bi target', target)
     gamma, pc, lJ = 4e-4, 1e-3, 2e-4
+    gpus.updateConsensus('main')  # as iterNewton does: the walkers are fixed during the steps
     gpus.calcEnergies('main')
     gpus.calcBicounts('main')
     gpus.bicounts_to_bimarg('main')
@@ -404,7 +405,7 @@ def run_kernels(args):
         E = torch.empty(N, device=dev)
         ws = torch.zeros(N + 2, dtype=torch.int64, device=dev)
         w = torch.rand(N, device=dev) + 0.5
-        wws = torch.zeros(int(_lib.query("mi3_weighted_marg_workspace", L, q)) // 8 + 2, dtype=torch.int64, device=dev)
+        wws = torch.zeros(int(_lib.query("mi3_weighted_marg_workspace", L, q, N)) // 8 + 2, dtype=torch.int64, device=dev)
         bi = torch.empty(npairs * q * q, device=dev)
         reps = 5 if N * npairs > 1e10 else 20
         t_plain = time_call(lambda: _lib.call("mi3_bicounts", seq.data_ptr(), N, N, out.data_ptr(), L, q, s), reps, st)
@@ -416,7 +417,7 @@ def run_kernels(args):
             assert torch.equal(out, ref) and int(status.item()) == 0, "tensor-core counts differ"
         t_e = time_call(lambda: _lib.call("mi3_energies", J.data_ptr(), seq.data_ptr(), N, N, E.data_ptr(), L, q,
                                           ws.data_ptr(), ws.numel() * 8, s), reps, st)
-        t_w = time_call(lambda: _lib.call("mi3_weighted_marg", w.data_ptr(), seq.data_ptr(), N, N, bi.data_ptr(), L, q,
+        t_w = time_call(lambda: _lib.call("mi3_weighted_marg", w.data_ptr(), seq.data_ptr(), N, N, bi.data_ptr(), L, q, None,
                                           wws.data_ptr(), wws.numel() * 8, s), reps, st)
         flops = 2.0 * N * npairs * q * q
         r = {"L": L, "q": q, "N": N, "counts_smem_ms": t_plain, "counts_tc_ms": t_tc, "energies_ms": t_e,
@@ -505,41 +506,58 @@ def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, 
 
 
 def run_inference(args):
-    """Quasi-Newton inference at the workload's shape, plain vs chosen, on
-    the same synthetic target: seconds per iteration (MCMC round + Newton
-    steps until Neff < 0.9 N) and the SSR of the sampled bimarginals after
-    each round.  plain: every round restarts the walkers from independent
-    sequences and runs 128 sweeps (the reference's recipe with a fixed
-    equilibration); chosen: walkers carried over between rounds
-    (reseed 'none'), 128 sweeps in the first round and args.chosen_sweeps
-    after that."""
+    """Quasi-Newton inference at the workload's shape on one synthetic
+    target: seconds per iteration (MCMC round + Newton steps until
+    Neff < 0.9 N) and the SSR of the sampled bimarginals after each round,
+    for these forms:
+      plain      every round restarts the walkers from independent sequences
+                 and runs 128 sweeps; round host work (gauge transform,
+                 statistics, J and sequence read-backs) in numpy as in the
+                 reference's NewtonSteps.py
+      plain_dev  the same sampling, with J resident on the device and the
+                 round's host work done there in FP64
+      chosen     J resident; walkers carried over between rounds (reseed
+                 'none'): 128 sweeps in the first round, args.chosen_sweeps
+                 after it
+      chosen_half  as chosen with half as many sweeps per round."""
     from mi3gpu_b200.inference import make_target, infer
     t0 = time.time()
     target, truth = make_target(args.L, args.q, args.msa, seed=1001)
     t_target = time.time() - t0
+    forms = (("plain", dict(reseed="independent", sweeps=128, device_resident=False)),
+             ("plain_dev", dict(reseed="independent", sweeps=128, device_resident=True)),
+             ("chosen", dict(reseed="none", sweeps=args.chosen_sweeps, sweeps_first=128, device_resident=True)),
+             ("chosen_half", dict(reseed="none", sweeps=max(1, args.chosen_sweeps // 2), sweeps_first=128,
+                                  device_resident=True)))
     out = {}
-    for name, kw in (("plain", dict(reseed="independent", sweeps=128)),
-                     ("chosen", dict(reseed="none", sweeps=args.chosen_sweeps, sweeps_first=128))):
+    for name, kw in forms:
         logs = []
+        w0 = time.time()
         res = infer(target, args.L, args.q, args.walkers, args.rounds, log=logs.append, **kw)
+        wall = time.time() - w0
         hist = res["history"]
         cum = np.cumsum([h["round_s"] for h in hist]).tolist()
-        out[name] = {"history": hist, "cum_s": cum, "s_per_iter": statistics.mean(h["round_s"] for h in hist),
-                     "s_per_iter_after_first": statistics.mean(h["round_s"] for h in hist[1:]) if len(hist) > 1
-                     else None, "final_ssr": hist[-1]["ssr"], "config": kw}
-    # wall seconds for the chosen form to reach the plain form's final SSR
-    tgt = out["plain"]["final_ssr"]
-    reach = next((c for h, c in zip(out["chosen"]["history"], out["chosen"]["cum_s"]) if h["ssr"] <= tgt), None)
+        after = [h["round_s"] for h in hist[1:]] or [hist[0]["round_s"]]
+        out[name] = {"ssr": [round(h["ssr"], 5) for h in hist], "round_s": [round(h["round_s"], 3) for h in hist],
+                     "mcmc_s": [round(h["mcmc_s"], 3) for h in hist],
+                     "newton_s": [round(h["newton_s"], 3) for h in hist],
+                     "newton_steps": [h["newton_steps"] for h in hist], "cum_s": cum,
+                     "s_per_iter": statistics.mean(after), "wall_s_all_rounds": wall,
+                     "final_ssr": hist[-1]["ssr"], "config": kw}
+    chosen = out["chosen"]
+    reach = {}
+    for base in ("plain", "plain_dev"):
+        tgt = out[base]["final_ssr"]
+        reach[base] = next((c for sv, c in zip(chosen["ssr"], chosen["cum_s"]) if sv <= tgt * (1 + 1e-3)), None)
     print(json.dumps({
         "metric": "s/iter (quasi-Newton round) and SSR, chosen vs plain", "unit": "s/iter",
-        "value": out["chosen"]["s_per_iter_after_first"] or out["chosen"]["s_per_iter"],
-        "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+        "value": chosen["s_per_iter"], "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
+        "data": "synthetic",
         "config": {"workload": f"inference L={args.L} q={args.q} walkers={args.walkers} msa={args.msa}, l1z 2e-4",
-                   "rounds": args.rounds},
-        "plain": out["plain"], "chosen": out["chosen"],
-        "s_per_iter_ratio_plain_over_chosen": out["plain"]["s_per_iter"] / (out["chosen"]["s_per_iter_after_first"]
-                                                                           or out["chosen"]["s_per_iter"]),
-        "chosen_s_to_plain_final_ssr": reach, "plain_s_total": out["plain"]["cum_s"][-1],
+                   "rounds": args.rounds, "s_per_iter": "mean round seconds after the first round"},
+        "forms": out,
+        "s_per_iter_ratio": {b: out[b]["s_per_iter"] / chosen["s_per_iter"] for b in ("plain", "plain_dev")},
+        "chosen_s_to_reach_final_ssr_of": reach,
         "expected_min_ssr": float(np.sum(target * (1 - target)) / args.walkers), "target_build_s": t_target}))
 
 

@@ -98,8 +98,9 @@ size_t mi3_energies_workspace(uint32_t nseq);
 
 /* getEnergies (mcmc.cl:249-345) as launched by MCMCGPU.calcEnergies
  * (mcmcGPU.py:536-553): E[n] = sum_{i<j} J[pair(i,j)][q*s_i+s_j] for the
- * first nseq sequences of a buffer of row length buflen.  Accumulated in
- * double and fixed point (deterministic), rounded once to float.  The
+ * first nseq sequences of a buffer of row length buflen.  Each site's row
+ * of at most 16 couplings per tile is summed in float, rows in double, tiles
+ * in 64-bit fixed point (deterministic); rounded once to float.  The
  * workspace (device, >= mi3_energies_workspace(nseq) bytes, 8-byte aligned)
  * is clobbered. */
 int mi3_energies(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
@@ -125,6 +126,22 @@ int mi3_energies(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32
 int mi3_energies_noalloc(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
                          float *energies, uint32_t L, uint32_t q, void *stream);
 
+/* Bytes of workspace mi3_energies_cons needs (256-byte aligned). */
+size_t mi3_energies_cons_workspace(uint32_t L, uint32_t q, uint32_t nseq);
+
+/* mi3_energies with the pair work limited to pairs where neither residue is
+ * its site's reference residue cons[i] (device, L bytes, e.g. from
+ * mi3_site_consensus): the couplings are moved in FP64 to the gauge where
+ * row cons[i] and column cons[j] of every pair block are zero (rounded once
+ * to float, in the workspace), the removed parts summed as site fields and
+ * a constant in FP64.  Same energies as mi3_energies up to that rounding:
+ * |E - E_exact| <= 2^-20 * sum_{i<j} |J'(s_i,s_j)|, with |J'| <= 4 max|J|.
+ * L*q*8 + 8 <= 200 KiB.  No counterpart in the reference (an addition of
+ * this library). */
+int mi3_energies_cons(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
+                      float *energies, uint32_t L, uint32_t q, const uint8_t *cons, void *workspace,
+                      size_t ws_bytes, void *stream);
+
 /* ------------------------------------------------------------ bimarginals */
 
 /* countBivariate (mcmc.cl:462-516) as launched by MCMCGPU.calcBicounts
@@ -145,19 +162,38 @@ int mi3_bicounts_tc(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint
 int mi3_bicounts_to_bimarg(const uint32_t *bicount, float *bimarg, uint32_t nseq, uint32_t L,
                            uint32_t q, void *stream);
 
-/* Bytes of workspace mi3_weighted_marg needs. */
-size_t mi3_weighted_marg_workspace(uint32_t L, uint32_t q);
+/* Bytes of workspace mi3_weighted_marg needs for nseq sequences:
+ * 256 + 8*L*q (padded to 256) + 4 * nPairs * q*q per chunk of up to 65536
+ * sequences. */
+size_t mi3_weighted_marg_workspace(uint32_t L, uint32_t q, uint32_t nseq);
 
 /* weightedMarg (mcmc.cl:646-718), MCMCGPU.weightedMarg (mcmcGPU.py:634-661):
  * unnormalised bi[pair][q*a+b] = sum_n w_n [s_i=a][s_j=b] for weights >= 0.
  * Reads the seq main layout directly (no transposed copy needed).  Sums are
  * accumulated as integers in fixed point (each weight rounded to 2^-s,
- * s >= 16 - log2(max w)), so the result is deterministic.  The workspace
- * (>= mi3_weighted_marg_workspace(L,q) bytes, 256-byte aligned) is
+ * s >= 15 - log2(max w)): per chunk of sequences in uint32, then across
+ * chunks in uint64 in a fixed order, so the result is deterministic.
+ * cons (device, L bytes, nullable): a reference residue per site, for
+ * example from mi3_site_consensus.  With it, only pairs where neither site
+ * holds its reference residue are histogrammed; the other bins are rebuilt
+ * exactly from per-site sums, so the result is bit-identical to the call
+ * without cons, and faster when the reference residues are frequent (it is
+ * ignored for q > 64 or L*q*4 + L > 160 KiB).  The workspace
+ * (>= mi3_weighted_marg_workspace(L,q,nseq) bytes, 256-byte aligned) is
  * clobbered. */
 int mi3_weighted_marg(const float *weights, const uint32_t *seqmem, uint32_t buflen,
-                      uint32_t nseq, float *bimarg, uint32_t L, uint32_t q, void *workspace,
-                      size_t ws_bytes, void *stream);
+                      uint32_t nseq, float *bimarg, uint32_t L, uint32_t q, const uint8_t *cons,
+                      void *workspace, size_t ws_bytes, void *stream);
+
+/* Bytes of workspace mi3_site_consensus needs: 8*L*q. */
+size_t mi3_site_consensus_workspace(uint32_t L, uint32_t q);
+
+/* cons[i] = the most frequent residue at site i among the first nseq
+ * sequences (the lowest on ties); L*q*4 + L <= 160 KiB.  No counterpart in
+ * the reference: the consensus residues let the pair kernels skip work (see
+ * mi3_weighted_marg and mi3_energies_cons). */
+int mi3_site_consensus(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t L, uint32_t q,
+                       uint8_t *cons, void *workspace, size_t ws_bytes, void *stream);
 
 /* renormalize_bimarg (mcmc.cl:753-759), MCMCGPU.renormalize_bimarg
  * (mcmcGPU.py:663-668), same summation tree as the reference. */
@@ -292,6 +328,32 @@ int mi3_mh_independence(uint32_t *seq, const uint32_t *prop, uint32_t buflen, ui
 
 /* addFloatBufs (mcmc.cl:720-727), MCMCGPU.addFloatBuf (mcmcGPU.py:670-685). */
 int mi3_add_float_bufs(float *dst, const float *src, uint32_t n, void *stream);
+
+/* ---- per-round host work on the device (FP64) ---------------------------
+ * The reference runs these on the host in numpy each round
+ * (NewtonSteps.py:618 fieldlessGaugeEven before sampling; :33-54
+ * bimarg_stats / printstats after it); the device forms keep J resident. */
+
+/* Bytes of workspace mi3_gauge_fieldless_even needs: 8*(nPairs*(2q+1) + L*q). */
+size_t mi3_gauge_workspace(uint32_t L, uint32_t q);
+
+/* Jout = fieldlessGaugeEven(0, J)[1] (changeGauge.py:37-155: zero gauge with
+ * the fields folded evenly into the couplings) computed in FP64 and rounded
+ * once to float; Jout may equal J.  J, Jout: nPairs x q*q floats. */
+int mi3_gauge_fieldless_even(const float *J, float *Jout, uint32_t L, uint32_t q, void *workspace,
+                             size_t ws_bytes, void *stream);
+
+/* Bytes of workspace mi3_bimarg_stats needs: 48 * nPairs. */
+size_t mi3_bimarg_stats_workspace(uint32_t L);
+
+/* bimarg_stats + the X statistic of printstats (NewtonSteps.py:33-54) in
+ * FP64 into out[6] (device, 8-byte aligned): SSR = sum (t-m)^2, max |t-m|,
+ * mean |t-m|/t over entries with t > 0.01f, the number of those entries,
+ * X_model = sum J (m - m_a m_b), X_target = sum J (t - t_a t_b) (m_a, m_b the
+ * pair's row and column sums).  J may be NULL (then out[4] = out[5] = 0).
+ * Deterministic (fixed reduction order). */
+int mi3_bimarg_stats(const float *target, const float *model, const float *J, uint32_t L, uint32_t q,
+                     double *out, void *workspace, size_t ws_bytes, void *stream);
 
 #ifdef __cplusplus
 }

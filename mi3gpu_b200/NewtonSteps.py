@@ -91,6 +91,9 @@ def iterNewton(param, bimarg_model, gpus, log, fused=False):
     if param.distribute_jstep not in (None, 'all'):
         raise NotImplementedError("distribute_jstep other than 'all' needs the large sequence buffers")
 
+    # the walkers are fixed during the Newton steps: their consensus residues
+    # let the energy and weighted-bimarginal passes skip most pairs
+    gpus.updateConsensus(seqbuf)
     gpus.calcEnergies(seqbuf)
     gpus.calcBicounts(seqbuf)
     gpus.bicounts_to_bimarg(seqbuf)
@@ -143,6 +146,18 @@ def iterNewton(param, bimarg_model, gpus, log, fused=False):
 
     log(f"Performed {i} coupling update steps")
 
+    if param.device_resident:
+        # trial J = J + dJ formed in place on every device (the reference reads
+        # bi, J, dJ back, adds them on the host and sends J down again)
+        gpus.addFloatBuf('J', 'dJ')
+        st = gpus.bimargStats('bi', 'bi target', None)[0].read()
+        log(f"Predicted statistics after perturbing J: SSR {st[0]:.4f}")
+        if not np.isfinite(wsum) or wsum == 0:
+            raise Exception("Error: Divergence. Decrease gamma or increase pc-damping")
+        log(f"Total Newton-step running time: {time.time() - s:.1f} s")
+        gpus.logProfile()
+        return i, None, None
+
     bi, J, dJ = gpus.head_gpu.readBufs(['bi', 'J', 'dJ'])
     bimarg_model, trialJ = bi[0], J[0] + dJ[0]
     weights = gpus.collect(wbufname)
@@ -176,7 +191,8 @@ def runMCMC(gpus, couplings, runName, param, log):
     nloop = param.equiltime
     trackequil = param.trackequil or 0
     outdir = param.outdir
-    gpus.setBuf('J', couplings)
+    if couplings is not None:  # None: J is already resident on the devices
+        gpus.setBuf('J', couplings)
 
     if nloop == 'auto':
         equil_dir = None
@@ -228,7 +244,16 @@ def runMCMC(gpus, couplings, runName, param, log):
         step = int(nloop)
         e_rho = [spearmanr(ei, equil_e[-1]) for ei in equil_e]
 
-    if param.beta is None:
+    if param.beta is None and param.device_resident:
+        # bimarginals stay on the device ('bi'); only the energies come back
+        gpus.calcBicounts('main')
+        gpus.calcEnergies('main')
+        gpus.bicounts_to_bimarg('main')
+        if gpus.ngpus > 1:
+            gpus.merge_bimarg()
+        es = gpus.collect('E main')
+        bimarg_model, bicount = None, None
+    elif param.beta is None:
         gpus.calcBicounts('main')
         gpus.calcEnergies('main')
         bicount, es = gpus.collect(['bicount', 'E main'])
@@ -250,6 +275,8 @@ def NewtonSteps(runName, param, bimarg_model, gpus, log):
     outdir = param.outdir
     if param.newtonSteps != 1:
         Jsteps, newJ, bimarg_p = iterNewton(param, bimarg_model, gpus, log, fused=bool(param.fused))
+        if outdir is not None and param.device_resident:
+            (bimarg_p,), (newJ,) = gpus.head_gpu.readBufs(['bi', 'J'])
         if outdir is not None:
             np.save(outdir / runName / 'predictedBimarg', bimarg_p)
             np.save(outdir / runName / 'perturbedJ', newJ)
@@ -260,16 +287,49 @@ def NewtonSteps(runName, param, bimarg_model, gpus, log):
     return Jsteps, newJ
 
 
+def _device_stats_line(name, jstep, gpus, energies, e_rho):
+    """printstats (NewtonSteps.py:43-80) from the device's FP64 statistics:
+    SSR, rel% and max% of bimarg_stats, X of model and target, plus the
+    first entries of the bimarginals and couplings."""
+    st = gpus.bimargStats('bi', 'bi target', 'J')[0].read()
+    ssr, maxd, ferr, xm, xt = float(st[0]), float(st[1]) * 100, float(st[2]) * 100, float(st[4]), float(st[5])
+    head = gpus.head_gpu.gpus[0]
+    rhostr = '(none)'
+    if e_rho is not None:
+        rho = [r[0] for r in e_rho]
+        rhostr = np.array2string(np.array(rho), precision=2, floatmode='fixed', suppress_small=True)[1:-1]
+    lowE, meanE, stdE = np.min(energies), np.mean(energies), np.std(energies)
+    line = (f"{name} {jstep: 6d} Error: SSR:{ssr:6.3f}   rel%:{ferr:5.2f}   max%:{maxd:5.2f}   "
+            f"X:{xm: 6.1f} ({xt: 6.1f})\n"
+            f"{name} bimarg: {printsome(head.peekBuf('bi'))} ...\n"
+            f"{name}      J: {printsome(head.peekBuf('J'))} ...\n"
+            f"{name} min(E) = {lowE:.4f}     mean(E) = {meanE:.4f}     std(E) = {stdE:.4f}\n"
+            f"{name} E Autocorr vs time: {rhostr}")
+    return ssr, line
+
+
 def MCMCstep(runName, Jstep, couplings, param, gpus, log):
     """One round: re-gauge J, equilibrate, report, Newton-update
-    (NewtonSteps.py:610-687)."""
+    (NewtonSteps.py:610-687).
+
+    With param.device_resident the couplings never leave the devices:
+    `couplings` is ignored (J is on the devices), the gauge transform and the
+    statistics run there in FP64, and sequences are read back only when they
+    are saved or needed for reseeding.  The returned J is then None."""
     outdir = param.outdir
     L, q = param.L, param.q
     bimarg_target = param.bimarg
+    dev = bool(param.device_resident)
 
     log("")
     log(f"Gradient Descent step {runName}")
-    couplings = fieldlessGaugeEven(np.zeros((L, q)), couplings)[1].astype('<f4')
+    if dev:
+        gpus.gaugeJ('J')
+        couplings = gpus.head_gpu.readBufs('J')[0] if outdir is not None else None
+        run_J = None
+    else:
+        couplings = fieldlessGaugeEven(np.zeros((L, q)), couplings)[1].astype('<f4')
+        run_J = couplings
     if outdir is not None:
         rundir = outdir / runName
         rundir.mkdir(parents=True, exist_ok=True)
@@ -279,18 +339,26 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
 
     start_time = time.time()
     (bimarg_model, bicount, sampledenergies, e_rho, ptinfo,
-     equilsteps) = runMCMC(gpus, couplings, runName, param, log)
+     equilsteps) = runMCMC(gpus, run_J, runName, param, log)
     dt = time.time() - start_time
     MC_s = equilsteps * param.nsteps * np.float64(gpus.nwalkers) / dt
     log(f"Total MCMC running time: {dt:.1f} s    ({MC_s:.3g} MC/s)")
 
-    seqs = gpus.collect('seq main')
-    log(printstats(runName, Jstep, bimarg_target, bimarg_model, couplings, sampledenergies, e_rho))
+    seqs = None
+    if not dev or outdir is not None or param.reseed in ('single_random', 'single_best'):
+        seqs = gpus.collect('seq main')
+    if dev:
+        ssr, line = _device_stats_line(runName, Jstep, gpus, sampledenergies, e_rho)
+        log(line)
+        if outdir is not None:
+            bimarg_model = gpus.head_gpu.collect('bi')
+    else:
+        log(printstats(runName, Jstep, bimarg_target, bimarg_model, couplings, sampledenergies, e_rho))
+        ssr = np.sum((bimarg_target - bimarg_model) ** 2)
     if outdir is not None:
         np.save(outdir / runName / 'seqs', seqs)
 
     ns_delta = param.newton_delta or 32
-    ssr = np.sum((bimarg_target - bimarg_model) ** 2)
     if param.last_ssr is not None:
         if ssr > (param.last_ssr + param.min_ssr) / 2:
             param.newtonSteps = max(ns_delta, param.newtonSteps - int(1.5 * ns_delta))
@@ -314,6 +382,8 @@ def newtonMCMC(param, gpus, start_run, Jstep, log):
     'single_random', 'none'."""
     J = param.couplings
     gpus.setBuf('bi target', param.bimarg)
+    if param.device_resident:
+        gpus.setBuf('J', np.asarray(J, dtype='<f4'))
     param.max_newtonSteps = param.newtonSteps
     param.min_ssr = np.inf
     seqs, es = None, None
@@ -341,4 +411,6 @@ def newtonMCMC(param, gpus, start_run, Jstep, log):
             param.equiltime = param.equiltime_first
         Jstep, seqs, es, J = MCMCstep(runname, Jstep, J, param, gpus, log)
         param.equiltime = equil
+    if param.device_resident:
+        J = gpus.head_gpu.readBufs('J')[0]  # trial J of the last round, as the host path returns
     return J

@@ -23,11 +23,15 @@ SIGNATURES = {
     "mi3_energies_workspace": (c.c_size_t, [_u32]),
     "mi3_energies": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),
     "mi3_energies_noalloc": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp]),
+    "mi3_energies_cons_workspace": (c.c_size_t, [_u32, _u32, _u32]),
+    "mi3_energies_cons": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp, c.c_size_t, _vp]),
     "mi3_bicounts": (c.c_int, [_vp, _u32, _u32, _vp, _u32, _u32, _vp]),
     "mi3_bicounts_tc": (c.c_int, [_vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp]),
     "mi3_bicounts_to_bimarg": (c.c_int, [_vp, _vp, _u32, _u32, _u32, _vp]),
-    "mi3_weighted_marg_workspace": (c.c_size_t, [_u32, _u32]),
-    "mi3_weighted_marg": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),
+    "mi3_weighted_marg_workspace": (c.c_size_t, [_u32, _u32, _u32]),
+    "mi3_weighted_marg": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp, c.c_size_t, _vp]),
+    "mi3_site_consensus_workspace": (c.c_size_t, [_u32, _u32]),
+    "mi3_site_consensus": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _vp, _vp, c.c_size_t, _vp]),
     "mi3_renormalize_bimarg": (c.c_int, [_vp, _u32, _u32, _vp]),
     "mi3_repack_seqs_T": (c.c_int, [_vp, _u32, _vp, _u32, _u32, _vp]),
     "mi3_update_j": (c.c_int, [_vp, _vp, _f32, _f32, _vp, _vp, _u32, _u32, _vp]),
@@ -47,6 +51,10 @@ SIGNATURES = {
     "mi3_weight_stats": (c.c_int, [_vp, _u32, _vp, _vp, _vp, c.c_size_t, _vp]),
     "mi3_weights_fused": (c.c_int, [_f32, _vp, _vp, _u32, _vp, _vp, _vp, _vp, c.c_size_t, _vp]),
     "mi3_add_float_bufs": (c.c_int, [_vp, _vp, _u32, _vp]),
+    "mi3_gauge_workspace": (c.c_size_t, [_u32, _u32]),
+    "mi3_gauge_fieldless_even": (c.c_int, [_vp, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),
+    "mi3_bimarg_stats_workspace": (c.c_size_t, [_u32]),
+    "mi3_bimarg_stats": (c.c_int, [_vp, _vp, _vp, _u32, _u32, _vp, _vp, c.c_size_t, _vp]),
     "mi3_made_forward": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _u32, _u32] + [_vp] * 12 + [_vp]),
     "mi3_made_backward": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _u32, _u32] + [_vp] * 21 + [_vp]),
     "mi3_made_adam": (c.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _u64, _f32, _f32, _f32, _f32, _u32, _vp]),

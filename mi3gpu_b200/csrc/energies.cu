@@ -2,11 +2,13 @@
 //
 // Slice-tiled (tiling.cuh): a CTA holds the couplings of one block pair in
 // shared memory and streams a chunk of sequences through it; each thread
-// sums its sequence's B*B gathered couplings in double and adds the slice
-// total to a per-sequence 64-bit fixed-point accumulator (scale 2^40) with an
-// integer atomic.  Integer addition is associative, so the result does not
-// depend on CTA order: energies are deterministic, and accurate to ~1e-12
-// absolute before the final rounding to float.  The reference sums each
+// sums its sequence's gathered couplings (float within a site row of at most
+// B terms, double across rows) and adds the slice total to a per-sequence
+// 64-bit fixed-point accumulator (scale 2^40) with an integer atomic.
+// Integer addition is associative, so the result does not depend on CTA
+// order: energies are deterministic.  The float row sums bound the error at
+// about B*2^-24 of the largest row sum per row, far below the final
+// rounding to float for the energies the sampler meets.  The reference sums each
 // sequence serially with Kahan compensation in float (getEnergiesf,
 // mcmc.cl:249-336); this result is at least as accurate.
 #include <mutex>
@@ -18,11 +20,94 @@ namespace mi3 {
 constexpr double FIX_SCALE = 1099511627776.0;  // 2^40
 constexpr double FIX_INV = 1.0 / 1099511627776.0;
 
-template <int B>
-__global__ void __launch_bounds__(512) k_energies(const float *__restrict__ J,
-                                                  const uint32_t *__restrict__ seq, uint32_t buflen,
-                                                  uint32_t nseq, unsigned long long *acc, uint32_t L,
-                                                  uint32_t q, SliceGeom g) {
+// Energy of one sequence over the pairs of one slice: each site row of B
+// couplings is summed in float (at most B terms) and the row sums in double.
+// CONS: the table is in the consensus gauge (tiling.cuh), so pairs where
+// either residue is its site's consensus contribute zero and are skipped.
+template <int B, int K, bool CONS>
+__device__ __forceinline__ double slice_energy(const float *js, const uint32_t (&wI)[B / 4],
+                                               const uint32_t (&wJ)[B / 4], const uint32_t (&cI)[B / 4],
+                                               const uint32_t (&cJ)[B / 4], uint32_t q, uint32_t qq,
+                                               uint32_t i0, uint32_t j0, uint32_t L) {
+    uint32_t col[B];
+    slice_cols<B>(wJ, q, qq, col);
+    double e = 0.0;
+    if constexpr (!CONS) {
+#pragma unroll
+        for (int ii = 0; ii < B; ++ii) {
+            if (K == SLICE_EDGE && i0 + ii >= L) break;
+            const uint32_t row = slice_row<B>(wI, ii, q, qq);
+            float r = 0.0f;
+#pragma unroll
+            for (int jj = 0; jj < B; ++jj)
+                if (slice_pair_valid<K>(ii, jj, i0, j0, L)) r += js[row + col[jj]];
+            e += (double)r;
+        }
+    } else {
+        uint32_t mI[B / 4], mJ[B / 4];
+        cons_masks<B>(wI, cI, mI);
+        cons_masks<B>(wJ, cJ, mJ);
+        const uint32_t cb = cons_bits<B>(mJ);
+        const uint32_t base = (uint32_t)__cvta_generic_to_shared(js);
+#pragma unroll
+        for (int ii = 0; ii < B; ++ii) {
+            if (K == SLICE_EDGE && i0 + ii >= L) break;
+            const uint32_t row = slice_row<B>(wI, ii, q, qq);
+            const uint32_t rb = cons_off<B>(mI, ii) ? cb : 0u;  // active columns of this row
+            float v[B];
+#pragma unroll
+            for (int jj = 0; jj < B; ++jj)
+                v[jj] = slice_pair_valid<K>(ii, jj, i0, j0, L) ? lds_if(base + 4u * (row + col[jj]), rb & (1u << jj))
+                                                               : 0.0f;
+            float r = 0.0f;
+#pragma unroll
+            for (int jj = 0; jj < B; ++jj) r += v[jj];
+            e += (double)r;
+        }
+    }
+    return e;
+}
+
+template <int B, int K, bool CONS>
+__device__ __forceinline__ void energies_chunk(const float *js, const uint32_t *__restrict__ seq, uint32_t buflen,
+                                               uint32_t nbeg, uint32_t nend, unsigned long long *acc,
+                                               uint32_t L, uint32_t q, uint32_t bi, uint32_t bj,
+                                               const uint32_t (&cI)[B / 4], const uint32_t (&cJ)[B / 4]) {
+    const uint32_t qq = q * q, swords = (L - 1) / 4 + 1;
+    const uint32_t i0 = bi * B, j0 = bj * B;
+    if constexpr (B <= 8 || !CONS) {
+        // two sequences per thread: two independent gather/add chains in flight
+        for (uint32_t n = nbeg + threadIdx.x; n < nend; n += 2 * blockDim.x) {
+            const uint32_t n2 = n + blockDim.x;
+            const bool two = n2 < nend;
+            uint32_t wI[B / 4], wJ[B / 4], vI[B / 4], vJ[B / 4];
+            load_block_words<B>(seq, buflen, n, bi, swords, wI);
+            load_block_words<B>(seq, buflen, n, bj, swords, wJ);
+            load_block_words<B>(seq, buflen, two ? n2 : n, bi, swords, vI);
+            load_block_words<B>(seq, buflen, two ? n2 : n, bj, swords, vJ);
+            const double e1 = slice_energy<B, K, CONS>(js, wI, wJ, cI, cJ, q, qq, i0, j0, L);
+            const double e2 = slice_energy<B, K, CONS>(js, vI, vJ, cI, cJ, q, qq, i0, j0, L);
+            atomicAdd(&acc[n], (unsigned long long)__double2ll_rn(e1 * FIX_SCALE));
+            if (two) atomicAdd(&acc[n2], (unsigned long long)__double2ll_rn(e2 * FIX_SCALE));
+        }
+    } else {
+        // 16-site blocks with consensus masks: one sequence per thread keeps
+        // the offsets and masks in registers
+        for (uint32_t n = nbeg + threadIdx.x; n < nend; n += blockDim.x) {
+            uint32_t wI[B / 4], wJ[B / 4];
+            load_block_words<B>(seq, buflen, n, bi, swords, wI);
+            load_block_words<B>(seq, buflen, n, bj, swords, wJ);
+            const double e1 = slice_energy<B, K, CONS>(js, wI, wJ, cI, cJ, q, qq, i0, j0, L);
+            atomicAdd(&acc[n], (unsigned long long)__double2ll_rn(e1 * FIX_SCALE));
+        }
+    }
+}
+
+template <int B, bool CONS>
+__global__ void __launch_bounds__(512, 2) k_energies(const float *__restrict__ J,
+                                                     const uint32_t *__restrict__ seq, uint32_t buflen,
+                                                     uint32_t nseq, unsigned long long *acc, uint32_t L,
+                                                     uint32_t q, SliceGeom g, const uint8_t *__restrict__ cons) {
     extern __shared__ __align__(16) float js[];  // [B*B][q*q]
     const uint32_t qq = q * q;
     const uint32_t s = blockIdx.x % g.nslices;
@@ -43,38 +128,25 @@ __global__ void __launch_bounds__(512) k_energies(const float *__restrict__ J,
         uint32_t cnt = (jhi - jlo) * qq;
         for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) dst[k] = __ldg(&src[k]);
     }
+    uint32_t cI[B / 4] = {}, cJ[B / 4] = {};
+    if constexpr (CONS) {
+        load_cons_words<B>(cons, bi, L, cI);
+        load_cons_words<B>(cons, bj, L, cJ);
+    }
     __syncthreads();
 
-    const uint32_t swords = (L - 1) / 4 + 1;
     const uint32_t nbeg = chunk * g.chunk;
     const uint32_t nend = min(nseq, nbeg + g.chunk);
-    // two sequences per thread: two independent gather/add chains in flight
-    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += 2 * blockDim.x) {
-        const uint32_t n2 = n + blockDim.x;
-        const bool two = n2 < nend;
-        uint32_t wI[B / 4], wJ[B / 4], vI[B / 4], vJ[B / 4];
-        load_block_words<B>(seq, buflen, n, bi, swords, wI);
-        load_block_words<B>(seq, buflen, n, bj, swords, wJ);
-        load_block_words<B>(seq, buflen, two ? n2 : n, bi, swords, vI);
-        load_block_words<B>(seq, buflen, two ? n2 : n, bj, swords, vJ);
-        double e1 = 0.0, e2 = 0.0;
-#pragma unroll
-        for (int ii = 0; ii < B; ++ii) {
-            uint32_t i = i0 + ii;
-            if (i >= L) break;
-            const float *row1 = js + (size_t)ii * B * qq + block_byte<B>(wI, ii, q - 1) * q;
-            const float *row2 = js + (size_t)ii * B * qq + block_byte<B>(vI, ii, q - 1) * q;
-#pragma unroll
-            for (int jj = 0; jj < B; ++jj) {
-                uint32_t j = j0 + jj;
-                if (j < L && j > i) {
-                    e1 += (double)row1[(size_t)jj * qq + block_byte<B>(wJ, jj, q - 1)];
-                    e2 += (double)row2[(size_t)jj * qq + block_byte<B>(vJ, jj, q - 1)];
-                }
-            }
-        }
-        atomicAdd(&acc[n], (unsigned long long)__double2ll_rn(e1 * FIX_SCALE));
-        if (two) atomicAdd(&acc[n2], (unsigned long long)__double2ll_rn(e2 * FIX_SCALE));
+    switch (slice_kind(bi, bj, j0, B, L)) {
+        case SLICE_FULL:
+            energies_chunk<B, SLICE_FULL, CONS>(js, seq, buflen, nbeg, nend, acc, L, q, bi, bj, cI, cJ);
+            break;
+        case SLICE_DIAG:
+            energies_chunk<B, SLICE_DIAG, CONS>(js, seq, buflen, nbeg, nend, acc, L, q, bi, bj, cI, cJ);
+            break;
+        default:
+            energies_chunk<B, SLICE_EDGE, CONS>(js, seq, buflen, nbeg, nend, acc, L, q, bi, bj, cI, cJ);
+            break;
     }
 }
 
@@ -83,16 +155,118 @@ __global__ void k_energies_final(const unsigned long long *__restrict__ acc, flo
     if (k < n) E[k] = (float)((double)(long long)acc[k] * FIX_INV);
 }
 
-template <int B>
+template <int B, bool CONS>
 static int launch_energies(const float *J, const uint32_t *seq, uint32_t buflen, uint32_t nseq,
-                           unsigned long long *acc, uint32_t L, uint32_t q, cudaStream_t st) {
+                           unsigned long long *acc, uint32_t L, uint32_t q, const uint8_t *cons, cudaStream_t st) {
     SliceGeom g = make_geom(L, B, nseq, 148 * 8, 2048);
     size_t smem = (size_t)B * B * q * q * 4;
-    cudaFuncSetAttribute(k_energies<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_energies<B, CONS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     uint64_t nblk = (uint64_t)g.nslices * g.nchunks;
     if (nblk > 0x7fffffffull) return fail(MI3_ERR_ARG, "mi3_energies: grid too large");
-    k_energies<B><<<(uint32_t)nblk, 512, smem, st>>>(J, seq, buflen, nseq, acc, L, q, g);
+    k_energies<B, CONS><<<(uint32_t)nblk, 512, smem, st>>>(J, seq, buflen, nseq, acc, L, q, g, cons);
     return check_launch("mi3_energies");
+}
+
+template <bool CONS>
+static int dispatch_energies(const float *J, const uint32_t *seq, uint32_t buflen, uint32_t nseq,
+                             unsigned long long *acc, uint32_t L, uint32_t q, const uint8_t *cons,
+                             cudaStream_t st) {
+    switch (pick_block(q, 116 * 1024, 16)) {
+        case 16: return launch_energies<16, CONS>(J, seq, buflen, nseq, acc, L, q, cons, st);
+        case 8: return launch_energies<8, CONS>(J, seq, buflen, nseq, acc, L, q, cons, st);
+        case 4: return launch_energies<4, CONS>(J, seq, buflen, nseq, acc, L, q, cons, st);
+        default: return fail(MI3_ERR_ARG, "mi3_energies: q too large");
+    }
+}
+
+// ------------------------------------------------------- consensus gauge
+// J'(a,b) = J(a,b) - J(a,c_j) - J(c_i,b) + J(c_i,c_j), computed in double and
+// rounded once; row c_i and column c_j of J' are exactly zero.  The removed
+// parts: x_i(a) = J(a,c_j) - J(c_i,c_j) for site i, y_j(b) = J(c_i,b) -
+// J(c_i,c_j) for site j, and the constant J(c_i,c_j), so that
+// J(a,b) = J'(a,b) + x_i(a) + y_j(b) + J(c_i,c_j).
+__global__ void k_cons_gauge(const float *__restrict__ J, const uint8_t *__restrict__ cons, float *Jc,
+                             uint32_t L, uint32_t q) {
+    const uint32_t p = blockIdx.x;
+    __shared__ uint32_t ij[2];
+    if (threadIdx.x == 0) {
+        uint32_t r = 0;
+        uint64_t start = 0;
+        while (r + 1 < L && p >= start + (L - 1 - r)) {
+            start += L - 1 - r;
+            ++r;
+        }
+        ij[0] = r;
+        ij[1] = r + 1 + (uint32_t)(p - start);
+    }
+    __syncthreads();
+    const uint32_t qq = q * q;
+    const uint32_t ci = min((uint32_t)cons[ij[0]], q - 1), cj = min((uint32_t)cons[ij[1]], q - 1);
+    const float *Jp = J + (size_t)p * qq;
+    const double cc = Jp[ci * q + cj];
+    for (uint32_t e = threadIdx.x; e < qq; e += blockDim.x) {
+        const uint32_t a = e / q, b = e - a * q;
+        const double v = ((double)Jp[e] - (double)Jp[a * q + cj]) - ((double)Jp[ci * q + b] - cc);
+        Jc[(size_t)p * qq + e] = (float)v;
+    }
+}
+
+// Site fields of the consensus gauge, h[k][a] = sum over the pairs of site k
+// of its x or y part, and the per-site share of the constant (pairs (k, j>k)).
+__global__ void k_cons_fields(const float *__restrict__ J, const uint8_t *__restrict__ cons, double *h,
+                              double *cpart, uint32_t L, uint32_t q) {
+    const uint32_t k = blockIdx.x, qq = q * q;
+    const uint32_t ck = min((uint32_t)cons[k], q - 1);
+    for (uint32_t a = threadIdx.x; a < q; a += blockDim.x) {
+        double acc = 0.0;
+        for (uint32_t i = 0; i < k; ++i) {  // pair (i, k): site k is the column
+            const float *Jp = J + pair_index(i, k, L) * qq;
+            const uint32_t ci = min((uint32_t)cons[i], q - 1);
+            acc += (double)Jp[ci * q + a] - (double)Jp[ci * q + ck];
+        }
+        for (uint32_t j = k + 1; j < L; ++j) {  // pair (k, j): site k is the row
+            const float *Jp = J + pair_index(k, j, L) * qq;
+            const uint32_t cj = min((uint32_t)cons[j], q - 1);
+            acc += (double)Jp[a * q + cj] - (double)Jp[ck * q + cj];
+        }
+        h[(size_t)k * q + a] = acc;
+    }
+    if (threadIdx.x == 0) {
+        double c = 0.0;
+        for (uint32_t j = k + 1; j < L; ++j)
+            c += (double)J[pair_index(k, j, L) * qq + ck * q + min((uint32_t)cons[j], q - 1)];
+        cpart[k] = c;
+    }
+}
+
+// E[n] = pair sums (fixed point) + sum_i h[i][s_i] + constant.
+__global__ void __launch_bounds__(256) k_energies_final_cons(const unsigned long long *__restrict__ acc,
+                                                             const uint32_t *__restrict__ seq, uint32_t buflen,
+                                                             const double *__restrict__ h,
+                                                             const double *__restrict__ cpart, float *E,
+                                                             uint32_t n, uint32_t L, uint32_t q) {
+    extern __shared__ double hs[];  // [L*q] fields, then the constant
+    for (uint32_t k = threadIdx.x; k < L * q; k += blockDim.x) hs[k] = h[k];
+    if (threadIdx.x == 0) {
+        double c = 0.0;
+        for (uint32_t k = 0; k < L; ++k) c += cpart[k];
+        hs[L * q] = c;
+    }
+    __syncthreads();
+    const uint32_t swords = (L - 1) / 4 + 1;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        double e = (double)(long long)acc[m] * FIX_INV;
+        double f = 0.0;
+        for (uint32_t w = 0; w < swords; ++w) {
+            const uint32_t word = __ldg(&seq[(size_t)w * buflen + m]);
+#pragma unroll
+            for (uint32_t t = 0; t < 4; ++t) {
+                const uint32_t site = 4 * w + t;
+                if (site < L) f += hs[site * q + min((word >> (8 * t)) & 0xffu, q - 1)];
+            }
+        }
+        E[m] = (float)(e + f + hs[L * q]);
+    }
 }
 
 }  // namespace mi3
@@ -116,15 +290,7 @@ extern "C" int mi3_energies(const float *J, const uint32_t *seqmem, uint32_t buf
     auto *acc = reinterpret_cast<unsigned long long *>(workspace);
     if (cudaMemsetAsync(acc, 0, (size_t)nseq * 8, st) != cudaSuccess)
         return check_launch("mi3_energies: memset");
-    uint32_t B = pick_block(q, 116 * 1024);
-    int rc;
-    switch (B) {
-        case 32: rc = launch_energies<32>(J, seqmem, buflen, nseq, acc, L, q, st); break;
-        case 16: rc = launch_energies<16>(J, seqmem, buflen, nseq, acc, L, q, st); break;
-        case 8: rc = launch_energies<8>(J, seqmem, buflen, nseq, acc, L, q, st); break;
-        case 4: rc = launch_energies<4>(J, seqmem, buflen, nseq, acc, L, q, st); break;
-        default: return fail(MI3_ERR_ARG, "mi3_energies: q too large");
-    }
+    int rc = dispatch_energies<false>(J, seqmem, buflen, nseq, acc, L, q, nullptr, st);
     if (rc) return rc;
     k_energies_final<<<(nseq + 255) / 256, 256, 0, st>>>(acc, energies, nseq);
     return check_launch("mi3_energies: final");
@@ -188,14 +354,57 @@ extern "C" int mi3_energies_noalloc(const float *J, const uint32_t *seqmem, uint
     // the accumulators keep the previous call's sums: clear the part used
     if (cudaMemsetAsync(acc, 0, (size_t)nseq * 8, st) != cudaSuccess)
         return check_launch("mi3_energies_noalloc: memset");
-    switch (pick_block(q, 116 * 1024)) {
-        case 32: rc = launch_energies<32>(J, seqmem, buflen, nseq, acc, L, q, st); break;
-        case 16: rc = launch_energies<16>(J, seqmem, buflen, nseq, acc, L, q, st); break;
-        case 8: rc = launch_energies<8>(J, seqmem, buflen, nseq, acc, L, q, st); break;
-        case 4: rc = launch_energies<4>(J, seqmem, buflen, nseq, acc, L, q, st); break;
-        default: return fail(MI3_ERR_ARG, "mi3_energies_noalloc: q too large");
-    }
+    rc = dispatch_energies<false>(J, seqmem, buflen, nseq, acc, L, q, nullptr, st);
     if (rc) return rc;
     k_energies_final<<<(nseq + 255) / 256, 256, 0, st>>>(acc, energies, nseq);
     return check_launch("mi3_energies_noalloc: final");
+}
+
+// ---------------------------------------------------------------------------
+// Energies in the consensus gauge: the same values as mi3_energies (up to
+// the rounding of the regauged couplings to float), with the pair work
+// limited to the pairs where neither residue is its site's consensus.
+extern "C" size_t mi3_energies_cons_workspace(uint32_t L, uint32_t q, uint32_t nseq) {
+    const size_t acc = ((size_t)nseq * 8 + 255) & ~size_t(255);
+    const size_t jc = ((size_t)npairs_of(L) * q * q * 4 + 255) & ~size_t(255);
+    return acc + jc + (size_t)L * q * 8 + (size_t)L * 8;
+}
+
+extern "C" int mi3_energies_cons(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
+                                 float *energies, uint32_t L, uint32_t q, const uint8_t *cons, void *workspace,
+                                 size_t ws_bytes, void *stream) {
+    if (!J || !seqmem || !energies || !cons || !workspace)
+        return fail(MI3_ERR_ARG, "mi3_energies_cons: null pointer");
+    if (L < 2 || q < 1 || q > 255 || nseq > buflen) return fail(MI3_ERR_ARG, "mi3_energies_cons: bad L/q/nseq");
+    if ((size_t)(L * q + 1) * 8 > 200 * 1024) return fail(MI3_ERR_ARG, "mi3_energies_cons: L*q too large");
+    if (nseq == 0) return MI3_OK;
+    if (ws_bytes < mi3_energies_cons_workspace(L, q, nseq))
+        return fail(MI3_ERR_WORKSPACE, "mi3_energies_cons: workspace too small");
+    if (!aligned(workspace, 256)) return fail(MI3_ERR_ALIGN, "mi3_energies_cons: workspace must be 256B aligned");
+    cudaStream_t st = as_stream(stream);
+    unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
+    auto *acc = reinterpret_cast<unsigned long long *>(ws);
+    ws += ((size_t)nseq * 8 + 255) & ~size_t(255);
+    float *Jc = reinterpret_cast<float *>(ws);
+    ws += ((size_t)npairs_of(L) * q * q * 4 + 255) & ~size_t(255);
+    double *h = reinterpret_cast<double *>(ws);
+    double *cpart = h + (size_t)L * q;
+    const uint64_t np = npairs_of(L);
+    if (np > 0x7fffffffull) return fail(MI3_ERR_ARG, "mi3_energies_cons: L too large");
+    k_cons_gauge<<<(uint32_t)np, 256, 0, st>>>(J, cons, Jc, L, q);
+    int rc = check_launch("mi3_energies_cons: gauge");
+    if (rc) return rc;
+    k_cons_fields<<<L, 32, 0, st>>>(J, cons, h, cpart, L, q);
+    rc = check_launch("mi3_energies_cons: fields");
+    if (rc) return rc;
+    if (cudaMemsetAsync(acc, 0, (size_t)nseq * 8, st) != cudaSuccess)
+        return check_launch("mi3_energies_cons: memset");
+    rc = dispatch_energies<true>(Jc, seqmem, buflen, nseq, acc, L, q, cons, st);
+    if (rc) return rc;
+    const size_t smem = (size_t)(L * q + 1) * 8;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_energies_final_cons, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const uint32_t grid = std::min<uint32_t>((nseq + 255) / 256, 148 * 4);
+    k_energies_final_cons<<<grid, 256, smem, st>>>(acc, seqmem, buflen, h, cpart, energies, nseq, L, q);
+    return check_launch("mi3_energies_cons: final");
 }

@@ -23,6 +23,6 @@ int check_launch(const char *what) {
 
 extern "C" const char *mi3_last_error(void) { return mi3::g_last_error.c_str(); }
 
-extern "C" int mi3_abi_version(void) { return 1; }
+extern "C" int mi3_abi_version(void) { return 2; }
 
 extern "C" uint64_t mi3_jrows_stride(uint32_t L, uint32_t q) { return mi3::jrow_stride(L, q); }

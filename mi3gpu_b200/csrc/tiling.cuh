@@ -39,11 +39,12 @@ __host__ __device__ __forceinline__ uint64_t pair_index(uint32_t i, uint32_t j, 
     return (uint64_t)i * (2 * L - i - 1) / 2 + (j - i - 1);
 }
 
-// Largest block size whose slice of q*q-entry pairs fits in `budget` bytes.
-inline uint32_t pick_block(uint32_t q, size_t budget) {
+// Largest block size (at most max_b) whose slice of q*q-entry pairs fits in
+// `budget` bytes.
+inline uint32_t pick_block(uint32_t q, size_t budget, uint32_t max_b = 32) {
     const uint32_t cands[4] = {32, 16, 8, 4};
     for (uint32_t B : cands)
-        if ((size_t)B * B * q * q * 4 <= budget) return B;
+        if (B <= max_b && (size_t)B * B * q * q * 4 <= budget) return B;
     return 0;
 }
 
@@ -79,6 +80,110 @@ __device__ __forceinline__ void load_block_words(const uint32_t *__restrict__ se
 template <int B>
 __device__ __forceinline__ uint32_t block_byte(const uint32_t (&w)[B / 4], int k, uint32_t qm1) {
     return min((w[k >> 2] >> (8 * (k & 3))) & 0xffu, qm1);
+}
+
+// Slice kinds: the B x B pairs of an off-diagonal block pair inside the
+// sequence (every pair valid), a diagonal block pair inside the sequence
+// (pairs jj > ii), and a block pair that crosses the end of the sequence
+// (each pair tested).  Specialising on the kind removes the per-pair tests
+// from the first two, which are all but a few slices.
+enum SliceKind { SLICE_FULL = 0, SLICE_DIAG = 1, SLICE_EDGE = 2 };
+
+__device__ __forceinline__ int slice_kind(uint32_t bi, uint32_t bj, uint32_t j0, uint32_t B, uint32_t L) {
+    if (j0 + B > L) return SLICE_EDGE;
+    return bi == bj ? SLICE_DIAG : SLICE_FULL;
+}
+
+// Whether pair (ii, jj) of a slice of kind K is a real pair i < j < L.
+template <int K>
+__device__ __forceinline__ bool slice_pair_valid(int ii, int jj, uint32_t i0, uint32_t j0, uint32_t L) {
+    if constexpr (K == SLICE_FULL) return true;
+    if constexpr (K == SLICE_DIAG) return jj > ii;
+    return (j0 + jj < L) && (j0 + jj > i0 + ii);
+}
+
+// 32-bit shared-memory offsets of one sequence in a slice table laid out as
+// [ii][jj][a][b]: col[jj] = jj*q*q + s_j, and the row of site ii is
+// ii*B*q*q + s_i*q.
+template <int B>
+__device__ __forceinline__ void slice_cols(const uint32_t (&wJ)[B / 4], uint32_t q, uint32_t qq,
+                                           uint32_t (&col)[B]) {
+#pragma unroll
+    for (int jj = 0; jj < B; ++jj) col[jj] = (uint32_t)jj * qq + block_byte<B>(wJ, jj, q - 1);
+}
+
+template <int B>
+__device__ __forceinline__ uint32_t slice_row(const uint32_t (&wI)[B / 4], int ii, uint32_t q, uint32_t qq) {
+    return (uint32_t)ii * B * qq + block_byte<B>(wI, ii, q - 1) * q;
+}
+
+// ---------------------------------------------------------------- consensus
+// Consensus decomposition.  Every site i has a reference residue c_i (any
+// choice is exact; the most frequent residue makes it fastest).  A pair
+// kernel then visits only the pairs where neither site holds its c:
+//   - pair histograms: the bins of row c_i and column c_j are rebuilt
+//     afterwards from per-site totals (integer arithmetic, exact);
+//   - energies: couplings are first moved to the gauge where row c_i and
+//     column c_j of every pair block are zero, the removed parts becoming
+//     site fields and a constant.
+// Consensus residues of block b packed like sequence words (byte k of word w
+// is site b*B + 4w + k); 0xff past the last site.
+template <int B>
+__device__ __forceinline__ void load_cons_words(const uint8_t *__restrict__ cons, uint32_t b, uint32_t L,
+                                                uint32_t (&c)[B / 4]) {
+#pragma unroll
+    for (int k = 0; k < B / 4; ++k) {
+        uint32_t w = 0;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            uint32_t site = b * B + 4 * k + t;
+            uint32_t v = site < L ? (uint32_t)__ldg(&cons[site]) : 0xffu;
+            w |= v << (8 * t);
+        }
+        c[k] = w;
+    }
+}
+
+// Per-byte "residue differs from the consensus" masks (0xff / 0x00 bytes).
+template <int B>
+__device__ __forceinline__ void cons_masks(const uint32_t (&w)[B / 4], const uint32_t (&c)[B / 4],
+                                           uint32_t (&m)[B / 4]) {
+#pragma unroll
+    for (int k = 0; k < B / 4; ++k) m[k] = __vcmpne4(w[k], c[k]);
+}
+
+template <int B>
+__device__ __forceinline__ bool cons_off(const uint32_t (&m)[B / 4], int k) {
+    return (m[k >> 2] >> (8 * (k & 3))) & 1u;
+}
+
+// Bit jj set when site jj of the block differs from its consensus.
+template <int B>
+__device__ __forceinline__ uint32_t cons_bits(const uint32_t (&m)[B / 4]) {
+    uint32_t b = 0;
+#pragma unroll
+    for (int k = 0; k < B; ++k) b |= ((m[k >> 2] >> (8 * (k & 3))) & 1u) << k;
+    return b;
+}
+
+// Predicated shared-memory access: one bit test selects the lanes, so the
+// masked-off lanes cost no shared-memory bandwidth and no branch.
+__device__ __forceinline__ float lds_if(uint32_t saddr, uint32_t bit) {
+    float v;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\tmov.f32 %0, 0f00000000;\n\t"
+        "@p ld.shared.f32 %0, [%1];\n\t}"
+        : "=f"(v)
+        : "r"(saddr), "r"(bit));
+    return v;
+}
+
+// (volatile asm keeps its order against the barriers around the pass; no
+// memory clobber, so registers stay live across it)
+__device__ __forceinline__ void red_add_if(uint32_t saddr, uint32_t inc, uint32_t bit) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\t@p red.shared.add.u32 [%0], %1;\n\t}" ::"r"(saddr),
+        "r"(inc), "r"(bit));
 }
 
 }  // namespace mi3

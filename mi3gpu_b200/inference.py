@@ -52,7 +52,7 @@ def make_target(L, q, n_msa, seed, sweeps=None, contact_sigma=0.5, device=0):
 
 def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e-4, damping=1e-3,
           reg=('l1z', (2e-4,)), seed=1234, device=0, log=print, fused=True, outdir=None, reseed='independent',
-          sweeps_first=None):
+          sweeps_first=None, device_resident=True):
     """Run `rounds` quasi-Newton iterations from the independent model;
     returns the per-round history (SSR, wall seconds of MCMC and Newton
     phases) as recorded by NewtonSteps.MCMCstep.
@@ -61,7 +61,9 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
     sequences each round (`sweeps` sweeps of equilibration); reseed='none'
     keeps the walkers from the previous round, so after a first round of
     `sweeps_first` sweeps each round only re-equilibrates to the slightly
-    changed couplings."""
+    changed couplings.  device_resident keeps J on the device between
+    rounds (gauge transform and statistics in FP64 there); False runs the
+    round's host work in numpy as the reference does."""
     unimarg = potts.getUnimarg(target)
     J0 = potts.independent_couplings(unimarg)
     nsteps = 8 * L
@@ -71,6 +73,7 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
                   distribute_jstep='all', L=L, q=q, couplings=J0, nsteps=nsteps,
                   equiltime=max(1, sweeps * L // nsteps), trackequil=0, outdir=outdir, mcmcsteps=rounds,
                   newton_delta=32, reseed=reseed, rngseed=seed + 1, unimarg=unimarg, fused=fused, init_indep=True,
+                  device_resident=device_resident,
                   equiltime_first=None if sweeps_first is None else max(1, sweeps_first * L // nsteps)))
     g = MCMCGPU((device, 0), L, q, nwalkers, 512, outdir, 1024, seed + 1)
     gpus = GPU_node([g])

@@ -145,7 +145,7 @@ class MCMCGPU:
         self._setupBuffer('status', '<i4', (1,))
         self._setupWorkspace('ws energies', _lib.query('mi3_energies_workspace', nseq))
         self._setupWorkspace('ws reduce', _lib.query('mi3_weight_stats_workspace', nseq))
-        self._setupWorkspace('ws wmarg', _lib.query('mi3_weighted_marg_workspace', L, q))
+        self._setupWorkspace('ws wmarg', _lib.query('mi3_weighted_marg_workspace', L, q, nseq))
         self.fillBuf('status', 0)
         self.unpackedJ = False
         self.repackedSeqT = {'main': False}
@@ -387,12 +387,61 @@ class MCMCGPU:
                   self._s)
         return self.logevt('bicounts_to_bimarg', s)
 
+    # Consensus decomposition thresholds: the fraction of site pairs at which
+    # neither residue is its site's consensus, below which the consensus
+    # kernels are used.  Measured at L=232 q=21 with 59% of pairs left: the
+    # energy pass drops from 9.8 to 8.5 ms; the weighted histogram does not
+    # gain (its masked shared-memory reductions become divergent branches,
+    # which costs what the saved bank conflicts give back), so it keeps the
+    # direct kernel unless nearly all pairs are skipped.
+    CONS_ENERGY_MAX_ACTIVE = 0.75
+    CONS_WMARG_MAX_ACTIVE = 0.2
+
+    def updateConsensus(self, seqbufname='main'):
+        """Most frequent residue of every site of the walkers -> 'cons', and
+        the fraction of site pairs where neither residue is the consensus.
+        When that fraction is small enough, the energies of 'dJ' (through the
+        consensus gauge) and weightedMarg (bins rebuilt exactly from site
+        sums) skip the other pairs; the residues only steer the work split,
+        so stale ones stay correct.  No counterpart in the reference."""
+        L, q = self.L, self.q
+        if L * q * 4 + L > 160 * 1024 or (L * q + 1) * 8 > 200 * 1024:
+            return None  # shapes the consensus kernels do not take
+        if 'cons' not in self.bufs:
+            self._setupBuffer('cons', '<u1', (L,))
+            self._setupWorkspace('ws cons', _lib.query('mi3_site_consensus_workspace', L, q))
+            self._setupWorkspace('ws energies cons', _lib.query('mi3_energies_cons_workspace', L, q,
+                                                                self.nseq['main']))
+        nseq = self.nseq[seqbufname]
+        s = self._begin()
+        _lib.call('mi3_site_consensus', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, L, q, self._ptr('cons'),
+                  self._ptr('ws cons'), self._wsbytes('ws cons'), self._s)
+        evt = self.logevt('updateConsensus', s)
+        # the workspace holds the per-site residue counts (uint64, L x q)
+        with torch.cuda.stream(self.stream):
+            counts = self.bufs['ws cons'][:L * q].to('cpu').numpy().reshape(L, q).astype(np.float64)
+        off = 1.0 - counts.max(axis=1) / max(1, nseq)
+        active = (off.sum() ** 2 - (off ** 2).sum()) / (L * (L - 1))
+        self.consActive = float(active)
+        self.consEnergies = active <= self.CONS_ENERGY_MAX_ACTIVE
+        self.consWmarg = active <= self.CONS_WMARG_MAX_ACTIVE
+        return evt
+
     def calcEnergies(self, seqbufname, Jbufname='J', wait_for=None):
         nseq = self.nseq[seqbufname]
         s = self._begin()
-        _lib.call('mi3_energies', self._ptr(Jbufname), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
-                  self.Ebufs[seqbufname].data_ptr(), self.L, self.q, self._ptr('ws energies'),
-                  self._wsbytes('ws energies'), self._s)
+        # the consensus gauge rounds the regauged couplings (|J'| <= 4 max|J|)
+        # to float once: used for the small reweighting energies of dJ, where
+        # that is far below the step's statistical error; energies of J keep
+        # the exact table
+        if getattr(self, 'consEnergies', False) and Jbufname == 'dJ':
+            _lib.call('mi3_energies_cons', self._ptr(Jbufname), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
+                      self.Ebufs[seqbufname].data_ptr(), self.L, self.q, self._ptr('cons'),
+                      self._ptr('ws energies cons'), self._wsbytes('ws energies cons'), self._s)
+        else:
+            _lib.call('mi3_energies', self._ptr(Jbufname), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
+                      self.Ebufs[seqbufname].data_ptr(), self.L, self.q, self._ptr('ws energies'),
+                      self._wsbytes('ws energies'), self._s)
         return self.logevt('getEnergies', s)
 
     def min_buf(self, buf, wait_for=None):
@@ -440,8 +489,10 @@ class MCMCGPU:
         self.require('Jstep')
         nseq = self.nseq[seqbufname]
         s = self._begin()
+        cons = self._ptr('cons') if getattr(self, 'consWmarg', False) else None
         _lib.call('mi3_weighted_marg', self._ptr('weights'), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
-                  self._ptr('bi'), self.L, self.q, self._ptr('ws wmarg'), self._wsbytes('ws wmarg'), self._s)
+                  self._ptr('bi'), self.L, self.q, cons, self._ptr('ws wmarg'), self._wsbytes('ws wmarg'),
+                  self._s)
         return self.logevt('weightedMarg', s)
 
     def renormalize_bimarg(self, wait_for=None):
@@ -469,6 +520,42 @@ class MCMCGPU:
         _lib.call('mi3_add_float_bufs', selfbuf.data_ptr(), otherbuf.data_ptr(), self.nPairs * self.q * self.q,
                   self._s)
         return self.logevt('addbibuf', s)
+
+    # ------------------------------------------------------------ round work on the device
+    def gaugeJ(self, Jbufname='J', outbufname=None):
+        """J -> fieldlessGaugeEven(0, J) (changeGauge.py:137-155) in FP64 on
+        the device, in place unless outbufname is given; the reference does
+        this on the host before every round (NewtonSteps.py:618)."""
+        if 'ws gauge' not in self.bufs:
+            self._setupWorkspace('ws gauge', _lib.query('mi3_gauge_workspace', self.L, self.q))
+        out = outbufname or Jbufname
+        s = self._begin()
+        _lib.call('mi3_gauge_fieldless_even', self._ptr(Jbufname), self._ptr(out), self.L, self.q,
+                  self._ptr('ws gauge'), self._wsbytes('ws gauge'), self._s)
+        if out.split()[0] == 'J':
+            self.unpackedJ = None
+        return self.logevt('gaugeJ', s)
+
+    def bimargStats(self, model='bi', target='bi target', Jbufname='J'):
+        """FP64 (SSR, max|t-m|, mean rel. error over t > 0.01, its count,
+        X_model, X_target) of bimarg_stats / printstats (NewtonSteps.py:33-54)
+        into 'stats64'; returns the FutureBuf of that buffer."""
+        if 'ws stats' not in self.bufs:
+            self._setupWorkspace('ws stats', _lib.query('mi3_bimarg_stats_workspace', self.L))
+            self._setupBuffer('stats64', '<f8', (6,))
+        s = self._begin()
+        _lib.call('mi3_bimarg_stats', self._ptr(target), self._ptr(model),
+                  self._ptr(Jbufname) if Jbufname else None, self.L, self.q, self._ptr('stats64'),
+                  self._ptr('ws stats'), self._wsbytes('ws stats'), self._s)
+        self.logevt('bimargStats', s)
+        return self.getBuf('stats64')
+
+    def peekBuf(self, bufname, n=5):
+        """First n elements of a float buffer (a few bytes read back)."""
+        dev = self.bufs[bufname]
+        with torch.cuda.stream(self.stream):
+            host = dev[:n].to('cpu', non_blocking=False)
+        return host.numpy().copy()
 
     # ------------------------------------------------------------ Newton step
     def updateJ(self, gamma, pc, Jbuf='dJ', wait_for=None):

@@ -84,6 +84,10 @@ class GPU_node:
         for gpu in self.gpus:
             gpu.runMCMC()
 
+    def updateConsensus(self, seqbufname='main'):
+        for gpu in self.gpus:
+            gpu.updateConsensus(seqbufname)
+
     def calcEnergies(self, seqbufname, Jbufname='J'):
         for gpu in self.gpus:
             gpu.calcEnergies(seqbufname, Jbufname)
@@ -137,6 +141,15 @@ class GPU_node:
     def renormalize_bimarg(self):
         for gpu in self.gpus:
             gpu.renormalize_bimarg()
+
+    def gaugeJ(self, Jbufname='J'):
+        """Every device holds the same J: re-gauge each copy in place."""
+        for gpu in self.gpus:
+            gpu.gaugeJ(Jbufname)
+
+    def bimargStats(self, model='bi', target='bi target', Jbufname='J'):
+        """FP64 statistics of the head device's (merged) bimarginals."""
+        return [self.gpus[0].bimargStats(model, target, Jbufname)]
 
     def getBuf(self, bufname):
         return [gpu.getBuf(bufname) for gpu in self.gpus]

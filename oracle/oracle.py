@@ -306,3 +306,50 @@ def repack_seqs_T(seqmem, L):
     out = np.zeros((L, buf4len), np.uint8)
     lib().mi3o_repack_seqs_T(np.ascontiguousarray(seqmem).reshape(-1), buf4len, out.reshape(-1), buf4len, L)
     return out.view("<u4")
+
+
+# ---------------------------------------------------------------------------
+# Host routines of the reference's round loop, restated in float64 numpy.
+
+def gauge_fieldless_even(J, L, q, h=None):
+    """fieldlessGaugeEven(h, J) of the reference (changeGauge.py:37-155):
+    zeroJGauge (row/column means of each pair moved into the fields), the
+    fields centred (zeroGauge), then each field h_i(a) spread evenly over
+    the L-1 couplings of site i.  Returns the float64 couplings."""
+    Jx = np.asarray(J, np.float64).reshape(L * (L - 1) // 2, q, q)
+    h = np.zeros((L, q)) if h is None else np.asarray(h, np.float64)
+    m1, m2 = Jx.mean(axis=1), Jx.mean(axis=2)   # mean over a (per b), over b (per a)
+    mJ = m1.mean(axis=1)
+    J0 = Jx - m1[:, None, :] - m2[:, :, None] + mJ[:, None, None]
+    h0 = h - np.sum(mJ) / L
+    i, j = np.triu_indices(L, k=1)
+    np.add.at(h0, j, m1)
+    np.add.at(h0, i, m2)
+    h0 = h0 - h0.mean(axis=1, keepdims=True)
+    hd = h0 / (L - 1)
+    out = J0 + hd[i][:, :, None] + hd[j][:, None, :]
+    return out.reshape(-1, q * q)
+
+
+def bimarg_stats_f64(target, model, J=None):
+    """bimarg_stats and the X statistic of printstats (NewtonSteps.py:33-54)
+    in float64: (SSR, max|t-m|, mean |t-m|/t over t > 0.01f, count,
+    X_model, X_target)."""
+    t32 = np.asarray(target, np.float32)
+    t, m = t32.astype(np.float64), np.asarray(model, np.float32).astype(np.float64)
+    d = t - m
+    top = t32 > np.float32(0.01)
+    cnt = int(np.sum(top))
+    rel = float(np.mean(np.abs(d[top]) / t[top])) if cnt else 0.0
+    xm = xt = 0.0
+    if J is not None:
+        npair, qq = t.shape
+        q = int(round(qq ** 0.5))
+        Jd = np.asarray(J, np.float32).astype(np.float64)
+
+        def indep(f):
+            fx = f.reshape(npair, q, q)
+            return (fx.sum(axis=2)[:, :, None] * fx.sum(axis=1)[:, None, :]).reshape(npair, qq)
+        xm = float(np.sum(Jd * (m - indep(m))))
+        xt = float(np.sum(Jd * (t - indep(t))))
+    return (float(np.sum(d * d)), float(np.max(np.abs(d))), rel, cnt, xm, xt)

@@ -117,6 +117,22 @@ class FakeMCMCGPU:
     def fillSeqs(self, seq):
         self.setBuf('seq main', np.tile(np.asarray(seq, '<u1'), (self.nwalkers, 1)))
 
+    def addFloatBuf(self, dst, src):
+        self.bufs[dst] = (self.bufs[dst] + self.bufs[src]).astype('<f4')
+
+    def updateConsensus(self, seqbufname='main'):
+        pass
+
+    def gaugeJ(self, Jbufname='J'):
+        self.bufs[Jbufname] = oracle.gauge_fieldless_even(self.bufs[Jbufname], self.L, self.q).astype('<f4')
+
+    def bimargStats(self, model='bi', target='bi target', Jbufname='J'):
+        J = self.bufs[Jbufname] if Jbufname else None
+        return _Fut(np.array(oracle.bimarg_stats_f64(self.bufs[target], self.bufs[model], J)))
+
+    def peekBuf(self, name, n=5):
+        return np.asarray(self.bufs[name]).reshape(-1)[:n].copy()
+
     def addBiBuffer(self, name, other):
         self.bufs[name] = self.bufs[name] + other
 

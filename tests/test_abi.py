@@ -36,7 +36,7 @@ def test_binding_covers_header():
 
 def test_abi_version_and_sizes():
     lib = _lib.load()
-    assert lib.mi3_abi_version() == 1
+    assert lib.mi3_abi_version() == 2
     assert lib.mi3_jrows_stride(232, 21) == 232 * 441  # already a multiple of 4
     assert lib.mi3_jrows_stride(93, 21) % 4 == 0 and lib.mi3_jrows_stride(93, 21) >= 93 * 441
     assert lib.mi3_energies_workspace(1 << 20) == 8 << 20
@@ -47,7 +47,7 @@ def test_abi_version_and_sizes():
     ("mi3_metropolis", (None, None, 0, None, 10, None, 1.0, None, 512, 10, 4, None, None)),
     ("mi3_energies", (None, None, 10, 10, None, 10, 4, None, 0, None)),
     ("mi3_bicounts", (None, 10, 10, None, 10, 4, None)),
-    ("mi3_weighted_marg", (None, None, 10, 10, None, 10, 4, None, 0, None)),
+    ("mi3_weighted_marg", (None, None, 10, 10, None, 10, 4, None, None, 0, None)),
     ("mi3_update_j", (None, None, 0.1, 0.1, None, None, 10, 4, None)),
     ("mi3_reg_l1z", (None, 0.1, 0.1, 0.1, None, None, 10, 4, None)),
     ("mi3_init_rng", (None, 10, 0, 1, None)),

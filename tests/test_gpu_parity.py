@@ -33,8 +33,8 @@ pytestmark = pytest.mark.gpu
 SHAPES = [(10, 5, 512), (48, 4, 1024), (37, 21, 512), (93, 4, 512), (64, 8, 640)]
 
 
-def _wmarg_ws(L, q):
-    return empty((int(_lib.query("mi3_weighted_marg_workspace", L, q)) // 8 + 1,), np.int64)
+def _wmarg_ws(L, q, N):
+    return empty((int(_lib.query("mi3_weighted_marg_workspace", L, q, N)) // 8 + 1,), np.int64)
 
 
 def _seqs(L, q, N, seed):
@@ -186,9 +186,9 @@ def test_weighted_marg(cuda, L, q, N):
     mem = oracle.pack_seqs(seqs)
     w = np.random.default_rng(11).uniform(0.01, 3.0, size=N).astype("<f4")
     out = empty((L * (L - 1) // 2, q * q), np.float32)
-    ws = _wmarg_ws(L, q)
+    ws = _wmarg_ws(L, q, N)
     dw, dm = dev(w), dev(mem)
-    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, ws.data_ptr(),
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, None, ws.data_ptr(),
               ws.numel() * 8, stream())
     ref = oracle.weighted_marg_f64(w, mem, L, q)
     tot = ref.sum(axis=1, keepdims=True)
@@ -196,7 +196,7 @@ def test_weighted_marg(cuda, L, q, N):
     assert (np.abs(got - ref) / tot).max() < 1e-5
     # integer (fixed-point) accumulation: a second call gives identical bits
     out2 = empty((L * (L - 1) // 2, q * q), np.float32)
-    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out2.data_ptr(), L, q, ws.data_ptr(),
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out2.data_ptr(), L, q, None, ws.data_ptr(),
               ws.numel() * 8, stream())
     np.testing.assert_array_equal(host(out2), got)
 
@@ -209,9 +209,9 @@ def test_weighted_marg_c1_shape_and_wide_weights(cuda):
     mem = oracle.pack_seqs(seqs)
     w = np.exp(np.random.default_rng(22).uniform(-14, 0, size=N)).astype("<f4")
     out = empty((L * (L - 1) // 2, q * q), np.float32)
-    ws = _wmarg_ws(L, q)
+    ws = _wmarg_ws(L, q, N)
     dw, dm = dev(w), dev(mem)
-    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, ws.data_ptr(),
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, None, ws.data_ptr(),
               ws.numel() * 8, stream())
     ref = oracle.weighted_marg_f64(w, mem, L, q)
     assert (np.abs(host(out) - ref) / ref.sum(axis=1, keepdims=True)).max() < 1e-5
@@ -223,9 +223,9 @@ def test_weighted_marg_golden(cuda, golden):
         N, L = seqs.shape
         q = int(round(np.sqrt(J.shape[1])))
         out = empty((L * (L - 1) // 2, q * q), np.float32)
-        ws = _wmarg_ws(L, q)
+        ws = _wmarg_ws(L, q, N)
         _lib.call("mi3_weighted_marg", dev(w).data_ptr(), dev(oracle.pack_seqs(seqs)).data_ptr(), N, N,
-                  out.data_ptr(), L, q, ws.data_ptr(), ws.numel() * 8, stream())
+                  out.data_ptr(), L, q, None, ws.data_ptr(), ws.numel() * 8, stream())
         ref = golden[f"m{tag}_wcounts"]
         assert (np.abs(host(out) - ref) / ref.sum(axis=1, keepdims=True)).max() < 1e-5
 
@@ -409,3 +409,164 @@ def test_bicounts_tensorcore_golden_and_partial(cuda, golden):
     dm = dev(mem)
     _lib.call("mi3_bicounts_tc", dm.data_ptr(), N, 777, out.data_ptr(), L, q, status.data_ptr(), stream())
     np.testing.assert_array_equal(host(out, np.uint32), oracle.bicounts(mem, L, q, nseq=777))
+
+
+@pytest.mark.parametrize("L,q", [(9, 4), (13, 21), (48, 4), (232, 21), (5, 2)])
+def test_gauge_fieldless_even_vs_oracle(cuda, L, q):
+    """FP64 device gauge transform vs the oracle's float64 restatement of
+    fieldlessGaugeEven: equal after rounding to float up to one ulp."""
+    rng = np.random.default_rng(L * q)
+    npair = L * (L - 1) // 2
+    J = (rng.normal(0, 0.3, size=(npair, q * q)) + rng.normal(0, 1, size=(npair, 1))).astype("<f4")
+    ref = oracle.gauge_fieldless_even(J, L, q).astype("<f4")
+    ws = empty((int(_lib.query("mi3_gauge_workspace", L, q)) // 8 + 1,), np.int64)
+    dJ = dev(J)
+    out = empty(J.shape, np.float32)
+    _lib.call("mi3_gauge_fieldless_even", dJ.data_ptr(), out.data_ptr(), L, q, ws.data_ptr(), ws.numel() * 8,
+              stream())
+    got = host(out, np.float32)
+    np.testing.assert_allclose(got, ref, rtol=2.5e-7, atol=1e-7 * np.abs(ref).max())
+    # in place gives the same values
+    _lib.call("mi3_gauge_fieldless_even", dJ.data_ptr(), dJ.data_ptr(), L, q, ws.data_ptr(), ws.numel() * 8,
+              stream())
+    np.testing.assert_array_equal(host(dJ, np.float32), got)
+    # the gauge is idempotent up to rounding: zero row/column means already
+    g2 = oracle.gauge_fieldless_even(got, L, q)
+    np.testing.assert_allclose(g2, got, atol=1e-6 * np.abs(ref).max() + 1e-7)
+
+
+@pytest.mark.parametrize("L,q", [(9, 4), (13, 21), (232, 21), (2, 3)])
+@pytest.mark.parametrize("with_J", [True, False])
+def test_bimarg_stats_vs_oracle(cuda, L, q, with_J):
+    rng = np.random.default_rng(L + q)
+    npair = L * (L - 1) // 2
+    t = rng.dirichlet(np.full(q * q, 0.5), size=npair).astype("<f4")
+    m = (t * rng.uniform(0.7, 1.3, size=t.shape)).astype("<f4")
+    J = rng.normal(size=t.shape).astype("<f4")
+    ref = oracle.bimarg_stats_f64(t, m, J if with_J else None)
+    ws = empty((int(_lib.query("mi3_bimarg_stats_workspace", L)) // 8 + 1,), np.int64)
+    out = empty((6,), np.float64)
+    dt, dm, dj = dev(t), dev(m), dev(J)
+    _lib.call("mi3_bimarg_stats", dt.data_ptr(), dm.data_ptr(), dj.data_ptr() if with_J else None, L, q,
+              out.data_ptr(), ws.data_ptr(), ws.numel() * 8, stream())
+    got = host(out, np.float64)
+    np.testing.assert_allclose(got[[0, 2, 4, 5]], np.array(ref)[[0, 2, 4, 5]], rtol=1e-11, atol=1e-13)
+    assert got[1] == ref[1] and got[3] == ref[3]
+    # deterministic: a second call gives the same bits
+    _lib.call("mi3_bimarg_stats", dt.data_ptr(), dm.data_ptr(), dj.data_ptr() if with_J else None, L, q,
+              out.data_ptr(), ws.data_ptr(), ws.numel() * 8, stream())
+    np.testing.assert_array_equal(host(out, np.float64), got)
+
+
+@pytest.mark.parametrize("L,q,N", [(20, 4, 200000), (64, 21, 300000), (232, 21, 200000)])
+def test_weighted_marg_many_chunks(cuda, L, q, N):
+    """Sizes whose histograms are split over many sequence chunks (the last
+    one at the 65536-sequence fixed-point cap): per-chunk partial sums
+    combined in fixed order, within 1e-5 of each pair's total and
+    bit-identical on a second call."""
+    seqs = _seqs(L, q, N, 31)
+    mem = oracle.pack_seqs(seqs)
+    w = np.exp(np.random.default_rng(32).normal(0, 1.0, size=N)).astype("<f4")
+    out = empty((L * (L - 1) // 2, q * q), np.float32)
+    ws = _wmarg_ws(L, q, N)
+    dw, dm = dev(w), dev(mem)
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, None, ws.data_ptr(),
+              ws.numel() * 8, stream())
+    got = host(out)
+    ref = oracle.weighted_marg_f64(w, mem, L, q)
+    assert (np.abs(got - ref) / ref.sum(axis=1, keepdims=True)).max() < 1e-5
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, None, ws.data_ptr(),
+              ws.numel() * 8, stream())
+    np.testing.assert_array_equal(host(out), got)
+    # a workspace one byte short is rejected
+    with pytest.raises(_lib.Mi3Error):
+        _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, out.data_ptr(), L, q, None, ws.data_ptr(),
+                  int(_lib.query("mi3_weighted_marg_workspace", L, q, N)) - 1, stream())
+
+
+def _potts_like_seqs(L, q, N, seed, conc=2.0):
+    """Sequences with per-site skewed residue frequencies (a frequent
+    residue per site, as in equilibrated walkers)."""
+    rng = np.random.default_rng(seed)
+    p = rng.dirichlet(np.full(q, 1.0 / conc), size=L)
+    u = rng.random((N, L))
+    return (u[:, :, None] > np.cumsum(p, axis=1)[None]).sum(axis=2).clip(0, q - 1).astype("<u1")
+
+
+@pytest.mark.parametrize("L,q,N", [(10, 5, 512), (37, 21, 1000), (9, 2, 3000), (232, 21, 4096)])
+def test_site_consensus(cuda, L, q, N):
+    seqs = _potts_like_seqs(L, q, N, L + q)
+    cons = empty((L,), np.uint8)
+    ws = empty((int(_lib.query("mi3_site_consensus_workspace", L, q)) // 8 + 1,), np.int64)
+    _lib.call("mi3_site_consensus", dev(oracle.pack_seqs(seqs)).data_ptr(), N, N, L, q, cons.data_ptr(),
+              ws.data_ptr(), ws.numel() * 8, stream())
+    counts = np.stack([np.bincount(seqs[:, i], minlength=q) for i in range(L)])
+    np.testing.assert_array_equal(host(cons), counts.argmax(axis=1))  # argmax: lowest index on ties
+
+
+@pytest.mark.parametrize("L,q,N", [(10, 5, 512), (48, 4, 1024), (37, 21, 1000), (93, 4, 3000), (64, 8, 640),
+                                   (9, 2, 3000), (20, 4, 200000), (64, 21, 300000), (29, 11, 5000)])
+@pytest.mark.parametrize("which", ["consensus", "arbitrary"])
+def test_weighted_marg_consensus_bitexact(cuda, L, q, N, which):
+    """Skipping the consensus pairs and rebuilding their bins from site
+    sums gives the same bits as the direct histogram, for the true
+    consensus and for an arbitrary residue per site (including values >= q,
+    which never match)."""
+    seqs = _potts_like_seqs(L, q, N, 7 * L + q)
+    mem = oracle.pack_seqs(seqs)
+    w = np.exp(np.random.default_rng(L).normal(0, 1.5, size=N)).astype("<f4")
+    if which == "consensus":
+        cons = np.stack([np.bincount(seqs[:, i], minlength=q) for i in range(L)]).argmax(axis=1).astype("u1")
+    else:
+        cons = np.random.default_rng(q).integers(0, q + 2, size=L).astype("u1")
+    ws = _wmarg_ws(L, q, N)
+    dw, dm, dc = dev(w), dev(mem), dev(cons)
+    a = empty((L * (L - 1) // 2, q * q), np.float32)
+    b = empty((L * (L - 1) // 2, q * q), np.float32)
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, a.data_ptr(), L, q, None, ws.data_ptr(),
+              ws.numel() * 8, stream())
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, b.data_ptr(), L, q, dc.data_ptr(),
+              ws.data_ptr(), ws.numel() * 8, stream())
+    np.testing.assert_array_equal(host(b), host(a))
+    if N * L * L < 4e9:
+        ref = oracle.weighted_marg_f64(w, mem, L, q)
+        assert (np.abs(host(b) - ref) / ref.sum(axis=1, keepdims=True)).max() < 1e-5
+
+
+@pytest.mark.parametrize("L,q,N", [(10, 5, 512), (48, 4, 1024), (37, 21, 1000), (93, 4, 3000), (64, 8, 640),
+                                   (9, 2, 3000), (232, 21, 2048), (29, 11, 5000)])
+@pytest.mark.parametrize("which", ["consensus", "arbitrary"])
+def test_energies_consensus_gauge(cuda, L, q, N, which):
+    """Energies through the consensus gauge against the FP64 oracle, for
+    the true consensus and for arbitrary reference residues.  The regauged
+    couplings J' are rounded once to float (<= 2^-25 |J'| each) and summed
+    in float rows of at most 16 terms (<= 2^-21 of the absolute row sum), and
+    the energy is rounded once to float at the end, so
+    |E - E64| <= 2^-20 * sum_pairs |J'(s_i, s_j)| + 2^-24 |E64|."""
+    seqs = _potts_like_seqs(L, q, N, 3 * L + q)
+    mem = oracle.pack_seqs(seqs)
+    rng = np.random.default_rng(L * q)
+    J = rng.normal(0, 0.3, size=(L * (L - 1) // 2, q * q)).astype("<f4")
+    if which == "consensus":
+        cons = np.stack([np.bincount(seqs[:, i], minlength=q) for i in range(L)]).argmax(axis=1).astype("u1")
+    else:
+        cons = rng.integers(0, q + 2, size=L).astype("u1")
+    ws = empty((int(_lib.query("mi3_energies_cons_workspace", L, q, N)) // 8 + 1,), np.int64)
+    E = empty((N,), np.float32)
+    _lib.call("mi3_energies_cons", dev(J).data_ptr(), dev(mem).data_ptr(), N, N, E.data_ptr(), L, q,
+              dev(cons).data_ptr(), ws.data_ptr(), ws.numel() * 8, stream())
+    e64 = oracle.energies_f64(J, mem, L, q)
+    got = host(E).astype(np.float64)
+    # the regauged table in float64: J'(a,b) = J(a,b) - J(a,c_j) - J(c_i,b) + J(c_i,c_j)
+    c = np.minimum(cons.astype(np.int64), q - 1)
+    i, j = np.triu_indices(L, k=1)
+    Jx = J.astype(np.float64).reshape(-1, q, q)
+    P = np.arange(Jx.shape[0])
+    Jg = Jx - Jx[P, :, c[j]][:, :, None] - Jx[P, c[i], :][:, None, :] + Jx[P, c[i], c[j]][:, None, None]
+    eabs = oracle.energies_f64(np.abs(Jg).reshape(-1, q * q).astype("<f4"), mem, L, q)
+    assert np.all(np.abs(got - e64) <= 2.0 ** -20 * eabs * 1.01 + 2.0 ** -24 * np.abs(e64) + 1e-9)
+    # deterministic
+    E2 = empty((N,), np.float32)
+    _lib.call("mi3_energies_cons", dev(J).data_ptr(), dev(mem).data_ptr(), N, N, E2.data_ptr(), L, q,
+              dev(cons).data_ptr(), ws.data_ptr(), ws.numel() * 8, stream())
+    np.testing.assert_array_equal(host(E2), host(E))

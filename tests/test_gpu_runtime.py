@@ -97,3 +97,30 @@ def test_runtime_regularizers_dispatch(cuda):
         gpus.reg(name, (4e-3, 1e-2) + args)
         after = gpus.collect('dJ')
         assert np.isfinite(after).all() and not np.array_equal(after, before), name
+
+
+def test_device_resident_rounds_on_gpu(cuda):
+    """Rounds with J kept on the device (FP64 gauge and statistics there)
+    follow the reference-shaped host loop: same Newton step counts, SSR per
+    round within float rounding of the gauge, and J after the last round."""
+    from mi3gpu_b200.inference import infer
+    L, q, N = 20, 4, 4096
+    truth = potts.synthetic_ground_truth(L, q, seed=21, contact_sigma=0.5)
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 5)
+    node = GPU_node([g])
+    node.initMCMC(4 * L)
+    node.setBuf('J', truth)
+    node.setSeqs('main', np.zeros((N, L), '<u1'))
+    for _ in range(40):
+        node.runMCMC()
+    node.calcBicounts('main')
+    target = potts.mutation_pc(node.collect('bicount') / N, N).astype('<f4')
+    res = {}
+    for dev in (False, True):
+        logs = []
+        res[dev] = infer(target, L, q, N, 3, sweeps=32, newtonsteps=64, gamma=4e-3, damping=1e-2,
+                         reg=('l1z', (1e-3,)), seed=3, log=logs.append, reseed='none', device_resident=dev)
+    hh, hd = res[False]['history'], res[True]['history']
+    assert [h['newton_steps'] for h in hh] == [h['newton_steps'] for h in hd]
+    np.testing.assert_allclose([h['ssr'] for h in hd], [h['ssr'] for h in hh], rtol=1e-3)
+    np.testing.assert_allclose(res[True]['J'], res[False]['J'], rtol=1e-3, atol=1e-5)

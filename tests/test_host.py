@@ -145,3 +145,36 @@ def test_newtonMCMC_rounds_over_fake_device():
     J = NewtonSteps.newtonMCMC(p, gpus, 0, 0, logs.append)
     assert J.shape == J0.shape and np.isfinite(J).all() and np.abs(J).max() > 0
     assert len(p.history) == 2 and all(np.isfinite(h['ssr']) for h in p.history)
+
+
+def test_device_resident_rounds_match_host_rounds():
+    """The device-resident round loop (J kept on the device, gauge and SSR
+    computed there) follows the same trajectory as the reference-shaped
+    host loop over the same device calls."""
+    L, q, N = 6, 3, 512
+    J0 = np.zeros((L * (L - 1) // 2, q * q), '<f4')
+    truth = potts.synthetic_ground_truth(L, q, seed=9, contact_sigma=0.5)
+    out = {}
+    for dev in (False, True):
+        g = FakeMCMCGPU(L, q, N, seed=4)
+        gpus = GPU_node([g])
+        gpus.initMCMC(4 * L)
+        gpus.initJstep()
+        gpus.setBuf('J', truth)
+        gpus.setSeqs('main', np.zeros((N, L), '<u1'))
+        for _ in range(30):
+            gpus.runMCMC()
+        gpus.calcBicounts('main')
+        target = potts.mutation_pc(gpus.collect('bicount') / N, N).astype('<f4')
+        p = _param(L, q, N, target, J0, newtonSteps=16)
+        p.unimarg = potts.getUnimarg(target)
+        p.reseed = 'none'
+        p.device_resident = dev
+        gpus.prepare_indep(p.unimarg)
+        logs = []
+        J = NewtonSteps.newtonMCMC(p, gpus, 0, 0, logs.append)
+        out[dev] = (J, [h['ssr'] for h in p.history], [h['newton_steps'] for h in p.history])
+    (Jh, sh, nh), (Jd, sd, nd) = out[False], out[True]
+    assert nh == nd
+    np.testing.assert_allclose(sd, sh, rtol=1e-5)
+    np.testing.assert_allclose(Jd, Jh, rtol=1e-4, atol=1e-6)

@@ -196,3 +196,33 @@ def test_min_weights_stats():
     s = oracle.weight_stats(w)
     s64 = oracle.weight_stats_f64(w)
     np.testing.assert_allclose(s, s64, rtol=1e-5)
+
+
+def test_gauge_fieldless_even_matches_reference(golden):
+    """The oracle's gauge transform against the reference's own
+    fieldlessGaugeEven on the golden (h, J)."""
+    h, J = golden["g_h"], golden["g_J"]
+    L, q = h.shape
+    out = oracle.gauge_fieldless_even(J, L, q, h=h)
+    np.testing.assert_allclose(out, golden["g_fe_J"], rtol=0, atol=1e-12)
+
+
+def test_bimarg_stats_f64_matches_host_formula():
+    from mi3gpu_b200.potts import bimarg_stats
+    rng = np.random.default_rng(11)
+    L, q = 9, 5
+    npair = L * (L - 1) // 2
+    t = rng.dirichlet(np.ones(q * q), size=npair).astype("<f4")
+    m = (t * rng.uniform(0.8, 1.2, size=t.shape)).astype("<f4")
+    J = rng.normal(size=t.shape).astype("<f4")
+    ssr, maxd, rel, cnt, xm, xt = oracle.bimarg_stats_f64(t, m, J)
+    ferr, ssr2, maxd2 = bimarg_stats(t.astype(np.float64), m.astype(np.float64))
+    assert abs(ssr - ssr2) <= 1e-14 * ssr2 and maxd == maxd2
+    np.testing.assert_allclose(rel, ferr, rtol=1e-12)
+    assert cnt == int(np.sum(t > np.float32(0.01)))
+    # X with the pair's own marginals, summed over all pairs
+    t64, m64, J64 = t.astype(np.float64), m.astype(np.float64), J.astype(np.float64)
+    xm2 = sum(float(np.sum(J64[p].reshape(q, q) * (m64[p].reshape(q, q) - np.outer(m64[p].reshape(q, q).sum(1),
+                                                                               m64[p].reshape(q, q).sum(0)))))
+              for p in range(npair))
+    np.testing.assert_allclose(xm, xm2, rtol=1e-10)
