@@ -32,12 +32,36 @@ __device__ __forceinline__ int fixed_shift(float wmax, uint32_t chunk) {
 // Increments of one sequence into the slice's histograms.  CONS: only the
 // pairs where neither residue is its site's consensus (the others are
 // rebuilt from site totals after the pass).
-template <int B, int K, bool CONS>
+template <int B, int K, bool CONS, bool ROT>
 __device__ __forceinline__ void slice_hist(uint32_t *h, const uint32_t (&wI)[B / 4], const uint32_t (&wJ)[B / 4],
                                            const uint32_t (&cI)[B / 4], const uint32_t (&cJ)[B / 4],
                                            uint32_t inc, uint32_t q, uint32_t qq, uint32_t i0, uint32_t j0,
                                            uint32_t L) {
     uint32_t col[B];
+    if constexpr (ROT && !CONS && K == SLICE_FULL) {
+        // Column order rotated by lane: at step t lane l updates column
+        // (t + l) mod B, so one warp instruction spreads over B pair tables
+        // and lanes rarely hit the same bin (same-bin lanes with different
+        // increments are serialised by the shared-memory atomic unit; equal
+        // increments, as in plain counts, are not, so counts keep the
+        // unrotated order, which has fewer bank conflicts).
+        const uint32_t rot = threadIdx.x & (B - 1);
+#pragma unroll
+        for (int t = 0; t < B; ++t) {
+            const uint32_t jj = (t + rot) & (B - 1);
+            uint32_t w = wJ[0];
+#pragma unroll
+            for (int k = 1; k < B / 4; ++k) w = ((jj >> 2) == (uint32_t)k) ? wJ[k] : w;
+            col[t] = jj * qq + min((w >> (8 * (jj & 3))) & 0xffu, q - 1);
+        }
+#pragma unroll
+        for (int ii = 0; ii < B; ++ii) {
+            const uint32_t row = slice_row<B>(wI, ii, q, qq);
+#pragma unroll
+            for (int t = 0; t < B; ++t) atomicAdd(&h[row + col[t]], inc);
+        }
+        return;
+    }
     slice_cols<B>(wJ, q, qq, col);
     if constexpr (!CONS) {
 #pragma unroll
@@ -82,7 +106,7 @@ __device__ __forceinline__ void hist_chunk(uint32_t *h, const uint32_t *__restri
             load_block_words<B>(seq, buflen, n, bj, swords, wJ);
             uint32_t inc = 1u;
             if constexpr (WEIGHTED) inc = __float2uint_rn(__ldg(&weights[n]) * scale);
-            slice_hist<B, K, CONS>(h, wI, wJ, cI, cJ, inc, q, qq, i0, j0, L);
+            slice_hist<B, K, CONS, false>(h, wI, wJ, cI, cJ, inc, q, qq, i0, j0, L);
         }
         return;
     }
@@ -100,8 +124,9 @@ __device__ __forceinline__ void hist_chunk(uint32_t *h, const uint32_t *__restri
             inc1 = __float2uint_rn(__ldg(&weights[n]) * scale);
             inc2 = two ? __float2uint_rn(__ldg(&weights[n2]) * scale) : 0u;
         }
-        slice_hist<B, K, CONS>(h, wI, wJ, cI, cJ, inc1, q, qq, i0, j0, L);
-        if (two) slice_hist<B, K, CONS>(h, vI, vJ, cI, cJ, inc2, q, qq, i0, j0, L);
+        constexpr bool ROT = WEIGHTED && B <= 8;
+        slice_hist<B, K, CONS, ROT>(h, wI, wJ, cI, cJ, inc1, q, qq, i0, j0, L);
+        if (two) slice_hist<B, K, CONS, ROT>(h, vI, vJ, cI, cJ, inc2, q, qq, i0, j0, L);
     }
 }
 
