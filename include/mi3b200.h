@@ -85,6 +85,22 @@ int mi3_metropolis(const float *Jrows, uint32_t *rngstates, uint32_t position_of
                    float beta, uint32_t *seqmem, uint32_t nseqs, uint32_t L, uint32_t q,
                    int32_t *status, void *stream);
 
+/* mi3_metropolis with an explicit tile plan: walkers per CTA (multiple of
+ * 32 in [64, 512] dividing nseqs), sites per coupling chunk (multiple of 4,
+ * <= L rounded up to 4) and ring stages ([2, 8]); all three 0 = the
+ * built-in choice.  Same results for every plan (the plan only changes the
+ * schedule).  No counterpart in the reference (its work-group size is a
+ * launch parameter, mcmcGPU.py:1140-1163). */
+int mi3_metropolis_plan(const float *Jrows, uint32_t *rngstates, uint32_t position_offset,
+                        const uint32_t *position_list, uint32_t nsteps, const float *betas,
+                        float beta, uint32_t *seqmem, uint32_t nseqs, uint32_t L, uint32_t q,
+                        uint32_t walkers_per_cta, uint32_t sites_per_chunk, uint32_t stages,
+                        int32_t *status, void *stream);
+
+/* Valid tile plans for a shape, as (walkers_per_cta, sites_per_chunk,
+ * stages) triples into plans[3*max] (nullable); returns how many exist. */
+uint32_t mi3_metropolis_plans(uint32_t L, uint32_t q, uint32_t nseqs, uint32_t *plans, uint32_t max);
+
 /* gen_indep (mcmc.cl:170-244) as launched by MCMCGPU.gen_indep
  * (mcmcGPU.py:380-390); cprob is (L, q-1) cumulative probabilities
  * (MCMCGPU.prepare_indep, mcmcGPU.py:375-378). */
@@ -354,6 +370,49 @@ size_t mi3_bimarg_stats_workspace(uint32_t L);
  * Deterministic (fixed reduction order). */
 int mi3_bimarg_stats(const float *target, const float *model, const float *J, uint32_t L, uint32_t q,
                      double *out, void *workspace, size_t ws_bytes, void *stream);
+
+/* mi3_weights_fused with the reference energy read from device memory
+ * (*ref_dev, which must not alias minout): lets a captured Newton loop carry
+ * the previous step's min(0, dE) without a host round trip. */
+int mi3_weights_fused_dev(const float *ref_dev, const float *dE, float *weights, uint32_t n, float *minout,
+                          float *out2, double *out2_f64, void *workspace, size_t ws_bytes, void *stream);
+
+/* ---- whole rounds as CUDA graphs ---------------------------------------
+ * No counterpart in the reference (its round loop is host Python,
+ * NewtonSteps.py:610-767).  Capture is in relaxed mode; graphs and execs
+ * are opaque cudaGraph_t / cudaGraphExec_t handles. */
+int mi3_capture_begin(void *stream);
+int mi3_capture_end(void *stream, void **graph_out);
+int mi3_graph_instantiate(void *graph, void **exec_out);
+int mi3_graph_launch(void *exec, void *stream);
+int mi3_graph_destroy(void *graph, void *exec);
+
+/* Add a conditional WHILE node at the capture position of `stream` (its
+ * condition is 1 at every launch) and start capturing the loop body on
+ * body_stream; *handle_out is the condition handle for mi3_newton_control. */
+int mi3_capture_while_begin(void *stream, void *body_stream, unsigned long long *handle_out);
+/* End the body capture begun by mi3_capture_while_begin. */
+int mi3_capture_while_end(void *body_stream);
+
+/* End-of-step control of a captured Newton loop (NewtonSteps.py:234-246):
+ * ++*count; *ref = *minout (the next step's reference energy); the loop
+ * continues while Neff = s^2/s2 (wstats64 = {s, s2}) >= neff_min and
+ * *count < *max_steps (device word), and stops on non-finite or zero sums
+ * (*stopped, if given, becomes 1 at a normal stop and 2 on divergence). */
+int mi3_newton_control(unsigned long long handle, const double *wstats64, const float *minout, float *ref,
+                       uint32_t *count, const uint32_t *max_steps, double neff_min, uint32_t *stopped,
+                       void *stream);
+
+/* The round-to-round Newton budget of MCMCstep (NewtonSteps.py:664-683) on
+ * the device.  after = 0 (before the loop): *budget -= 1.5*delta (not below
+ * delta) when stats[0] (this round's SSR) > (state[0] + state[1]) / 2, then
+ * state = {SSR, min(state[1], SSR)} (state[0] = NaN before the first round).
+ * after = 1: *budget = min(2048, (*count - 1) + delta). */
+int mi3_newton_adapt(uint32_t after, const double *stats, const uint32_t *count, uint32_t *budget,
+                     double *state, uint32_t delta, void *stream);
+
+/* cudaMemsetAsync, for callers without a runtime binding (graph memset nodes). */
+int mi3_memset(void *ptr, int value, size_t nbytes, void *stream);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,9 @@ SIGNATURES = {
     "mi3_jrows_stride": (_u64, [_u32, _u32]),
     "mi3_unpack_j": (c.c_int, [_vp, _vp, _u32, _u32, _vp]),
     "mi3_metropolis": (c.c_int, [_vp, _vp, _u32, _vp, _u32, _vp, _f32, _vp, _u32, _u32, _u32, _vp, _vp]),
+    "mi3_metropolis_plan": (c.c_int, [_vp, _vp, _u32, _vp, _u32, _vp, _f32, _vp, _u32, _u32, _u32, _u32, _u32,
+                                      _u32, _vp, _vp]),
+    "mi3_metropolis_plans": (_u32, [_u32, _u32, _u32, _vp, _u32]),
     "mi3_gen_indep": (c.c_int, [_vp, _u32, _u32, _vp, _vp, _u32, _u32, _vp]),
     "mi3_energies_workspace": (c.c_size_t, [_u32]),
     "mi3_energies": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),
@@ -51,6 +54,17 @@ SIGNATURES = {
     "mi3_weight_stats": (c.c_int, [_vp, _u32, _vp, _vp, _vp, c.c_size_t, _vp]),
     "mi3_weights_fused": (c.c_int, [_f32, _vp, _vp, _u32, _vp, _vp, _vp, _vp, c.c_size_t, _vp]),
     "mi3_add_float_bufs": (c.c_int, [_vp, _vp, _u32, _vp]),
+    "mi3_weights_fused_dev": (c.c_int, [_vp, _vp, _vp, _u32, _vp, _vp, _vp, _vp, c.c_size_t, _vp]),
+    "mi3_capture_begin": (c.c_int, [_vp]),
+    "mi3_capture_end": (c.c_int, [_vp, c.POINTER(_vp)]),
+    "mi3_graph_instantiate": (c.c_int, [_vp, c.POINTER(_vp)]),
+    "mi3_graph_launch": (c.c_int, [_vp, _vp]),
+    "mi3_graph_destroy": (c.c_int, [_vp, _vp]),
+    "mi3_capture_while_begin": (c.c_int, [_vp, _vp, c.POINTER(c.c_ulonglong)]),
+    "mi3_capture_while_end": (c.c_int, [_vp]),
+    "mi3_newton_control": (c.c_int, [c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, c.c_double, _vp, _vp]),
+    "mi3_newton_adapt": (c.c_int, [_u32, _vp, _vp, _vp, _vp, _u32, _vp]),
+    "mi3_memset": (c.c_int, [_vp, c.c_int, c.c_size_t, _vp]),
     "mi3_gauge_workspace": (c.c_size_t, [_u32, _u32]),
     "mi3_gauge_fieldless_even": (c.c_int, [_vp, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),
     "mi3_bimarg_stats_workspace": (c.c_size_t, [_u32]),

@@ -252,10 +252,67 @@ extern "C" int mi3_unpack_j(const float *J, float *Jrows, uint32_t L, uint32_t q
     return check_launch("mi3_unpack_j");
 }
 
-extern "C" int mi3_metropolis(const float *Jrows, uint32_t *rngstates, uint32_t position_offset,
-                              const uint32_t *position_list, uint32_t nsteps, const float *betas,
-                              float beta, uint32_t *seqmem, uint32_t nseqs, uint32_t L, uint32_t q,
-                              int32_t *status, void *stream) {
+namespace mi3 {
+
+// A caller-chosen plan (walkers per CTA, sites per chunk, stages), checked
+// against the kernel's limits; zeros leave the choice to pick_metro_config.
+static int make_metro_config(uint32_t L, uint32_t q, uint32_t nseqs, uint32_t NW, uint32_t M, uint32_t S,
+                             MetroConfig &cfg) {
+    if (NW == 0 && M == 0 && S == 0) {
+        if (!pick_metro_config(L, q, nseqs, cfg))
+            return fail(MI3_ERR_ARG, "mi3_metropolis: L/q too large for the shared-memory plan");
+        return MI3_OK;
+    }
+    const uint32_t Lr = (L + 3) & ~3u, sw = (L - 1) / 4 + 1, qq = q * q;
+    if (NW < 64 || NW > 512 || NW % 32 || nseqs % NW)
+        return fail(MI3_ERR_ARG, "mi3_metropolis: walkers per CTA must be a multiple of 32 in [64, 512] dividing nseqs");
+    if (M < 4 || M % 4 || M > Lr) return fail(MI3_ERR_ARG, "mi3_metropolis: sites per chunk must be a multiple of 4 <= L");
+    if (S < 2 || S > 8) return fail(MI3_ERR_ARG, "mi3_metropolis: stages must be in [2, 8]");
+    const uint32_t stage_floats = ((M * qq) + 31) & ~31u;
+    const size_t sm = metro_smem(NW, S, stage_floats, sw);
+    if (sm > 227 * 1024) return fail(MI3_ERR_ARG, "mi3_metropolis: plan exceeds shared memory");
+    cfg = MetroConfig{NW, M, (L + M - 1) / M, S, stage_floats, sm};
+    return MI3_OK;
+}
+
+}  // namespace mi3
+
+extern "C" uint32_t mi3_metropolis_plans(uint32_t L, uint32_t q, uint32_t nseqs, uint32_t *plans, uint32_t max) {
+    uint32_t n = 0;
+    if (L < 2 || q < 2 || q > 255 || nseqs == 0) return 0;
+    const uint32_t Lr = (L + 3) & ~3u;
+    const uint32_t nws[4] = {128, 256, 384, 512};
+    for (uint32_t NW : nws) {
+        if (nseqs % NW) continue;
+        for (uint32_t S = 2; S <= 6; ++S) {
+            // chunk sizes: stage buffers of about 8, 16, 24, 32, 48 KB
+            const uint32_t kb[5] = {8, 16, 24, 32, 48};
+            uint32_t last = 0;
+            for (uint32_t t = 0; t < 5; ++t) {
+                uint32_t M = (kb[t] * 1024) / (q * q * 4);
+                M = std::min(std::max<uint32_t>(4, M & ~3u), Lr);
+                if (M == last) continue;
+                last = M;
+                MetroConfig cfg;
+                if (make_metro_config(L, q, nseqs, NW, M, S, cfg) != MI3_OK) continue;
+                if (plans && n < max) {
+                    plans[3 * n] = NW;
+                    plans[3 * n + 1] = M;
+                    plans[3 * n + 2] = S;
+                }
+                ++n;
+            }
+        }
+    }
+    set_error("");
+    return n;
+}
+
+extern "C" int mi3_metropolis_plan(const float *Jrows, uint32_t *rngstates, uint32_t position_offset,
+                                   const uint32_t *position_list, uint32_t nsteps, const float *betas,
+                                   float beta, uint32_t *seqmem, uint32_t nseqs, uint32_t L, uint32_t q,
+                                   uint32_t walkers_per_cta, uint32_t sites_per_chunk, uint32_t stages,
+                                   int32_t *status, void *stream) {
     if (!Jrows || !rngstates || !position_list || !seqmem || !status)
         return fail(MI3_ERR_ARG, "mi3_metropolis: null pointer");
     if (L < 2 || q < 2 || q > 255) return fail(MI3_ERR_ARG, "mi3_metropolis: bad L/q");
@@ -265,8 +322,8 @@ extern "C" int mi3_metropolis(const float *Jrows, uint32_t *rngstates, uint32_t 
         return fail(MI3_ERR_ALIGN, "mi3_metropolis: Jrows/rngstates must be 16B aligned");
     if (nsteps == 0) return MI3_OK;
     MetroConfig cfg;
-    if (!pick_metro_config(L, q, nseqs, cfg))
-        return fail(MI3_ERR_ARG, "mi3_metropolis: L/q too large for the shared-memory plan");
+    int rc = make_metro_config(L, q, nseqs, walkers_per_cta, sites_per_chunk, stages, cfg);
+    if (rc) return rc;
     cudaFuncSetAttribute(k_metropolis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
     MetroParams p;
     p.Jrows = Jrows;
@@ -288,4 +345,12 @@ extern "C" int mi3_metropolis(const float *Jrows, uint32_t *rngstates, uint32_t 
     p.status = status;
     k_metropolis<<<nseqs / cfg.NW, cfg.NW + 32, cfg.smem, as_stream(stream)>>>(p);
     return check_launch("mi3_metropolis");
+}
+
+extern "C" int mi3_metropolis(const float *Jrows, uint32_t *rngstates, uint32_t position_offset,
+                              const uint32_t *position_list, uint32_t nsteps, const float *betas,
+                              float beta, uint32_t *seqmem, uint32_t nseqs, uint32_t L, uint32_t q,
+                              int32_t *status, void *stream) {
+    return mi3_metropolis_plan(Jrows, rngstates, position_offset, position_list, nsteps, betas, beta, seqmem,
+                               nseqs, L, q, 0, 0, 0, status, stream);
 }

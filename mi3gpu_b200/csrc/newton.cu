@@ -128,8 +128,9 @@ __device__ __forceinline__ float warp_min(float v) {
 
 // in = dE when RM_WEIGHTS (weights computed as exp(-dE + ref)), else weights.
 __global__ void __launch_bounds__(RED_THREADS) k_reduce(const float *__restrict__ in, uint32_t n,
-                                                        float ref, uint32_t mode, RedOut o,
-                                                        unsigned char *ws) {
+                                                        float ref_host, const float *ref_dev, uint32_t mode,
+                                                        RedOut o, unsigned char *ws) {
+    const float ref = ref_dev ? *ref_dev : ref_host;
     unsigned int *ticket = reinterpret_cast<unsigned int *>(ws);
     double *part = reinterpret_cast<double *>(ws + 16);
     __shared__ double s_sum[RED_THREADS / 32], s_sum2[RED_THREADS / 32];
@@ -235,12 +236,12 @@ __global__ void k_add(float *dst, const float *__restrict__ src, uint32_t n) {
 static size_t red_ws_bytes() { return 16 + (size_t)RED_BLOCKS * 4 * sizeof(double); }
 
 static int launch_reduce(const float *in, uint32_t n, float ref, uint32_t mode, RedOut o, void *ws,
-                         size_t ws_bytes, cudaStream_t st, const char *what) {
+                         size_t ws_bytes, cudaStream_t st, const char *what, const float *ref_dev = nullptr) {
     if (ws_bytes < red_ws_bytes()) return fail(MI3_ERR_WORKSPACE, std::string(what) + ": workspace too small");
     if (!aligned(ws, 16)) return fail(MI3_ERR_ALIGN, std::string(what) + ": workspace alignment");
     uint32_t blocks = std::min<uint32_t>(RED_BLOCKS, std::max<uint32_t>(1, (n + RED_THREADS - 1) / RED_THREADS));
     if (cudaMemsetAsync(ws, 0, 16, st) != cudaSuccess) return check_launch(what);
-    k_reduce<<<blocks, RED_THREADS, 0, st>>>(in, n, ref, mode, o, reinterpret_cast<unsigned char *>(ws));
+    k_reduce<<<blocks, RED_THREADS, 0, st>>>(in, n, ref, ref_dev, mode, o, reinterpret_cast<unsigned char *>(ws));
     return check_launch(what);
 }
 
@@ -331,6 +332,17 @@ extern "C" int mi3_weights_fused(float ref_E, const float *dE, float *weights, u
     RedOut o{weights, minout, out2, out2_f64};
     return launch_reduce(dE, n, ref_E, RM_WEIGHTS | RM_MIN | RM_STATS, o, workspace, ws_bytes,
                          as_stream(stream), "mi3_weights_fused");
+}
+
+extern "C" int mi3_weights_fused_dev(const float *ref_dev, const float *dE, float *weights, uint32_t n,
+                                     float *minout, float *out2, double *out2_f64, void *workspace,
+                                     size_t ws_bytes, void *stream) {
+    if (!ref_dev || !dE || !weights || !minout || !out2 || !workspace)
+        return fail(MI3_ERR_ARG, "mi3_weights_fused_dev: null pointer");
+    if (ref_dev == minout) return fail(MI3_ERR_ARG, "mi3_weights_fused_dev: ref_dev must not alias minout");
+    RedOut o{weights, minout, out2, out2_f64};
+    return launch_reduce(dE, n, 0.0f, RM_WEIGHTS | RM_MIN | RM_STATS, o, workspace, ws_bytes, as_stream(stream),
+                         "mi3_weights_fused_dev", ref_dev);
 }
 
 extern "C" int mi3_add_float_bufs(float *dst, const float *src, uint32_t n, void *stream) {

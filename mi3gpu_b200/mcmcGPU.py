@@ -356,21 +356,24 @@ class MCMCGPU:
         self.repackedSeqT['main'] = False
         s = self._begin()
         betas = self._ptr('Bs') if getattr(self, 'tempering', False) else None
-        _lib.call('mi3_metropolis', self._ptr('Junpacked'), self._ptr('rngstates'), int(rngoffset),
+        plan = getattr(self, 'metro_plan', None) or (0, 0, 0)  # set by autotune.Autotuner.tune
+        _lib.call('mi3_metropolis_plan', self._ptr('Junpacked'), self._ptr('rngstates'), int(rngoffset),
                   self._ptr('randpos'), self.nsteps, betas, self.beta, self._ptr('seq main'),
-                  self.nseq['main'], self.L, self.q, self._ptr('status'), self._s)
+                  self.nseq['main'], self.L, self.q, plan[0], plan[1], plan[2], self._ptr('status'), self._s)
         return self.logevt('mcmc', s)
 
     # ------------------------------------------------------------ statistics
     # alphabet sizes for which the tcgen05 one-hot GEMM counts beat the
-    # shared-memory histogram (measured on B200: 8x at q=4, 2.3x at q=8,
-    # 3x slower at q=21); both give identical integers.
-    TENSOR_COUNT_Q = range(4, 13)
+    # shared-memory histogram when nothing was tuned (measured on B200 at
+    # 2^18 walkers: 1.3x at q=4, even at q=8, 3x slower at q=21); both give
+    # identical integers.
+    TENSOR_COUNT_Q = range(4, 7)
 
     def calcBicounts(self, seqbufname, wait_for=None, tensor=None):
         nseq = self.nseq[seqbufname]
         if tensor is None:
-            tensor = self.q in self.TENSOR_COUNT_Q
+            tuned = getattr(self, 'count_kernel', None)  # set by autotune.Autotuner.tune
+            tensor = (tuned == 'tc') if tuned else self.q in self.TENSOR_COUNT_Q
         s = self._begin()
         if tensor:
             _lib.call('mi3_bicounts_tc', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, self._ptr('bicount'),

@@ -79,3 +79,22 @@ def test_bad_shapes_rejected():
     with pytest.raises(_lib.Mi3Error) as e:
         _lib.call("mi3_metropolis", p, p, 0, p, 10, None, 1.0, p, 512, 10, 300, p, None)  # q > 255
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("L,q,N", [(232, 21, 1 << 20), (99, 4, 1 << 18), (48, 4, 16384), (150, 8, 4096),
+                                   (512, 21, 1 << 21), (2, 2, 128)])
+def test_metropolis_plans_host_query(L, q, N):
+    """The plan enumeration is host code: every plan respects the kernel's
+    limits (walkers per CTA divide N, chunk a multiple of 4 within the row,
+    2-8 stages, shared memory within 227 KB)."""
+    from mi3gpu_b200.autotune import sampler_plans
+    plans = sampler_plans(L, q, N)
+    assert plans, "no plan for a supported shape"
+    sw = (L - 1) // 4 + 1
+    for nw, m, st in plans:
+        assert nw % 32 == 0 and 64 <= nw <= 512 and N % nw == 0
+        assert m % 4 == 0 and 4 <= m <= ((L + 3) // 4) * 4
+        assert 2 <= st <= 8
+        stage_floats = (m * q * q + 31) // 32 * 32
+        smem = 128 * ((16 * st + 4 + 127) // 128) + st * stage_floats * 4 + 256 * 4 + sw * nw * 4
+        assert smem <= 227 * 1024

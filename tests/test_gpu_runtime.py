@@ -124,3 +124,42 @@ def test_device_resident_rounds_on_gpu(cuda):
     assert [h['newton_steps'] for h in hh] == [h['newton_steps'] for h in hd]
     np.testing.assert_allclose([h['ssr'] for h in hd], [h['ssr'] for h in hh], rtol=1e-3)
     np.testing.assert_allclose(res[True]['J'], res[False]['J'], rtol=1e-3, atol=1e-5)
+
+
+def test_sampler_plans_same_trajectory_and_autotuner(cuda, tmp_path):
+    """Every tile plan of the sampler gives the same walkers and RNG states
+    (the plan changes only the schedule); the autotuner picks one of them,
+    caches it and installs it on the device object."""
+    import torch
+    from mi3gpu_b200 import _lib
+    from mi3gpu_b200.autotune import Autotuner, sampler_plans
+    for L, q, N in [(37, 21, 1024), (48, 4, 2048)]:
+        g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 3)
+        node = GPU_node([g])
+        node.initMCMC(2 * L)
+        node.setBuf('J', potts.synthetic_ground_truth(L, q, seed=L, contact_sigma=0.4))
+        node.setSeqs('main', np.random.default_rng(L).integers(0, q, size=(N, L)).astype('<u1'))
+        g.unpackJ()
+        pos = torch.from_numpy(np.random.default_rng(q).integers(0, L, size=3 * L).astype(np.int32)).to(g.device)
+        seq0, rng0 = g.bufs['seq main'].clone(), g.bufs['rngstates'].clone()
+        outs = []
+        for plan in [(0, 0, 0)] + sampler_plans(L, q, N):
+            seq, rng = seq0.clone(), rng0.clone()
+            st = torch.zeros(1, dtype=torch.int32, device=g.device)
+            _lib.call('mi3_metropolis_plan', g._ptr('Junpacked'), rng.data_ptr(), 0, pos.data_ptr(), 3 * L,
+                      None, 1.0, seq.data_ptr(), N, L, q, *plan, st.data_ptr(), g.stream.cuda_stream)
+            g.stream.synchronize()
+            assert int(st.item()) == 0
+            outs.append((plan, seq, rng))
+        for plan, seq, rng in outs[1:]:
+            assert torch.equal(seq, outs[0][1]) and torch.equal(rng, outs[0][2]), plan
+        cache = tmp_path / "tune.json"
+        t = Autotuner(cache)
+        chosen = t.tune(g)
+        assert tuple(chosen["metropolis_plan"]) in set(sampler_plans(L, q, N))
+        assert chosen["count_kernel"] in ("smem", "tc")
+        # tuning left the chain where it was; a run with the tuned plan works
+        assert torch.equal(g.bufs['seq main'], seq0)
+        node.runMCMC()
+        g.wait()
+        assert Autotuner(cache).table == t.table
