@@ -431,6 +431,78 @@ def run_kernels(args):
                       "fp8_peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (of measured)", "rows": rows}))
 
 
+def run_batched(args):
+    """Many independent problems (L ~ U[50,300], q in {4, 8, 21}, walkers
+    log-uniform in [2^14, 2^17]): quasi-Newton rounds with one CUDA-graph
+    launch per round for the whole batch (walkers carried over, tuned
+    kernel schedules), against the same problems driven by the host loop
+    one problem at a time (inference.infer, device-resident; the consensus
+    energies are off in both so that both arms compute the same numbers).
+    Same seeds, same kernels: both arms give the same results."""
+    import torch
+    from mi3gpu_b200.autotune import Autotuner
+    from mi3gpu_b200.batched import BatchedRounds, random_problems
+    from mi3gpu_b200.inference import infer
+    from mi3gpu_b200.mcmcGPU import MCMCGPU
+    MCMCGPU.CONS_ENERGY_MAX_ACTIVE = -1.0
+    t0 = time.time()
+    probs = random_problems(args.problems, seed=2000, msa=1 << 14, sweeps=256)
+    t_targets = time.time() - t0
+    shapes = [(p.L, p.q, p.N) for p in probs]
+    t0 = time.time()
+    br = BatchedRounds(probs, sweeps=args.chosen_sweeps, sweeps_first=args.first_sweeps, reseed='none',
+                       tuner=Autotuner(ROOT / "_build" / "autotune.json") if not args.no_tune else None)
+    t_tune = time.time() - t0
+    rounds = []
+    for r in range(args.rounds):
+        t0 = time.time()
+        rec = br.run_round()
+        if r == 0:
+            rec["capture_s"] = time.time() - t0 - rec["wall_s"]
+        rounds.append(rec)
+    upd_first = br.site_updates_per_round(first=True)
+    upd = br.site_updates_per_round(first=False)
+    steady = rounds[1:] or rounds
+    gpu_s = statistics.mean(r["gpu_ms"] for r in steady) / 1e3
+    batched = {
+        "s_per_round": gpu_s, "s_per_round_wall": statistics.mean(r["wall_s"] for r in steady),
+        "first_round_s": rounds[0]["gpu_ms"] / 1e3, "capture_s": rounds[0].get("capture_s"),
+        "site_updates_per_round": upd, "sampling_site_updates_per_s_incl_newton": upd / gpu_s,
+        "newton_steps_total_per_round": [sum(p["newton_steps"] for p in r["problems"]) for r in rounds],
+        "tuning_s": t_tune, "graph_launches_per_round": 1}
+    ssr_b = [[h["ssr"] for h in p.history] for p in probs]
+    plans = {f"L{p.L}q{p.q}N{p.N}": br.tuning.get(id(p)) for p in probs[:8]}
+    targets = [(p.target, p.L, p.q, p.N) for p in probs]
+    br.close()
+    del br, probs
+    torch.cuda.empty_cache()
+    # host-driven arm: the same problems (same targets and seeds) one after
+    # another, same rounds
+    ssr_h = []
+    per_round = [0.0] * args.rounds
+    for k, (tgt, L, q, N) in enumerate(targets):
+        res = infer(tgt, L, q, N, args.rounds, sweeps=args.chosen_sweeps, sweeps_first=args.first_sweeps,
+                    newtonsteps=1024, seed=2000 + 1000 + k, log=lambda *a: None, reseed='none',
+                    device_resident=True)
+        for r, h in enumerate(res["history"]):
+            per_round[r] += h["round_s"]
+        ssr_h.append([h["ssr"] for h in res["history"]])
+        torch.cuda.empty_cache()
+    host_s = statistics.mean(per_round[1:] or per_round)
+    same = all(a == b for a, b in zip(ssr_b, ssr_h))
+    print(json.dumps({
+        "metric": "s per quasi-Newton round of a batch of independent problems, one graph launch vs host loop",
+        "unit": "s/round", "value": gpu_s, "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"batched {args.problems} problems, L~U[50,300], q in {{4,8,21}}, "
+                               f"walkers logU[2^14,2^17], {args.chosen_sweeps} sweeps/round after a "
+                               f"{args.first_sweeps}-sweep first round, l1z 2e-4", "rounds": args.rounds,
+                   "shapes": shapes},
+        "batched": batched, "host_loop": {"s_per_round": host_s, "first_round_s": per_round[0]},
+        "speedup_host_over_batched": host_s / gpu_s, "identical_ssr_histories": same,
+        "tuned_plans_sample": plans, "target_build_s": t_targets}))
+
+
 def energy_autocorr(Es):
     """Energy autocorrelation across walkers, rho(t) = corr(E_0, E_t), and
     tau_int = 1 + 2 sum_t rho(t) summed until rho first drops below 0.05."""
@@ -575,11 +647,14 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--newton-steps", type=int, default=10, help="quasi-Newton steps to time (0: skip)")
-    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned"],
+    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned", "batched"],
                     help="inference: run full quasi-Newton rounds and report s/iter and SSR")
     ap.add_argument("--rounds", type=int, default=4, help="inference rounds (--mode inference)")
     ap.add_argument("--msa", type=int, default=1 << 16, help="synthetic MSA size (--mode inference)")
     ap.add_argument("--chosen-sweeps", type=int, default=16, help="sweeps per round after the first (chosen form)")
+    ap.add_argument("--first-sweeps", type=int, default=128, help="sweeps in the first round (--mode batched)")
+    ap.add_argument("--problems", type=int, default=64, help="problems in the batch (--mode batched)")
+    ap.add_argument("--no-tune", action="store_true", help="built-in kernel schedules (--mode batched)")
     args = ap.parse_args()
     rank, world, _ = env_rank()
 
@@ -617,6 +692,9 @@ def main():
         return
     if args.mode == "learned":
         run_learned(args)
+        return
+    if args.mode == "batched":
+        run_batched(args)
         return
     out, J = run_gpu(args)
     if rank == 0:

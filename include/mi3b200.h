@@ -411,6 +411,11 @@ int mi3_newton_control(unsigned long long handle, const double *wstats64, const 
 int mi3_newton_adapt(uint32_t after, const double *stats, const uint32_t *count, uint32_t *budget,
                      double *state, uint32_t delta, void *stream);
 
+/* A new non-blocking stream of the current device / its destruction (capture
+ * needs streams that no other part of the process uses). */
+int mi3_stream_create(void **stream_out);
+int mi3_stream_destroy(void *stream);
+
 /* cudaMemsetAsync, for callers without a runtime binding (graph memset nodes). */
 int mi3_memset(void *ptr, int value, size_t nbytes, void *stream);
 

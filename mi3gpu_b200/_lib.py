@@ -65,6 +65,8 @@ SIGNATURES = {
     "mi3_newton_control": (c.c_int, [c.c_ulonglong, _vp, _vp, _vp, _vp, _vp, c.c_double, _vp, _vp]),
     "mi3_newton_adapt": (c.c_int, [_u32, _vp, _vp, _vp, _vp, _u32, _vp]),
     "mi3_memset": (c.c_int, [_vp, c.c_int, c.c_size_t, _vp]),
+    "mi3_stream_create": (c.c_int, [c.POINTER(_vp)]),
+    "mi3_stream_destroy": (c.c_int, [_vp]),
     "mi3_gauge_workspace": (c.c_size_t, [_u32, _u32]),
     "mi3_gauge_fieldless_even": (c.c_int, [_vp, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),
     "mi3_bimarg_stats_workspace": (c.c_size_t, [_u32]),

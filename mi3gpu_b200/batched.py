@@ -62,7 +62,9 @@ class Problem:
             'ssr state': torch.tensor([float('nan'), float('inf')], dtype=torch.float64, device=dev),
         }
         self.randpos_round = None
-        self.body_stream = torch.cuda.Stream(device=dev)
+        # capture streams of this problem's branch and of its Newton-loop body
+        self.cap_stream = _new_stream(dev)
+        self.body_stream = _new_stream(dev)
         self.history = []
 
     def round_positions(self, ncalls):
@@ -87,6 +89,15 @@ def _p(t):
     return t.data_ptr()
 
 
+def _new_stream(device):
+    """A stream of our own (torch.cuda.Stream hands out pooled streams, which
+    alias once more than 32 are in use; a capturing stream must not)."""
+    with torch.cuda.device(device):
+        h = ctypes.c_void_p()
+        _lib.call('mi3_stream_create', ctypes.byref(h))
+        return torch.cuda.ExternalStream(h.value, device=device)
+
+
 class BatchedRounds:
     """Quasi-Newton rounds of many problems, one graph launch per round.
 
@@ -104,7 +115,7 @@ class BatchedRounds:
         self.reseed = reseed
         self.sweeps, self.sweeps_first = int(sweeps), int(sweeps_first)
         self.device = torch.device('cuda', device) if isinstance(device, int) else device
-        self.origin = torch.cuda.Stream(device=self.device)
+        self.origin = _new_stream(self.device)
         self.tuning = {}
         if tuner is not None:
             for pr in self.problems:
@@ -121,7 +132,7 @@ class BatchedRounds:
         return max(1, sweeps * pr.L // pr.nsteps)
 
     def _capture_problem(self, pr, ncalls):
-        g, s, L, q, N = pr.gpu, pr.gpu.stream.cuda_stream, pr.L, pr.q, pr.N
+        g, s, L, q, N = pr.gpu, pr.cap_stream.cuda_stream, pr.L, pr.q, pr.N
         npq = g.nPairs * q * q
         b = g.bufs
         c = pr.ctl
@@ -196,10 +207,10 @@ class BatchedRounds:
             fork.record(o)
             joins = []
             for pr in self.problems:
-                pr.gpu.stream.wait_event(fork)
+                pr.cap_stream.wait_event(fork)
                 self._capture_problem(pr, self._ncalls(pr, sweeps))
                 e = torch.cuda.Event()
-                e.record(pr.gpu.stream)
+                e.record(pr.cap_stream)
                 joins.append(e)
             for e in joins:
                 o.wait_event(e)
@@ -256,14 +267,20 @@ class BatchedRounds:
         for graph, exec_ in self.graphs.values():
             _lib.call('mi3_graph_destroy', graph, exec_)
         self.graphs = {}
+        torch.cuda.synchronize(self.device)
+        for st in [self.origin] + [x for pr in self.problems for x in (pr.cap_stream, pr.body_stream)]:
+            _lib.call('mi3_stream_destroy', st.cuda_stream)
+        self.origin = None
+        for pr in self.problems:
+            pr.cap_stream = pr.body_stream = None
 
 
 def random_problems(n, seed=2000, L_range=(50, 300), qs=(4, 8, 21), walkers_log2=(14, 17), msa=1 << 14,
-                    device=0, contact_sigma=0.5):
+                    device=0, contact_sigma=0.5, sweeps=None):
     """Batch of synthetic problems: L ~ U[L_range], q from qs, walkers
     log-uniform in [2^lo, 2^hi] rounded to a multiple of 2048; each target
     from a ground truth built as potts.synthetic_ground_truth (seed + k)
-    sampled by the plain sampler."""
+    sampled by the plain sampler (`sweeps` sweeps, default max(256, 4L))."""
     from .inference import make_target
     rng = np.random.default_rng(seed)
     out = []
@@ -272,6 +289,7 @@ def random_problems(n, seed=2000, L_range=(50, 300), qs=(4, 8, 21), walkers_log2
         q = int(rng.choice(qs))
         N = int(2 ** rng.uniform(*walkers_log2))
         N = max(2048, (N // 2048) * 2048)
-        target, _ = make_target(L, q, msa, seed=seed + k, contact_sigma=contact_sigma, device=device)
+        target, _ = make_target(L, q, msa, seed=seed + k, sweeps=sweeps, contact_sigma=contact_sigma,
+                                device=device)
         out.append(Problem(target, L, q, N, seed=seed + 1000 + k, device=device))
     return out

@@ -156,6 +156,22 @@ extern "C" int mi3_newton_adapt(uint32_t after, const double *stats, const uint3
     return check_launch("mi3_newton_adapt");
 }
 
+// Dedicated non-blocking streams for capture (pooled streams of a framework
+// may alias each other, and a stream cannot capture two graphs at once).
+extern "C" int mi3_stream_create(void **stream_out) {
+    if (!stream_out) return fail(MI3_ERR_ARG, "mi3_stream_create: null pointer");
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(MI3_ERR_CUDA, std::string("mi3_stream_create: ") + cudaGetErrorString(e));
+    *stream_out = st;
+    return MI3_OK;
+}
+
+extern "C" int mi3_stream_destroy(void *stream) {
+    if (stream) cudaStreamDestroy(as_stream(stream));
+    return check_launch("mi3_stream_destroy");
+}
+
 extern "C" int mi3_memset(void *ptr, int value, size_t nbytes, void *stream) {
     if (!ptr && nbytes) return fail(MI3_ERR_ARG, "mi3_memset: null pointer");
     if (nbytes == 0) return MI3_OK;
