@@ -577,6 +577,30 @@ def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, 
                       "tau_gain_per_second": res["plain"]["tau_int_s"] / res["learned"]["tau_int_s"]}))
 
 
+def headline_inference(args):
+    """The s/iter half of the headline metric, compact enough for the
+    default run: the plain form (independent reseed every round, 128
+    sweeps, round host work in numpy as the reference does it) for 2 rounds
+    and the chosen form (walkers carried over, 128 sweeps in the first round
+    and args.chosen_sweeps after, round work on the device) for 3 rounds on
+    the same synthetic target; s/iter of each = its last round, SSR after
+    round 2 of each (the same J updates).  --mode inference runs the full
+    comparison."""
+    from mi3gpu_b200.inference import make_target, infer
+    target, _ = make_target(args.L, args.q, args.msa, seed=1001)
+    plain = infer(target, args.L, args.q, args.walkers, 2, reseed="independent", sweeps=128,
+                  device_resident=False, log=lambda *a: None)["history"]
+    chosen = infer(target, args.L, args.q, args.walkers, 3, reseed="none", sweeps=args.chosen_sweeps,
+                   sweeps_first=128, device_resident=True, log=lambda *a: None)["history"]
+    p_s, c_s = plain[-1]["round_s"], chosen[-1]["round_s"]
+    return {"unit": "s/iter", "plain": p_s, "chosen": c_s, "plain_over_chosen": p_s / c_s,
+            "ssr_round2": {"plain": plain[1]["ssr"], "chosen": chosen[1]["ssr"]},
+            "plain_form": "reseed independent, 128 sweeps/round, host round work",
+            "chosen_form": f"walkers carried over, {args.chosen_sweeps} sweeps/round after a 128-sweep "
+                           "first round, device-resident round work",
+            "newton_steps": {"plain": plain[-1]["newton_steps"], "chosen": chosen[-1]["newton_steps"]}}
+
+
 def run_inference(args):
     """Quasi-Newton inference at the workload's shape on one synthetic
     target: seconds per iteration (MCMC round + Newton steps until
@@ -655,6 +679,7 @@ def main():
     ap.add_argument("--first-sweeps", type=int, default=128, help="sweeps in the first round (--mode batched)")
     ap.add_argument("--problems", type=int, default=64, help="problems in the batch (--mode batched)")
     ap.add_argument("--no-tune", action="store_true", help="built-in kernel schedules (--mode batched)")
+    ap.add_argument("--no-inference", action="store_true", help="skip the s/iter comparison of the default run")
     args = ap.parse_args()
     rank, world, _ = env_rank()
 
@@ -697,6 +722,8 @@ def main():
         run_batched(args)
         return
     out, J = run_gpu(args)
+    if rank == 0 and world == 1 and not args.no_inference:
+        out["s_per_iter"] = headline_inference(args)
     if rank == 0:
         if not args.no_cpu:
             r = cpu_generator_rate(J, args.L, args.q, args.cpu_seconds, os.cpu_count() or 1)
