@@ -625,6 +625,9 @@ def run_inference(args):
              ("chosen", dict(reseed="none", sweeps=args.chosen_sweeps, sweeps_first=128, device_resident=True)),
              ("chosen_half", dict(reseed="none", sweeps=max(1, args.chosen_sweeps // 2), sweeps_first=128,
                                   device_resident=True)))
+    if args.forms:
+        keep = args.forms.split(",")
+        forms = tuple(f for f in forms if f[0] in keep)
     out = {}
     for name, kw in forms:
         logs = []
@@ -642,7 +645,8 @@ def run_inference(args):
                      "final_ssr": hist[-1]["ssr"], "config": kw}
     chosen = out["chosen"]
     reach = {}
-    for base in ("plain", "plain_dev"):
+    bases = [b for b in ("plain", "plain_dev") if b in out]
+    for base in bases:
         tgt = out[base]["final_ssr"]
         reach[base] = next((c for sv, c in zip(chosen["ssr"], chosen["cum_s"]) if sv <= tgt * (1 + 1e-3)), None)
     print(json.dumps({
@@ -652,7 +656,7 @@ def run_inference(args):
         "config": {"workload": f"inference L={args.L} q={args.q} walkers={args.walkers} msa={args.msa}, l1z 2e-4",
                    "rounds": args.rounds, "s_per_iter": "mean round seconds after the first round"},
         "forms": out,
-        "s_per_iter_ratio": {b: out[b]["s_per_iter"] / chosen["s_per_iter"] for b in ("plain", "plain_dev")},
+        "s_per_iter_ratio": {b: out[b]["s_per_iter"] / chosen["s_per_iter"] for b in bases},
         "chosen_s_to_reach_final_ssr_of": reach,
         "expected_min_ssr": float(np.sum(target * (1 - target)) / args.walkers), "target_build_s": t_target}))
 
@@ -680,6 +684,7 @@ def main():
     ap.add_argument("--problems", type=int, default=64, help="problems in the batch (--mode batched)")
     ap.add_argument("--no-tune", action="store_true", help="built-in kernel schedules (--mode batched)")
     ap.add_argument("--no-inference", action="store_true", help="skip the s/iter comparison of the default run")
+    ap.add_argument("--forms", default="", help="comma list of forms for --mode inference (default: all)")
     args = ap.parse_args()
     rank, world, _ = env_rank()
 
