@@ -155,6 +155,15 @@ def run_gpu(args):
     gpus.gen_indep('main')
     gpus.setBuf('J', J)
     gpus.wait()
+    tuned = None
+    if not args.no_tune:
+        # sampler tile plan and count kernel picked by timing every candidate
+        # on scratch copies of the walkers (outside the timed region)
+        from mi3gpu_b200.autotune import Autotuner
+        t0 = time.time()
+        tuned = Autotuner(ROOT / "_build" / "autotune.json").tune(gpu)
+        tuned = {"metropolis_plan": list(tuned["metropolis_plan"]), "count_kernel": tuned["count_kernel"],
+                 "tuning_s": round(time.time() - t0, 1)}
 
     s = gpu.stream
     kernel_ms = []
@@ -255,7 +264,8 @@ def run_gpu(args):
             "data": "synthetic (ground-truth Potts model of the workload's shape; independent-site start)",
             "config": {"workload": WORKLOAD, "L": L, "q": q, "walkers_per_gpu": N, "nsteps_per_call": args.nsteps,
                        "parallelism": f"walkers x{world} (independent RNG spans)",
-                       "l2": "inputs larger than L2 (sequence buffer 243 MB); couplings stay L2-resident by design"},
+                       "l2": "inputs larger than L2 (sequence buffer 243 MB); couplings stay L2-resident by design",
+                       "tuned": tuned},
             "e2e": {"value": e2e_value, "unit": "site-updates/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                     "path": "GPU_node.setBuf('J') + runMCMC() + MCMCGPU.getBuf('seq main') (pinned, packed words)"},
@@ -587,11 +597,13 @@ def headline_inference(args):
     round 2 of each (the same J updates).  --mode inference runs the full
     comparison."""
     from mi3gpu_b200.inference import make_target, infer
+    from mi3gpu_b200.autotune import Autotuner
+    tuner = None if args.no_tune else Autotuner(ROOT / "_build" / "autotune.json")
     target, _ = make_target(args.L, args.q, args.msa, seed=1001)
     plain = infer(target, args.L, args.q, args.walkers, 2, reseed="independent", sweeps=128,
-                  device_resident=False, log=lambda *a: None)["history"]
+                  device_resident=False, log=lambda *a: None, tuner=tuner)["history"]
     chosen = infer(target, args.L, args.q, args.walkers, 3, reseed="none", sweeps=args.chosen_sweeps,
-                   sweeps_first=128, device_resident=True, log=lambda *a: None)["history"]
+                   sweeps_first=128, device_resident=True, log=lambda *a: None, tuner=tuner)["history"]
     p_s, c_s = plain[-1]["round_s"], chosen[-1]["round_s"]
     return {"unit": "s/iter", "plain": p_s, "chosen": c_s, "plain_over_chosen": p_s / c_s,
             "ssr_round2": {"plain": plain[1]["ssr"], "chosen": chosen[1]["ssr"]},
@@ -617,6 +629,8 @@ def run_inference(args):
                  after it
       chosen_half  as chosen with half as many sweeps per round."""
     from mi3gpu_b200.inference import make_target, infer
+    from mi3gpu_b200.autotune import Autotuner
+    tuner = None if args.no_tune else Autotuner(ROOT / "_build" / "autotune.json")
     t0 = time.time()
     target, truth = make_target(args.L, args.q, args.msa, seed=1001)
     t_target = time.time() - t0
@@ -632,7 +646,7 @@ def run_inference(args):
     for name, kw in forms:
         logs = []
         w0 = time.time()
-        res = infer(target, args.L, args.q, args.walkers, args.rounds, log=logs.append, **kw)
+        res = infer(target, args.L, args.q, args.walkers, args.rounds, log=logs.append, tuner=tuner, **kw)
         wall = time.time() - w0
         hist = res["history"]
         cum = np.cumsum([h["round_s"] for h in hist]).tolist()
@@ -682,7 +696,7 @@ def main():
     ap.add_argument("--chosen-sweeps", type=int, default=16, help="sweeps per round after the first (chosen form)")
     ap.add_argument("--first-sweeps", type=int, default=128, help="sweeps in the first round (--mode batched)")
     ap.add_argument("--problems", type=int, default=64, help="problems in the batch (--mode batched)")
-    ap.add_argument("--no-tune", action="store_true", help="built-in kernel schedules (--mode batched)")
+    ap.add_argument("--no-tune", action="store_true", help="built-in kernel schedules instead of autotuned ones")
     ap.add_argument("--no-inference", action="store_true", help="skip the s/iter comparison of the default run")
     ap.add_argument("--forms", default="", help="comma list of forms for --mode inference (default: all)")
     args = ap.parse_args()

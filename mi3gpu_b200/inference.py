@@ -52,7 +52,7 @@ def make_target(L, q, n_msa, seed, sweeps=None, contact_sigma=0.5, device=0):
 
 def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e-4, damping=1e-3,
           reg=('l1z', (2e-4,)), seed=1234, device=0, log=print, fused=True, outdir=None, reseed='independent',
-          sweeps_first=None, device_resident=True):
+          sweeps_first=None, device_resident=True, tuner=None):
     """Run `rounds` quasi-Newton iterations from the independent model;
     returns the per-round history (SSR, wall seconds of MCMC and Newton
     phases) as recorded by NewtonSteps.MCMCstep.
@@ -63,7 +63,9 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
     `sweeps_first` sweeps each round only re-equilibrates to the slightly
     changed couplings.  device_resident keeps J on the device between
     rounds (gauge transform and statistics in FP64 there); False runs the
-    round's host work in numpy as the reference does."""
+    round's host work in numpy as the reference does.  tuner: an
+    autotune.Autotuner whose sampler plan and count kernel are installed
+    (results do not depend on them)."""
     unimarg = potts.getUnimarg(target)
     J0 = potts.independent_couplings(unimarg)
     nsteps = 8 * L
@@ -80,6 +82,12 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
     gpus.initMCMC(nsteps)
     gpus.initJstep()
     gpus.prepare_indep(unimarg)
+    if tuner is not None:
+        # tune on walkers and couplings of the right kind (both are set again
+        # by the round loop)
+        gpus.setBuf('J', J0)
+        gpus.gen_indep('main')
+        tuner.tune(g)
     t0 = time.time()
     J = NewtonSteps.newtonMCMC(p, gpus, 0, 0, log)
     total = time.time() - t0
