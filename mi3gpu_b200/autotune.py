@@ -58,17 +58,18 @@ class Autotuner:
         tmp.write_text(json.dumps(self.table, indent=1, sort_keys=True))
         os.replace(tmp, self.cache_path)
 
-    def sampler_plan(self, gpu, probe_steps=None, reps=3):
+    def sampler_plan(self, gpu, probe_steps=None, reps=2):
         """Fastest sampler plan for gpu's shape; times `reps` launches of
-        probe_steps proposals per walker for every plan on scratch copies of
-        the walkers and RNG states.  Returns (plan, {plan: ms})."""
+        probe_steps proposals per walker (default two sweeps) for every plan
+        on scratch copies of the walkers and RNG states.  Returns
+        (plan, {plan: ms})."""
         key = self._key("metropolis", gpu)
         if key in self.table:
             return tuple(self.table[key]["plan"]), self.table[key].get("ms", {})
         gpu.require('MCMC')
         gpu.unpackJ()
         L, q, N = gpu.L, gpu.q, gpu.nseq['main']
-        steps = int(probe_steps or min(gpu.nsteps, 4 * L))
+        steps = int(probe_steps or min(gpu.nsteps, 2 * L))
         with torch.cuda.stream(gpu.stream):
             seq = gpu.bufs['seq main'].clone()
             rng = gpu.bufs['rngstates'].clone()
