@@ -1,0 +1,128 @@
+"""One device per process: the reference's GPU_node over torch.distributed.
+
+The reference spreads walkers over the GPUs of a node (node_manager.py) and
+over nodes with MPI (mpi_manager.py).  Here each process drives one device
+(launched one rank per GPU, as torchrun does) and RankNode stands in for the
+node object that NewtonSteps talks to.  Walkers shard across ranks with
+disjoint slices of the MWC64X period (node_manager.py:73-81); sampling has
+no exchange.  The quasi-Newton phase has three, all collectives over the
+process group (NCCL on GPUs, gloo in the CPU tests):
+
+  * merge_bimarg: sum of the (weighted) bimarginals, then the same
+    renormalisation on every rank (node_manager.py:254-304);
+  * the reference energy of the next step: min over ranks of min(0, dE);
+  * the weight sums behind Neff: FP64 sum over ranks.
+
+Every rank then holds the same J, dJ and bimarginals and takes the same
+number of Newton steps, because each computes the stop rule from the same
+reduced numbers.  Collectives are issued on the device's own stream.
+"""
+import numpy as np
+import torch
+import torch.distributed as dist
+
+from .node_manager import GPU_node
+
+
+def _as_tensor(buf):
+    """The device buffer as a tensor sharing its memory (numpy buffers of
+    the CPU test device are wrapped without a copy)."""
+    if isinstance(buf, torch.Tensor):
+        return buf
+    return torch.from_numpy(buf)
+
+
+class RankNode(GPU_node):
+    def __init__(self, gpu, group=None):
+        super().__init__([gpu])
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        n = torch.tensor([gpu.nwalkers], dtype=torch.int64)
+        ns = [torch.zeros_like(n) for _ in range(self.world)]
+        if self._backend() == 'nccl':
+            n, ns = n.to(gpu.device), [x.to(gpu.device) for x in ns]
+        dist.all_gather(ns, n, group=group)
+        self.walkers_per_rank = [int(x.item()) for x in ns]
+
+    def _backend(self):
+        return dist.get_backend(self.group)
+
+    # -------------------------------------------------------- shape
+    @property
+    def head_gpu(self):
+        return GPU_node([self.gpus[0]])
+
+    @property
+    def nwalkers(self):
+        return sum(self.walkers_per_rank)
+
+    @property
+    def nseq(self):
+        return {'main': self.nwalkers}
+
+    @property
+    def ngpus(self):
+        return self.world
+
+    def setSeqs(self, bufname, seqs, log=None):
+        """This rank's own walkers (node_manager.py:190-221 splits a global
+        array across the devices of one process; here every rank passes its
+        share)."""
+        seqs = seqs[0] if isinstance(seqs, (list, tuple)) else seqs
+        g = self.gpus[0]
+        if seqs.shape[0] != g.nseq[bufname]:
+            raise Exception("Expected {} sequences on rank {}, got {}".format(g.nseq[bufname], self.rank,
+                                                                              seqs.shape[0]))
+        g.setBuf('seq ' + bufname, seqs)
+
+    def initMCMC(self, nsteps):
+        span = np.uint64(2 ** 63) // np.uint64(self.world)
+        self.gpus[0].initMCMC(nsteps, np.uint64(self.rank) * span, span)
+
+    # -------------------------------------------------------- exchanges
+    def _reduce(self, bufname, op):
+        g = self.gpus[0]
+        t = _as_tensor(g.bufs[bufname])
+        stream = getattr(g, 'stream', None)
+        if isinstance(stream, torch.cuda.Stream) or isinstance(stream, torch.cuda.ExternalStream):
+            with torch.cuda.stream(stream):
+                dist.all_reduce(t, op=op, group=self.group)
+        else:
+            dist.all_reduce(t, op=op, group=self.group)
+
+    def merge_bimarg(self):
+        self._reduce('bi', dist.ReduceOp.SUM)
+        self.gpus[0].renormalize_bimarg()
+
+    def getBuf(self, bufname):
+        if bufname == 'minout':
+            self._reduce('minout', dist.ReduceOp.MIN)
+        elif bufname in ('weightstats', 'weightstats64'):
+            self._reduce(bufname, dist.ReduceOp.SUM)
+        return super().getBuf(bufname)
+
+    def _gather(self, arr):
+        out = [None] * self.world
+        dist.all_gather_object(out, arr, group=self.group)
+        return out
+
+    def collect(self, bufs):
+        single = isinstance(bufs, str)
+        names = [bufs] if single else list(bufs)
+        local = [super(RankNode, self).collect(n) for n in names]
+        ret = []
+        for name, a in zip(names, local):
+            kind = name.split()[0]
+            if kind == 'bicount':
+                t = torch.from_numpy(np.ascontiguousarray(a).astype(np.int64))
+                if self._backend() == 'nccl':
+                    t = t.to(self.gpus[0].device)
+                dist.all_reduce(t, group=self.group)
+                a = t.cpu().numpy().astype(a.dtype)
+            elif kind in ('E', 'weights', 'Bs', 'seq'):
+                a = np.concatenate(self._gather(np.asarray(a)), axis=0)
+            elif kind == 'bi':
+                a = np.mean(np.stack(self._gather(np.asarray(a))), axis=0).astype(np.asarray(a).dtype)
+            ret.append(a)
+        return ret[0] if single else ret

@@ -81,3 +81,142 @@ def test_two_rank_reductions_match_single_process():
     for r in (x for x in res if "rank" in x):
         expect = oracle.init_rng(1, r["rank"] * span, span // (2 * n_per))[0]
         np.testing.assert_array_equal(r["first_state"], expect)
+
+
+def _newton_worker(rank, world, port, out):
+    """iterNewton through RankNode over two FakeMCMCGPU halves of the
+    walkers; rank 0 reports the result."""
+    import torch.distributed as dist
+    from mi3gpu_b200 import NewtonSteps, potts
+    from mi3gpu_b200.distributed import RankNode
+    from tests.fake_device import FakeMCMCGPU
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    L, q, N = 8, 3, 1024
+    n_per = N // world
+    J = potts.synthetic_ground_truth(L, q, seed=5, contact_sigma=0.4)
+    seqs = np.random.default_rng(4).integers(0, q, size=(N, L)).astype('<u1')
+    g = FakeMCMCGPU(L, q, n_per, seed=2 + rank)
+    node = RankNode(g)
+    node.initMCMC(4 * L)
+    node.initJstep()
+    node.setSeqs('main', seqs[rank * n_per:(rank + 1) * n_per])
+    node.setBuf('J', J)
+    node.calcBicounts('main')
+    f0 = node.collect('bicount') / N
+    target = potts.mutation_pc(f0 * np.exp(np.random.default_rng(3).normal(0, 0.2, f0.shape)), N).astype('<f4')
+    target /= target.sum(axis=1, keepdims=True)
+    node.setBuf('bi target', target)
+    p = NewtonSteps.Param(bimarg=target, gamma0=4e-3, newtonSteps=12, pcdamping=1e-2, fracNeff=0.5,
+                          nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all')
+    steps, Jt, bt = NewtonSteps.iterNewton(p, f0, node, lambda *a: None)
+    out.put(dict(rank=rank, steps=steps, J=Jt, bi=bt, f0=f0, target=target))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def _guarded(fn, rank, world, port, out):
+    """Report a worker's exception instead of leaving the parent waiting."""
+    try:
+        fn(rank, world, port, out)
+    except BaseException as e:  # noqa: BLE001 - forwarded to the test
+        out.put(dict(rank=rank, error=repr(e)))
+        raise
+
+
+def test_two_rank_newton_phase_matches_single_process():
+    """The Newton phase with walkers split over two gloo ranks (bimarginals
+    summed, min dE and FP64 weight sums reduced across ranks) takes the same
+    steps and reaches the same couplings as one process holding all walkers;
+    both ranks end with identical couplings."""
+    from mi3gpu_b200 import GPU_node, NewtonSteps
+    from tests.fake_device import FakeMCMCGPU
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_guarded, args=(_newton_worker, r, 2, port, out)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted([out.get(timeout=180) for _ in range(2)], key=lambda r: r["rank"])
+    assert not any("error" in r for r in res), res
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    np.testing.assert_array_equal(res[0]["J"], res[1]["J"])
+    assert res[0]["steps"] == res[1]["steps"]
+    # one process with all walkers
+    from mi3gpu_b200 import potts
+    L, q, N = 8, 3, 1024
+    J = potts.synthetic_ground_truth(L, q, seed=5, contact_sigma=0.4)
+    seqs = np.random.default_rng(4).integers(0, q, size=(N, L)).astype('<u1')
+    g = FakeMCMCGPU(L, q, N, seed=2)
+    node = GPU_node([g])
+    node.initMCMC(4 * L)
+    node.initJstep()
+    node.setSeqs('main', seqs)
+    node.setBuf('J', J)
+    node.calcBicounts('main')
+    np.testing.assert_allclose(node.collect('bicount') / N, res[0]["f0"])
+    node.setBuf('bi target', res[0]["target"])
+    p = NewtonSteps.Param(bimarg=res[0]["target"], gamma0=4e-3, newtonSteps=12, pcdamping=1e-2, fracNeff=0.5,
+                          nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all')
+    steps, Jt, bt = NewtonSteps.iterNewton(p, res[0]["f0"], node, lambda *a: None)
+    assert steps == res[0]["steps"]
+    np.testing.assert_allclose(res[0]["J"], Jt, rtol=1e-4, atol=1e-6)
+    np.testing.assert_allclose(res[0]["bi"], bt, rtol=1e-4, atol=1e-6)
+
+
+def _rounds_worker(rank, world, port, out):
+    """Two device-resident rounds (sampling on each rank's own walkers,
+    Newton phase reduced across ranks) through RankNode."""
+    import torch.distributed as dist
+    from mi3gpu_b200 import NewtonSteps, potts
+    from mi3gpu_b200.distributed import RankNode
+    from tests.fake_device import FakeMCMCGPU
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    L, q, n_per = 6, 3, 256
+    truth = potts.synthetic_ground_truth(L, q, seed=9, contact_sigma=0.5)
+    target = potts.mutation_pc(np.full((L * (L - 1) // 2, q * q), 1.0 / (q * q)) *
+                               np.exp(np.random.default_rng(1).normal(0, 0.3, (L * (L - 1) // 2, q * q))),
+                               1000).astype('<f4')
+    target /= target.sum(axis=1, keepdims=True)
+    g = FakeMCMCGPU(L, q, n_per, seed=4 + rank)
+    node = RankNode(g)
+    node.initMCMC(4 * L)
+    node.initJstep()
+    p = NewtonSteps.Param()
+    p.update(dict(bimarg=target, gamma0=4e-3, newtonSteps=16, pcdamping=1e-2, fracNeff=0.9, nwalkers=node.nwalkers,
+                  reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all', L=L, q=q,
+                  couplings=np.zeros((L * (L - 1) // 2, q * q), '<f4'), nsteps=4 * L, equiltime=4, trackequil=0,
+                  outdir=None, mcmcsteps=2, newton_delta=8, reseed='none', rngseed=3, init_indep=True,
+                  device_resident=True, unimarg=potts.getUnimarg(target)))
+    node.prepare_indep(p.unimarg)
+    J = NewtonSteps.newtonMCMC(p, node, 0, 0, lambda *a: None)
+    out.put(dict(rank=rank, J=J, ssr=[h['ssr'] for h in p.history], steps=[h['newton_steps'] for h in p.history],
+                 N=node.nwalkers))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_device_resident_rounds_agree():
+    """Rounds over two ranks: each samples its own walkers (disjoint RNG
+    spans), the Newton phase is reduced across ranks, and both ranks end
+    every round with the same statistics and the same couplings."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_guarded, args=(_rounds_worker, r, 2, port, out)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted([out.get(timeout=180) for _ in range(2)], key=lambda r: r["rank"])
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert not any("error" in r for r in res), res
+    assert res[0]["N"] == res[1]["N"] == 512
+    assert res[0]["ssr"] == res[1]["ssr"] and res[0]["steps"] == res[1]["steps"]
+    assert all(np.isfinite(res[0]["ssr"]))
+    np.testing.assert_array_equal(res[0]["J"], res[1]["J"])
