@@ -400,7 +400,8 @@ def run_kernels(args):
     st = torch.cuda.current_stream(dev)
     s = st.cuda_stream
     rows = []
-    for (L, q, N) in [(232, 21, 1 << 20), (99, 4, 1 << 18), (48, 4, 16384), (512, 21, 1 << 19), (128, 8, 1 << 18)]:
+    for (L, q, N) in [(232, 21, 1 << 20), (99, 4, 1 << 18), (48, 4, 16384), (512, 21, 1 << 19), (128, 8, 1 << 18),
+                      (150, 5, 1 << 18), (150, 6, 1 << 18), (150, 12, 1 << 18)]:
         g = torch.Generator(device=dev)
         g.manual_seed(L * q)
         sw = (L - 1) // 4 + 1
@@ -429,9 +430,19 @@ def run_kernels(args):
                                           ws.data_ptr(), ws.numel() * 8, s), reps, st)
         t_w = time_call(lambda: _lib.call("mi3_weighted_marg", w.data_ptr(), seq.data_ptr(), N, N, bi.data_ptr(), L, q, None,
                                           wws.data_ptr(), wws.numel() * 8, s), reps, st)
+        t_wtc = None
+        if 4 <= q <= 32:
+            wst = torch.zeros(int(_lib.query("mi3_weighted_marg_tc_workspace", L, q)) // 8 + 2, dtype=torch.int64,
+                              device=dev)
+            bi_tc = torch.empty_like(bi)
+            t_wtc = time_call(lambda: _lib.call("mi3_weighted_marg_tc", w.data_ptr(), seq.data_ptr(), N, N,
+                                                bi_tc.data_ptr(), L, q, wst.data_ptr(), wst.numel() * 8,
+                                                status.data_ptr(), s), reps, st)
+            assert torch.equal(bi_tc, bi) and int(status.item()) == 0, "tensor-core weighted bimarginals differ"
+            del wst, bi_tc
         flops = 2.0 * N * npairs * q * q
         r = {"L": L, "q": q, "N": N, "counts_smem_ms": t_plain, "counts_tc_ms": t_tc, "energies_ms": t_e,
-             "weighted_ms": t_w, "counts_GBps_smem": N * L / t_plain / 1e6}
+             "weighted_ms": t_w, "weighted_tc_ms": t_wtc, "counts_GBps_smem": N * L / t_plain / 1e6}
         if t_tc:
             r.update(counts_GBps_tc=N * L / t_tc / 1e6, tc_tflops=flops / t_tc / 1e9,
                      tc_frac_of_fp8=flops / t_tc / 1e9 / fp8_peak)

@@ -201,6 +201,21 @@ int mi3_weighted_marg(const float *weights, const uint32_t *seqmem, uint32_t buf
                       uint32_t nseq, float *bimarg, uint32_t L, uint32_t q, const uint8_t *cons,
                       void *workspace, size_t ws_bytes, void *stream);
 
+/* Bytes of workspace mi3_weighted_marg_tc needs: 256 + 8 * nPairs * q*q. */
+size_t mi3_weighted_marg_tc_workspace(uint32_t L, uint32_t q);
+
+/* weightedMarg (mcmc.cl:646-718) on the tensor cores: the same fixed-point
+ * weights as mi3_weighted_marg, split into three byte planes, each an
+ * integer one-hot GEMM X^T diag(w_p) X (tcgen05.mma.kind::i8, s32
+ * accumulators, exact), recombined into 64-bit sums -- bit-identical to
+ * mi3_weighted_marg.  4 <= q <= 32.  *status (int32, device, zeroed by the
+ * caller) receives MI3_STATUS_TIMEOUT_FULL if a bounded wait for the tensor
+ * cores gave up.  No counterpart in the reference (its kernel is the
+ * shared-memory histogram). */
+int mi3_weighted_marg_tc(const float *weights, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq,
+                         float *bimarg, uint32_t L, uint32_t q, void *workspace, size_t ws_bytes,
+                         int32_t *status, void *stream);
+
 /* Bytes of workspace mi3_site_consensus needs: 8*L*q. */
 size_t mi3_site_consensus_workspace(uint32_t L, uint32_t q);
 

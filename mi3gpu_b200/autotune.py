@@ -1,10 +1,10 @@
 """Autotuner for the shape-dependent choices of the B200 kernels.
 
 The sampler's tile plan (walkers per CTA, sites per streamed coupling chunk,
-ring stages; `mi3_metropolis_plans` lists the valid ones) and the bimarginal
-count kernel (shared-memory histogram or tcgen05 one-hot GEMM, which give the
-same integers) are picked per (L, q, walkers) by timing every candidate once
-on the device, from the caller's own walker state copied to scratch buffers
+ring stages; `mi3_metropolis_plans` lists the valid ones), the bimarginal
+count kernel and the weighted-bimarginal kernel (shared-memory histogram or
+tcgen05 one-hot GEMM, which give the same integers) are picked per
+(L, q, walkers) by timing every candidate once on the device, from the caller's own walker state copied to scratch buffers
 so the chain itself is not advanced.  Results are kept in memory and, when a
 cache path is given, in a JSON file keyed by device name and shape.
 
@@ -102,6 +102,7 @@ class Autotuner:
             return self.table[key]["kernel"]
         if not 4 <= gpu.q <= 32:
             self.table[key] = {"kernel": "smem"}
+            self._save()
             return "smem"
         times = {}
         for kind in ("smem", "tc"):
@@ -113,9 +114,41 @@ class Autotuner:
         self._save()
         return best
 
+    def wmarg_kernel(self, gpu, reps=3):
+        """'tc' or 'smem': the faster weighted-bimarginal kernel for gpu's
+        shape (identical results), timed with scratch weights."""
+        key = self._key("wmarg", gpu)
+        if key in self.table:
+            return self.table[key]["kernel"]
+        if not 4 <= gpu.q <= 32 or 'weights' not in gpu.bufs:
+            self.table[key] = {"kernel": "smem"}
+            self._save()
+            return "smem"
+        with torch.cuda.stream(gpu.stream):
+            saved = gpu.bufs['weights'].clone()
+            gen = torch.Generator(device='cpu').manual_seed(gpu.L)
+            w = torch.exp(-0.5 * torch.rand(saved.numel(), generator=gen)).to(gpu.device)
+            gpu.bufs['weights'].copy_(w)
+        prev = getattr(gpu, 'wmarg_kernel', None)
+        times = {}
+        for kind in ("smem", "tc"):
+            gpu.wmarg_kernel = kind
+            fn = (lambda: gpu.weightedMarg('main'))
+            fn()
+            times[kind] = _events_time(gpu.stream, fn, reps)
+        gpu.wmarg_kernel = prev
+        with torch.cuda.stream(gpu.stream):
+            gpu.bufs['weights'].copy_(saved)
+        best = min(times, key=times.get)
+        self.table[key] = {"kernel": best, "ms": times}
+        self._save()
+        return best
+
     def tune(self, gpu):
         """Tune every choice for gpu and install them on it."""
         plan, _ = self.sampler_plan(gpu)
         gpu.metro_plan = tuple(plan)
         gpu.count_kernel = self.count_kernel(gpu)
-        return {"metropolis_plan": gpu.metro_plan, "count_kernel": gpu.count_kernel}
+        gpu.wmarg_kernel = self.wmarg_kernel(gpu)
+        return {"metropolis_plan": gpu.metro_plan, "count_kernel": gpu.count_kernel,
+                "wmarg_kernel": gpu.wmarg_kernel}

@@ -173,8 +173,13 @@ class BatchedRounds:
              g._wsbytes('ws energies'), bs)
         call('mi3_weights_fused_dev', _p(c['ref']), _p(b['E main']), _p(b['weights']), N, _p(b['minout']),
              _p(b['weightstats']), _p(b['weightstats64']), _p(b['ws reduce']), g._wsbytes('ws reduce'), bs)
-        call('mi3_weighted_marg', _p(b['weights']), _p(b['seq main']), N, N, _p(b['bi']), L, q, None,
-             _p(b['ws wmarg']), g._wsbytes('ws wmarg'), bs)
+        wk = getattr(g, 'wmarg_kernel', None)
+        if (wk == 'tc') if wk else q in g.TENSOR_WMARG_Q:
+            call('mi3_weighted_marg_tc', _p(b['weights']), _p(b['seq main']), N, N, _p(b['bi']), L, q,
+                 *self._ws(g, 'ws wmarg tc', 'mi3_weighted_marg_tc_workspace', L, q), _p(b['status']), bs)
+        else:
+            call('mi3_weighted_marg', _p(b['weights']), _p(b['seq main']), N, N, _p(b['bi']), L, q, None,
+                 _p(b['ws wmarg']), g._wsbytes('ws wmarg'), bs)
         call('mi3_renormalize_bimarg', _p(b['bi']), L, q, bs)
         call('mi3_newton_control', handle.value, _p(b['weightstats64']), _p(b['minout']), _p(c['ref']),
              _p(c['count']), _p(c['budget']), self.frac * N, _p(c['stopped']), bs)
@@ -199,6 +204,8 @@ class BatchedRounds:
             # workspaces are created before capture (no allocation inside it)
             self._ws(pr.gpu, 'ws gauge', 'mi3_gauge_workspace', pr.L, pr.q)
             self._ws(pr.gpu, 'ws stats', 'mi3_bimarg_stats_workspace', pr.L)
+            if 4 <= pr.q <= 32:
+                self._ws(pr.gpu, 'ws wmarg tc', 'mi3_weighted_marg_tc_workspace', pr.L, pr.q)
         torch.cuda.synchronize(self.device)
         o = self.origin
         fork = torch.cuda.Event()

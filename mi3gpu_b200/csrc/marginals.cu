@@ -20,15 +20,6 @@ namespace mi3 {
 // bin cannot overflow, and the CTA flushes into a u64 accumulator with
 // integer atomics -- the sums are exact integers, so the result does not
 // depend on the order of the atomics (deterministic).
-__device__ __forceinline__ int fixed_shift(float wmax, uint32_t chunk) {
-    if (!(wmax > 0.0f)) return 40;
-    // chunk * (wmax * 2^s + 1/2) <= 2^32 - 1: the rounded increments of a
-    // whole chunk fit a u32 bin
-    double lim = (4294967295.0 - (double)chunk) / ((double)chunk * (double)wmax);
-    int s = (int)floor(log2(lim));
-    return min(s, 40);
-}
-
 // Increments of one sequence into the slice's histograms.  CONS: only the
 // pairs where neither residue is its site's consensus (the others are
 // rebuilt from site totals after the pass).
@@ -108,25 +99,25 @@ __device__ __forceinline__ void hist_chunk(uint32_t *h, const uint32_t *__restri
             if constexpr (WEIGHTED) inc = __float2uint_rn(__ldg(&weights[n]) * scale);
             slice_hist<B, K, CONS, false>(h, wI, wJ, cI, cJ, inc, q, qq, i0, j0, L);
         }
-        return;
-    }
-    // two sequences per thread: two independent atomic streams in flight
-    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += 2 * blockDim.x) {
-        const uint32_t n2 = n + blockDim.x;
-        const bool two = n2 < nend;
-        uint32_t wI[B / 4], wJ[B / 4], vI[B / 4], vJ[B / 4];
-        load_block_words<B>(seq, buflen, n, bi, swords, wI);
-        load_block_words<B>(seq, buflen, n, bj, swords, wJ);
-        load_block_words<B>(seq, buflen, two ? n2 : n, bi, swords, vI);
-        load_block_words<B>(seq, buflen, two ? n2 : n, bj, swords, vJ);
-        uint32_t inc1 = 1u, inc2 = 1u;
-        if constexpr (WEIGHTED) {
-            inc1 = __float2uint_rn(__ldg(&weights[n]) * scale);
-            inc2 = two ? __float2uint_rn(__ldg(&weights[n2]) * scale) : 0u;
+    } else {
+        // two sequences per thread: two independent atomic streams in flight
+        for (uint32_t n = nbeg + threadIdx.x; n < nend; n += 2 * blockDim.x) {
+            const uint32_t n2 = n + blockDim.x;
+            const bool two = n2 < nend;
+            uint32_t wI[B / 4], wJ[B / 4], vI[B / 4], vJ[B / 4];
+            load_block_words<B>(seq, buflen, n, bi, swords, wI);
+            load_block_words<B>(seq, buflen, n, bj, swords, wJ);
+            load_block_words<B>(seq, buflen, two ? n2 : n, bi, swords, vI);
+            load_block_words<B>(seq, buflen, two ? n2 : n, bj, swords, vJ);
+            uint32_t inc1 = 1u, inc2 = 1u;
+            if constexpr (WEIGHTED) {
+                inc1 = __float2uint_rn(__ldg(&weights[n]) * scale);
+                inc2 = two ? __float2uint_rn(__ldg(&weights[n2]) * scale) : 0u;
+            }
+            constexpr bool ROT = WEIGHTED && B <= 8;
+            slice_hist<B, K, CONS, ROT>(h, wI, wJ, cI, cJ, inc1, q, qq, i0, j0, L);
+            if (two) slice_hist<B, K, CONS, ROT>(h, vI, vJ, cI, cJ, inc2, q, qq, i0, j0, L);
         }
-        constexpr bool ROT = WEIGHTED && B <= 8;
-        slice_hist<B, K, CONS, ROT>(h, wI, wJ, cI, cJ, inc1, q, qq, i0, j0, L);
-        if (two) slice_hist<B, K, CONS, ROT>(h, vI, vJ, cI, cJ, inc2, q, qq, i0, j0, L);
     }
 }
 
@@ -520,6 +511,17 @@ extern "C" int mi3_bicounts(const uint32_t *seqmem, uint32_t buflen, uint32_t ns
     return dispatch_pairhist<false>(seqmem, buflen, nseq, nullptr, nullptr, bicount, L, q, nullptr,
                                     as_stream(stream));
 }
+
+namespace mi3 {
+uint32_t wmarg_fixed_chunk(uint32_t L, uint32_t q, uint32_t nseq) {
+    switch (pick_block(q, 116 * 1024, 16)) {
+        case 16: return pairhist_geom<16, true>(L, nseq).chunk;
+        case 8: return pairhist_geom<8, true>(L, nseq).chunk;
+        case 4: return pairhist_geom<4, true>(L, nseq).chunk;
+        default: return WMARG_CHUNK;
+    }
+}
+}  // namespace mi3
 
 extern "C" size_t mi3_weighted_marg_workspace(uint32_t L, uint32_t q, uint32_t nseq) {
     uint32_t nchunks = 1;

@@ -82,6 +82,21 @@ __device__ __forceinline__ uint32_t block_byte(const uint32_t (&w)[B / 4], int k
     return min((w[k >> 2] >> (8 * (k & 3))) & 0xffu, qm1);
 }
 
+// Fixed-point scale of the weighted histograms: increments are
+// round(w * 2^s), with s chosen from the largest weight so that a whole
+// chunk of `chunk` sequences fits a u32 bin:
+// chunk * (wmax * 2^s + 1/2) <= 2^32 - 1.
+__device__ __forceinline__ int fixed_shift(float wmax, uint32_t chunk) {
+    if (!(wmax > 0.0f)) return 40;
+    double lim = (4294967295.0 - (double)chunk) / ((double)chunk * (double)wmax);
+    int s = (int)floor(log2(lim));
+    return min(s, 40);
+}
+
+// The chunk length that sets that scale for mi3_weighted_marg on a shape
+// (every weighted-histogram kernel uses it, so all give identical integers).
+uint32_t wmarg_fixed_chunk(uint32_t L, uint32_t q, uint32_t nseq);
+
 // Slice kinds: the B x B pairs of an off-diagonal block pair inside the
 // sequence (every pair valid), a diagonal block pair inside the sequence
 // (pairs jj > ii), and a block pair that crosses the end of the sequence

@@ -368,6 +368,10 @@ class MCMCGPU:
     # 2^18 walkers: 1.3x at q=4, even at q=8, 3x slower at q=21); both give
     # identical integers.
     TENSOR_COUNT_Q = range(4, 7)
+    # the same for the weighted bimarginals (three byte-plane integer GEMMs
+    # against the shared-memory fixed-point histogram, identical results):
+    # 2.1x at q=4, 1.2x at q=5, slower from q=6 on
+    TENSOR_WMARG_Q = range(4, 6)
 
     def calcBicounts(self, seqbufname, wait_for=None, tensor=None):
         nseq = self.nseq[seqbufname]
@@ -493,9 +497,18 @@ class MCMCGPU:
         nseq = self.nseq[seqbufname]
         s = self._begin()
         cons = self._ptr('cons') if getattr(self, 'consWmarg', False) else None
-        _lib.call('mi3_weighted_marg', self._ptr('weights'), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
-                  self._ptr('bi'), self.L, self.q, cons, self._ptr('ws wmarg'), self._wsbytes('ws wmarg'),
-                  self._s)
+        tuned = getattr(self, 'wmarg_kernel', None)  # set by autotune.Autotuner.tune
+        tensor = (tuned == 'tc') if tuned else self.q in self.TENSOR_WMARG_Q
+        if tensor and cons is None:
+            if 'ws wmarg tc' not in self.bufs:
+                self._setupWorkspace('ws wmarg tc', _lib.query('mi3_weighted_marg_tc_workspace', self.L, self.q))
+            _lib.call('mi3_weighted_marg_tc', self._ptr('weights'), self.seqbufs[seqbufname].data_ptr(), nseq,
+                      nseq, self._ptr('bi'), self.L, self.q, self._ptr('ws wmarg tc'),
+                      self._wsbytes('ws wmarg tc'), self._ptr('status'), self._s)
+        else:
+            _lib.call('mi3_weighted_marg', self._ptr('weights'), self.seqbufs[seqbufname].data_ptr(), nseq,
+                      nseq, self._ptr('bi'), self.L, self.q, cons, self._ptr('ws wmarg'),
+                      self._wsbytes('ws wmarg'), self._s)
         return self.logevt('weightedMarg', s)
 
     def renormalize_bimarg(self, wait_for=None):

@@ -570,3 +570,37 @@ def test_energies_consensus_gauge(cuda, L, q, N, which):
     _lib.call("mi3_energies_cons", dev(J).data_ptr(), dev(mem).data_ptr(), N, N, E2.data_ptr(), L, q,
               dev(cons).data_ptr(), ws.data_ptr(), ws.numel() * 8, stream())
     np.testing.assert_array_equal(host(E2), host(E))
+
+
+@pytest.mark.parametrize("L,q,N", [(10, 5, 512), (48, 4, 1024), (37, 21, 1000), (93, 4, 3000), (64, 8, 640),
+                                   (20, 4, 200000), (29, 11, 5000), (232, 21, 2048), (99, 4, 1 << 16)])
+def test_weighted_marg_tensorcore_bitexact(cuda, L, q, N):
+    """tcgen05 integer one-hot GEMM (three weight byte planes) gives the
+    same bits as the shared-memory fixed-point histogram, and both are
+    within 1e-5 of each pair's total of the FP64 oracle."""
+    seqs = _potts_like_seqs(L, q, N, 11 * L + q)
+    mem = oracle.pack_seqs(seqs)
+    w = np.exp(np.random.default_rng(L + N).normal(0, 2.0, size=N)).astype("<f4")
+    dw, dm = dev(w), dev(mem)
+    a = empty((L * (L - 1) // 2, q * q), np.float32)
+    b = empty((L * (L - 1) // 2, q * q), np.float32)
+    ws = _wmarg_ws(L, q, N)
+    _lib.call("mi3_weighted_marg", dw.data_ptr(), dm.data_ptr(), N, N, a.data_ptr(), L, q, None, ws.data_ptr(),
+              ws.numel() * 8, stream())
+    wst = empty((int(_lib.query("mi3_weighted_marg_tc_workspace", L, q)) // 8 + 1,), np.int64)
+    status = empty((1,), np.int32)
+    _lib.call("mi3_weighted_marg_tc", dw.data_ptr(), dm.data_ptr(), N, N, b.data_ptr(), L, q, wst.data_ptr(),
+              wst.numel() * 8, status.data_ptr(), stream())
+    assert int(host(status, np.int32)[0]) == 0
+    np.testing.assert_array_equal(host(b), host(a))
+    if N * L * L < 4e9:
+        ref = oracle.weighted_marg_f64(w, mem, L, q)
+        assert (np.abs(host(b) - ref) / ref.sum(axis=1, keepdims=True)).max() < 1e-5
+
+
+def test_weighted_marg_tensorcore_rejects_bad_q(cuda):
+    ws = empty((16,), np.int64)
+    st = empty((1,), np.int32)
+    with pytest.raises(_lib.Mi3Error):
+        _lib.call("mi3_weighted_marg_tc", ws.data_ptr(), ws.data_ptr(), 512, 512, ws.data_ptr(), 10, 2,
+                  ws.data_ptr(), 128, st.data_ptr(), stream())
