@@ -430,6 +430,14 @@ def run_kernels(args):
                                           ws.data_ptr(), ws.numel() * 8, s), reps, st)
         t_w = time_call(lambda: _lib.call("mi3_weighted_marg", w.data_ptr(), seq.data_ptr(), N, N, bi.data_ptr(), L, q, None,
                                           wws.data_ptr(), wws.numel() * 8, s), reps, st)
+        t_etc = None
+        if 4 <= q <= 32:
+            E_tc = torch.empty_like(E)
+            t_etc = time_call(lambda: _lib.call("mi3_energies_tc", J.data_ptr(), seq.data_ptr(), N, N, E_tc.data_ptr(),
+                                                L, q, ws.data_ptr(), ws.numel() * 8, status.data_ptr(), s), reps, st)
+            assert int(status.item()) == 0
+            e_err = float(((E_tc - E).abs() / E.abs().clamp(min=1.0)).max())
+            del E_tc
         t_wtc = None
         if 4 <= q <= 32:
             wst = torch.zeros(int(_lib.query("mi3_weighted_marg_tc_workspace", L, q)) // 8 + 2, dtype=torch.int64,
@@ -442,7 +450,8 @@ def run_kernels(args):
             del wst, bi_tc
         flops = 2.0 * N * npairs * q * q
         r = {"L": L, "q": q, "N": N, "counts_smem_ms": t_plain, "counts_tc_ms": t_tc, "energies_ms": t_e,
-             "weighted_ms": t_w, "weighted_tc_ms": t_wtc, "counts_GBps_smem": N * L / t_plain / 1e6}
+             "weighted_ms": t_w, "weighted_tc_ms": t_wtc, "energies_tc_ms": t_etc,
+             "energies_tc_max_rel_diff": e_err if t_etc else None, "counts_GBps_smem": N * L / t_plain / 1e6}
         if t_tc:
             r.update(counts_GBps_tc=N * L / t_tc / 1e6, tc_tflops=flops / t_tc / 1e9,
                      tc_frac_of_fp8=flops / t_tc / 1e9 / fp8_peak)

@@ -123,6 +123,19 @@ int mi3_energies(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32
                  float *energies, uint32_t L, uint32_t q, void *workspace, size_t ws_bytes,
                  void *stream);
 
+/* getEnergies (mcmc.cl:249-345) on the tensor cores: per tile of row and
+ * column sites a BF16 one-hot GEMM X_I (J_hi + J_lo)_IJ (tcgen05, FP32
+ * accumulation in tensor memory) whose epilogue adds, per sequence, the
+ * column its own residues select; tiles are combined in 64-bit fixed point
+ * as in mi3_energies.  |E - E_exact| <= 2^-15 sum_{i<j} |J(s_i,s_j)| +
+ * 2^-24 |E| (hi + lo carries J to 2^-17; FP32 sums of at most 3*128/q
+ * terms).  4 <= q <= 32; the workspace holds nseq uint64 (as
+ * mi3_energies_workspace).  *status (int32, device, zeroed by the caller)
+ * receives MI3_STATUS_TIMEOUT_FULL if a bounded wait gave up.  No
+ * counterpart in the reference. */
+int mi3_energies_tc(const float *J, const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, float *energies,
+                    uint32_t L, uint32_t q, void *workspace, size_t ws_bytes, int32_t *status, void *stream);
+
 /* Capacity of mi3_energies_noalloc, in sequences. */
 #define MI3_ENERGIES_NOALLOC_MAX_SEQ (1u << 20)
 

@@ -26,6 +26,7 @@ SIGNATURES = {
     "mi3_energies_workspace": (c.c_size_t, [_u32]),
     "mi3_energies": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),
     "mi3_energies_noalloc": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp]),
+    "mi3_energies_tc": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, c.c_size_t, _vp, _vp]),
     "mi3_energies_cons_workspace": (c.c_size_t, [_u32, _u32, _u32]),
     "mi3_energies_cons": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp, c.c_size_t, _vp]),
     "mi3_bicounts": (c.c_int, [_vp, _u32, _u32, _vp, _u32, _u32, _vp]),

@@ -604,3 +604,29 @@ def test_weighted_marg_tensorcore_rejects_bad_q(cuda):
     with pytest.raises(_lib.Mi3Error):
         _lib.call("mi3_weighted_marg_tc", ws.data_ptr(), ws.data_ptr(), 512, 512, ws.data_ptr(), 10, 2,
                   ws.data_ptr(), 128, st.data_ptr(), stream())
+
+
+@pytest.mark.parametrize("L,q,N", [(10, 5, 512), (48, 4, 1024), (37, 21, 1000), (93, 4, 3000), (64, 8, 640),
+                                   (29, 11, 5000), (99, 4, 1 << 16), (150, 6, 4096), (33, 32, 700)])
+def test_energies_tensorcore_vs_fp64(cuda, L, q, N):
+    """BF16 hi/lo one-hot GEMM energies (tcgen05) against the FP64 oracle
+    within the stated bound 2^-15 sum|J(s_i,s_j)| + 2^-24 |E|, and
+    deterministic."""
+    seqs = _potts_like_seqs(L, q, N, 13 * L + q)
+    mem = oracle.pack_seqs(seqs)
+    J = np.random.default_rng(L * q + 1).normal(0, 0.3, size=(L * (L - 1) // 2, q * q)).astype("<f4")
+    ws = empty((N + 1,), np.int64)
+    st = empty((1,), np.int32)
+    E = empty((N,), np.float32)
+    dJ, dm = dev(J), dev(mem)
+    _lib.call("mi3_energies_tc", dJ.data_ptr(), dm.data_ptr(), N, N, E.data_ptr(), L, q, ws.data_ptr(),
+              ws.numel() * 8, st.data_ptr(), stream())
+    assert int(host(st, np.int32)[0]) == 0
+    e64 = oracle.energies_f64(J, mem, L, q)
+    eabs = oracle.energies_f64(np.abs(J), mem, L, q)
+    got = host(E).astype(np.float64)
+    assert np.all(np.abs(got - e64) <= 2.0 ** -15 * eabs + 2.0 ** -24 * np.abs(e64) + 1e-9)
+    E2 = empty((N,), np.float32)
+    _lib.call("mi3_energies_tc", dJ.data_ptr(), dm.data_ptr(), N, N, E2.data_ptr(), L, q, ws.data_ptr(),
+              ws.numel() * 8, st.data_ptr(), stream())
+    np.testing.assert_array_equal(host(E2), host(E))
