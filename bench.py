@@ -455,10 +455,19 @@ def run_kernels(args):
         if t_tc:
             r.update(counts_GBps_tc=N * L / t_tc / 1e6, tc_tflops=flops / t_tc / 1e9,
                      tc_frac_of_fp8=flops / t_tc / 1e9 / fp8_peak)
+        if t_wtc:
+            # three int8 byte planes: 3x the one-hot MACs, at the 8-bit peak
+            r.update(wmarg_tc_tops=3 * flops / t_wtc / 1e9, wmarg_tc_frac_of_int8=3 * flops / t_wtc / 1e9 / fp8_peak)
+        if t_etc:
+            # energies: 2 N (Lq)^2 / 2 over the tile triangle, x2 for hi and lo, at the bf16 peak
+            eflops = 2.0 * 2.0 * N * npairs * q * q
+            r.update(energies_tc_tflops=eflops / t_etc / 1e9,
+                     energies_tc_frac_of_bf16=eflops / t_etc / 1e9 / peaks.get("bf16_tflops", 1590.0))
         rows.append(r)
         del seqb, seq, out, J, E, ws, w, wws, bi
     print(json.dumps({"mode": "kernels", "fp8_peak_tflops": fp8_peak,
-                      "fp8_peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (of measured)", "rows": rows}))
+                      "fp8_peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (of measured)",
+                      "bf16_peak_tflops": peaks.get("bf16_tflops", 1590.0), "rows": rows}))
 
 
 def run_batched(args):
