@@ -44,17 +44,23 @@ class Autotuner:
         self.cache_path = Path(cache_path) if cache_path else None
         self.table = {}
         if self.cache_path is not None and self.cache_path.exists():
-            self.table = json.loads(self.cache_path.read_text())
+            try:
+                self.table = json.loads(self.cache_path.read_text())
+            except (ValueError, OSError):
+                self.table = {}  # unreadable cache: tune again
 
     def _key(self, kind, gpu, extra=""):
         name = torch.cuda.get_device_name(gpu.device).replace(" ", "_")
         return f"{name}/{kind}/L{gpu.L}/q{gpu.q}/N{gpu.nseq['main']}{extra}"
 
     def _save(self):
+        """Write the table atomically; processes sharing the file (one per
+        GPU) each write a private temporary and the last rename wins, so a
+        reader sees some complete table."""
         if self.cache_path is None:
             return
         self.cache_path.parent.mkdir(parents=True, exist_ok=True)
-        tmp = self.cache_path.with_suffix('.tmp')
+        tmp = self.cache_path.with_name(f"{self.cache_path.name}.{os.getpid()}.tmp")
         tmp.write_text(json.dumps(self.table, indent=1, sort_keys=True))
         os.replace(tmp, self.cache_path)
 

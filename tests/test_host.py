@@ -178,3 +178,27 @@ def test_device_resident_rounds_match_host_rounds():
     assert nh == nd
     np.testing.assert_allclose(sd, sh, rtol=1e-5)
     np.testing.assert_allclose(Jd, Jh, rtol=1e-4, atol=1e-6)
+
+
+def test_autotuner_cache_roundtrip_and_concurrent_writers(tmp_path):
+    """The tuning cache survives a reload, tolerates a corrupt file and is
+    written atomically through per-process temporaries."""
+    import json
+    import os
+    from mi3gpu_b200.autotune import Autotuner
+    path = tmp_path / "tune.json"
+    a = Autotuner(path)
+    a.table["dev/metropolis/L10/q4/N512"] = {"plan": [128, 12, 2]}
+    a._save()
+    assert Autotuner(path).table == a.table
+    assert not any(p.name.endswith(".tmp") for p in tmp_path.iterdir())
+    path.write_text("{not json")
+    assert Autotuner(path).table == {}
+    # two writers: each renames its own temporary, the file stays complete
+    b, c = Autotuner(path), Autotuner(path)
+    b.table["x"] = {"kernel": "smem"}
+    c.table["y"] = {"kernel": "tc"}
+    b._save()
+    c._save()
+    assert json.loads(path.read_text()) in (b.table, c.table)
+    assert os.path.exists(path)
