@@ -123,6 +123,10 @@ class BatchedRounds:
         for pr in self.problems:
             pr.gpu.gen_indep('main')
             pr.ctl['budget'].fill_(self.newton_max)
+            # the round's site list, sized for the longer round: graphs keep
+            # its address, so it is never reallocated
+            n = max(self._ncalls(pr, self.sweeps), self._ncalls(pr, self.sweeps_first)) * pr.nsteps
+            pr.randpos_round = torch.zeros(n, dtype=torch.int32, device=pr.gpu.device)
         torch.cuda.synchronize(self.device)
         self.graphs = {}
         self.rounds_done = 0
@@ -198,9 +202,6 @@ class BatchedRounds:
 
     def _build(self, key, sweeps):
         for pr in self.problems:
-            n = self._ncalls(pr, sweeps) * pr.nsteps
-            if pr.randpos_round is None or pr.randpos_round.numel() < n:
-                pr.randpos_round = torch.zeros(max(n, 1), dtype=torch.int32, device=pr.gpu.device)
             # workspaces are created before capture (no allocation inside it)
             self._ws(pr.gpu, 'ws gauge', 'mi3_gauge_workspace', pr.L, pr.q)
             self._ws(pr.gpu, 'ws stats', 'mi3_bimarg_stats_workspace', pr.L)
