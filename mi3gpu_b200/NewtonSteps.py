@@ -376,20 +376,31 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
     return Jstep + Jsteps, seqs, sampledenergies, newJ
 
 
-def newtonMCMC(param, gpus, start_run, Jstep, log):
+def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
     """Round loop (NewtonSteps.py:689-767) for the reseed strategies that
     need no file input: 'independent', 'single_indep', 'single_best',
-    'single_random', 'none'."""
+    'single_random', 'none'.
+
+    param.checkpoint (a path) writes a checkpoint after every round;
+    resume (a state from checkpoint.load) continues a run from one, on the
+    same trajectory as if it had not stopped."""
+    from . import checkpoint
     J = param.couplings
     gpus.setBuf('bi target', param.bimarg)
+    rng = np.random.RandomState(param.rngseed)
+    seqs, es = None, None
+    fresh = resume is None
+    if fresh:
+        param.max_newtonSteps = param.newtonSteps
+        param.min_ssr = np.inf
+    else:
+        start_run, Jstep, J, seqs, es = checkpoint.restore(resume, gpus, param, rng)
+        log(f"Continuing from a checkpoint before round {start_run}")
     if param.device_resident:
         gpus.setBuf('J', np.asarray(J, dtype='<f4'))
-    param.max_newtonSteps = param.newtonSteps
-    param.min_ssr = np.inf
-    seqs, es = None, None
-    rng = np.random.RandomState(param.rngseed)
     for i in range(start_run, param.mcmcsteps):
         runname = f'run_{i:02d}'
+        first = fresh and i == start_run
         seed = None
         if param.seedseq is not None:
             seed, param.seedseq = param.seedseq, None
@@ -402,15 +413,19 @@ def newtonMCMC(param, gpus, start_run, Jstep, log):
             seed = seqs[np.argmin(es)]
         if seed is not None:
             gpus.fillSeqs(seed)
-        elif param.reseed == 'independent' or (param.reseed == 'none' and i == start_run and param.init_indep):
+        elif param.reseed == 'independent' or (param.reseed == 'none' and first and param.init_indep):
             # 'none' keeps the walkers from round to round; they start from
             # independent-site sequences when init_indep is set
             gpus.gen_indep('main')
         equil = param.equiltime
-        if i == start_run and param.equiltime_first is not None:
+        if first and param.equiltime_first is not None:
             param.equiltime = param.equiltime_first
         Jstep, seqs, es, J = MCMCstep(runname, Jstep, J, param, gpus, log)
         param.equiltime = equil
+        if param.checkpoint:
+            keep = param.reseed in ('single_random', 'single_best')
+            checkpoint.save(param.checkpoint, gpus, param, i + 1, Jstep, J, rng,
+                            seqs if keep else None, es if keep else None)
     if param.device_resident:
         J = gpus.head_gpu.readBufs('J')[0]  # trial J of the last round, as the host path returns
     return J

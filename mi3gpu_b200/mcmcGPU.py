@@ -773,6 +773,32 @@ class MCMCGPU:
     def storeSeqs(self, seqs=None, wait_for=None):
         raise NotImplementedError("large sequence buffers are not part of the single-device path")
 
+    # ------------------------------------------------------------ checkpoints
+    _STATE_BUFS = ('seq main', 'rngstates', 'randpos')
+
+    def state_dict(self):
+        """Host copy of the sampling state: walkers, MWC64X states, the site
+        list with its read offset and the MT19937 state that refills it
+        (checkpoint.py)."""
+        self.stream.synchronize()
+        out = {name: self.bufs[name].cpu().numpy().copy() for name in self._STATE_BUFS if name in self.bufs}
+        out['randpos_offset'] = int(getattr(self, 'randpos_offset', 0))
+        out['rngstate'] = self.rngstate.get_state()
+        return out
+
+    def load_state_dict(self, d):
+        for name in self._STATE_BUFS:
+            if name in d:
+                src = torch.from_numpy(np.ascontiguousarray(d[name]))
+                if src.shape != self.bufs[name].shape or src.dtype != self.bufs[name].dtype:
+                    raise ValueError(f"state of {name!r} does not match this device's buffer")
+                with torch.cuda.stream(self.stream):
+                    self.bufs[name].copy_(src.to(self.device))
+        self.stream.synchronize()
+        self.randpos_offset = int(d['randpos_offset'])
+        self.rngstate.set_state(d['rngstate'])
+        self.repackedSeqT['main'] = False
+
     def wait(self):
         self.stream.synchronize()
         while self._pending_host:

@@ -136,6 +136,19 @@ class FakeMCMCGPU:
     def addBiBuffer(self, name, other):
         self.bufs[name] = self.bufs[name] + other
 
+    def state_dict(self):
+        out = {k: np.array(self.bufs[k], copy=True) for k in ('seq main', 'rngstates', 'randpos') if k in self.bufs}
+        out['randpos_offset'] = int(self.randpos_offset)
+        out['rngstate'] = self.rngstate.get_state()
+        return out
+
+    def load_state_dict(self, d):
+        for k in ('seq main', 'rngstates', 'randpos'):
+            if k in d:
+                self.bufs[k] = np.array(d[k], copy=True)
+        self.randpos_offset = int(d['randpos_offset'])
+        self.rngstate.set_state(d['rngstate'])
+
     def logProfile(self):
         pass
 

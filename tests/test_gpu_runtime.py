@@ -163,3 +163,40 @@ def test_sampler_plans_same_trajectory_and_autotuner(cuda, tmp_path):
         node.runMCMC()
         g.wait()
         assert Autotuner(cache).table == t.table
+
+
+def test_checkpoint_resume_on_gpu_bit_identical(cuda, tmp_path):
+    """On the device: three rounds straight equal two rounds + checkpoint +
+    a third round continued from it in new device objects."""
+    from mi3gpu_b200 import checkpoint
+    L, q, N = 20, 4, 2048
+    truth = potts.synthetic_ground_truth(L, q, seed=31, contact_sigma=0.5)
+
+    def run(rounds, path, resume=None):
+        g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 17)
+        node = GPU_node([g])
+        node.initMCMC(4 * L)
+        node.initJstep()
+        node.setBuf('J', truth)
+        node.setSeqs('main', np.zeros((N, L), '<u1'))
+        for _ in range(20):
+            node.runMCMC()
+        node.calcBicounts('main')
+        target = potts.mutation_pc(node.collect('bicount') / N, N).astype('<f4')
+        uni = potts.getUnimarg(target)
+        p = NewtonSteps.Param()
+        p.update(dict(bimarg=target, gamma0=4e-3, newtonSteps=64, pcdamping=1e-2, fracNeff=0.9, nwalkers=N,
+                      reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all', L=L, q=q,
+                      couplings=potts.independent_couplings(uni), nsteps=4 * L, equiltime=8, trackequil=0,
+                      outdir=None, mcmcsteps=rounds, newton_delta=32, reseed='none', rngseed=5, unimarg=uni,
+                      fused=True, init_indep=True, device_resident=True, checkpoint=str(path)))
+        node.prepare_indep(uni)
+        J = NewtonSteps.newtonMCMC(p, node, 0, 0, lambda *a: None,
+                                   resume=checkpoint.load(resume) if resume else None)
+        return J, [h['ssr'] for h in p.history]
+
+    J3, s3 = run(3, tmp_path / "a.pkl")
+    run(2, tmp_path / "b.pkl")
+    J3b, s3b = run(3, tmp_path / "c.pkl", resume=tmp_path / "b.pkl")
+    np.testing.assert_array_equal(J3b, J3)
+    assert s3b == s3

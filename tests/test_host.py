@@ -202,3 +202,51 @@ def test_autotuner_cache_roundtrip_and_concurrent_writers(tmp_path):
     c._save()
     assert json.loads(path.read_text()) in (b.table, c.table)
     assert os.path.exists(path)
+
+
+def _ckpt_run(tmp_path, rounds, dev, reseed, resume_from=None, ckpt_name="ck.pkl"):
+    from mi3gpu_b200 import checkpoint
+    L, q, N = 6, 3, 512
+    truth = potts.synthetic_ground_truth(L, q, seed=9, contact_sigma=0.5)
+    g = FakeMCMCGPU(L, q, N, seed=4)
+    gpus = GPU_node([g])
+    gpus.initMCMC(4 * L)
+    gpus.initJstep()
+    gpus.setBuf('J', truth)
+    gpus.setSeqs('main', np.zeros((N, L), '<u1'))
+    for _ in range(20):
+        gpus.runMCMC()
+    gpus.calcBicounts('main')
+    target = potts.mutation_pc(gpus.collect('bicount') / N, N).astype('<f4')
+    p = _param(L, q, N, target, np.zeros((L * (L - 1) // 2, q * q), '<f4'), newtonSteps=16)
+    p.unimarg = potts.getUnimarg(target)
+    p.reseed, p.device_resident, p.init_indep, p.mcmcsteps = reseed, dev, True, rounds
+    p.checkpoint = str(tmp_path / ckpt_name)
+    gpus.prepare_indep(p.unimarg)
+    state = checkpoint.load(resume_from) if resume_from else None
+    J = NewtonSteps.newtonMCMC(p, gpus, 0, 0, lambda *a: None, resume=state)
+    return J, p.history
+
+
+@pytest.mark.parametrize("dev", [False, True])
+@pytest.mark.parametrize("reseed", ["none", "independent", "single_random"])
+def test_checkpoint_resume_is_bit_identical(tmp_path, dev, reseed):
+    """Three rounds straight vs two rounds, a checkpoint, and the third round
+    continued from it in a fresh process state: the same couplings and the
+    same history, bit for bit."""
+    J3, h3 = _ckpt_run(tmp_path, 3, dev, reseed, ckpt_name="a.pkl")
+    _ckpt_run(tmp_path, 2, dev, reseed, ckpt_name="b.pkl")
+    J3b, h3b = _ckpt_run(tmp_path, 3, dev, reseed, resume_from=tmp_path / "b.pkl", ckpt_name="c.pkl")
+    np.testing.assert_array_equal(J3b, J3)
+    assert [h['ssr'] for h in h3b] == [h['ssr'] for h in h3]
+    assert [h['newton_steps'] for h in h3b] == [h['newton_steps'] for h in h3]
+
+
+def test_checkpoint_rejects_other_shapes(tmp_path):
+    from mi3gpu_b200 import checkpoint
+    _ckpt_run(tmp_path, 1, False, "none", ckpt_name="s.pkl")
+    state = checkpoint.load(tmp_path / "s.pkl")
+    state['shape'] = (7, 3, 512)
+    with pytest.raises(ValueError):
+        checkpoint.restore(state, GPU_node([FakeMCMCGPU(6, 3, 512, seed=1)]), NewtonSteps.Param(L=6, q=3),
+                           np.random.RandomState(0))
