@@ -832,23 +832,44 @@ def unpackJ_CPU(couplings):
     return full
 
 
-def setup_GPU_context(param, log):
-    """Select the CUDA devices to use (mcmcGPU.py:1038-1100 counterpart).
-    param.gpuspec: None (all visible devices) or a comma separated list of
-    device indices.  No run-time compilation: the kernels are prebuilt."""
+def printGPUs(log):
+    """List the visible CUDA devices (mcmcGPU.py:58-64 lists OpenCL platforms)."""
+    for n in range(torch.cuda.device_count()):
+        printDevice(log, torch.device('cuda', n))
+        log("")
+
+
+def setup_GPU_context(scriptpath, scriptfile, param, log):
+    """Select the CUDA devices to use, with the reference's signature and
+    return shape (mcmcGPU.py:1038-1100): (context data, devices, (info,
+    build log)).  There is no run-time compilation -- the kernels are
+    prebuilt for sm_100a -- so scriptpath/scriptfile are not read and the
+    context data is None.  param.gpuspec: None (all visible devices) or a
+    comma separated list of device indices (an OpenCL "platform:device"
+    entry uses its device index)."""
     if not torch.cuda.is_available():
         raise Exception("Error: No GPUs found")
     _lib.load()
     if param.get('gpuspec') is not None:
-        devs = [int(x.split(':')[-1]) for x in str(param['gpuspec']).split(',')]
+        try:
+            devs = [int(x.split(':')[-1]) for x in str(param['gpuspec']).split(',')]
+        except ValueError:
+            raise Exception("Error: GPU specification must be a comma separated list of devices, eg '0,1'")
+        for d in devs:
+            if not 0 <= d < torch.cuda.device_count():
+                raise Exception("No GPU with specification {}".format(d))
     else:
         devs = list(range(torch.cuda.device_count()))
+    if not devs:
+        raise Exception("Error: No GPUs found")
     log("Using CUDA devices {}".format(devs))
-    return devs
+    info = "libmi3b200 ABI {} (sm_100a)".format(_lib.load().mi3_abi_version())
+    return None, [torch.device('cuda', d) for d in devs], (info, "")
 
 
-def initGPU(devnum, device, nwalkers, param, log):
-    """(mcmcGPU.py:1102-1119 counterpart)"""
+def initGPU(devnum, cldat, device, nwalkers, param, log):
+    """(mcmcGPU.py:1102-1119) -- cldat is setup_GPU_context's context data
+    (unused)."""
     wgsize = param.get('wgsize', 512)
     if wgsize not in [1 << n for n in range(32)]:
         raise Exception("wgsize must be a power of two")

@@ -200,3 +200,23 @@ def test_checkpoint_resume_on_gpu_bit_identical(cuda, tmp_path):
     J3b, s3b = run(3, tmp_path / "c.pkl", resume=tmp_path / "b.pkl")
     np.testing.assert_array_equal(J3b, J3)
     assert s3b == s3
+
+
+def test_reference_setup_and_init_signatures(cuda):
+    """Mi3.py's device set-up calls, with the reference's signatures:
+    setup_GPU_context(scriptpath, scriptfile, param, log) and
+    initGPU(devnum, cldat, device, nwalkers, param, log)."""
+    from mi3gpu_b200 import initGPU, setup_GPU_context
+    logs = []
+    p = NewtonSteps.Param(L=12, q=4, gpuspec='0', wgsize=512, outdir=None, rngseed=3, profile=False, beta=None)
+    cldat, devices, (info, buildlog) = setup_GPU_context(None, None, p, logs.append)
+    assert len(devices) == 1 and "sm_100a" in info
+    gpus = GPU_node([initGPU(i, cldat, d, 1024, p, logs.append) for i, d in enumerate(devices)])
+    gpus.initMCMC(48)
+    gpus.setBuf('J', potts.synthetic_ground_truth(12, 4, seed=1, contact_sigma=0.3))
+    gpus.setSeqs('main', np.zeros((1024, 12), '<u1'))
+    gpus.runMCMC()
+    gpus.wait()
+    assert gpus.collect('seq main').shape == (1024, 12)
+    with pytest.raises(Exception):
+        setup_GPU_context(None, None, NewtonSteps.Param(gpuspec='99'), logs.append)

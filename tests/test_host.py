@@ -250,3 +250,24 @@ def test_checkpoint_rejects_other_shapes(tmp_path):
     with pytest.raises(ValueError):
         checkpoint.restore(state, GPU_node([FakeMCMCGPU(6, 3, 512, seed=1)]), NewtonSteps.Param(L=6, q=3),
                            np.random.RandomState(0))
+
+
+def test_auto_equilibration_runs_and_stops():
+    """equiltime='auto' (NewtonSteps.py:395-442): loops double until two
+    successive energy snapshots are uncorrelated with the current one
+    (Spearman p > 0.02) after min_equil calls, or max_equil is reached."""
+    L, q, N = 6, 3, 512
+    truth = potts.synthetic_ground_truth(L, q, seed=9, contact_sigma=0.5)
+    g = FakeMCMCGPU(L, q, N, seed=4)
+    gpus = GPU_node([g])
+    gpus.initMCMC(2 * L)
+    gpus.initJstep()
+    p = _param(L, q, N, np.full((L * (L - 1) // 2, q * q), 1.0 / (q * q), '<f4'), truth, newtonSteps=4)
+    p.equiltime, p.min_equil, p.max_equil = 'auto', 16, 64
+    logs = []
+    gpus.setSeqs('main', np.zeros((N, L), '<u1'))
+    out = NewtonSteps.runMCMC(gpus, truth, 'run_00', p, logs.append)
+    steps = out[5]
+    assert 16 <= steps <= 64 + 32
+    assert any("Equilibrated" in s or "Max Steps" in s for s in logs)
+    assert out[3] is not None and len(out[3]) >= 2  # energy autocorrelations recorded
