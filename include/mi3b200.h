@@ -55,6 +55,17 @@ const char *mi3_last_error(void);
 /* ABI version of this library. */
 int mi3_abi_version(void);
 
+/* Test hook for the failure path of the device-side bounded waits: one
+ * thread waits on an mbarrier that nothing completes, with the wait routine
+ * the sampler and the tensor-core kernels use, and gives up after limit_ns
+ * (<= 2 s): *status (int32, zeroed by the caller) becomes
+ * MI3_STATUS_TIMEOUT_FULL and *waited_ns (uint64) the time waited.  With
+ * abort_after_ns > 0 another warp raises the CTA's abort flag after that
+ * time, which ends the wait early.  Nothing faults or hangs: the kernel
+ * returns and the context stays usable. */
+int mi3_probe_bounded_wait(int32_t *status, uint64_t limit_ns, uint64_t abort_after_ns,
+                           unsigned long long *waited_ns, void *stream);
+
 /* ---------------------------------------------------------------- sampler */
 
 /* initRNG2 (mcmc.cl:349-356) as launched by MCMCGPU._initMCMC_RNG

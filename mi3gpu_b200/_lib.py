@@ -15,6 +15,7 @@ _vp, _u32, _u64, _f32, _i32 = c.c_void_p, c.c_uint32, c.c_uint64, c.c_float, c.c
 SIGNATURES = {
     "mi3_last_error": (c.c_char_p, []),
     "mi3_abi_version": (c.c_int, []),
+    "mi3_probe_bounded_wait": (c.c_int, [_vp, _u64, _u64, _vp, _vp]),
     "mi3_init_rng": (c.c_int, [_vp, _u32, _u64, _u64, _vp]),
     "mi3_jrows_stride": (_u64, [_u32, _u32]),
     "mi3_unpack_j": (c.c_int, [_vp, _vp, _u32, _u32, _vp]),

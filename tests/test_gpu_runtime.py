@@ -220,3 +220,41 @@ def test_reference_setup_and_init_signatures(cuda):
     assert gpus.collect('seq main').shape == (1024, 12)
     with pytest.raises(Exception):
         setup_GPU_context(None, None, NewtonSteps.Param(gpuspec='99'), logs.append)
+
+
+def test_bounded_wait_gives_up_and_context_survives(cuda):
+    """The device-side failure path, exercised without a fault: a wait on an
+    mbarrier that nothing completes gives up after its limit (or as soon as
+    the CTA's abort flag rises), writes MI3_STATUS_TIMEOUT_FULL, and the
+    kernel returns; the device keeps working and MCMCGPU turns the status
+    word into an exception."""
+    import torch
+    from mi3gpu_b200 import _lib
+    dev = torch.device('cuda', 0)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    for limit, abort in [(50_000_000, 0), (1_000_000_000, 20_000_000)]:
+        st = torch.zeros(1, dtype=torch.int32, device=dev)
+        waited = torch.zeros(1, dtype=torch.int64, device=dev)
+        _lib.call('mi3_probe_bounded_wait', st.data_ptr(), limit, abort, waited.data_ptr(), s)
+        torch.cuda.synchronize(dev)
+        assert int(st.item()) == 1  # MI3_STATUS_TIMEOUT_FULL
+        w = int(waited.item())
+        if abort:
+            assert abort <= w < limit // 2, w
+        else:
+            assert limit <= w < 20 * limit, w
+    # the context still runs kernels
+    L, q, N = 12, 4, 512
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 3)
+    node = GPU_node([g])
+    node.initMCMC(2 * L)
+    node.setBuf('J', potts.synthetic_ground_truth(L, q, seed=2, contact_sigma=0.3))
+    node.setSeqs('main', np.zeros((N, L), '<u1'))
+    node.runMCMC()
+    node.wait()
+    # a status word set by a kernel surfaces as an exception on the host
+    _lib.call('mi3_probe_bounded_wait', g._ptr('status'), 10_000_000, 0, waited.data_ptr(), g.stream.cuda_stream)
+    with pytest.raises(RuntimeError):
+        g.wait()
+    with pytest.raises(_lib.Mi3Error):
+        _lib.call('mi3_probe_bounded_wait', st.data_ptr(), 3_000_000_000, 0, waited.data_ptr(), s)
