@@ -773,7 +773,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_inference:
         out["s_per_iter"] = headline_inference(args)
     if rank == 0:
-        if not args.no_cpu:
+        if not args.no_cpu and world == 1:  # the CPU baseline is an N=1 figure
             r = cpu_generator_rate(J, args.L, args.q, args.cpu_seconds, os.cpu_count() or 1)
             if r is not None:
                 out["cpu_baseline"] = {"value": r[0], "unit": "site-updates/s", "cores": os.cpu_count() or 1,
