@@ -542,6 +542,46 @@ def run_batched(args):
         "tuned_plans_sample": plans, "target_build_s": t_targets}))
 
 
+def run_graph_small(args):
+    """The small workload (L=48, q=4, 16384 walkers, 64 sweeps per round, a
+    2^14-sequence synthetic MSA): quasi-Newton rounds driven by the host
+    loop (device-resident, one launch and one sync per Newton step) against
+    the same rounds recorded once as a CUDA graph (batched.BatchedRounds
+    with one problem: one launch per round).  Same seeds, same kernels, same
+    results; the difference is launch and synchronisation overhead.  Both
+    arms are timed by the wall clock around a round (the host loop's own
+    round_s), the graph's device time is reported beside it."""
+    import torch
+    from mi3gpu_b200.batched import BatchedRounds, Problem
+    from mi3gpu_b200.inference import make_target, infer
+    from mi3gpu_b200.mcmcGPU import MCMCGPU
+    MCMCGPU.CONS_ENERGY_MAX_ACTIVE = -1.0  # the graph uses the direct energy kernel
+    L, q, N, sweeps, rounds = 48, 4, 16384, 64, args.rounds
+    target, _ = make_target(L, q, 1 << 14, seed=1000)
+    res = infer(target, L, q, N, rounds, sweeps=sweeps, sweeps_first=sweeps, reseed='none', seed=77,
+                device_resident=True, log=lambda *a: None)
+    host = [h["round_s"] for h in res["history"]]
+    pr = Problem(target, L, q, N, seed=77)
+    br = BatchedRounds([pr], sweeps=sweeps, sweeps_first=sweeps, reseed='none')
+    recs = [br.run_round() for _ in range(rounds)]
+    graph = [r["wall_s"] for r in recs]  # wall clock, like the host loop's round_s
+    graph_dev = [r["gpu_ms"] / 1e3 for r in recs]
+    same = [h["ssr"] for h in pr.history] == [h["ssr"] for h in res["history"]]
+    steps = [h["newton_steps"] for h in res["history"]]
+    br.close()
+    print(json.dumps({
+        "metric": "s per quasi-Newton round, host loop vs one graph launch", "unit": "s/round",
+        "value": statistics.mean(graph[1:] or graph), "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"inference L={L} q={q} walkers={N}, {sweeps} sweeps/round, msa 2^14, l1z 2e-4",
+                   "rounds": rounds},
+        "host_loop_s_per_round": statistics.mean(host[1:] or host), "graph_s_per_round":
+            statistics.mean(graph[1:] or graph), "speedup": statistics.mean(host[1:] or host) /
+            statistics.mean(graph[1:] or graph), "graph_device_s_per_round": statistics.mean(graph_dev[1:] or graph_dev),
+        "newton_steps_per_round": steps,
+        "identical_ssr_histories": same}))
+
+
 def energy_autocorr(Es):
     """Energy autocorrelation across walkers, rho(t) = corr(E_0, E_t), and
     tau_int = 1 + 2 sum_t rho(t) summed until rho first drops below 0.05."""
@@ -718,7 +758,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--newton-steps", type=int, default=10, help="quasi-Newton steps to time (0: skip)")
-    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned", "batched"],
+    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned", "batched", "graph_small"],
                     help="inference: run full quasi-Newton rounds and report s/iter and SSR")
     ap.add_argument("--rounds", type=int, default=4, help="inference rounds (--mode inference)")
     ap.add_argument("--msa", type=int, default=1 << 16, help="synthetic MSA size (--mode inference)")
@@ -768,6 +808,9 @@ def main():
         return
     if args.mode == "batched":
         run_batched(args)
+        return
+    if args.mode == "graph_small":
+        run_graph_small(args)
         return
     out, J = run_gpu(args)
     if rank == 0 and world == 1 and not args.no_inference:
