@@ -88,8 +88,21 @@ def iterNewton(param, bimarg_model, gpus, log, fused=False):
     s = time.time()
 
     seqbuf, wbufname, ebufname, etmpname = 'main', 'weights', 'E main', 'E tmp'
-    if param.distribute_jstep not in (None, 'all'):
-        raise NotImplementedError("distribute_jstep other than 'all' needs the large sequence buffers")
+    allgpus = gpus
+    mode = param.distribute_jstep or 'all'
+    if mode != 'all':
+        # the Newton phase runs on the head device (or node) over every
+        # walker, gathered into its large buffer (NewtonSteps.py:181-195)
+        if mode == 'head_gpu':
+            gpus = allgpus.head_gpu
+            log("Transferring sequences to gpu 0")
+        elif mode == 'head_node':
+            gpus = allgpus.head_node
+            log("Transferring sequences to node 0")
+        else:
+            raise ValueError(f"unknown distribute_jstep {mode!r}")
+        allgpus.gatherLarge(gpus)
+        seqbuf, wbufname, ebufname, etmpname = 'large', 'weights large', 'E large', 'E tmp large'
 
     # the walkers are fixed during the Newton steps: their consensus residues
     # let the energy and weighted-bimarginal passes skip most pairs
@@ -150,6 +163,8 @@ def iterNewton(param, bimarg_model, gpus, log, fused=False):
         # trial J = J + dJ formed in place on every device (the reference reads
         # bi, J, dJ back, adds them on the host and sends J down again)
         gpus.addFloatBuf('J', 'dJ')
+        if gpus is not allgpus:
+            allgpus.shareJ(gpus)
         st = gpus.bimargStats('bi', 'bi target', None)[0].read()
         log(f"Predicted statistics after perturbing J: SSR {st[0]:.4f}")
         if not np.isfinite(wsum) or wsum == 0:

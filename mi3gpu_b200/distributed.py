@@ -16,6 +16,13 @@ process group (NCCL on GPUs, gloo in the CPU tests):
 Every rank then holds the same J, dJ and bimarginals and takes the same
 number of Newton steps, because each computes the stop rule from the same
 reduced numbers.  Collectives are issued on the device's own stream.
+
+With distribute_jstep 'head_gpu' the reference gathers all walkers on its
+first GPU and runs the Newton phase there while the others wait
+(NewtonSteps.py:181-195).  Here every rank gathers all walkers into its own
+large buffer (one broadcast per rank) and runs that same head-device phase,
+with no collective inside the loop; the couplings are then broadcast from
+rank 0, so all ranks continue from identical J by construction.
 """
 import numpy as np
 import torch
@@ -54,6 +61,12 @@ class RankNode(GPU_node):
         return GPU_node([self.gpus[0]])
 
     @property
+    def head_node(self):
+        # the reference accepts 'head_node' only across MPI nodes (Mi3.py:452-455);
+        # the ranks of one launch are one node
+        raise Exception('"head_node" needs ranks on several nodes; use "head_gpu" or "all"')
+
+    @property
     def nwalkers(self):
         return sum(self.walkers_per_rank)
 
@@ -81,15 +94,46 @@ class RankNode(GPU_node):
         self.gpus[0].initMCMC(nsteps, np.uint64(self.rank) * span, span)
 
     # -------------------------------------------------------- exchanges
-    def _reduce(self, bufname, op):
-        g = self.gpus[0]
-        t = _as_tensor(g.bufs[bufname])
-        stream = getattr(g, 'stream', None)
-        if isinstance(stream, torch.cuda.Stream) or isinstance(stream, torch.cuda.ExternalStream):
+    def _collective(self, fn):
+        stream = getattr(self.gpus[0], 'stream', None)
+        if isinstance(stream, (torch.cuda.Stream, torch.cuda.ExternalStream)):
             with torch.cuda.stream(stream):
-                dist.all_reduce(t, op=op, group=self.group)
+                fn()
         else:
-            dist.all_reduce(t, op=op, group=self.group)
+            fn()
+
+    def _reduce(self, bufname, op):
+        t = _as_tensor(self.gpus[0].bufs[bufname])
+        self._collective(lambda: dist.all_reduce(t, op=op, group=self.group))
+
+    def gatherLarge(self, target):
+        """All ranks' walkers, in rank order, into this rank's large buffer
+        (target must be this rank's head_gpu)."""
+        g = self.gpus[0]
+        if target.gpus != [g]:
+            raise ValueError("RankNode gathers into its own device only (head_gpu)")
+        total = self.nwalkers
+        if 'large' not in g.nseq:
+            g.initLargeBufs(total)
+        if g.nseq['large'] != total:
+            raise Exception("Expected {} total sequences, got {}".format(g.nseq['large'], total))
+        g.wait()
+        g.clearLargeSeqs()
+        mine = _as_tensor(g.packedSeqs('main'))
+        for r, n in enumerate(self.walkers_per_rank):
+            buf = mine.contiguous() if r == self.rank else torch.empty((mine.shape[0], n), dtype=mine.dtype,
+                                                                         device=mine.device)
+            self._collective(lambda: dist.broadcast(buf, src=r, group=self.group))
+            g.storeSeqs(buf)
+        g.wait()
+
+    def shareJ(self, head):
+        """Rank 0's couplings to every rank (after the head-device phase)."""
+        g = self.gpus[0]
+        g.wait()
+        t = _as_tensor(g.bufs['J'])
+        self._collective(lambda: dist.broadcast(t, src=0, group=self.group))
+        g.wait()
 
     def merge_bimarg(self):
         self._reduce('bi', dist.ReduceOp.SUM)

@@ -52,7 +52,7 @@ def make_target(L, q, n_msa, seed, sweeps=None, contact_sigma=0.5, device=0):
 
 def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e-4, damping=1e-3,
           reg=('l1z', (2e-4,)), seed=1234, device=0, log=print, fused=True, outdir=None, reseed='independent',
-          sweeps_first=None, device_resident=True, tuner=None):
+          sweeps_first=None, device_resident=True, tuner=None, distribute_jstep='all'):
     """Run `rounds` quasi-Newton iterations from the independent model;
     returns the per-round history (SSR, wall seconds of MCMC and Newton
     phases) as recorded by NewtonSteps.MCMCstep.
@@ -65,14 +65,16 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
     rounds (gauge transform and statistics in FP64 there); False runs the
     round's host work in numpy as the reference does.  tuner: an
     autotune.Autotuner whose sampler plan and count kernel are installed
-    (results do not depend on them)."""
+    (results do not depend on them).  distribute_jstep: 'all' runs the
+    Newton steps over the walkers where they are; 'head_gpu' first gathers
+    them into the device's large buffer, as the reference's option does."""
     unimarg = potts.getUnimarg(target)
     J0 = potts.independent_couplings(unimarg)
     nsteps = 8 * L
     p = NewtonSteps.Param()
     p.update(dict(bimarg=target, gamma0=gamma, newtonSteps=newtonsteps, pcdamping=damping, fracNeff=0.9,
                   nwalkers=nwalkers, reg=reg[0] if reg else None, regarg=reg[1] if reg else None, beta=None,
-                  distribute_jstep='all', L=L, q=q, couplings=J0, nsteps=nsteps,
+                  distribute_jstep=distribute_jstep, L=L, q=q, couplings=J0, nsteps=nsteps,
                   equiltime=max(1, sweeps * L // nsteps), trackequil=0, outdir=outdir, mcmcsteps=rounds,
                   newton_delta=32, reseed=reseed, rngseed=seed + 1, unimarg=unimarg, fused=fused, init_indep=True,
                   device_resident=device_resident,

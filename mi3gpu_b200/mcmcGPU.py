@@ -143,9 +143,8 @@ class MCMCGPU:
         self._setupBuffer('minout', '<f4', (1,))
         # library-side state: sampler status word and reduction/energy workspaces
         self._setupBuffer('status', '<i4', (1,))
-        self._setupWorkspace('ws energies', _lib.query('mi3_energies_workspace', nseq))
-        self._setupWorkspace('ws reduce', _lib.query('mi3_weight_stats_workspace', nseq))
-        self._setupWorkspace('ws wmarg', _lib.query('mi3_weighted_marg_workspace', L, q, nseq))
+        self._ws_nseq = 0
+        self._sizeWorkspaces(nseq)
         self.fillBuf('status', 0)
         self.unpackedJ = False
         self.repackedSeqT = {'main': False}
@@ -227,6 +226,32 @@ class MCMCGPU:
         with torch.cuda.device(self.device):
             self.bufs[name] = torch.zeros(max(int(nbytes), 16) // 8 + 2, dtype=torch.int64, device=self.device)
 
+    def _sizeWorkspaces(self, nseq):
+        """(Re)allocate the workspaces whose size grows with the number of
+        sequences a call may process (main, or the large buffer)."""
+        if nseq <= self._ws_nseq:
+            return
+        self._ws_nseq = nseq
+        L, q = self.L, self.q
+        self._setupWorkspace('ws energies', _lib.query('mi3_energies_workspace', nseq))
+        self._setupWorkspace('ws reduce', _lib.query('mi3_weight_stats_workspace', nseq))
+        self._setupWorkspace('ws wmarg', _lib.query('mi3_weighted_marg_workspace', L, q, nseq))
+        if 'ws energies cons' in self.bufs:
+            self._setupWorkspace('ws energies cons', _lib.query('mi3_energies_cons_workspace', L, q, nseq))
+
+    def _span(self, seqbufname):
+        """(sequences to process, row length) of a sequence buffer: all of
+        'main', or the stored part of 'large' (mcmcGPU.py:504-509)."""
+        if seqbufname == 'main':
+            n = self.nseq['main']
+            return n, n
+        self.require('Large')
+        return self.nstoredseqs, self.nseq[seqbufname]
+
+    @staticmethod
+    def _wbufname(seqbufname):
+        return 'weights' if seqbufname == 'main' else 'weights ' + seqbufname
+
     def _wsbytes(self, name):
         b = self.bufs[name]
         return b.numel() * b.element_size()
@@ -259,8 +284,26 @@ class MCMCGPU:
         self.nsteps = int(nsteps)
 
     def initLargeBufs(self, nseq_large):
-        raise NotImplementedError("large sequence buffers (distribute_jstep head_gpu/head_node) are not "
-                                  "part of the single-device path")
+        """Sequence buffers for more sequences than this device samples
+        (mcmcGPU.py:284-303): with distribute_jstep 'head_gpu' / 'head_node'
+        the walkers of every device are gathered here and the Newton steps
+        run over them.  Only the first nstoredseqs columns are used."""
+        self._initcomponent('Large')
+        nseq_large = int(nseq_large)
+        if nseq_large <= 0:
+            raise ValueError("the large buffer needs at least one sequence")
+        self.nseq['large'] = nseq_large
+        self._setupBuffer('seq large', '<u4', (self.SWORDS, nseq_large))
+        self._setupBuffer('seqL large', '<u4', (self.L, nseq_large // 4))
+        self._setupBuffer('E large', '<f4', (nseq_large,))
+        self._setupBuffer('E tmp large', '<f4', (nseq_large,))
+        self._setupBuffer('weights large', '<f4', (nseq_large,))
+        self.largebufs.extend(['seq large', 'seqL large', 'E large', 'weights large'])
+        self.nstoredseqs = 0
+        # zeroed, as in the reference: unused columns hold residue 0
+        self.fillBuf('seq large', 0)
+        self.repackedSeqT['large'] = False
+        self._sizeWorkspaces(nseq_large)
 
     def initSubseq(self):
         raise NotImplementedError("subsequence mode is not part of the single-device path")
@@ -293,7 +336,7 @@ class MCMCGPU:
         return bseqs[:, :self.L].copy()
 
     def repackseqs_T(self, bufname, wait_for=None):
-        nseq = self.nseq[bufname]
+        nseq = self.nseq[bufname]  # the whole buffer, stored or not (mcmcGPU.py:356-373)
         s = self._begin()
         _lib.call('mi3_repack_seqs_T', self._ptr('seq ' + bufname), nseq, self._ptr('seqL ' + bufname),
                   nseq // 4, self.L, self._s)
@@ -374,21 +417,21 @@ class MCMCGPU:
     TENSOR_WMARG_Q = range(4, 6)
 
     def calcBicounts(self, seqbufname, wait_for=None, tensor=None):
-        nseq = self.nseq[seqbufname]
+        nseq, buflen = self._span(seqbufname)
         if tensor is None:
             tuned = getattr(self, 'count_kernel', None)  # set by autotune.Autotuner.tune
             tensor = (tuned == 'tc') if tuned else self.q in self.TENSOR_COUNT_Q
         s = self._begin()
         if tensor:
-            _lib.call('mi3_bicounts_tc', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, self._ptr('bicount'),
-                      self.L, self.q, self._ptr('status'), self._s)
+            _lib.call('mi3_bicounts_tc', self.seqbufs[seqbufname].data_ptr(), buflen, nseq,
+                      self._ptr('bicount'), self.L, self.q, self._ptr('status'), self._s)
         else:
-            _lib.call('mi3_bicounts', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, self._ptr('bicount'),
+            _lib.call('mi3_bicounts', self.seqbufs[seqbufname].data_ptr(), buflen, nseq, self._ptr('bicount'),
                       self.L, self.q, self._s)
         return self.logevt('calcBicounts', s)
 
     def bicounts_to_bimarg(self, seqbufname='main', wait_for=None):
-        nseq = self.nseq[seqbufname]
+        nseq = self._span(seqbufname)[0]
         s = self._begin()
         _lib.call('mi3_bicounts_to_bimarg', self._ptr('bicount'), self._ptr('bi'), nseq, self.L, self.q,
                   self._s)
@@ -418,10 +461,10 @@ class MCMCGPU:
             self._setupBuffer('cons', '<u1', (L,))
             self._setupWorkspace('ws cons', _lib.query('mi3_site_consensus_workspace', L, q))
             self._setupWorkspace('ws energies cons', _lib.query('mi3_energies_cons_workspace', L, q,
-                                                                self.nseq['main']))
-        nseq = self.nseq[seqbufname]
+                                                                self._ws_nseq))
+        nseq, buflen = self._span(seqbufname)
         s = self._begin()
-        _lib.call('mi3_site_consensus', self.seqbufs[seqbufname].data_ptr(), nseq, nseq, L, q, self._ptr('cons'),
+        _lib.call('mi3_site_consensus', self.seqbufs[seqbufname].data_ptr(), buflen, nseq, L, q, self._ptr('cons'),
                   self._ptr('ws cons'), self._wsbytes('ws cons'), self._s)
         evt = self.logevt('updateConsensus', s)
         # the workspace holds the per-site residue counts (uint64, L x q)
@@ -435,18 +478,18 @@ class MCMCGPU:
         return evt
 
     def calcEnergies(self, seqbufname, Jbufname='J', wait_for=None):
-        nseq = self.nseq[seqbufname]
+        nseq, buflen = self._span(seqbufname)
         s = self._begin()
         # the consensus gauge rounds the regauged couplings (|J'| <= 4 max|J|)
         # to float once: used for the small reweighting energies of dJ, where
         # that is far below the step's statistical error; energies of J keep
         # the exact table
         if getattr(self, 'consEnergies', False) and Jbufname == 'dJ':
-            _lib.call('mi3_energies_cons', self._ptr(Jbufname), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
+            _lib.call('mi3_energies_cons', self._ptr(Jbufname), self.seqbufs[seqbufname].data_ptr(), buflen, nseq,
                       self.Ebufs[seqbufname].data_ptr(), self.L, self.q, self._ptr('cons'),
                       self._ptr('ws energies cons'), self._wsbytes('ws energies cons'), self._s)
         else:
-            _lib.call('mi3_energies', self._ptr(Jbufname), self.seqbufs[seqbufname].data_ptr(), nseq, nseq,
+            _lib.call('mi3_energies', self._ptr(Jbufname), self.seqbufs[seqbufname].data_ptr(), buflen, nseq,
                       self.Ebufs[seqbufname].data_ptr(), self.L, self.q, self._ptr('ws energies'),
                       self._wsbytes('ws energies'), self._s)
         return self.logevt('getEnergies', s)
@@ -454,47 +497,53 @@ class MCMCGPU:
     def min_buf(self, buf, wait_for=None):
         self.require('Jstep')
         buflen = int(np.prod(self.buf_spec[buf][1]))
+        if buf in ('E large', 'E tmp large', 'weights large'):
+            # the stored part only (the reference scans the whole buffer,
+            # which equals it once the buffer has been filled)
+            buflen = self.nstoredseqs
         s = self._begin()
         _lib.call('mi3_min_floats', self._ptr(buf), buflen, self._ptr('minout'), self._s)
         return self.logevt('min_buf', s)
 
     def weight_statistics(self, buf='main', wait_for=None):
         self.require('Jstep')
-        nseq = self.nseq[buf]
+        nseq = self._span(buf)[0]
         s = self._begin()
-        _lib.call('mi3_weight_stats', self._ptr('weights'), nseq, self._ptr('weightstats'),
+        _lib.call('mi3_weight_stats', self._ptr(self._wbufname(buf)), nseq, self._ptr('weightstats'),
                   self._ptr('weightstats64'), self._ptr('ws reduce'), self._wsbytes('ws reduce'), self._s)
         return self.logevt('weight_statistics', s)
 
     def dE_to_weights(self, buf='main', offset=0., wait_for=None):
         self.require('Jstep')
-        nseq = self.nseq[buf]
+        nseq = self._span(buf)[0]
         s = self._begin()
-        _lib.call('mi3_dE_to_weights', float(offset), self._ptr('E main'), self._ptr('weights'), nseq, self._s)
+        _lib.call('mi3_dE_to_weights', float(offset), self.Ebufs[buf].data_ptr(), self._ptr(self._wbufname(buf)),
+                  nseq, self._s)
         return self.logevt('dE_to_weights', s)
 
     def weights_fused(self, offset=0., buf='main'):
         """dE -> weights, minout = min(0, min dE), weightstats in one pass
         (same results as min_buf + dE_to_weights + weight_statistics)."""
         self.require('Jstep')
-        nseq = self.nseq[buf]
+        nseq = self._span(buf)[0]
         s = self._begin()
-        _lib.call('mi3_weights_fused', float(offset), self._ptr('E main'), self._ptr('weights'), nseq,
+        _lib.call('mi3_weights_fused', float(offset), self.Ebufs[buf].data_ptr(), self._ptr(self._wbufname(buf)), nseq,
                   self._ptr('minout'), self._ptr('weightstats'), self._ptr('weightstats64'),
                   self._ptr('ws reduce'), self._wsbytes('ws reduce'), self._s)
         return self.logevt('weights_fused', s)
 
     def fixed_beta_weights(self, ref_E, seqbufname='main', wait_for=None):
         self.require('Jstep')
-        nseq = self.nseq[seqbufname]
+        nseq = self._span(seqbufname)[0]
         s = self._begin()
         _lib.call('mi3_fixed_beta_weights', float(self.beta), float(ref_E), self.Ebufs[seqbufname].data_ptr(),
-                  self._ptr('weights'), nseq, self._s)
+                  self._ptr(self._wbufname(seqbufname)), nseq, self._s)
         return self.logevt('fixed_beta_weights', s)
 
     def weightedMarg(self, seqbufname='main', wait_for=None):
         self.require('Jstep')
-        nseq = self.nseq[seqbufname]
+        nseq, buflen = self._span(seqbufname)
+        wbuf = self._ptr(self._wbufname(seqbufname))
         s = self._begin()
         cons = self._ptr('cons') if getattr(self, 'consWmarg', False) else None
         tuned = getattr(self, 'wmarg_kernel', None)  # set by autotune.Autotuner.tune
@@ -502,11 +551,11 @@ class MCMCGPU:
         if tensor and cons is None:
             if 'ws wmarg tc' not in self.bufs:
                 self._setupWorkspace('ws wmarg tc', _lib.query('mi3_weighted_marg_tc_workspace', self.L, self.q))
-            _lib.call('mi3_weighted_marg_tc', self._ptr('weights'), self.seqbufs[seqbufname].data_ptr(), nseq,
+            _lib.call('mi3_weighted_marg_tc', wbuf, self.seqbufs[seqbufname].data_ptr(), buflen,
                       nseq, self._ptr('bi'), self.L, self.q, self._ptr('ws wmarg tc'),
                       self._wsbytes('ws wmarg tc'), self._ptr('status'), self._s)
         else:
-            _lib.call('mi3_weighted_marg', self._ptr('weights'), self.seqbufs[seqbufname].data_ptr(), nseq,
+            _lib.call('mi3_weighted_marg', wbuf, self.seqbufs[seqbufname].data_ptr(), buflen,
                       nseq, self._ptr('bi'), self.L, self.q, cons, self._ptr('ws wmarg'),
                       self._wsbytes('ws wmarg'), self._s)
         return self.logevt('weightedMarg', s)
@@ -665,13 +714,16 @@ class MCMCGPU:
             return FutureBuf(host, evt, post, self)
 
         shape = _full_shape(buftype, bufshape)
+        # the large buffers return only their stored part unless asked
+        # otherwise (mcmcGPU.py:845-867)
+        nret = self.nstoredseqs if (bufname in self.largebufs and truncateLarge) else None
 
         def post(b):
             a = b.numpy().view(_base_dtype(buftype))
             a = a[:int(np.prod(shape))].reshape(shape)
             if bufname.split()[0] == 'seq':
-                return self.unpackSeqs_4(a)
-            return a.copy()
+                return self.unpackSeqs_4(a)[:nret]
+            return a[:nret].copy()
         return FutureBuf(host, evt, post, self)
 
     def setBuf(self, bufname, buf, wait_for=None):
@@ -713,6 +765,8 @@ class MCMCGPU:
         self.logevt('setBuf', s, raw.size)
         if bufname.split()[0] == 'J':
             self.unpackedJ = None
+        if bufname == 'seq large':
+            self.nstoredseqs = bufshape[1]
         if bufname.split()[0] == 'seq':
             self.repackedSeqT[bufname.split()[1]] = False
         return evt
@@ -770,8 +824,75 @@ class MCMCGPU:
         nseq = self.nseq[seqbufname]
         self.setBuf('seq ' + seqbufname, np.tile(np.asarray(startseq, dtype='<u1'), (nseq, 1)))
 
+    def packedSeqs(self, bufname='main'):
+        """The device sequence buffer 'seq <bufname>' as a (SWORDS, nseq)
+        int32 tensor view (4 residues per word, walker-minor)."""
+        n = self.nseq[bufname]
+        return self.bufs['seq ' + bufname][:self.SWORDS * n].view(self.SWORDS, n)
+
+    def _largeCols(self, offset, n):
+        """Columns [offset, offset+n) of 'seq large' as a (SWORDS, n) view."""
+        return self.packedSeqs('large')[:, offset:offset + n]
+
     def storeSeqs(self, seqs=None, wait_for=None):
-        raise NotImplementedError("large sequence buffers are not part of the single-device path")
+        """Append sequences to the large buffer after the ones stored so far
+        (mcmcGPU.py:934-978): the walkers of 'seq main' when seqs is None, a
+        host (n, L) uint8 array, or -- not in the reference -- a packed
+        (SWORDS, n) device tensor, which may live on another device (a peer
+        copy), so walkers can be gathered without passing through the host."""
+        self.require('Large')
+        offset = self.nstoredseqs
+        if seqs is None:
+            src = self.packedSeqs('main')
+        elif isinstance(seqs, torch.Tensor):
+            if seqs.dim() != 2 or seqs.shape[0] != self.SWORDS or seqs.element_size() != 4:
+                raise ValueError(f"expected packed sequences of shape ({self.SWORDS}, n) with 4-byte words")
+            src = seqs.view(torch.int32)
+        else:
+            seqs = np.asarray(seqs)
+            if seqs.ndim != 2 or seqs.shape[1] != self.L:
+                raise Exception("Sequences have wrong length: {} vs {}".format(seqs.shape[-1], self.L))
+            if seqs.dtype != np.dtype('u1'):
+                raise ValueError("seqs must have u1 dtype")
+            src = torch.from_numpy(self.packSeqs_4(seqs).view(np.int32)).pin_memory()
+        n = int(src.shape[1])
+        if offset + n > self.nseq['large']:
+            raise Exception("cannot store seqs past end of large buffer")
+        s = self._begin()
+        with torch.cuda.stream(self.stream):
+            # a device tensor is read in this device's stream order: writes to
+            # it from another stream must be complete (GPU_node.gatherLarge
+            # waits for the source device first)
+            self._largeCols(offset, n).copy_(src, non_blocking=True)
+        evt = self.logevt('storeSeqs', s, 4 * self.SWORDS * n)
+        if not src.is_cuda:
+            # keep the pinned staging copy alive until the copy has run
+            self._pending_host.append(src)
+        self.nstoredseqs += n
+        self.repackedSeqT['large'] = False
+        return evt
+
+    def clearLargeSeqs(self):
+        """Forget the stored sequences (mcmcGPU.py:980-983)."""
+        self.require('Large')
+        self.nstoredseqs = 0
+        self.repackedSeqT['large'] = False
+
+    def restoreSeqs(self, offset=0, wait_for=None):
+        """Copy nseq['main'] stored sequences, from column `offset` of the
+        large buffer, back into 'seq main' (mcmcGPU.py:985-999, whose offset
+        is not defined in the reference; here it is an argument)."""
+        self.require('Large')
+        nseq = self.nseq['main']
+        if offset + nseq > self.nseq['large']:
+            raise Exception("cannot get seqs past end of large buffer")
+        if self.nstoredseqs < nseq:
+            raise Exception("not enough seqs stored in large buffer")
+        s = self._begin()
+        with torch.cuda.stream(self.stream):
+            self.packedSeqs('main').copy_(self._largeCols(offset, nseq), non_blocking=True)
+        self.repackedSeqT['main'] = False
+        return self.logevt('restoreSeqs', s, 4 * self.SWORDS * nseq)
 
     # ------------------------------------------------------------ checkpoints
     _STATE_BUFS = ('seq main', 'rngstates', 'randpos')

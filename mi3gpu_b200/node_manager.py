@@ -32,7 +32,10 @@ def skip_single(f):
 class GPU_node:
     def __init__(self, gpus):
         self.gpus = gpus
-        self.head_node = self
+
+    @property
+    def head_node(self):
+        return self  # one node (node_manager.py:47)
 
     @property
     def head_gpu(self):
@@ -44,7 +47,10 @@ class GPU_node:
 
     @property
     def nseq(self):
-        return {'main': sum(g.nseq['main'] for g in self.gpus)}
+        ret = {'main': sum(g.nseq['main'] for g in self.gpus)}
+        if 'large' in self.gpus[0].nseq:
+            ret['large'] = sum(g.nseq.get('large', 0) for g in self.gpus)
+        return ret
 
     @property
     def ngpus(self):
@@ -67,6 +73,65 @@ class GPU_node:
     def initJstep(self):
         for gpu in self.gpus:
             gpu.initJstep()
+
+    def initLargeBufs(self, nseq):
+        """Large sequence buffers on every device: one size for all, or one
+        per device (node_manager.py:87-93)."""
+        sizes = nseq if isinstance(nseq, (list, tuple)) else [nseq] * self.ngpus
+        for n, gpu in zip(sizes, self.gpus):
+            gpu.initLargeBufs(n)
+
+    def storeSeqs(self, seqs=None):
+        for gpu in self.gpus:
+            gpu.storeSeqs(seqs)
+
+    def clearLargeSeqs(self):
+        for gpu in self.gpus:
+            gpu.clearLargeSeqs()
+
+    def gatherLarge(self, target):
+        """Every device's walkers, in device order, into the large buffers of
+        `target` (a GPU_node over some of these devices, e.g. head_gpu), split
+        in order across its devices as np.split would.  The reference does
+        this through the host, collect('seq main') then
+        target.setSeqs('large', ...) (NewtonSteps.py:181-191); here the
+        columns are copied device to device.  Large buffers that do not exist
+        yet are created, one equal share per target device
+        (Mi3.py:450-457)."""
+        total = self.nwalkers
+        if 'large' not in target.gpus[0].nseq:
+            if total % target.ngpus:
+                raise Exception("{} walkers do not split over {} devices".format(total, target.ngpus))
+            target.initLargeBufs(total // target.ngpus)
+        sizes = [g.nseq['large'] for g in target.gpus]
+        if sum(sizes) != total:
+            raise Exception("Expected {} total sequences, got {}".format(sum(sizes), total))
+        self.wait()  # every device's walkers are final before they are read
+        target.clearLargeSeqs()
+        ti = 0
+        for g in self.gpus:
+            n, a = g.nseq['main'], 0
+            while a < n:
+                t = target.gpus[ti]
+                k = min(sizes[ti] - t.nstoredseqs, n - a)
+                if t is g and a == 0 and k == n:
+                    t.storeSeqs(None)  # this device's own walkers
+                else:
+                    t.storeSeqs(g.packedSeqs('main')[:, a:a + k])
+                a += k
+                if t.nstoredseqs == sizes[ti]:
+                    ti += 1
+        target.wait()
+
+    def shareJ(self, head):
+        """Copy the couplings of head's first device to every other device
+        (after a Newton phase that ran on `head` only)."""
+        src = head.gpus[0]
+        src.wait()
+        for g in self.gpus:
+            if g is not src:
+                g.setBuf('J', src.bufs['J'])
+        self.wait()
 
     def logProfile(self):
         for gpu in self.gpus:

@@ -27,6 +27,49 @@ class FakeMCMCGPU:
                      'seq main': np.zeros((oracle.swords(L), nseq), '<u4'), 'E main': np.zeros(nseq, '<f4'),
                      'minout': np.zeros(1, '<f4'), 'cprob': np.zeros((L, q - 1), '<f4')}
         self.calls = []
+        self.largebufs = []
+        self.nstoredseqs = 0
+
+    # sequence buffers: 'main', or the stored part of 'large'
+    def _seqs(self, name):
+        if name == 'main':
+            return self.bufs['seq main']
+        return self.bufs['seq ' + name][:, :self.nstoredseqs]
+
+    def _n(self, name):
+        return self.nseq['main'] if name == 'main' else self.nstoredseqs
+
+    @staticmethod
+    def _w(name):
+        return 'weights' if name == 'main' else 'weights ' + name
+
+    def initLargeBufs(self, n):
+        self.nseq['large'] = int(n)
+        self.bufs.update({'seq large': np.zeros((oracle.swords(self.L), n), '<u4'), 'E large': np.zeros(n, '<f4'),
+                          'E tmp large': np.zeros(n, '<f4'), 'weights large': np.zeros(n, '<f4')})
+        self.largebufs = ['seq large', 'E large', 'weights large']
+        self.nstoredseqs = 0
+
+    def packedSeqs(self, name='main'):
+        return self.bufs['seq ' + name].view(np.int32)
+
+    def storeSeqs(self, seqs=None):
+        if seqs is None:
+            seqs = self.bufs['seq main']
+        elif not isinstance(seqs, np.ndarray):  # a tensor of packed words
+            seqs = seqs.cpu().numpy()
+        seqs = np.asarray(seqs)
+        if seqs.dtype == np.uint8:
+            seqs = oracle.pack_seqs(seqs)
+        seqs = seqs.view('<u4')
+        n, off = seqs.shape[1], self.nstoredseqs
+        if off + n > self.nseq['large']:
+            raise Exception("cannot store seqs past end of large buffer")
+        self.bufs['seq large'][:, off:off + n] = seqs
+        self.nstoredseqs += n
+
+    def clearLargeSeqs(self):
+        self.nstoredseqs = 0
 
     def initMCMC(self, nsteps, rng_offset, rng_span):
         self.nsteps = int(nsteps)
@@ -56,14 +99,15 @@ class FakeMCMCGPU:
         self.calls.append('runMCMC')
 
     def calcEnergies(self, seqbufname, Jbufname='J'):
-        self.bufs['E main'] = oracle.energies_f64(self.bufs[Jbufname], self.bufs['seq main'], self.L,
-                                                  self.q).astype('<f4')
+        n = self._n(seqbufname)
+        self.bufs['E ' + seqbufname][:n] = oracle.energies_f64(self.bufs[Jbufname], self._seqs(seqbufname),
+                                                               self.L, self.q).astype('<f4')
 
     def calcBicounts(self, seqbufname):
-        self.bufs['bicount'] = oracle.bicounts(self.bufs['seq main'], self.L, self.q)
+        self.bufs['bicount'] = oracle.bicounts(self._seqs(seqbufname), self.L, self.q)
 
     def bicounts_to_bimarg(self, seqbufname='main'):
-        self.bufs['bi'] = oracle.bicounts_to_bimarg(self.bufs['bicount'], self.nwalkers)
+        self.bufs['bi'] = oracle.bicounts_to_bimarg(self.bufs['bicount'], self._n(seqbufname))
 
     def updateJ(self, gamma, pc, Jbuf='dJ'):
         self.bufs[Jbuf] = oracle.updatedJ(self.bufs['bi target'], self.bufs['bi'], gamma, pc, self.bufs[Jbuf])
@@ -72,23 +116,28 @@ class FakeMCMCGPU:
         self.bufs['dJ'] = oracle.reg_lz(self.bufs['bi'], gamma, pc, lJ, self.bufs['J'], self.bufs['dJ'], self.q, False)
 
     def min_buf(self, buf):
-        self.bufs['minout'][0] = oracle.min_floats(self.bufs[buf])
+        v = self.bufs[buf]
+        if buf in self.largebufs or buf == 'E tmp large':
+            v = v[:self.nstoredseqs]
+        self.bufs['minout'][0] = oracle.min_floats(v)
 
     def dE_to_weights(self, buf='main', offset=0.):
-        self.bufs['weights'] = oracle.dE_to_weights(offset, self.bufs['E main'])
+        n = self._n(buf)
+        self.bufs[self._w(buf)][:n] = oracle.dE_to_weights(offset, self.bufs['E ' + buf][:n])
 
     def weight_statistics(self, buf='main'):
-        self.bufs['weightstats'] = oracle.weight_stats(self.bufs['weights'])
-        self.bufs['weightstats64'] = oracle.weight_stats_f64(self.bufs['weights'])
+        w = self.bufs[self._w(buf)][:self._n(buf)]
+        self.bufs['weightstats'] = oracle.weight_stats(w)
+        self.bufs['weightstats64'] = oracle.weight_stats_f64(w)
 
     def weights_fused(self, offset=0., buf='main'):
-        self.min_buf('E main')
+        self.min_buf('E ' + buf)
         self.dE_to_weights(buf, offset)
         self.weight_statistics(buf)
 
     def weightedMarg(self, seqbufname='main'):
-        self.bufs['bi'] = oracle.weighted_marg_f64(self.bufs['weights'], self.bufs['seq main'], self.L,
-                                                   self.q).astype('<f4')
+        w = self.bufs[self._w(seqbufname)][:self._n(seqbufname)]
+        self.bufs['bi'] = oracle.weighted_marg_f64(w, self._seqs(seqbufname), self.L, self.q).astype('<f4')
 
     def renormalize_bimarg(self):
         self.bufs['bi'] = oracle.renormalize_bimarg(self.bufs['bi'], self.q)
@@ -102,6 +151,8 @@ class FakeMCMCGPU:
 
     def getBuf(self, name):
         v = self.bufs[name]
+        if name in self.largebufs:
+            v = v[..., :self.nstoredseqs]
         if name.startswith('seq'):
             return _Fut(oracle.unpack_seqs(v, self.L))
         return _Fut(np.array(v, copy=True))
@@ -109,7 +160,11 @@ class FakeMCMCGPU:
     def setBuf(self, name, v):
         if name.startswith('seq'):
             v = oracle.pack_seqs(v)
+        if hasattr(v, 'cpu'):  # a tensor from another device
+            v = v.cpu().numpy().view(self.bufs[name].dtype).reshape(self.bufs[name].shape)
         self.bufs[name] = np.array(v, copy=True)
+        if name == 'seq large':
+            self.nstoredseqs = self.bufs[name].shape[1]
 
     def fillBuf(self, name, val):
         self.bufs[name][...] = val

@@ -258,3 +258,104 @@ def test_bounded_wait_gives_up_and_context_survives(cuda):
         g.wait()
     with pytest.raises(_lib.Mi3Error):
         _lib.call('mi3_probe_bounded_wait', st.data_ptr(), 3_000_000_000, 0, waited.data_ptr(), s)
+
+
+@pytest.mark.parametrize("q", [5, 21])
+def test_large_buffer_kernels_match_main(cuda, q):
+    """The large sequence buffer (mcmcGPU.py:284-303, 934-999): walkers
+    stored from 'seq main' and from the host, read back truncated to the
+    stored part; energies, counts (both count kernels at q=5), weights,
+    weight statistics and weighted bimarginals over its stored columns
+    equal the same calls over a main buffer holding the same walkers, bit
+    for bit; restoreSeqs copies stored columns back into 'seq main'."""
+    from oracle import oracle
+    L, N = 37, 1024
+    n_extra = 1024
+    rng = np.random.default_rng(q)
+    J = potts.synthetic_ground_truth(L, q, seed=8, contact_sigma=0.4)
+    seqs = rng.integers(0, q, size=(N, L)).astype('<u1')
+    extra = rng.integers(0, q, size=(n_extra, L)).astype('<u1')
+    both = np.concatenate([seqs, extra])
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 3)
+    g.initMCMC(L, 0, 2 ** 62)
+    g.initJstep()
+    g.setBuf('seq main', seqs)
+    g.setBuf('J', J)
+    g.initLargeBufs(N + n_extra + 512)  # 512 columns left unused
+    g.storeSeqs()
+    g.storeSeqs(extra)
+    assert g.nstoredseqs == N + n_extra
+    np.testing.assert_array_equal(g.getBuf('seq large').read(), both)
+    assert g.getBuf('seq large', truncateLarge=False).read().shape == (N + n_extra + 512, L)
+    # the same walkers in the main buffer of a second device object
+    h = MCMCGPU((0, 0), L, q, N + n_extra, 512, None, 1024, 3)
+    h.initMCMC(L, 0, 2 ** 62)
+    h.initJstep()
+    h.setBuf('seq main', both)
+    h.setBuf('J', J)
+    for dev, buf in ((g, 'large'), (h, 'main')):
+        dev.calcEnergies(buf)
+    Eg, Eh = g.getBuf('E large').read(), h.getBuf('E main').read()
+    assert Eg.shape == (N + n_extra,)
+    np.testing.assert_array_equal(Eg, Eh)
+    for tensor in ([False, True] if q in MCMCGPU.TENSOR_COUNT_Q else [False]):
+        g.calcBicounts('large', tensor=tensor)
+        np.testing.assert_array_equal(g.getBuf('bicount').read(), oracle.bicounts(oracle.pack_seqs(both), L, q))
+    g.bicounts_to_bimarg('large')
+    h.calcBicounts('main')
+    h.bicounts_to_bimarg('main')
+    np.testing.assert_array_equal(g.getBuf('bi').read(), h.getBuf('bi').read())
+    dE = rng.normal(0, 0.5, size=N + n_extra).astype('<f4')
+    g.setBuf('E large', np.concatenate([dE, np.full(512, -50, '<f4')]))  # unused tail must not count
+    g.nstoredseqs = N + n_extra
+    h.setBuf('E main', dE)
+    for dev, buf, ebuf in ((g, 'large', 'E large'), (h, 'main', 'E main')):
+        dev.min_buf(ebuf)
+        dev.dE_to_weights(buf, 0.25)
+        dev.weight_statistics(buf)
+        dev.updateConsensus(buf)
+        dev.weightedMarg(buf)
+    assert g.getBuf('minout').read()[0] == h.getBuf('minout').read()[0] == min(0.0, float(dE.min()))
+    np.testing.assert_array_equal(g.getBuf('weights large').read(), h.getBuf('weights').read())
+    np.testing.assert_array_equal(g.getBuf('weightstats64').read(), h.getBuf('weightstats64').read())
+    np.testing.assert_array_equal(g.getBuf('bi').read(), h.getBuf('bi').read())
+    g.restoreSeqs(offset=n_extra)
+    np.testing.assert_array_equal(g.getBuf('seq main').read(), both[n_extra:n_extra + N])
+    with pytest.raises(Exception, match="past end"):
+        g.storeSeqs(extra[:600])
+
+
+@pytest.mark.parametrize("device_resident", [False, True])
+def test_head_gpu_newton_phase_equals_all(cuda, device_resident):
+    """distribute_jstep='head_gpu' on one device: the Newton phase over the
+    walkers copied into the large buffer takes the same steps to the same
+    couplings, bit for bit, as 'all' over the main buffer."""
+    L, q, N = 28, 5, 2048
+    truth = potts.synthetic_ground_truth(L, q, seed=17, contact_sigma=0.5)
+    seqs = np.random.default_rng(5).integers(0, q, size=(N, L)).astype('<u1')
+    res = []
+    for mode in ('all', 'head_gpu'):
+        g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 9)
+        node = GPU_node([g])
+        node.initMCMC(4 * L)
+        node.initJstep()
+        node.setSeqs('main', seqs)
+        node.setBuf('J', truth)
+        for _ in range(3):
+            node.runMCMC()
+        node.calcBicounts('main')
+        f0 = node.collect('bicount') / N
+        target = potts.mutation_pc(f0 * np.exp(np.random.default_rng(3).normal(0, 0.2, f0.shape)),
+                                   N).astype('<f4')
+        target /= target.sum(axis=1, keepdims=True)
+        node.setBuf('bi target', target)
+        p = NewtonSteps.Param(bimarg=target, gamma0=4e-3, newtonSteps=16, pcdamping=1e-2, fracNeff=0.5,
+                              nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep=mode,
+                              device_resident=device_resident)
+        steps, Jt, bt = NewtonSteps.iterNewton(p, f0, node, lambda *a: None, fused=True)
+        if device_resident:
+            Jt, bt = g.getBuf('J').read(), g.getBuf('bi').read()
+        res.append((steps, Jt, bt))
+    assert res[0][0] == res[1][0] >= 1
+    np.testing.assert_array_equal(res[0][1], res[1][1])
+    np.testing.assert_array_equal(res[0][2], res[1][2])

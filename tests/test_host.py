@@ -124,6 +124,108 @@ def test_iterNewton_over_fake_device_moves_toward_target():
     np.testing.assert_array_equal(J2, trialJ)
 
 
+def _two_device_node(L, q, n_per, seqs, J, target):
+    gs = [FakeMCMCGPU(L, q, n_per, seed=2 + k, gpunum=k) for k in range(2)]
+    node = GPU_node(gs)
+    node.initMCMC(4 * L)
+    node.initJstep()
+    node.setSeqs('main', seqs)
+    node.setBuf('J', J)
+    node.setBuf('bi target', target)
+    return node
+
+
+@pytest.mark.parametrize("device_resident", [False, True])
+def test_head_gpu_newton_phase_equals_one_device_over_all_walkers(device_resident):
+    """distribute_jstep='head_gpu' (NewtonSteps.py:181-195): two devices'
+    walkers gathered, in device order, into the head device's large buffer;
+    the Newton phase there takes the same steps to the same couplings, bit
+    for bit, as one device holding all walkers in its main buffer, and the
+    other device receives the new J."""
+    L, q, n_per = 8, 3, 512
+    N = 2 * n_per
+    rng = np.random.default_rng(4)
+    J = potts.synthetic_ground_truth(L, q, seed=5, contact_sigma=0.4)
+    seqs = rng.integers(0, q, size=(N, L)).astype('<u1')
+    f0 = oracle.bicounts(oracle.pack_seqs(seqs), L, q) / N
+    target = potts.mutation_pc(f0 * np.exp(rng.normal(0, 0.2, f0.shape)), N).astype('<f4')
+    target /= target.sum(axis=1, keepdims=True)
+    node = _two_device_node(L, q, n_per, seqs, J, target)
+    p = _param(L, q, N, target, J, newtonSteps=12)
+    p.update(distribute_jstep='head_gpu', device_resident=device_resident)
+    logs = []
+    steps, Jt, bt = NewtonSteps.iterNewton(p, f0, node, logs.append)
+    assert "Transferring sequences to gpu 0" in logs
+    head = node.gpus[0]
+    assert head.nstoredseqs == N
+    np.testing.assert_array_equal(head.getBuf('seq large').read(), seqs)
+    if device_resident:
+        Jt, bt = head.bufs['J'].copy(), head.bufs['bi'].copy()
+        np.testing.assert_array_equal(node.gpus[1].bufs['J'], Jt)
+
+    one = GPU_node([FakeMCMCGPU(L, q, N, seed=2)])
+    one.initMCMC(4 * L)
+    one.initJstep()
+    one.setSeqs('main', seqs)
+    one.setBuf('J', J)
+    one.setBuf('bi target', target)
+    s1, J1, b1 = NewtonSteps.iterNewton(_param(L, q, N, target, J, newtonSteps=12), f0, one, lambda *a: None)
+    assert steps == s1
+    np.testing.assert_array_equal(Jt, J1)
+    np.testing.assert_array_equal(bt, b1)
+
+
+def test_head_node_newton_phase_equals_all_on_the_same_devices():
+    """distribute_jstep='head_node' on one node: the walkers pass through
+    the large buffers split as np.split would, which for one node is the
+    same split as the main buffers, so the result equals 'all' bit for
+    bit."""
+    L, q, n_per = 6, 3, 512
+    N = 2 * n_per
+    rng = np.random.default_rng(7)
+    J = potts.synthetic_ground_truth(L, q, seed=6, contact_sigma=0.4)
+    seqs = rng.integers(0, q, size=(N, L)).astype('<u1')
+    f0 = oracle.bicounts(oracle.pack_seqs(seqs), L, q) / N
+    target = potts.mutation_pc(f0 * np.exp(rng.normal(0, 0.2, f0.shape)), N).astype('<f4')
+    target /= target.sum(axis=1, keepdims=True)
+    res = []
+    for mode in ('all', 'head_node'):
+        node = _two_device_node(L, q, n_per, seqs, J, target)
+        p = _param(L, q, N, target, J, newtonSteps=10)
+        p.update(distribute_jstep=mode)
+        res.append(NewtonSteps.iterNewton(p, f0, node, lambda *a: None))
+    assert res[0][0] == res[1][0]
+    np.testing.assert_array_equal(res[0][1], res[1][1])
+    np.testing.assert_array_equal(res[0][2], res[1][2])
+
+
+def test_large_buffer_bookkeeping_and_errors():
+    """storeSeqs appends after the stored part, clearLargeSeqs forgets it,
+    overfilling raises (mcmcGPU.py:934-983); an unknown distribute_jstep
+    is rejected."""
+    L, q, n = 6, 3, 512
+    g = FakeMCMCGPU(L, q, n, seed=1)
+    node = GPU_node([g])
+    rng = np.random.default_rng(2)
+    seqs = rng.integers(0, q, size=(n, L)).astype('<u1')
+    node.setSeqs('main', seqs)
+    node.initLargeBufs(n + n // 2)
+    assert node.nseq == {'main': n, 'large': n + n // 2}
+    node.storeSeqs()
+    extra = rng.integers(0, q, size=(n // 2, L)).astype('<u1')
+    g.storeSeqs(extra)
+    np.testing.assert_array_equal(g.getBuf('seq large').read(), np.concatenate([seqs, extra]))
+    with pytest.raises(Exception, match="past end"):
+        g.storeSeqs(extra[:1])
+    node.clearLargeSeqs()
+    assert g.nstoredseqs == 0
+    p = _param(L, q, n, np.zeros((L * (L - 1) // 2, q * q), '<f4'), np.zeros((L * (L - 1) // 2, q * q), '<f4'))
+    p.update(distribute_jstep='everywhere')
+    node.initJstep()
+    with pytest.raises(ValueError, match="distribute_jstep"):
+        NewtonSteps.iterNewton(p, None, node, lambda *a: None)
+
+
 def test_newtonMCMC_rounds_over_fake_device():
     L, q, N = 6, 3, 512
     J0 = np.zeros((L * (L - 1) // 2, q * q), '<f4')

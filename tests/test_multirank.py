@@ -83,7 +83,7 @@ def test_two_rank_reductions_match_single_process():
         np.testing.assert_array_equal(r["first_state"], expect)
 
 
-def _newton_worker(rank, world, port, out):
+def _newton_worker(rank, world, port, out, mode='all', device_resident=False):
     """iterNewton through RankNode over two FakeMCMCGPU halves of the
     walkers; rank 0 reports the result."""
     import torch.distributed as dist
@@ -109,11 +109,18 @@ def _newton_worker(rank, world, port, out):
     target /= target.sum(axis=1, keepdims=True)
     node.setBuf('bi target', target)
     p = NewtonSteps.Param(bimarg=target, gamma0=4e-3, newtonSteps=12, pcdamping=1e-2, fracNeff=0.5,
-                          nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all')
+                          nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep=mode,
+                          device_resident=device_resident)
     steps, Jt, bt = NewtonSteps.iterNewton(p, f0, node, lambda *a: None)
+    if device_resident:  # J += dJ in place, then shared from rank 0
+        Jt, bt = g.bufs['J'].copy(), g.bufs['bi'].copy()
     out.put(dict(rank=rank, steps=steps, J=Jt, bi=bt, f0=f0, target=target))
     dist.barrier()
     dist.destroy_process_group()
+
+
+def _newton_worker_head_gpu(rank, world, port, out):
+    _newton_worker(rank, world, port, out, mode='head_gpu', device_resident=True)
 
 
 def _guarded(fn, rank, world, port, out):
@@ -165,6 +172,45 @@ def test_two_rank_newton_phase_matches_single_process():
     assert steps == res[0]["steps"]
     np.testing.assert_allclose(res[0]["J"], Jt, rtol=1e-4, atol=1e-6)
     np.testing.assert_allclose(res[0]["bi"], bt, rtol=1e-4, atol=1e-6)
+
+
+def test_two_rank_head_gpu_newton_phase_equals_single_process():
+    """distribute_jstep='head_gpu' over two gloo ranks: every rank gathers
+    all walkers (one broadcast per rank) and runs the head device's Newton
+    phase with no collective in the loop; the couplings, bimarginals and
+    step count equal, bit for bit, those of one process holding all walkers,
+    and rank 0's J is shared with rank 1."""
+    from mi3gpu_b200 import GPU_node, NewtonSteps, potts
+    from tests.fake_device import FakeMCMCGPU
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_guarded, args=(_newton_worker_head_gpu, r, 2, port, out)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted([out.get(timeout=180) for _ in range(2)], key=lambda r: r["rank"])
+    assert not any("error" in r for r in res), res
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    np.testing.assert_array_equal(res[0]["J"], res[1]["J"])
+    assert res[0]["steps"] == res[1]["steps"]
+    L, q, N = 8, 3, 1024
+    J = potts.synthetic_ground_truth(L, q, seed=5, contact_sigma=0.4)
+    seqs = np.random.default_rng(4).integers(0, q, size=(N, L)).astype('<u1')
+    g = FakeMCMCGPU(L, q, N, seed=2)
+    node = GPU_node([g])
+    node.initMCMC(4 * L)
+    node.initJstep()
+    node.setSeqs('main', seqs)
+    node.setBuf('J', J)
+    node.setBuf('bi target', res[0]["target"])
+    p = NewtonSteps.Param(bimarg=res[0]["target"], gamma0=4e-3, newtonSteps=12, pcdamping=1e-2, fracNeff=0.5,
+                          nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all')
+    steps, Jt, bt = NewtonSteps.iterNewton(p, res[0]["f0"], node, lambda *a: None)
+    assert steps == res[0]["steps"]
+    np.testing.assert_array_equal(res[0]["J"], Jt)
+    np.testing.assert_array_equal(res[0]["bi"], bt)
 
 
 def _rounds_worker(rank, world, port, out):
