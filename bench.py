@@ -470,6 +470,79 @@ def run_kernels(args):
                       "bf16_peak_tflops": peaks.get("bf16_tflops", 1590.0), "rows": rows}))
 
 
+def run_msa(args):
+    """The run directories' 'seqs' files at L=232 q=21 with 2^20 walkers.
+    Kernels: walkers -> text lines (mi3_seqs_to_text) and back
+    (mi3_text_to_seqs), timed with CUDA events, against the HBM roofline:
+    per walker 4*SWORDS bytes of packed words one way and L+1 bytes of text
+    the other (both buffers exceed L2).  End to end: a file written or
+    loaded through GPU_node.writeSeqs / loadSeqs (device formatting,
+    parallel bzip2) against the reference's route for the same file
+    (collect the walkers to the host, format them in numpy, one bzip2 stream;
+    loadSeqs then setSeqs), both producing the same bytes."""
+    import tempfile
+    import torch
+    from mi3gpu_b200 import GPU_node, MCMCGPU, _lib, seqload
+    L, q, N = 232, 21, 1 << 20
+    sw = (L - 1) // 4 + 1
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 1)
+    node = GPU_node([g])
+    seqs = np.random.default_rng(0).integers(0, q, size=(N, L)).astype('u1')
+    node.setSeqs('main', seqs)
+    alpha = seqload.alpha21.encode()
+    text = torch.empty(N * (L + 1), dtype=torch.uint8, device=g.device)
+    back = torch.empty_like(g.bufs['seq main'])
+    st = torch.zeros(1, dtype=torch.int32, device=g.device)
+    bad = torch.zeros(1, dtype=torch.int64, device=g.device)
+    s = g.stream.cuda_stream
+    fmt_ms = time_call(lambda: _lib.call("mi3_seqs_to_text", g._ptr('seq main'), N, N, L, alpha, len(alpha),
+                                         text.data_ptr(), st.data_ptr(), s), 20, g.stream)
+    parse_ms = time_call(lambda: _lib.call("mi3_text_to_seqs", text.data_ptr(), N, L + 1, 0, L, alpha, len(alpha),
+                                           back.data_ptr(), N, 0, bad.data_ptr(), s), 20, g.stream)
+    assert torch.equal(back, g.bufs['seq main']) and int(st.item()) == 0 and int(bad.item()) == -1
+    nbytes = N * (4 * sw + L + 1)
+    out = {"mode": "msa", "config": {"workload": f"walkers <-> MSA text, L={L} q={q} walkers={N}",
+                                     "l2": "buffers larger than L2"},
+           "seqs_to_text_ms": fmt_ms, "text_to_seqs_ms": parse_ms,
+           "seqs_to_text_GBps": nbytes / fmt_ms / 1e6, "text_to_seqs_GBps": nbytes / parse_ms / 1e6,
+           "hbm_peak_GBps": hbm, "seqs_to_text_frac": nbytes / fmt_ms / 1e6 / hbm,
+           "text_to_seqs_frac": nbytes / parse_ms / 1e6 / hbm, "bytes_per_walker": 4 * sw + L + 1,
+           "host_cores": os.cpu_count()}
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        for zipf in (False, True):
+            tag = "bz2" if zipf else "plain"
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            node.writeSeqs(d / f"dev_{tag}", zipf=zipf)
+            out[f"write_{tag}_device_s"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            host = node.collect('seq main')
+            seqload.write_text(d / f"host_{tag}", [seqload.format_lines(host, seqload.alpha21)], zipf, threads=1)
+            out[f"write_{tag}_host_s"] = time.perf_counter() - t0
+            same = (d / f"dev_{tag}").read_bytes() == (d / f"host_{tag}").read_bytes() if not zipf else None
+            if zipf:
+                import bz2
+                same = bz2.decompress((d / "dev_bz2").read_bytes()) == bz2.decompress((d / "host_bz2").read_bytes())
+            out[f"write_{tag}_same_bytes"] = bool(same)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        node.loadSeqs(d / "dev_plain")
+        torch.cuda.synchronize()
+        out["load_plain_device_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        host, _, _ = seqload.loadSeqs(d / "dev_plain")
+        node.setSeqs('main', host)
+        torch.cuda.synchronize()
+        out["load_plain_host_s"] = time.perf_counter() - t0
+    out["write_bz2_speedup"] = out["write_bz2_host_s"] / out["write_bz2_device_s"]
+    out["write_plain_speedup"] = out["write_plain_host_s"] / out["write_plain_device_s"]
+    out["load_plain_speedup"] = out["load_plain_host_s"] / out["load_plain_device_s"]
+    print(json.dumps(out))
+
+
 def run_batched(args):
     """Many independent problems (L ~ U[50,300], q in {4, 8, 21}, walkers
     log-uniform in [2^14, 2^17]): quasi-Newton rounds with one CUDA-graph
@@ -758,7 +831,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--newton-steps", type=int, default=10, help="quasi-Newton steps to time (0: skip)")
-    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned", "batched", "graph_small"],
+    ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned", "batched", "graph_small",
+                                                           "msa"],
                     help="inference: run full quasi-Newton rounds and report s/iter and SSR")
     ap.add_argument("--rounds", type=int, default=4, help="inference rounds (--mode inference)")
     ap.add_argument("--msa", type=int, default=1 << 16, help="synthetic MSA size (--mode inference)")
@@ -811,6 +885,9 @@ def main():
         return
     if args.mode == "graph_small":
         run_graph_small(args)
+        return
+    if args.mode == "msa":
+        run_msa(args)
         return
     out, J = run_gpu(args)
     if rank == 0 and world == 1 and not args.no_inference:

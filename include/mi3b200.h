@@ -240,6 +240,30 @@ int mi3_weighted_marg_tc(const float *weights, const uint32_t *seqmem, uint32_t 
                          float *bimarg, uint32_t L, uint32_t q, void *workspace, size_t ws_bytes,
                          int32_t *status, void *stream);
 
+/* The walkers as the lines of an MSA text file, in the format of the
+ * reference's writeSeqs (mi3gpu/utils/seqload.py:378-411, no id field):
+ * line n = alpha[residue] for the L sites of walker n, then '\n', so text
+ * (device, 16-byte aligned) receives nseq*(L+1) bytes.  alpha is a HOST
+ * pointer to nalpha <= 256 characters.  A residue >= nalpha is written as
+ * '?' and *status (int32, device, zeroed by the caller) receives
+ * MI3_STATUS_BAD_INPUT. */
+int mi3_seqs_to_text(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t L,
+                     const char *alpha, uint32_t nalpha, uint8_t *text, int32_t *status, void *stream);
+
+/* MSA text lines back into walkers, the translation of the reference's
+ * loadSeqs (seqload.py:91-133, 196-246, 259-352): nseq lines of line_len =
+ * id_len + L + 1 bytes each (an id field of id_len bytes whose last byte is
+ * a space when id_len > 0, the L residues, '\n') from text (device,
+ * 16-byte aligned; headers and end-of-file fix-ups are the caller's) into
+ * columns [n0, n0+nseq) of seqmem.  alpha: HOST pointer, nalpha <= 255
+ * characters; a character maps to its (last) index in alpha.  *first_bad
+ * (uint64, device) receives the index of the first malformed line -- no
+ * '\n' at its end, no space ending its id field, or a character not in
+ * alpha -- or UINT64_MAX; the words of malformed lines are undefined. */
+int mi3_text_to_seqs(const uint8_t *text, uint32_t nseq, uint32_t line_len, uint32_t id_len, uint32_t L,
+                     const char *alpha, uint32_t nalpha, uint32_t *seqmem, uint32_t buflen, uint32_t n0,
+                     uint64_t *first_bad, void *stream);
+
 /* Bytes of workspace mi3_site_consensus needs: 8*L*q. */
 size_t mi3_site_consensus_workspace(uint32_t L, uint32_t q);
 

@@ -13,6 +13,7 @@ NewtonSteps (:595-608), singleNewton (:109-124) -- and drives a GPU_node
     in the reference either (undefined readGPUbufs / markSeqs / split).
 """
 import time
+from pathlib import Path
 
 import numpy as np
 from scipy.stats import spearmanr
@@ -197,7 +198,14 @@ def track_main_bufs(param, gpus, savedir=None, step=None):
             np.save(savedir / f'bimarg_{step}', bimarg_model)
         if 'E' in (param.tracked or ''):
             np.save(savedir / f'energies_{step}', energies)
+        if 'seq' in (param.tracked or ''):
+            gpus.writeSeqs(savedir / f'seqs_{step}', 'main', _alpha(param), zipf=True)
     return energies, bimarg_model
+
+
+def _alpha(param):
+    from .seqload import default_alpha
+    return param.alpha if param.alpha is not None else default_alpha(param.q)
 
 
 def runMCMC(gpus, couplings, runName, param, log):
@@ -360,18 +368,21 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
     log(f"Total MCMC running time: {dt:.1f} s    ({MC_s:.3g} MC/s)")
 
     seqs = None
-    if not dev or outdir is not None or param.reseed in ('single_random', 'single_best'):
+    if not dev or param.reseed in ('single_random', 'single_best'):
         seqs = gpus.collect('seq main')
     if dev:
         ssr, line = _device_stats_line(runName, Jstep, gpus, sampledenergies, e_rho)
-        log(line)
         if outdir is not None:
             bimarg_model = gpus.head_gpu.collect('bi')
     else:
-        log(printstats(runName, Jstep, bimarg_target, bimarg_model, couplings, sampledenergies, e_rho))
+        line = printstats(runName, Jstep, bimarg_target, bimarg_model, couplings, sampledenergies, e_rho)
         ssr = np.sum((bimarg_target - bimarg_model) ** 2)
+    log(line)
     if outdir is not None:
-        np.save(outdir / runName / 'seqs', seqs)
+        # writeStatus (NewtonSteps.py:76-94): the statistics, and the walkers
+        # as a bzip2 MSA in the reference's format, formatted on the devices
+        (outdir / runName / 'info.txt').write_text(line)
+        gpus.writeSeqs(outdir / runName / 'seqs', 'main', _alpha(param), zipf=True)
 
     ns_delta = param.newton_delta or 32
     if param.last_ssr is not None:
@@ -388,7 +399,45 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
                              round_s=time.time() - start_time)
     param.newtonSteps = min(2048, Jsteps + ns_delta)
     log(f"Increasing newtonsteps to {param.newtonSteps}")
+    if outdir is not None:
+        (outdir / runName / 'nsteps').write_text(str(Jsteps))
     return Jstep + Jsteps, seqs, sampledenergies, newJ
+
+
+def run_name_format(mcmcsteps):
+    """Run directory names, run_ with ceil(log10(rounds)) digits
+    (NewtonSteps.py:733)."""
+    return f'run_{{:0{int(np.ceil(np.log10(mcmcsteps)))}d}}'
+
+
+def last_run(outdir):
+    """The last run directory of an output directory and what the
+    reference's --finish reads from it (Mi3.py:377-390): (run directory,
+    its round index, its newtonsteps, its jstep)."""
+    runs = sorted(Path(outdir).glob('run_*'))
+    if not runs:
+        raise Exception(f"Did not find any runs in {outdir}")
+    rundir = runs[-1]
+    start = int(str(rundir).rpartition('_')[2])
+    return rundir, start, int((rundir / 'newtonsteps').read_text()), int((rundir / 'jstep').read_text())
+
+
+def finish(param, gpus, log):
+    """Continue an interrupted run from its output directory, as the
+    reference's `--finish` does (Mi3.py:373-402): the last run directory's
+    round is run again from its J.npy and newtonsteps, with its jstep, and
+    its walkers ('seqs', when the round got that far) loaded into the
+    devices; rounds then continue up to param.mcmcsteps.  The walkers' RNG
+    streams and the site list start afresh, as in the reference (a
+    checkpoint, checkpoint.py, continues bit for bit instead)."""
+    rundir, start, newtonsteps, jstep = last_run(param.outdir)
+    log(f"Continuing from {rundir}")
+    param.couplings = np.load(rundir / 'J.npy')
+    param.newtonSteps = newtonsteps
+    if (rundir / 'seqs').exists():
+        gpus.loadSeqs(rundir / 'seqs', 'main', _alpha(param))
+        param.init_indep = False  # reseed 'none' keeps the loaded walkers
+    return newtonMCMC(param, gpus, start, jstep, log)
 
 
 def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
@@ -413,8 +462,9 @@ def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
         log(f"Continuing from a checkpoint before round {start_run}")
     if param.device_resident:
         gpus.setBuf('J', np.asarray(J, dtype='<f4'))
+    name_fmt = run_name_format(param.mcmcsteps)
     for i in range(start_run, param.mcmcsteps):
-        runname = f'run_{i:02d}'
+        runname = name_fmt.format(i)
         first = fresh and i == start_run
         seed = None
         if param.seedseq is not None:
@@ -427,6 +477,10 @@ def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
         elif param.reseed == 'single_best' and seqs is not None:
             seed = seqs[np.argmin(es)]
         if seed is not None:
+            if param.outdir is not None:
+                rundir = Path(param.outdir) / runname
+                rundir.mkdir(parents=True, exist_ok=True)
+                (rundir / 'seedseq').write_text("".join(_alpha(param)[c] for c in seed))
             gpus.fillSeqs(seed)
         elif param.reseed == 'independent' or (param.reseed == 'none' and first and param.init_indep):
             # 'none' keeps the walkers from round to round; they start from

@@ -127,6 +127,27 @@ class RankNode(GPU_node):
             g.storeSeqs(buf)
         g.wait()
 
+    @property
+    def is_writer(self):
+        return self.rank == 0
+
+    def collectText(self, bufname='main', alpha=None):
+        """Every rank's walkers as MSA text lines, in rank order."""
+        return self._gather(self.gpus[0].getSeqsText(bufname, alpha).read())
+
+    def loadSeqs(self, fn, bufname='main', alpha=None, zipf=None):
+        """This rank's share of an MSA file: lines from the sum of the
+        previous ranks' walkers on (every rank reads the file)."""
+        from . import seqload
+        g = self.gpus[0]
+        msa = seqload.read_msa(fn, alpha if alpha is not None else seqload.default_alpha(g.q), zipf)
+        if msa.nseq != self.nwalkers or msa.eof_error is not None:
+            if msa.eof_error is not None:
+                seqload.check(msa)
+            raise Exception("Expected {} total sequences, got {}".format(self.nwalkers, msa.nseq))
+        g.setSeqsText(bufname, msa, sum(self.walkers_per_rank[:self.rank]))
+        return msa.headers
+
     def shareJ(self, head):
         """Rank 0's couplings to every rank (after the head-device phase)."""
         g = self.gpus[0]

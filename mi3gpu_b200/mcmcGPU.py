@@ -22,7 +22,7 @@ import numpy as np
 from numpy.random import RandomState
 import torch
 
-from . import _lib
+from . import _lib, seqload
 
 rng_buf_mul = 1024  # position-list blocks of 1024*nsteps (mcmcGPU.py:30)
 
@@ -893,6 +893,95 @@ class MCMCGPU:
             self.packedSeqs('main').copy_(self._largeCols(offset, nseq), non_blocking=True)
         self.repackedSeqT['main'] = False
         return self.logevt('restoreSeqs', s, 4 * self.SWORDS * nseq)
+
+    # ------------------------------------------------------------ MSA text
+    def _text_scratch(self, nbytes):
+        """Device byte buffer of at least nbytes (grown, never shrunk)."""
+        buf = self.bufs.get('text')
+        if buf is None or buf.numel() < nbytes:
+            with torch.cuda.device(self.device):
+                buf = torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=self.device)
+            self.bufs['text'] = buf
+            if 'status text' not in self.bufs:
+                self._setupBuffer('status text', '<i4', (1,))
+                self._setupBuffer('first bad', '<u8', (1,))
+        return buf
+
+    def getSeqsText(self, bufname='main', alpha=None):
+        """The walkers of 'seq <bufname>' as the lines of an MSA file in the
+        reference's format (mi3_seqs_to_text; seqload.py:378-411): a
+        FutureBuf whose read() returns nseq*(L+1) uint8 bytes (for 'large',
+        the stored part).  alpha defaults to seqload.default_alpha(q)."""
+        alpha = seqload._as_bytes(alpha if alpha is not None else seqload.default_alpha(self.q))
+        nseq, buflen = self._span(bufname)
+        nbytes = nseq * (self.L + 1)
+        dev = self._text_scratch(nbytes)
+        self.fillBuf('status text', 0)
+        s = self._begin()
+        _lib.call('mi3_seqs_to_text', self.seqbufs[bufname].data_ptr(), buflen, nseq, self.L, alpha, len(alpha),
+                  dev.data_ptr(), self._ptr('status text'), self._s)
+        host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        st = torch.empty(1, dtype=torch.int32, pin_memory=True)
+        with torch.cuda.stream(self.stream):
+            host.copy_(dev[:nbytes], non_blocking=True)
+            st.copy_(self.bufs['status text'], non_blocking=True)
+        evt = torch.cuda.Event()
+        evt.record(self.stream)
+        self.logevt('getSeqsText', s, nbytes)
+
+        def post(b):
+            if int(st[0]) != 0:
+                raise ValueError("a walker holds a residue outside the alphabet {!r}".format(alpha.decode()))
+            return b.numpy()
+        return FutureBuf(host, evt, post, self)
+
+    def _textToSeqs(self, msa, start, n, bufname, n0):
+        if msa.L != self.L:
+            raise Exception("Sequences have wrong length: {} vs {}".format(msa.L, self.L))
+        if msa.eof_error is not None or start + n > msa.nseq:
+            seqload.check(msa)  # raises the reference's error for this file
+            raise Exception("need {} sequences from line {}, the file has {}".format(n, start, msa.nseq))
+        nbytes = n * msa.line_len
+        dev = self._text_scratch(nbytes)
+        host = self._staging_for('text', nbytes)
+        host.numpy()[:] = msa.body[start * msa.line_len:(start + n) * msa.line_len]
+        s = self._begin()
+        with torch.cuda.stream(self.stream):
+            dev[:nbytes].copy_(host, non_blocking=True)
+        evt = torch.cuda.Event()
+        evt.record(self.stream)
+        self._staging['text'][1] = evt
+        _lib.call('mi3_text_to_seqs', dev.data_ptr(), n, msa.line_len, msa.id_len, self.L, msa.alpha,
+                  len(msa.alpha), self.seqbufs[bufname].data_ptr(), self.nseq[bufname], n0,
+                  self._ptr('first bad'), self._s)
+        self.logevt('setSeqsText', s, nbytes)
+        with torch.cuda.stream(self.stream):
+            first = int(self.bufs['first bad'].cpu()[0])
+        if first != -1:  # UINT64_MAX: every line is well formed
+            seqload.check(msa)
+            raise ValueError("Sequence {} is malformed".format(start + first + 1))
+        self.repackedSeqT[bufname] = False
+
+    def setSeqsText(self, bufname, msa, start=0):
+        """Lines [start, start + nseq) of a parsed MSA file (seqload.MSAText,
+        from seqload.read_msa) into 'seq <bufname>', translated on the
+        device (mi3_text_to_seqs).  A malformed file raises the reference's
+        error for it (seqload.py:196-336).  For 'large' the lines fill the
+        whole buffer and become its stored part."""
+        n = self.nseq[bufname]
+        self._textToSeqs(msa, start, n, bufname, 0)
+        if bufname == 'large':
+            self.nstoredseqs = n
+
+    def storeSeqsText(self, msa, start=0, n=None):
+        """Append lines [start, start + n) of a parsed MSA file to the large
+        buffer after its stored part (storeSeqs for file input)."""
+        self.require('Large')
+        n = msa.nseq - start if n is None else n
+        if self.nstoredseqs + n > self.nseq['large']:
+            raise Exception("cannot store seqs past end of large buffer")
+        self._textToSeqs(msa, start, n, 'large', self.nstoredseqs)
+        self.nstoredseqs += n
 
     # ------------------------------------------------------------ checkpoints
     _STATE_BUFS = ('seq main', 'rngstates', 'randpos')

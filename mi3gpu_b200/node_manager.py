@@ -9,6 +9,8 @@ for completeness rather than speed.
 """
 import numpy as np
 
+from . import seqload
+
 
 def sumarr(arrlist):
     tot = arrlist[0].copy()
@@ -122,6 +124,40 @@ class GPU_node:
                 if t.nstoredseqs == sizes[ti]:
                     ti += 1
         target.wait()
+
+    # ------------------------------------------------------ MSA files
+    is_writer = True  # this process writes the files
+
+    def collectText(self, bufname='main', alpha=None):
+        """Every device's walkers as MSA text lines, in device order."""
+        futs = [g.getSeqsText(bufname, alpha) for g in self.gpus]
+        return [f.read() for f in futs]
+
+    def writeSeqs(self, fn, bufname='main', alpha=None, zipf=None, headers=None, write_param=False):
+        """Write the walkers as an MSA file in the reference's format (what
+        writeSeqs(fn, collect('seq main'), alpha) writes, seqload.py:353-411),
+        formatting the lines on the devices."""
+        alpha = alpha if alpha is not None else seqload.default_alpha(self.gpus[0].q)
+        parts = self.collectText(bufname, alpha)
+        if self.is_writer:
+            seqload.write_text(fn, [seqload.header_bytes(alpha, headers, write_param)] + parts, zipf)
+
+    def loadSeqs(self, fn, bufname='main', alpha=None, zipf=None):
+        """Fill 'seq <bufname>' of every device, in order, from an MSA file
+        (as setSeqs(bufname, loadSeqs(fn)[0]) would), parsing the lines on
+        the devices; returns the file's headers."""
+        msa = fn if isinstance(fn, seqload.MSAText) else seqload.read_msa(
+            fn, alpha if alpha is not None else seqload.default_alpha(self.gpus[0].q), zipf)
+        total = self.nseq[bufname]
+        if msa.nseq != total or msa.eof_error is not None:
+            if msa.eof_error is not None:
+                seqload.check(msa)
+            raise Exception("Expected {} total sequences, got {}".format(total, msa.nseq))
+        start = 0
+        for g in self.gpus:
+            g.setSeqsText(bufname, msa, start)
+            start += g.nseq[bufname]
+        return msa.headers
 
     def shareJ(self, head):
         """Copy the couplings of head's first device to every other device

@@ -353,3 +353,41 @@ def bimarg_stats_f64(target, model, J=None):
         xm = float(np.sum(Jd * (m - indep(m))))
         xt = float(np.sum(Jd * (t - indep(t))))
     return (float(np.sum(d * d)), float(np.max(np.abs(d))), rel, cnt, xm, xt)
+
+
+# ---------------------------------------------------------------------------
+# MSA text lines (mi3gpu/utils/seqload.py), restated in numpy.
+
+def seqs_to_text(seqmem, L, alpha):
+    """The lines writeSeqs writes for packed walkers (seqload.py:378-411,
+    no id field): alpha[residue] for each site, then b'\\n'.  Returns
+    (bytes as uint8 array of N*(L+1), any residue >= len(alpha)); such a
+    residue is written as '?'."""
+    seqs = unpack_seqs(seqmem, L)
+    a = np.frombuffer(alpha.encode() if isinstance(alpha, str) else alpha, np.uint8)
+    table = np.full(256, ord('?'), np.uint8)
+    table[:a.size] = a
+    out = np.empty((seqs.shape[0], L + 1), np.uint8)
+    out[:, :L] = table[seqs]
+    out[:, L] = ord('\n')
+    return out.reshape(-1), bool((seqs >= a.size).any())
+
+
+def text_to_seqs(text, nlines, line_len, id_len, L, alpha):
+    """Lines of an MSA body back to packed walkers, as loadSeqs reads them
+    (seqload.py:196-246): every line ends in b'\\n', its id field (id_len
+    bytes) ends in a space, every residue is in alpha (the last index of a
+    repeated letter wins, as the reference's table assignment does).
+    Returns (packed (SWORDS, nlines) uint32, index of the first malformed
+    line or None); malformed lines pack as zeros."""
+    a = np.frombuffer(alpha.encode() if isinstance(alpha, str) else alpha, np.uint8)
+    lut = np.full(256, 255, np.uint8)
+    lut[a] = np.arange(a.size, dtype=np.uint8)
+    rows = np.asarray(text, np.uint8)[:nlines * line_len].reshape(nlines, line_len)
+    res = lut[rows[:, id_len:id_len + L]]
+    bad = (rows[:, -1] != ord('\n')) | (res == 255).any(axis=1)
+    if id_len:
+        bad |= rows[:, id_len - 1] != ord(' ')
+    res[bad] = 0
+    first = int(np.argmax(bad)) if bad.any() else None
+    return pack_seqs(res), first

@@ -71,6 +71,29 @@ class FakeMCMCGPU:
     def clearLargeSeqs(self):
         self.nstoredseqs = 0
 
+    def getSeqsText(self, bufname='main', alpha=None):
+        from mi3gpu_b200 import seqload
+        alpha = alpha if alpha is not None else seqload.default_alpha(self.q)
+        text, bad = oracle.seqs_to_text(self._seqs(bufname), self.L, alpha)
+        if bad:
+            raise ValueError("a walker holds a residue outside the alphabet")
+        return _Fut(text)
+
+    def setSeqsText(self, bufname, msa, start=0):
+        from mi3gpu_b200 import seqload
+        n = self.nseq[bufname]
+        if msa.eof_error is not None or start + n > msa.nseq:
+            seqload.check(msa)
+            raise Exception("not enough sequences")
+        mem, first = oracle.text_to_seqs(msa.lines(start, start + n).reshape(-1), n, msa.line_len, msa.id_len,
+                                         self.L, msa.alpha)
+        if first is not None:
+            seqload.check(msa)
+            raise ValueError("Sequence {} is malformed".format(start + first + 1))
+        self.bufs['seq ' + bufname] = mem
+        if bufname == 'large':
+            self.nstoredseqs = n
+
     def initMCMC(self, nsteps, rng_offset, rng_span):
         self.nsteps = int(nsteps)
         ws = int(rng_span) // (2 * self.nwalkers)

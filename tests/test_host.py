@@ -249,6 +249,72 @@ def test_newtonMCMC_rounds_over_fake_device():
     assert len(p.history) == 2 and all(np.isfinite(h['ssr']) for h in p.history)
 
 
+@pytest.mark.parametrize("device_resident", [False, True])
+def test_run_directories_in_reference_format_and_finish(tmp_path, device_resident):
+    """With outdir, every round writes what the reference writes
+    (NewtonSteps.py:76-94, 610-687): J.npy, newtonsteps, jstep, info.txt,
+    the walkers as a bzip2 MSA 'seqs' in the reference's text format,
+    nsteps, predictedBimarg.npy and perturbedJ.npy, in run_X directories
+    named as the reference names them; finish() then continues from the
+    last one as --finish does (Mi3.py:373-402): its J, jstep and
+    newtonsteps, and its walkers loaded from 'seqs'."""
+    from mi3gpu_b200 import seqload
+    L, q, N = 6, 3, 512
+    J0 = np.zeros((L * (L - 1) // 2, q * q), '<f4')
+    truth = potts.synthetic_ground_truth(L, q, seed=9, contact_sigma=0.5)
+
+    def node():
+        g = FakeMCMCGPU(L, q, N, seed=4)
+        gpus = GPU_node([g])
+        gpus.initMCMC(4 * L)
+        gpus.initJstep()
+        return g, gpus
+
+    g, gpus = node()
+    gpus.setBuf('J', truth)
+    gpus.setSeqs('main', np.zeros((N, L), '<u1'))
+    for _ in range(30):
+        gpus.runMCMC()
+    gpus.calcBicounts('main')
+    target = potts.mutation_pc(gpus.collect('bicount') / N, N).astype('<f4')
+    p = _param(L, q, N, target, J0, newtonSteps=16)
+    p.update(unimarg=potts.getUnimarg(target), reseed='none', device_resident=device_resident, outdir=tmp_path,
+             alpha="ABC", mcmcsteps=3)
+    gpus.prepare_indep(p.unimarg)
+    NewtonSteps.newtonMCMC(p, gpus, 0, 0, lambda *a: None)
+    runs = sorted(x.name for x in tmp_path.glob('run_*'))
+    assert runs == ['run_0', 'run_1', 'run_2']
+    for r in runs:
+        d = tmp_path / r
+        for f in ('J.npy', 'newtonsteps', 'jstep', 'info.txt', 'seqs', 'nsteps', 'predictedBimarg.npy',
+                  'perturbedJ.npy'):
+            assert (d / f).exists(), (r, f)
+        assert (d / 'seqs').read_bytes()[:3] == b"BZh"
+    seqs, ids, _ = seqload.loadSeqs(tmp_path / 'run_2' / 'seqs', "ABC")
+    assert seqs.shape == (N, L) and ids is None
+    np.testing.assert_array_equal(seqs, oracle.unpack_seqs(g.bufs['seq main'], L))
+
+    # finish: a fresh process continues from run_2 (rerunning it)
+    g2, gpus2 = node()
+    gpus2.prepare_indep(p.unimarg)
+    p2 = _param(L, q, N, target, None, newtonSteps=1)
+    p2.update(unimarg=p.unimarg, reseed='none', device_resident=device_resident, outdir=tmp_path, alpha="ABC",
+              mcmcsteps=2)  # nothing left to run: only the state is restored
+    logs = []
+    J = NewtonSteps.finish(p2, gpus2, logs.append)
+    assert "Continuing from" in logs[0] and logs[0].endswith('run_2')
+    np.testing.assert_array_equal(p2.couplings, np.load(tmp_path / 'run_2' / 'J.npy'))
+    assert p2.newtonSteps == int((tmp_path / 'run_2' / 'newtonsteps').read_text())
+    np.testing.assert_array_equal(oracle.unpack_seqs(g2.bufs['seq main'], L), seqs)
+    if not device_resident:
+        np.testing.assert_array_equal(J, p2.couplings)
+    jstep = (tmp_path / 'run_2' / 'jstep').read_text()
+    p2.mcmcsteps = 3  # now run the last round again, from the same jstep
+    NewtonSteps.finish(p2, gpus2, lambda *a: None)
+    assert (tmp_path / 'run_2' / 'jstep').read_text() == jstep
+    assert len(p2.history) == 1 and p2.history[0]['run'] == 'run_2'
+
+
 def test_device_resident_rounds_match_host_rounds():
     """The device-resident round loop (J kept on the device, gauge and SSR
     computed there) follows the same trajectory as the reference-shaped
