@@ -264,6 +264,13 @@ int mi3_text_to_seqs(const uint8_t *text, uint32_t nseq, uint32_t line_len, uint
                      const char *alpha, uint32_t nalpha, uint32_t *seqmem, uint32_t buflen, uint32_t n0,
                      uint64_t *first_bad, void *stream);
 
+/* copySubseq (mcmc.cl:99-122), MCMCGPU.copySubseq (mcmcGPU.py:1001-1014):
+ * every sequence of the large buffer (SWORDS, nlarge) takes, at each site i
+ * with marks[i] != 0 (marks: device, L bytes), the residue of sequence
+ * seqind of the small buffer (SWORDS, nsmall). */
+int mi3_copy_subseq(const uint32_t *small, uint32_t nsmall, uint32_t seqind, const uint8_t *marks,
+                    uint32_t *large, uint32_t nlarge, uint32_t L, void *stream);
+
 /* Bytes of workspace mi3_site_consensus needs: 8*L*q. */
 size_t mi3_site_consensus_workspace(uint32_t L, uint32_t q);
 

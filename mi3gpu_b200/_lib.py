@@ -37,6 +37,7 @@ SIGNATURES = {
     "mi3_weighted_marg": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp, c.c_size_t, _vp]),
     "mi3_weighted_marg_tc_workspace": (c.c_size_t, [_u32, _u32]),
     "mi3_weighted_marg_tc": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, c.c_size_t, _vp, _vp]),
+    "mi3_copy_subseq": (c.c_int, [_vp, _u32, _u32, _vp, _vp, _u32, _u32, _vp]),
     "mi3_seqs_to_text": (c.c_int, [_vp, _u32, _u32, _u32, c.c_char_p, _u32, _vp, _vp, _vp]),
     "mi3_text_to_seqs": (c.c_int, [_vp, _u32, _u32, _u32, _u32, c.c_char_p, _u32, _vp, _u32, _u32, _vp, _vp]),
     "mi3_site_consensus_workspace": (c.c_size_t, [_u32, _u32]),

@@ -95,3 +95,95 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
     total = time.time() - t0
     hist = p.history or []
     return dict(history=hist, total_s=total, J=J, expected_ssr=float(np.sum(target * (1 - target)) / nwalkers))
+
+
+# ---------------------------------------------------------------- other modes
+def _load_seqs_into_large(g, seqs, alpha):
+    """Sequences (an (N, L) uint8 array or an MSA file path) into the large
+    buffer of device g, which must hold exactly that many."""
+    from . import seqload
+    if isinstance(seqs, np.ndarray):
+        g.setBuf('seq large', seqs.astype('<u1', copy=False))
+    else:
+        msa = seqs if isinstance(seqs, seqload.MSAText) else seqload.read_msa(seqs, alpha)
+        g.setSeqsText('large', msa)
+
+
+def _count_seqs(seqs, alpha):
+    from . import seqload
+    if isinstance(seqs, np.ndarray):
+        return seqs.shape[0], None
+    msa = seqload.read_msa(seqs, alpha)
+    return msa.nseq, msa
+
+
+def sequence_energies(couplings, seqs, alpha=None, device=0):
+    """Potts energies of a set of sequences (the reference's `energies`
+    mode, Mi3.py:549-606): seqs is an (N, L) uint8 array or an MSA file in
+    the reference's format.  Any N: the sequences go to the device's large
+    buffer (the reference requires N to fill whole work groups)."""
+    from . import seqload
+    couplings = np.asarray(couplings, dtype='<f4')
+    L, q = potts.getLq(couplings)
+    alpha = alpha if alpha is not None else seqload.default_alpha(q)
+    n, msa = _count_seqs(seqs, alpha)
+    g = MCMCGPU((device, 0), L, q, 512, 512, None, 1024, 0)
+    g.initLargeBufs(n)
+    _load_seqs_into_large(g, seqs if msa is None else msa, alpha)
+    g.setBuf('J', couplings)
+    g.calcEnergies('large')
+    return g.getBuf('E large').read()
+
+
+def subseq_log_frequencies(couplings, backgroundseqs, subseqs, fixpos, iterbackgrounds=False, alpha=None,
+                           device=0):
+    """Log frequencies of subsequences at fixed sites given a sample of
+    background sequences (the reference's `subseq` mode, Mi3.py:876-976):
+    the marked sites of every sequence of the larger set are replaced by
+    those of each sequence of the smaller set in turn (copySubseq) and the
+    energies of the result are combined by log-sum-exp, with the
+    reference's own arithmetic (including that its default branch needs
+    both sets to be the same size).  Sequences are (N, L) uint8 arrays;
+    fixpos is a list of site indices."""
+    from scipy.special import logsumexp
+    from . import seqload
+    couplings = np.asarray(couplings, dtype='<f4')
+    L, q = potts.getLq(couplings)
+    alpha = alpha if alpha is not None else seqload.default_alpha(q)
+    bseqs, sseqs = np.asarray(backgroundseqs, '<u1'), np.asarray(subseqs, '<u1')
+    large, small = (sseqs, bseqs) if iterbackgrounds else (bseqs, sseqs)
+    ns = len(small)
+    if ns < 512 or ns % 512 != 0:  # whole work groups (Mi3.py:915-919)
+        n_new = ns - 1 + 512 - ((ns - 1) % 512)
+        small = np.concatenate([small, np.zeros((n_new - ns, L), dtype='u1')], axis=0)
+    g = MCMCGPU((device, 0), L, q, small.shape[0], 512, None, 1024, 0)
+    node = GPU_node([g])
+    g.initLargeBufs(large.shape[0])
+    g.initSubseq()
+    fixedpos = np.array([int(x) for x in fixpos])
+    if iterbackgrounds:
+        members = set(fixedpos.tolist())
+        fixedpos = np.array([i for i in range(L) if i not in members])
+    marks = np.zeros(L, dtype='u1')
+    marks[fixedpos] = 1
+    g.setBuf('seq main', small)
+    g.setBuf('seq large', large)
+    g.markPos(marks)
+    g.setBuf('J', couplings)
+    g.calcEnergies('main')
+    origEs = node.collect(['E main'])[0][:ns]
+    if iterbackgrounds:
+        logf = np.full(len(large), -np.inf)
+        for n, eo in enumerate(origEs):
+            g.copySubseq(n)
+            g.calcEnergies('large')
+            energies = g.getBuf('E large').read()
+            np.logaddexp(logf, eo - energies, out=logf)
+    else:
+        logf = np.zeros(len(large))
+        for n in range(ns):
+            g.copySubseq(n)
+            g.calcEnergies('large')
+            energies = g.getBuf('E large').read()
+            logf[n] = logsumexp(origEs - energies)
+    return logf

@@ -306,7 +306,31 @@ class MCMCGPU:
         self._sizeWorkspaces(nseq_large)
 
     def initSubseq(self):
-        raise NotImplementedError("subsequence mode is not part of the single-device path")
+        """The site marks of the subsequence splice (mcmcGPU.py:305-310)."""
+        self.require('Large')
+        self._initcomponent('Subseq')
+        self._setupBuffer('markpos', '<u1', (self.SBYTES,))
+        self.markPos(np.zeros(self.SBYTES, '<u1'))
+
+    def markPos(self, marks, wait_for=None):
+        """Mark the sites copySubseq replaces (mcmcGPU.py:919-925)."""
+        self.require('Subseq')
+        marks = np.asarray(marks).astype('<u1')
+        if len(marks) == self.L:
+            marks = np.concatenate([marks, np.zeros(self.SBYTES - self.L, '<u1')])
+        return self.setBuf('markpos', marks)
+
+    def copySubseq(self, seqind, wait_for=None):
+        """Every sequence of the large buffer takes the residues of main
+        sequence `seqind` at the marked sites (mcmcGPU.py:1001-1014)."""
+        self.require('Subseq')
+        if seqind >= self.nseq['main']:
+            raise Exception("given index is past end of main seq buffer")
+        s = self._begin()
+        _lib.call('mi3_copy_subseq', self._ptr('seq main'), self.nseq['main'], int(seqind), self._ptr('markpos'),
+                  self._ptr('seq large'), self.nseq['large'], self.L, self._s)
+        self.repackedSeqT['large'] = False
+        return self.logevt('copySubseq', s)
 
     def initJstep(self):
         self._initcomponent('Jstep')

@@ -83,6 +83,18 @@ class GPU_node:
         for n, gpu in zip(sizes, self.gpus):
             gpu.initLargeBufs(n)
 
+    def initSubseq(self):
+        for gpu in self.gpus:
+            gpu.initSubseq()
+
+    def markPos(self, marks):
+        for gpu in self.gpus:
+            gpu.markPos(marks)
+
+    def copySubseq(self, seqind):
+        for gpu in self.gpus:
+            gpu.copySubseq(seqind)
+
     def storeSeqs(self, seqs=None):
         for gpu in self.gpus:
             gpu.storeSeqs(seqs)

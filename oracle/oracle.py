@@ -391,3 +391,39 @@ def text_to_seqs(text, nlines, line_len, id_len, L, alpha):
     res[bad] = 0
     first = int(np.argmax(bad)) if bad.any() else None
     return pack_seqs(res), first
+
+
+def copy_subseq(small, seqind, marks, large, L):
+    """copySubseq (mcmc.cl:99-122): every sequence of `large` (packed) takes
+    the residues of small sequence `seqind` at the marked sites."""
+    big = unpack_seqs(large, L)
+    sub = unpack_seqs(small, L)[seqind]
+    m = np.asarray(marks[:L]).astype(bool)
+    big[:, m] = sub[m]
+    return pack_seqs(big)
+
+
+def subseq_log_frequencies(J, bseqs, sseqs, fixpos, iterbackgrounds, L, q):
+    """The subsequence-frequency computation of Mi3.py:906-974 in float64
+    (energies from energies_f64), with the reference's arithmetic."""
+    from scipy.special import logsumexp
+    large, small = (sseqs, bseqs) if iterbackgrounds else (bseqs, sseqs)
+    ns = len(small)
+    fixed = np.array([int(x) for x in fixpos])
+    if iterbackgrounds:
+        fixed = np.array([i for i in range(L) if i not in set(fixed.tolist())])
+    marks = np.zeros(L, np.uint8)
+    marks[fixed] = 1
+    smem, lmem = pack_seqs(np.asarray(small)), pack_seqs(np.asarray(large))
+    origEs = energies_f64(J, smem, L, q)
+    if iterbackgrounds:
+        logf = np.full(len(large), -np.inf)
+        for n, eo in enumerate(origEs):
+            lmem = copy_subseq(smem, n, marks, lmem, L)
+            np.logaddexp(logf, eo - energies_f64(J, lmem, L, q), out=logf)
+    else:
+        logf = np.zeros(len(large))
+        for n in range(ns):
+            lmem = copy_subseq(smem, n, marks, lmem, L)
+            logf[n] = logsumexp(origEs - energies_f64(J, lmem, L, q))
+    return logf
