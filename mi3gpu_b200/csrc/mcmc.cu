@@ -66,9 +66,30 @@ struct MetroParams {
 };
 
 // Shared memory: [full mbarriers S][empty mbarriers S][abort flag] (pad 128)
-//                [stage buffers S * stage_floats][pad STAGE_PAD][seq words SWORDS * NW]
+//                [stage buffers S * stage_floats][pad STAGE_PAD][seq words ceil(L/PK) * NW]
 // The pad absorbs gathers with an out-of-range residue byte (< 256 floats).
+//
+// PK residues per shared-memory word: 4 (bytes, the global layout) or, for
+// q <= 32, 6 (5 bits each) -- a walker's sequence then takes 2/3 of the
+// space, so more walkers fit per SM and a site block costs fewer word
+// loads.  The packing is internal: the kernel converts from and to the
+// global byte layout when it loads and stores the walkers, and the float
+// sums run over the same sites in the same order.
 constexpr uint32_t STAGE_PAD = 256;
+
+template <uint32_t PK>
+__device__ __forceinline__ uint32_t res_get(uint32_t w, uint32_t k) {
+    constexpr uint32_t BITS = PK == 4 ? 8 : 5;
+    return (w >> (BITS * k)) & ((1u << BITS) - 1);
+}
+
+template <uint32_t PK>
+__device__ __forceinline__ uint32_t res_set(uint32_t w, uint32_t k, uint32_t v) {
+    constexpr uint32_t BITS = PK == 4 ? 8 : 5, MASK = (1u << BITS) - 1;
+    return (w & ~(MASK << (BITS * k))) | ((v & MASK) << (BITS * k));
+}
+
+template <uint32_t PK>
 __global__ void __launch_bounds__(544, 1) k_metropolis(const MetroParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const uint32_t NW = blockDim.x - 32;  // consumer threads = walkers
@@ -82,7 +103,7 @@ __global__ void __launch_bounds__(544, 1) k_metropolis(const MetroParams p) {
     const uint32_t tid = threadIdx.x;
     const uint32_t warp = tid >> 5, lane = tid & 31;
     const uint32_t qq = p.q * p.q;
-    const uint32_t sw = (p.L - 1) / 4 + 1;
+    const uint32_t sw = (p.L - 1) / 4 + 1;  // global words (4 residues each)
 
     if (tid == 0) {
         for (uint32_t s = 0; s < S; ++s) {
@@ -132,7 +153,20 @@ __global__ void __launch_bounds__(544, 1) k_metropolis(const MetroParams p) {
 
     // -------------------------------------------------------- consumers
     const uint32_t g = blockIdx.x * NW + tid;
-    for (uint32_t w = 0; w < sw; ++w) seq_s[w * NW + tid] = p.seq[(size_t)w * p.nseqs + g];
+    if constexpr (PK == 4) {
+        for (uint32_t w = 0; w < sw; ++w) seq_s[w * NW + tid] = p.seq[(size_t)w * p.nseqs + g];
+    } else {
+        uint32_t gw = 0, acc = 0;
+        for (uint32_t j = 0; j < p.L; ++j) {
+            if ((j & 3) == 0) gw = p.seq[(size_t)(j >> 2) * p.nseqs + g];
+            const uint32_t k = j % PK;
+            acc = res_set<PK>(acc, k, getbyte(gw, j & 3));
+            if (k == PK - 1 || j == p.L - 1) {
+                seq_s[(j / PK) * NW + tid] = acc;
+                acc = 0;
+            }
+        }
+    }
     uint4 s4 = p.rng[g];
     Rng2 rng{s4.x, s4.y, s4.z, s4.w};
     const float B = p.betas ? p.betas[g] : p.beta;
@@ -149,10 +183,11 @@ __global__ void __launch_bounds__(544, 1) k_metropolis(const MetroParams p) {
         uint32_t r0, r1;
         rng_next2(rng, r0, r1);
         uint32_t mut = r0 % p.q;
-        uint32_t wpos = seq_s[(pos >> 2) * NW + tid];
+        const uint32_t pw = pos / PK, pk = pos - pw * PK;
+        uint32_t wpos = seq_s[pw * NW + tid];
         // residues are < q for valid input; the clamp keeps an invalid one
         // inside the stage buffer (an out-of-range s_m lands in the pad).
-        uint32_t cur = min(getbyte(wpos, pos & 3), p.q - 1);
+        uint32_t cur = min(res_get<PK>(wpos, pk), p.q - 1);
         uint32_t mq = mut * p.q, cq = cur * p.q;
         float dE = 0.0f;
         for (uint32_t c = 0; c < p.nchunks; ++c, ++k) {
@@ -164,26 +199,26 @@ __global__ void __launch_bounds__(544, 1) k_metropolis(const MetroParams p) {
                 break;
             }
             const float *Jc = stage + (size_t)s * p.stage_floats;
-            uint32_t m0 = c * p.M;
+            uint32_t m0 = c * p.M;  // a multiple of PK
             uint32_t nm = min(p.M, p.L - m0);
-            uint32_t nfull = nm >> 2;
-            const uint32_t *sq = seq_s + (m0 >> 2) * NW + tid;
+            uint32_t nfull = nm / PK;
+            const uint32_t *sq = seq_s + (m0 / PK) * NW + tid;
 #pragma unroll 2
             for (uint32_t w = 0; w < nfull; ++w) {
                 uint32_t word = sq[w * NW];
-                const float *Jm = Jc + w * 4 * qq;
+                const float *Jm = Jc + w * PK * qq;
 #pragma unroll
-                for (uint32_t b = 0; b < 4; ++b) {
-                    uint32_t sm = getbyte(word, b);
+                for (uint32_t b = 0; b < PK; ++b) {
+                    uint32_t sm = res_get<PK>(word, b);
                     dE += Jm[b * qq + mq + sm] - Jm[b * qq + cq + sm];
                 }
             }
-            uint32_t rem = nm & 3;
+            uint32_t rem = nm - nfull * PK;
             if (rem) {
                 uint32_t word = sq[nfull * NW];
-                const float *Jm = Jc + nfull * 4 * qq;
+                const float *Jm = Jc + nfull * PK * qq;
                 for (uint32_t b = 0; b < rem; ++b) {
-                    uint32_t sm = getbyte(word, b);
+                    uint32_t sm = res_get<PK>(word, b);
                     dE += Jm[b * qq + mq + sm] - Jm[b * qq + cq + sm];
                 }
             }
@@ -192,45 +227,71 @@ __global__ void __launch_bounds__(544, 1) k_metropolis(const MetroParams p) {
         }
         if (!ok) break;
         float x = -B * dE;
-        if (accept_exp(x, uniform_map(r1))) seq_s[(pos >> 2) * NW + tid] = setbyte(wpos, pos & 3, mut);
+        if (accept_exp(x, uniform_map(r1))) seq_s[pw * NW + tid] = res_set<PK>(wpos, pk, mut);
     }
-    for (uint32_t w = 0; w < sw; ++w) p.seq[(size_t)w * p.nseqs + g] = seq_s[w * NW + tid];
+    if constexpr (PK == 4) {
+        for (uint32_t w = 0; w < sw; ++w) p.seq[(size_t)w * p.nseqs + g] = seq_s[w * NW + tid];
+    } else {
+        uint32_t gw = 0, sword = 0;
+        for (uint32_t j = 0; j < p.L; ++j) {
+            const uint32_t k = j % PK;
+            if (k == 0) sword = seq_s[(j / PK) * NW + tid];
+            gw = setbyte(gw, j & 3, res_get<PK>(sword, k));
+            if ((j & 3) == 3 || j == p.L - 1) {
+                p.seq[(size_t)(j >> 2) * p.nseqs + g] = gw;
+                gw = 0;
+            }
+        }
+    }
     p.rng[g] = make_uint4(rng.x0, rng.x1, rng.c0, rng.c1);
 }
 
 struct MetroConfig {
     uint32_t NW, M, nchunks, stages, stage_floats;
     size_t smem;
+    uint32_t pk;  // residues per shared-memory word
 };
 
-static size_t metro_smem(uint32_t NW, uint32_t S, uint32_t stage_floats, uint32_t sw) {
+// 5-bit residues when they fit and chunks start on whole words of 6
+static uint32_t metro_pk(uint32_t q, uint32_t M) { return (q <= 32 && M % 12 == 0) ? 6 : 4; }
+
+static size_t metro_smem(uint32_t NW, uint32_t S, uint32_t stage_floats, uint32_t L, uint32_t pk) {
     size_t head = 128 * ((16 * S + 4 + 127) / 128);
-    return head + (size_t)S * stage_floats * 4 + STAGE_PAD * 4 + (size_t)sw * NW * 4;
+    return head + (size_t)S * stage_floats * 4 + STAGE_PAD * 4 + (size_t)((L + pk - 1) / pk) * NW * 4;
+}
+
+// Sites per chunk for a stage of about `bytes`: a multiple of 4 (16-byte
+// aligned bulk copies), of 12 when q <= 32 (whole 5-bit words), at most the
+// rounded row.
+static uint32_t metro_chunk(uint32_t L, uint32_t q, uint32_t bytes) {
+    const uint32_t Lr = (L + 3) & ~3u;
+    uint32_t M = bytes / (q * q * 4);
+    const uint32_t unit = (q <= 32 && M >= 12) ? 12 : 4;
+    M = std::max<uint32_t>(4, M - M % unit);
+    return std::min(M, Lr);
 }
 
 static bool pick_metro_config(uint32_t L, uint32_t q, uint32_t nseqs, MetroConfig &cfg) {
     const size_t SMEM_MAX = 227 * 1024;
     const uint32_t qq = q * q;
-    const uint32_t sw = (L - 1) / 4 + 1;
-    const uint32_t Lr = (L + 3) & ~3u;
-    // sites per chunk: stages of up to ~48 KB, multiple of 4, at most the
-    // (rounded) row; two stages first.  (Timing every plan at L=232/512,
-    // q=21 put two or three ~40 KB stages first: fewer, larger bulk copies
-    // per coupling row beat a deeper ring of small ones.)
-    uint32_t M = (48 * 1024) / (qq * 4);
-    M = std::max<uint32_t>(4, M & ~3u);
-    M = std::min(M, Lr);
-    uint32_t cands[3] = {512, 256, 128};
+    // sites per chunk: stages of up to ~48 KB, at most the (rounded) row;
+    // two stages first.  (Timing every plan at L=232/512, q=21 put two or
+    // three ~40 KB stages first: fewer, larger bulk copies per coupling row
+    // beat a deeper ring of small ones.)
+    const uint32_t M = metro_chunk(L, q, 48 * 1024);
+    const uint32_t step = metro_pk(q, M) == 6 ? 12 : 4;
+    uint32_t cands[4] = {512, 384, 256, 128};
     for (uint32_t NW : cands) {
         if (nseqs % NW) continue;
         // prefer enough CTAs to fill the SMs when walkers are few
         if (NW > 128 && nseqs / NW < 148) continue;
         for (uint32_t S = 2; S <= 4; ++S) {
-            for (uint32_t m = M; m >= 4; m -= 4) {
+            for (uint32_t m = M; m >= step; m -= step) {
                 uint32_t stage_floats = ((m * qq) + 31) & ~31u;
-                size_t sm = metro_smem(NW, S, stage_floats, sw);
+                const uint32_t pk = metro_pk(q, m);
+                size_t sm = metro_smem(NW, S, stage_floats, L, pk);
                 if (sm <= SMEM_MAX) {
-                    cfg = MetroConfig{NW, m, (L + m - 1) / m, S, stage_floats, sm};
+                    cfg = MetroConfig{NW, m, (L + m - 1) / m, S, stage_floats, sm, pk};
                     return true;
                 }
             }
@@ -266,15 +327,16 @@ static int make_metro_config(uint32_t L, uint32_t q, uint32_t nseqs, uint32_t NW
             return fail(MI3_ERR_ARG, "mi3_metropolis: L/q too large for the shared-memory plan");
         return MI3_OK;
     }
-    const uint32_t Lr = (L + 3) & ~3u, sw = (L - 1) / 4 + 1, qq = q * q;
+    const uint32_t Lr = (L + 3) & ~3u, qq = q * q;
     if (NW < 64 || NW > 512 || NW % 32 || nseqs % NW)
         return fail(MI3_ERR_ARG, "mi3_metropolis: walkers per CTA must be a multiple of 32 in [64, 512] dividing nseqs");
     if (M < 4 || M % 4 || M > Lr) return fail(MI3_ERR_ARG, "mi3_metropolis: sites per chunk must be a multiple of 4 <= L");
     if (S < 2 || S > 8) return fail(MI3_ERR_ARG, "mi3_metropolis: stages must be in [2, 8]");
     const uint32_t stage_floats = ((M * qq) + 31) & ~31u;
-    const size_t sm = metro_smem(NW, S, stage_floats, sw);
+    const uint32_t pk = metro_pk(q, M);
+    const size_t sm = metro_smem(NW, S, stage_floats, L, pk);
     if (sm > 227 * 1024) return fail(MI3_ERR_ARG, "mi3_metropolis: plan exceeds shared memory");
-    cfg = MetroConfig{NW, M, (L + M - 1) / M, S, stage_floats, sm};
+    cfg = MetroConfig{NW, M, (L + M - 1) / M, S, stage_floats, sm, pk};
     return MI3_OK;
 }
 
@@ -283,7 +345,6 @@ static int make_metro_config(uint32_t L, uint32_t q, uint32_t nseqs, uint32_t NW
 extern "C" uint32_t mi3_metropolis_plans(uint32_t L, uint32_t q, uint32_t nseqs, uint32_t *plans, uint32_t max) {
     uint32_t n = 0;
     if (L < 2 || q < 2 || q > 255 || nseqs == 0) return 0;
-    const uint32_t Lr = (L + 3) & ~3u;
     const uint32_t nws[4] = {128, 256, 384, 512};
     for (uint32_t NW : nws) {
         if (nseqs % NW) continue;
@@ -292,8 +353,7 @@ extern "C" uint32_t mi3_metropolis_plans(uint32_t L, uint32_t q, uint32_t nseqs,
             const uint32_t kb[5] = {8, 16, 24, 32, 48};
             uint32_t last = 0;
             for (uint32_t t = 0; t < 5; ++t) {
-                uint32_t M = (kb[t] * 1024) / (q * q * 4);
-                M = std::min(std::max<uint32_t>(4, M & ~3u), Lr);
+                const uint32_t M = metro_chunk(L, q, kb[t] * 1024);
                 if (M == last) continue;
                 last = M;
                 MetroConfig cfg;
@@ -327,7 +387,8 @@ extern "C" int mi3_metropolis_plan(const float *Jrows, uint32_t *rngstates, uint
     MetroConfig cfg;
     int rc = make_metro_config(L, q, nseqs, walkers_per_cta, sites_per_chunk, stages, cfg);
     if (rc) return rc;
-    cudaFuncSetAttribute(k_metropolis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
+    auto kernel = cfg.pk == 6 ? k_metropolis<6> : k_metropolis<4>;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
     MetroParams p;
     p.Jrows = Jrows;
     p.stride = jrow_stride(L, q);
@@ -346,7 +407,7 @@ extern "C" int mi3_metropolis_plan(const float *Jrows, uint32_t *rngstates, uint
     p.stages = cfg.stages;
     p.stage_floats = cfg.stage_floats;
     p.status = status;
-    k_metropolis<<<nseqs / cfg.NW, cfg.NW + 32, cfg.smem, as_stream(stream)>>>(p);
+    kernel<<<nseqs / cfg.NW, cfg.NW + 32, cfg.smem, as_stream(stream)>>>(p);
     return check_launch("mi3_metropolis");
 }
 

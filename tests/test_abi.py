@@ -86,15 +86,18 @@ def test_bad_shapes_rejected():
 def test_metropolis_plans_host_query(L, q, N):
     """The plan enumeration is host code: every plan respects the kernel's
     limits (walkers per CTA divide N, chunk a multiple of 4 within the row,
-    2-8 stages, shared memory within 227 KB)."""
+    2-8 stages, shared memory within 227 KB with the walkers held at 4
+    residues per word, or 6 (5 bits each) when q <= 32 and the chunk is a
+    multiple of 12)."""
     from mi3gpu_b200.autotune import sampler_plans
     plans = sampler_plans(L, q, N)
     assert plans, "no plan for a supported shape"
-    sw = (L - 1) // 4 + 1
     for nw, m, st in plans:
         assert nw % 32 == 0 and 64 <= nw <= 512 and N % nw == 0
         assert m % 4 == 0 and 4 <= m <= ((L + 3) // 4) * 4
         assert 2 <= st <= 8
+        pk = 6 if q <= 32 and m % 12 == 0 else 4
+        words = (L + pk - 1) // pk
         stage_floats = (m * q * q + 31) // 32 * 32
-        smem = 128 * ((16 * st + 4 + 127) // 128) + st * stage_floats * 4 + 256 * 4 + sw * nw * 4
+        smem = 128 * ((16 * st + 4 + 127) // 128) + st * stage_floats * 4 + 256 * 4 + words * nw * 4
         assert smem <= 227 * 1024
