@@ -68,6 +68,7 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
     (results do not depend on them).  distribute_jstep: 'all' runs the
     Newton steps over the walkers where they are; 'head_gpu' first gathers
     them into the device's large buffer, as the reference's option does."""
+    potts.check_target(target)  # as the reference's set-up does (Mi3.py:1029-1034)
     unimarg = potts.getUnimarg(target)
     J0 = potts.independent_couplings(unimarg)
     nsteps = 8 * L

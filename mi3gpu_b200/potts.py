@@ -5,6 +5,7 @@ Shapes follow the reference: couplings/bimarginals (nPairs, q*q) with pairs
 
 Restated from the reference's utilities (numpy, FP64):
   getLq, getUnimarg, indepF, validate_bimarg  -- utils/potts_common.py:24-100
+  check_target                                -- Mi3.py:1029-1034
   zeroJGauge, zeroGauge, fieldlessGaugeEven  -- utils/changeGauge.py:37-155
   mutation_pc                                -- utils/pseudocount.py:8-24
 plus the synthetic ground-truth generator for the benchmark workloads.
@@ -46,10 +47,12 @@ def indepF(fab):
 
 def validate_bimarg(ff, eps=1e-5):
     """Unimarginals implied by every bimarginal row agree and sum to 1
-    (potts_common.py:50-76).  Raises ValueError otherwise."""
+    (potts_common.py:50-76): the first failing check, in the reference's
+    order (the sums, then pair by pair the i and j marginals), raises its
+    ValueError with the reference's message."""
     L, q = getLq(ff)
     fx = np.asarray(ff).reshape((L * (L - 1) // 2, q, q))
-    uni = np.empty((L, q))
+    uni = np.empty((L, q), dtype=fx.dtype)
     uni[0] = fx[0].sum(axis=1)
     uni[1:] = fx[:L - 1].sum(axis=1)
     delta = np.abs(uni.sum(axis=1) - 1)
@@ -58,9 +61,28 @@ def validate_bimarg(ff, eps=1e-5):
     i, j = pair_indices(L)
     di = np.abs(uni[i] - fx.sum(axis=2))
     dj = np.abs(uni[j] - fx.sum(axis=1))
-    if di.max() > eps or dj.max() > eps:
-        n = int(np.argmax(np.maximum(di.max(axis=1), dj.max(axis=1))))
-        raise ValueError("inconsistent unimarg for bimarg {} ({},{})".format(n, i[n], j[n]))
+    bad = np.flatnonzero((di.max(axis=1) > eps) | (dj.max(axis=1) > eps))
+    if bad.size:
+        n = int(bad[0])
+        if di[n].max() > eps:
+            m = int(np.argmax(di[n]))
+            raise ValueError("inconsitent i unimarg {:.5f} with delta {:.5f} for bimarg {} ({},{})".format(
+                uni[i[n]][m], di[n][m], n, i[n], j[n]))
+        m = int(np.argmax(dj[n]))
+        raise ValueError("inconsitent j unimarg {:.5f} with delta {:.5f} for bimarg {} ({},{})".format(
+            uni[j[n]][m], dj[n][m], n, i[n], j[n]))
+
+
+def check_target(bimarg):
+    """The target checks of the reference's inference set-up
+    (Mi3.py:1029-1034): float32, every entry in (0, 1], consistent
+    marginals."""
+    bimarg = np.asarray(bimarg)
+    if bimarg.dtype != np.dtype('<f4'):
+        raise Exception("Bimarg must be in 'f4' format")
+    if np.any((bimarg <= 0) | (bimarg > 1)):
+        raise Exception("All bimarg must be 0 < f < 1")
+    validate_bimarg(bimarg)
 
 
 def _impute(h, J):

@@ -359,3 +359,25 @@ def test_head_gpu_newton_phase_equals_all(cuda, device_resident):
     assert res[0][0] == res[1][0] >= 1
     np.testing.assert_array_equal(res[0][1], res[1][1])
     np.testing.assert_array_equal(res[0][2], res[1][2])
+
+
+def test_device_bimarginals_pass_the_reference_checks(cuda):
+    """Bimarginals the device produces -- counted (bicounts_to_bimarg) and
+    weighted then renormalised (weightedMarg + renormalize_bimarg) -- pass
+    the reference's consistency checks (potts_common.py:50-76)."""
+    L, q, N = 33, 21, 4096
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 5)
+    node = GPU_node([g])
+    node.initMCMC(2 * L)
+    node.initJstep()
+    node.setSeqs('main', np.random.default_rng(3).integers(0, q, size=(N, L)).astype('<u1'))
+    node.setBuf('J', potts.synthetic_ground_truth(L, q, seed=4, contact_sigma=0.5))
+    for _ in range(4):
+        node.runMCMC()
+    node.calcBicounts('main')
+    node.bicounts_to_bimarg('main')
+    potts.validate_bimarg(node.collect('bi'))
+    g.setBuf('weights', np.random.default_rng(6).uniform(0.1, 3.0, size=N).astype('<f4'))
+    node.weightedMarg('main')
+    node.renormalize_bimarg()
+    potts.validate_bimarg(node.collect('bi'))

@@ -226,3 +226,56 @@ def test_bimarg_stats_f64_matches_host_formula():
                                                                                m64[p].reshape(q, q).sum(0)))))
               for p in range(npair))
     np.testing.assert_allclose(xm, xm2, rtol=1e-10)
+
+
+def test_validate_bimarg_matches_reference_messages():
+    """potts.validate_bimarg accepts and rejects what the reference's
+    validate_bimarg does (potts_common.py:50-76), with its messages
+    (tests/golden/validate_vectors.npz)."""
+    from pathlib import Path
+    from mi3gpu_b200 import potts
+    g = np.load(Path(__file__).parent / "golden" / "validate_vectors.npz")
+    tags = sorted({k[:-3] for k in g.files if k.endswith("_in")})
+    assert len(tags) == 5
+    for tag in tags:
+        want = str(g[tag + "_msg"])
+        if not want:
+            potts.validate_bimarg(g[tag + "_in"])
+        else:
+            with pytest.raises(ValueError) as e:
+                potts.validate_bimarg(g[tag + "_in"])
+            assert str(e.value) == want, tag
+
+
+def test_check_target_rejects_what_the_reference_rejects():
+    from pathlib import Path
+    from mi3gpu_b200 import potts
+    g = np.load(Path(__file__).parent / "golden" / "validate_vectors.npz")
+    ff = g["valid_in"]
+    potts.check_target(ff)
+    with pytest.raises(Exception, match="'f4' format"):
+        potts.check_target(ff.astype('f8'))
+    z = ff.copy()
+    z[3, 5] = 0
+    with pytest.raises(Exception, match="0 < f < 1"):
+        potts.check_target(z)
+
+
+def test_gauge_change_shifts_every_energy_by_one_constant():
+    """The intent of the reference's changeGauge.test_transform
+    (changeGauge.py:181-201): a gauge change leaves energy differences
+    unchanged.  Couplings uniform on [0, 1) (the reference test's, far from
+    any gauge) moved to the fieldless-even gauge (FP64 oracle): the energies
+    of random sequences, summed in FP64, all shift by one constant."""
+    L, q = 9, 5
+    rng = np.random.default_rng(1234)
+    J = rng.random((L * (L - 1) // 2, q * q))
+    Jg = oracle.gauge_fieldless_even(J, L, q)
+    seqs = rng.integers(0, q, size=(200, L))
+    pairs = [(i, j) for i in range(L - 1) for j in range(i + 1, L)]
+
+    def energies(C):
+        return sum(C[p, q * seqs[:, i] + seqs[:, j]] for p, (i, j) in enumerate(pairs))
+    d = energies(Jg) - energies(J)
+    assert abs(d.mean()) > 1.0  # the gauge did move the couplings
+    assert np.ptp(d) < 1e-9 * np.abs(d).max()
