@@ -440,10 +440,36 @@ def finish(param, gpus, log):
     return newtonMCMC(param, gpus, start, jstep, log)
 
 
+def preOpt(param, gpus, log):
+    """Pre-optimisation (NewtonSteps.py:274-296): one Newton phase on the
+    walkers already in the devices' main buffers (loaded sequences), before
+    the first round; writes a 'preopt' status directory when param.outdir
+    is set.  Returns (J after it, Newton steps taken)."""
+    J = param.couplings
+    log("Pre-Optimization:")
+    gpus.setBuf('J', np.asarray(J, dtype='<f4'))
+    gpus.calcBicounts('main')
+    gpus.calcEnergies('main')
+    bicount, es = gpus.collect(['bicount', 'E main'])
+    bimarg = bicount.astype(np.float32) / np.float32(np.sum(bicount[0, :]))
+    if param.outdir is not None:
+        d = Path(param.outdir) / 'preopt'
+        d.mkdir(parents=True, exist_ok=True)
+        (d / 'info.txt').write_text(printstats('preopt', 0, param.bimarg, bimarg, J, es, None))
+        gpus.writeSeqs(d / 'seqs', 'main', _alpha(param), zipf=True)
+    Jsteps, newJ = NewtonSteps('preopt', param, bimarg, gpus, log)
+    if newJ is None:  # device-resident: J + dJ stays on the devices
+        newJ = gpus.head_gpu.readBufs('J')[0]
+    return newJ, Jsteps
+
+
 def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
-    """Round loop (NewtonSteps.py:689-767) for the reseed strategies that
-    need no file input: 'independent', 'single_indep', 'single_best',
-    'single_random', 'none'.
+    """Round loop (NewtonSteps.py:689-767) with the reseed strategies
+    'independent', 'single_indep', 'single_best', 'single_random', 'none'
+    and 'msa' (param.seedmsa: the seed sequences, one (n, L) uint8 array
+    per device or one array for all, reset into the walkers every round;
+    they are copied to the devices once and restored there), and the
+    pre-optimisation of param.preopt.
 
     param.checkpoint (a path) writes a checkpoint after every round;
     resume (a state from checkpoint.load) continues a run from one, on the
@@ -462,6 +488,12 @@ def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
         log(f"Continuing from a checkpoint before round {start_run}")
     if param.device_resident:
         gpus.setBuf('J', np.asarray(J, dtype='<f4'))
+    if fresh and param.preopt:
+        J, Jsteps = preOpt(param, gpus, log)
+        Jstep += Jsteps
+    elif fresh:
+        log("No Pre-optimization")
+    seed_snapshot = None
     name_fmt = run_name_format(param.mcmcsteps)
     for i in range(start_run, param.mcmcsteps):
         runname = name_fmt.format(i)
@@ -476,15 +508,24 @@ def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
             seed = seqs[rng.randint(0, seqs.shape[0])]
         elif param.reseed == 'single_best' and seqs is not None:
             seed = seqs[np.argmin(es)]
-        if seed is not None:
+        if param.reseed == 'msa' and seed is None:
+            # the seed MSA: uploaded once, then restored on the devices
+            if seed_snapshot is None:
+                gpus.setSeqs('main', param.seedmsa)
+                seed_snapshot = gpus.snapshotSeqs()
+            else:
+                gpus.restoreSnapshot(seed_snapshot)
+        elif seed is not None:
             if param.outdir is not None:
                 rundir = Path(param.outdir) / runname
                 rundir.mkdir(parents=True, exist_ok=True)
                 (rundir / 'seedseq').write_text("".join(_alpha(param)[c] for c in seed))
             gpus.fillSeqs(seed)
-        elif param.reseed == 'independent' or (param.reseed == 'none' and first and param.init_indep):
+        elif param.reseed == 'independent' or (param.reseed == 'none' and first and param.init_indep
+                                                and not param.preopt):
             # 'none' keeps the walkers from round to round; they start from
-            # independent-site sequences when init_indep is set
+            # independent-site sequences when init_indep is set (not after a
+            # pre-optimisation, which ran on the loaded walkers)
             gpus.gen_indep('main')
         equil = param.equiltime
         if first and param.equiltime_first is not None:

@@ -854,6 +854,19 @@ class MCMCGPU:
         n = self.nseq[bufname]
         return self.bufs['seq ' + bufname][:self.SWORDS * n].view(self.SWORDS, n)
 
+    def snapshotSeqs(self, bufname='main'):
+        """A device copy of the walkers of 'seq <bufname>' (restoreSnapshot
+        puts it back without a host round trip)."""
+        with torch.cuda.stream(self.stream):
+            return self.packedSeqs(bufname).clone()
+
+    def restoreSnapshot(self, snap, bufname='main'):
+        s = self._begin()
+        with torch.cuda.stream(self.stream):
+            self.packedSeqs(bufname).copy_(snap, non_blocking=True)
+        self.repackedSeqT[bufname] = False
+        return self.logevt('restoreSnapshot', s, snap.numel() * 4)
+
     def _largeCols(self, offset, n):
         """Columns [offset, offset+n) of 'seq large' as a (SWORDS, n) view."""
         return self.packedSeqs('large')[:, offset:offset + n]

@@ -322,6 +322,13 @@ class GPU_node:
         for gpu in self.gpus:
             gpu.fillSeqs(seq)
 
+    def snapshotSeqs(self, bufname='main'):
+        return [gpu.snapshotSeqs(bufname) for gpu in self.gpus]
+
+    def restoreSnapshot(self, snaps, bufname='main'):
+        for gpu, snap in zip(self.gpus, snaps):
+            gpu.restoreSnapshot(snap, bufname)
+
     def reduce_node_bimarg(self):
         """Pairwise tree sum of 'bi' onto device 0 (node_manager.py:254-281)."""
         self.wait()

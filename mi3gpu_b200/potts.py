@@ -140,6 +140,13 @@ def fieldlessGaugeEven(h, J):
     return fieldlessGaugeDistributed(*zeroGauge(h, J))
 
 
+def repeatseqs(seqs, n):
+    """n sequences by repeating the given ones in order (Mi3.py:1206-1207):
+    the seed MSA of reseed 'msa'."""
+    seqs = np.asarray(seqs)
+    return np.repeat(seqs, (n - 1) // seqs.shape[0] + 1, axis=0)[:n, :]
+
+
 def mutation_pc(ff, N, mode='jeffreys'):
     """Covariance-preserving pseudocount (pseudocount.py:8-24): mix the
     bimarginals with uniform residues at rate mu = q/(2N+q) (Jeffreys) or

@@ -71,6 +71,12 @@ class FakeMCMCGPU:
     def clearLargeSeqs(self):
         self.nstoredseqs = 0
 
+    def snapshotSeqs(self, bufname='main'):
+        return self.bufs['seq ' + bufname].copy()
+
+    def restoreSnapshot(self, snap, bufname='main'):
+        self.bufs['seq ' + bufname] = snap.copy()
+
     def getSeqsText(self, bufname='main', alpha=None):
         from mi3gpu_b200 import seqload
         alpha = alpha if alpha is not None else seqload.default_alpha(self.q)

@@ -381,3 +381,20 @@ def test_device_bimarginals_pass_the_reference_checks(cuda):
     node.weightedMarg('main')
     node.renormalize_bimarg()
     potts.validate_bimarg(node.collect('bi'))
+
+
+def test_seed_snapshot_restores_walkers_on_device(cuda):
+    """snapshotSeqs / restoreSnapshot (the seed MSA of reseed 'msa'): a
+    device copy of the walkers, put back after sampling moved them."""
+    L, q, N = 19, 21, 1024
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, 2)
+    node = GPU_node([g])
+    node.initMCMC(2 * L)
+    seed = potts.repeatseqs(np.random.default_rng(1).integers(0, q, size=(300, L)).astype('<u1'), N)
+    node.setSeqs('main', seed)
+    snap = node.snapshotSeqs()
+    node.setBuf('J', potts.synthetic_ground_truth(L, q, seed=2, contact_sigma=0.5))
+    node.runMCMC()
+    assert not np.array_equal(node.collect('seq main'), seed)
+    node.restoreSnapshot(snap)
+    np.testing.assert_array_equal(node.collect('seq main'), seed)

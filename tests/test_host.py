@@ -439,3 +439,77 @@ def test_auto_equilibration_runs_and_stops():
     assert 16 <= steps <= 64 + 32
     assert any("Equilibrated" in s or "Max Steps" in s for s in logs)
     assert out[3] is not None and len(out[3]) >= 2  # energy autocorrelations recorded
+
+
+def _round_setup(L=6, q=3, N=512, seed=4):
+    J0 = np.zeros((L * (L - 1) // 2, q * q), '<f4')
+    truth = potts.synthetic_ground_truth(L, q, seed=9, contact_sigma=0.5)
+    g = FakeMCMCGPU(L, q, N, seed=seed)
+    gpus = GPU_node([g])
+    gpus.initMCMC(4 * L)
+    gpus.initJstep()
+    gpus.setBuf('J', truth)
+    gpus.setSeqs('main', np.zeros((N, L), '<u1'))
+    for _ in range(30):
+        gpus.runMCMC()
+    gpus.calcBicounts('main')
+    target = potts.mutation_pc(gpus.collect('bicount') / N, N).astype('<f4')
+    p = _param(L, q, N, target, J0, newtonSteps=16)
+    p.unimarg = potts.getUnimarg(target)
+    gpus.prepare_indep(p.unimarg)
+    return g, gpus, p
+
+
+@pytest.mark.parametrize("device_resident", [False, True])
+def test_preopt_runs_a_newton_phase_on_the_loaded_walkers(tmp_path, device_resident):
+    """param.preopt (NewtonSteps.py:274-296, 716-720): one Newton phase on
+    the walkers in the main buffers before round 0, written to 'preopt/',
+    its steps counted in the jstep of run 0; reseed 'none' then keeps those
+    walkers (no independent restart)."""
+    g, gpus, p = _round_setup()
+    loaded = g.bufs['seq main'].copy()
+    p.update(preopt=True, reseed='none', init_indep=True, outdir=tmp_path, alpha="ABC", mcmcsteps=2,
+             device_resident=device_resident)
+    seen = []
+    orig = NewtonSteps.MCMCstep
+
+    def spy(runName, Jstep, couplings, param, gpus_, log):
+        seen.append((runName, Jstep, g.bufs['seq main'].copy()))
+        return orig(runName, Jstep, couplings, param, gpus_, log)
+    NewtonSteps.MCMCstep = spy
+    try:
+        logs = []
+        NewtonSteps.newtonMCMC(p, gpus, 0, 0, logs.append)
+    finally:
+        NewtonSteps.MCMCstep = orig
+    assert "Pre-Optimization:" in logs
+    for f in ('info.txt', 'seqs', 'predictedBimarg.npy', 'perturbedJ.npy'):
+        assert (tmp_path / 'preopt' / f).exists(), f
+    assert seen[0][1] > 0  # run 0 starts after the pre-optimisation's steps
+    assert (tmp_path / 'run_0' / 'jstep').read_text() == str(seen[0][1])
+    np.testing.assert_array_equal(seen[0][2], loaded)
+
+
+def test_reseed_msa_restarts_every_round_from_the_seed_msa():
+    """reseed 'msa' (NewtonSteps.py:761-762): every round starts from the
+    seed sequences (uploaded once, restored on the device afterwards)."""
+    L, q, N = 6, 3, 512
+    g, gpus, p = _round_setup(L, q, N)
+    seedmsa = potts.repeatseqs(np.random.default_rng(8).integers(0, q, size=(100, L)).astype('<u1'), N)
+    assert seedmsa.shape == (N, L)
+    p.update(reseed='msa', seedmsa=seedmsa, mcmcsteps=3)
+    seen = []
+    orig = NewtonSteps.MCMCstep
+
+    def spy(runName, Jstep, couplings, param, gpus_, log):
+        seen.append(g.bufs['seq main'].copy())
+        return orig(runName, Jstep, couplings, param, gpus_, log)
+    NewtonSteps.MCMCstep = spy
+    try:
+        NewtonSteps.newtonMCMC(p, gpus, 0, 0, lambda *a: None)
+    finally:
+        NewtonSteps.MCMCstep = orig
+    assert len(seen) == 3
+    for s in seen:
+        np.testing.assert_array_equal(s, oracle.pack_seqs(seedmsa))
+    assert not np.array_equal(g.bufs['seq main'], oracle.pack_seqs(seedmsa))  # the walkers did move
