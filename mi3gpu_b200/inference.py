@@ -188,3 +188,86 @@ def subseq_log_frequencies(couplings, backgroundseqs, subseqs, fixpos, iterbackg
             energies = g.getBuf('E large').read()
             logf[n] = logsumexp(origEs - energies)
     return logf
+
+
+def equilibrate(couplings, nwalkers, equiltime, nsteps=None, seqs=None, seedseq=None, unimarg=None, alpha=None,
+                outdir=None, trackequil=0, tracked='', min_equil=64, max_equil=32768, beta=None, seed=1234,
+                device=0, log=print):
+    """A round of sampling from a Potts model, the reference's `gen` mode
+    (Mi3.py:724-870): the walkers start from `seqs` (an (N, L) uint8 array
+    or an MSA file), from one `seedseq`, or from independent-site sequences
+    of `unimarg` ((L, q) marginals); they run `equiltime` sampler calls of
+    `nsteps` steps ('auto': until the energies decorrelate,
+    NewtonSteps.runMCMC); the result is (bimarg, bicount, energies, walkers)
+    and, with outdir, the reference's files: bicounts (text), bimarg.npy,
+    energies.npy and seqs (MSA text)."""
+    from . import seqload
+    from pathlib import Path
+    couplings = np.asarray(couplings, dtype='<f4')
+    L, q = potts.getLq(couplings)
+    alpha = alpha if alpha is not None else seqload.default_alpha(q)
+    nsteps = nsteps or L
+    g = MCMCGPU((device, 0), L, q, nwalkers, 512, None, 1024, seed + 1, beta=beta)
+    gpus = GPU_node([g])
+    gpus.initMCMC(nsteps)
+    if beta is not None:
+        gpus.initJstep()
+    if seedseq is not None:
+        gpus.fillSeqs(np.asarray(seedseq, '<u1'))
+    elif seqs is not None:
+        if isinstance(seqs, np.ndarray):
+            gpus.setSeqs('main', seqs.astype('<u1', copy=False))
+        else:
+            gpus.loadSeqs(seqs, 'main', alpha)
+    elif unimarg is not None:
+        gpus.prepare_indep(np.asarray(unimarg, 'f4'))
+        gpus.gen_indep('main')
+    else:
+        raise ValueError("give seqs, seedseq or unimarg for the starting walkers")
+    outdir = Path(outdir) if outdir is not None else None
+    p = NewtonSteps.Param(equiltime=equiltime, trackequil=trackequil, tracked=tracked, outdir=outdir,
+                          min_equil=min_equil, max_equil=max_equil, beta=beta, nsteps=nsteps, alpha=alpha, q=q,
+                          device_resident=False)
+    if outdir is not None:
+        outdir.mkdir(parents=True, exist_ok=True)
+    bimarg, bicount, energies, e_rho, _, _ = NewtonSteps.runMCMC(gpus, couplings, 'gen', p, log)
+    walkers = gpus.collect('seq main')
+    if outdir is not None:
+        if bicount is not None:
+            np.savetxt(outdir / 'bicounts', bicount, fmt='%d')
+        np.save(outdir / 'bimarg', bimarg)
+        np.save(outdir / 'energies', energies)
+        gpus.writeSeqs(outdir / 'seqs', 'main', alpha)
+    log("Mean energy:", np.mean(energies))
+    return bimarg, bicount, energies, walkers
+
+
+def benchmark_mcmc(couplings, nwalkers, nsteps, nloop, seqs=None, seedseq=None, device=0, log=print):
+    """The reference's `benchmark` mode (Mi3.py:610-722): nloop sampler
+    calls of nsteps steps after a warm-up of as many, timed by the wall
+    clock; returns MC steps per second."""
+    couplings = np.asarray(couplings, dtype='<f4')
+    L, q = potts.getLq(couplings)
+    g = MCMCGPU((device, 0), L, q, nwalkers, 512, None, 1024, 1)
+    gpus = GPU_node([g])
+    gpus.initMCMC(nsteps)
+    if seqs is not None:
+        gpus.setSeqs('main', np.asarray(seqs, '<u1'))
+    elif seedseq is not None:
+        gpus.fillSeqs(np.asarray(seedseq, '<u1'))
+    else:
+        raise Exception("'seqs' or 'seedseq' option required")
+    gpus.setBuf('J', couplings)
+
+    def run():
+        for _ in range(nloop):
+            gpus.runMCMC()
+        gpus.wait()
+    run()
+    t0 = time.perf_counter()
+    run()
+    dt = time.perf_counter() - t0
+    total = nwalkers * nloop * np.float64(nsteps)
+    log(f"MC steps computed: {total}")
+    log(f"MC steps per second: {total / dt:g}")
+    return total / dt

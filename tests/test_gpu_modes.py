@@ -76,3 +76,28 @@ def test_subseq_log_frequencies_match_oracle(cuda, iterbackgrounds):
     want = oracle.subseq_log_frequencies(J, bseqs, sseqs, fixpos, iterbackgrounds, L, q)
     assert got.shape == want.shape
     np.testing.assert_allclose(got, want, rtol=0, atol=2e-4)
+
+
+def test_equilibrate_gen_mode_outputs(cuda, tmp_path):
+    """The reference's `gen` mode (Mi3.py:724-870): walkers from
+    independent-site sequences, fixed or automatic equilibration, and the
+    files it writes -- bicounts (text), bimarg.npy, energies.npy, seqs -- all
+    consistent with the final walkers (counts bit-exact, energies against
+    the FP64 oracle)."""
+    from mi3gpu_b200.inference import benchmark_mcmc, equilibrate
+    L, q, N = 20, 4, 4096
+    J = potts.synthetic_ground_truth(L, q, seed=31, contact_sigma=0.5)
+    uni = np.full((L, q), 1.0 / q)
+    for equiltime in (6, 'auto'):
+        out = tmp_path / str(equiltime)
+        bim, bic, E, walkers = equilibrate(J, N, equiltime, unimarg=uni, alpha="ACGT", outdir=out,
+                                           log=lambda *a: None)
+        mem = oracle.pack_seqs(walkers)
+        np.testing.assert_array_equal(bic, oracle.bicounts(mem, L, q))
+        np.testing.assert_array_equal(np.loadtxt(out / 'bicounts').astype(np.uint32), bic)
+        np.testing.assert_array_equal(np.load(out / 'bimarg.npy'), bim)
+        ref = oracle.energies_f64(J, mem, L, q)
+        assert (np.abs(np.load(out / 'energies.npy') - ref) / np.maximum(1, np.abs(ref))).max() <= 1e-5
+        np.testing.assert_array_equal(seqload.loadSeqs(out / 'seqs', "ACGT")[0], walkers)
+    rate = benchmark_mcmc(J, N, L, 3, seedseq=np.zeros(L, 'u1'), log=lambda *a: None)
+    assert rate > 1e8
