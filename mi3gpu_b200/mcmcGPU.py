@@ -739,8 +739,11 @@ class MCMCGPU:
 
         shape = _full_shape(buftype, bufshape)
         # the large buffers return only their stored part unless asked
-        # otherwise (mcmcGPU.py:845-867)
-        nret = self.nstoredseqs if (bufname in self.largebufs and truncateLarge) else None
+        # otherwise (mcmcGPU.py:845-867) -- those indexed by sequence: the
+        # transposed 'seqL large' (sites first) is returned whole
+        nret = None
+        if bufname in self.largebufs and truncateLarge and bufname != 'seqL large':
+            nret = self.nstoredseqs
 
         def post(b):
             a = b.numpy().view(_base_dtype(buftype))
