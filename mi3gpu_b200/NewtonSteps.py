@@ -382,7 +382,8 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
         # writeStatus (NewtonSteps.py:76-94): the statistics, and the walkers
         # as a bzip2 MSA in the reference's format, formatted on the devices
         (outdir / runName / 'info.txt').write_text(line)
-        gpus.writeSeqs(outdir / runName / 'seqs', 'main', _alpha(param), zipf=True)
+        # compressed and written while the devices run the Newton phase
+        gpus.writeSeqs(outdir / runName / 'seqs', 'main', _alpha(param), zipf=True, background=True)
 
     ns_delta = param.newton_delta or 32
     if param.last_ssr is not None:
@@ -538,4 +539,6 @@ def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
                             seqs if keep else None, es if keep else None)
     if param.device_resident:
         J = gpus.head_gpu.readBufs('J')[0]  # trial J of the last round, as the host path returns
+    if hasattr(gpus, 'flushWrites'):
+        gpus.flushWrites()
     return J

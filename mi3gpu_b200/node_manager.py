@@ -145,14 +145,31 @@ class GPU_node:
         futs = [g.getSeqsText(bufname, alpha) for g in self.gpus]
         return [f.read() for f in futs]
 
-    def writeSeqs(self, fn, bufname='main', alpha=None, zipf=None, headers=None, write_param=False):
+    def writeSeqs(self, fn, bufname='main', alpha=None, zipf=None, headers=None, write_param=False,
+                  background=False):
         """Write the walkers as an MSA file in the reference's format (what
         writeSeqs(fn, collect('seq main'), alpha) writes, seqload.py:353-411),
-        formatting the lines on the devices."""
+        formatting the lines on the devices.  background=True returns once
+        the lines are in host memory and leaves compression and the file
+        write to a background thread (overlapping the devices' next work);
+        flushWrites() waits for them and raises their errors."""
         alpha = alpha if alpha is not None else seqload.default_alpha(self.gpus[0].q)
         parts = self.collectText(bufname, alpha)
-        if self.is_writer:
-            seqload.write_text(fn, [seqload.header_bytes(alpha, headers, write_param)] + parts, zipf)
+        if not self.is_writer:
+            return
+        parts = [seqload.header_bytes(alpha, headers, write_param)] + parts
+        if not background:
+            seqload.write_text(fn, parts, zipf)
+            return
+        pending = self.__dict__.setdefault('_pending_writes', [])
+        pending.append(seqload.background_writer().submit(seqload.write_text, fn, parts, zipf))
+
+    def flushWrites(self):
+        """Wait for the background file writes of writeSeqs."""
+        pending = self.__dict__.get('_pending_writes') or []
+        self._pending_writes = []
+        for f in pending:
+            f.result()
 
     def loadSeqs(self, fn, bufname='main', alpha=None, zipf=None):
         """Fill 'seq <bufname>' of every device, in order, from an MSA file

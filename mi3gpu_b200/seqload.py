@@ -35,6 +35,7 @@ Walkers that live on a device are turned into these lines there
 import bz2
 import json
 import os
+import threading
 from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
@@ -275,7 +276,20 @@ def header_bytes(alpha=alpha21, headers=None, write_param=False):
 def write_text(fn, parts, zipf=None, threads=None):
     """Write byte blocks (bytes or uint8 arrays) in order; bzip2 (zipf True)
     compresses blocks of 8 MiB as independent streams in parallel threads
-    (the compressor releases the interpreter lock)."""
+    (the compressor releases the interpreter lock).  The file appears under
+    its name only when complete (written to a temporary name, then
+    renamed)."""
+    fn = Path(fn)
+    tmp = fn.with_name(f"{fn.name}.{os.getpid()}.{threading.get_ident()}.tmp")
+    try:
+        _write_parts(tmp, parts, zipf, threads)
+        os.replace(tmp, fn)
+    finally:
+        if tmp.exists():
+            tmp.unlink()
+
+
+def _write_parts(fn, parts, zipf, threads):
     views = [memoryview(np.ascontiguousarray(p, np.uint8) if not isinstance(p, (bytes, bytearray)) else p)
              for p in parts]
     if not zipf:
@@ -298,6 +312,18 @@ def write_text(fn, parts, zipf=None, threads=None):
     with open(fn, 'wb') as f, ThreadPoolExecutor(max_workers=max(1, workers)) as ex:
         for data in ex.map(lambda b: bz2.compress(b"".join(b)), blocks):
             f.write(data)
+
+
+_writer = None
+
+
+def background_writer():
+    """One thread that runs file writes in submission order (each write
+    compresses with its own pool of threads)."""
+    global _writer
+    if _writer is None:
+        _writer = ThreadPoolExecutor(max_workers=1, thread_name_prefix="msa-writer")
+    return _writer
 
 
 def writeSeqs(fn, seqs, alpha=alpha21, ids=None, headers=None, write_param=False, zipf=None):

@@ -106,3 +106,26 @@ def test_headers_and_param_alphabet(tmp_path):
     np.testing.assert_array_equal(back, seqs)
     assert headers[1:] == ["made here\n", "second\n"]
     assert headers[0].startswith("PARAM")
+
+
+def test_background_writes_and_atomic_files(tmp_path):
+    """GPU_node.writeSeqs(background=True): the file appears complete once
+    flushWrites returns, no temporary file is left, and an error in the
+    background write is raised by flushWrites."""
+    from mi3gpu_b200 import GPU_node
+    from tests.fake_device import FakeMCMCGPU
+    L, q, N = 9, 4, 512
+    g = FakeMCMCGPU(L, q, N, seed=1)
+    node = GPU_node([g])
+    seqs = np.random.default_rng(2).integers(0, q, size=(N, L)).astype('u1')
+    node.setSeqs('main', seqs)
+    node.writeSeqs(tmp_path / "a", alpha="ACGT", zipf=True, background=True)
+    node.writeSeqs(tmp_path / "b", alpha="ACGT", background=True)
+    node.flushWrites()
+    for name in ("a", "b"):
+        np.testing.assert_array_equal(seqload.loadSeqs(tmp_path / name, "ACGT")[0], seqs)
+    assert sorted(p.name for p in tmp_path.iterdir()) == ["a", "b"]
+    node.writeSeqs(tmp_path / "missing_dir" / "c", alpha="ACGT", background=True)
+    with pytest.raises(FileNotFoundError):
+        node.flushWrites()
+    node.flushWrites()  # nothing pending any more
