@@ -400,8 +400,11 @@ def run_kernels(args):
     st = torch.cuda.current_stream(dev)
     s = st.cuda_stream
     rows = []
-    for (L, q, N) in [(232, 21, 1 << 20), (99, 4, 1 << 18), (48, 4, 16384), (512, 21, 1 << 19), (128, 8, 1 << 18),
-                      (150, 5, 1 << 18), (150, 6, 1 << 18), (150, 12, 1 << 18)]:
+    shapes = [(232, 21, 1 << 20), (99, 4, 1 << 18), (48, 4, 16384), (512, 21, 1 << 19), (128, 8, 1 << 18),
+              (150, 5, 1 << 18), (150, 6, 1 << 18), (150, 12, 1 << 18)]
+    if args.shape:
+        shapes = [tuple(int(x) for x in args.shape.split(","))]
+    for (L, q, N) in shapes:
         g = torch.Generator(device=dev)
         g.manual_seed(L * q)
         sw = (L - 1) // 4 + 1
@@ -541,6 +544,110 @@ def run_msa(args):
     out["write_plain_speedup"] = out["write_plain_host_s"] / out["write_plain_device_s"]
     out["load_plain_speedup"] = out["load_plain_host_s"] / out["load_plain_device_s"]
     print(json.dumps(out))
+
+
+def run_streams(args):
+    """The HBM-stream kernels of the quasi-Newton step and the round at
+    L=232, q=21 with 2^20 walkers: CUDA-event time per launch (after a
+    warm-up; every buffer is larger than L2 or read once per launch) and
+    achieved GB/s = algorithmic bytes / time, against the measured HBM
+    copy bandwidth.  Algorithmic bytes: each coupling-sized array (nPairs x
+    q^2 floats, 47.3 MB) read or written once, per-walker arrays (4 MB)
+    likewise, sequences 4*SWORDS bytes per walker."""
+    import torch
+    from mi3gpu_b200 import _lib
+    L, q, N = args.L, args.q, args.walkers
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream(dev)
+    s = st.cuda_stream
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    g = torch.Generator(device=dev).manual_seed(5)
+    npairs, qq, sw = L * (L - 1) // 2, q * q, (L - 1) // 4 + 1
+    nJ = npairs * qq
+    rnd = lambda n, lo=0.0, hi=1.0: torch.rand(n, device=dev, generator=g) * (hi - lo) + lo
+    bt, bi, J, dJ = rnd(nJ, 1e-4, 1e-2), rnd(nJ, 1e-4, 1e-2), rnd(nJ, -0.1, 0.1), rnd(nJ, -0.01, 0.01)
+    Jo = torch.empty_like(J)
+    cnt = torch.randint(0, N, (nJ,), device=dev, dtype=torch.int32, generator=g)
+    dE = rnd(N, -2.0, 2.0)
+    w = torch.empty(N, device=dev)
+    out2 = torch.empty(2, device=dev)
+    out2d = torch.empty(2, device=dev, dtype=torch.float64)
+    minout = torch.empty(1, device=dev)
+    wsr = torch.zeros(int(_lib.query("mi3_weight_stats_workspace", N)) // 8 + 2, dtype=torch.int64, device=dev)
+    wsg = torch.zeros(int(_lib.query("mi3_gauge_workspace", L, q)) // 8 + 2, dtype=torch.int64, device=dev)
+    wss = torch.zeros(int(_lib.query("mi3_bimarg_stats_workspace", L)) // 8 + 2, dtype=torch.int64, device=dev)
+    stats = torch.empty(6, device=dev, dtype=torch.float64)
+    stride = int(_lib.query("mi3_jrows_stride", L, q))
+    Jrows = torch.empty(L * stride, device=dev)
+    seq = torch.randint(0, q, (sw * 4, N), dtype=torch.uint8, device=dev, generator=g)
+    seq[L:] = 0
+    seq = seq.view(sw, 4, N).permute(0, 2, 1).contiguous().view(torch.int32).view(sw, N)
+    seqL = torch.empty((L, N // 4), dtype=torch.int32, device=dev)
+    rng = torch.zeros(N * 4, dtype=torch.int32, device=dev)
+    cprob = torch.cumsum(torch.full((L, q), 1.0 / q, device=dev), 1)[:, :q - 1].contiguous()
+    seq2 = torch.empty_like(seq)
+    MB = 1e6
+    Jb, Wb, Sb = nJ * 4, N * 4, sw * N * 4
+    calls = [
+        ("k_update_j", 4 * Jb, lambda: _lib.call("mi3_update_j", bt.data_ptr(), bi.data_ptr(), 4e-4, 1e-3,
+                                                 J.data_ptr(), Jo.data_ptr(), L, q, s)),
+        ("k_reg_lz (l1z)", 4 * Jb, lambda: _lib.call("mi3_reg_l1z", bi.data_ptr(), 4e-4, 1e-3, 2e-4, J.data_ptr(),
+                                                    dJ.data_ptr(), L, q, s)),
+        ("k_renormalize", 2 * Jb, lambda: _lib.call("mi3_renormalize_bimarg", bi.data_ptr(), L, q, s)),
+        ("k_bicounts_to_bimarg", 2 * Jb, lambda: _lib.call("mi3_bicounts_to_bimarg", cnt.data_ptr(), Jo.data_ptr(),
+                                                           N, L, q, s)),
+        ("k_add_float_bufs", 3 * Jb, lambda: _lib.call("mi3_add_float_bufs", Jo.data_ptr(), dJ.data_ptr(), nJ, s)),
+        ("gauge (fieldless even)", 2 * Jb, lambda: _lib.call("mi3_gauge_fieldless_even", J.data_ptr(),
+                                                              Jo.data_ptr(), L, q, wsg.data_ptr(),
+                                                              wsg.numel() * 8, s)),
+        ("bimarg stats (FP64)", 3 * Jb, lambda: _lib.call("mi3_bimarg_stats", bt.data_ptr(), bi.data_ptr(),
+                                                           J.data_ptr(), L, q, stats.data_ptr(), wss.data_ptr(),
+                                                           wss.numel() * 8, s)),
+        ("k_unpack_j", Jb + L * stride * 4, lambda: _lib.call("mi3_unpack_j", J.data_ptr(), Jrows.data_ptr(), L, q,
+                                                              s)),
+        ("weights fused (k_reduce)", 2 * Wb, lambda: _lib.call("mi3_weights_fused", 0.0, dE.data_ptr(),
+                                                               w.data_ptr(), N, minout.data_ptr(),
+                                                               out2.data_ptr(), out2d.data_ptr(), wsr.data_ptr(),
+                                                               wsr.numel() * 8, s)),
+        ("k_dE_to_weights", 2 * Wb, lambda: _lib.call("mi3_dE_to_weights", 0.0, dE.data_ptr(), w.data_ptr(), N,
+                                                      s)),
+        ("weight stats", Wb, lambda: _lib.call("mi3_weight_stats", w.data_ptr(), N, out2.data_ptr(),
+                                               out2d.data_ptr(), wsr.data_ptr(), wsr.numel() * 8, s)),
+        ("k_min_floats", Wb, lambda: _lib.call("mi3_min_floats", dE.data_ptr(), N, minout.data_ptr(), s)),
+        ("k_repack_T", 2 * Sb, lambda: _lib.call("mi3_repack_seqs_T", seq.data_ptr(), N, seqL.data_ptr(), N // 4,
+                                                 L, s)),
+        ("k_init_rng", 4 * N * 4, lambda: _lib.call("mi3_init_rng", rng.data_ptr(), N, 0, (2 ** 63) // (2 * N),
+                                                    s)),
+        ("k_gen_indep", Sb + 2 * 4 * N * 4, lambda: _lib.call("mi3_gen_indep", seq2.data_ptr(), N, N,
+                                                              rng.data_ptr(), cprob.data_ptr(), L, q, s)),
+    ]
+    # L2 flushed before every timed launch (a 256 MB write), the launch
+    # alone between the events
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+
+    def time_flushed(fn, reps=10):
+        fn()
+        fn()
+        tot = 0.0
+        for r in range(reps):
+            flush.fill_(float(r))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / reps
+
+    rows = []
+    for name, nbytes, fn in calls:
+        ms = time_flushed(fn)
+        rows.append({"kernel": name, "ms": ms, "algorithmic_MB": nbytes / MB, "GBps": nbytes / ms / 1e6,
+                     "frac_of_hbm": nbytes / ms / 1e6 / hbm})
+    print(json.dumps({"mode": "streams", "config": {"workload": f"HBM-stream kernels, L={L} q={q} walkers={N}",
+                                                    "l2": "flushed (256 MB write) before every timed launch"},
+                      "hbm_peak_GBps": hbm, "rows": rows}))
 
 
 def run_batched(args):
@@ -832,7 +939,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--newton-steps", type=int, default=10, help="quasi-Newton steps to time (0: skip)")
     ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned", "batched", "graph_small",
-                                                           "msa"],
+                                                           "msa", "streams"],
                     help="inference: run full quasi-Newton rounds and report s/iter and SSR")
     ap.add_argument("--rounds", type=int, default=4, help="inference rounds (--mode inference)")
     ap.add_argument("--msa", type=int, default=1 << 16, help="synthetic MSA size (--mode inference)")
@@ -842,6 +949,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="built-in kernel schedules instead of autotuned ones")
     ap.add_argument("--no-inference", action="store_true", help="skip the s/iter comparison of the default run")
     ap.add_argument("--forms", default="", help="comma list of forms for --mode inference (default: all)")
+    ap.add_argument("--shape", default="", help="L,q,N: one shape for --mode kernels")
     args = ap.parse_args()
     rank, world, _ = env_rank()
 
@@ -888,6 +996,9 @@ def main():
         return
     if args.mode == "msa":
         run_msa(args)
+        return
+    if args.mode == "streams":
+        run_streams(args)
         return
     out, J = run_gpu(args)
     if rank == 0 and world == 1 and not args.no_inference:

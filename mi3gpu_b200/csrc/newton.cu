@@ -125,6 +125,11 @@ __device__ __forceinline__ float warp_min(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_down_sync(0xffffffffu, v, o));
     return v;
 }
+__device__ __forceinline__ double warp_min_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
 
 // in = dE when RM_WEIGHTS (weights computed as exp(-dE + ref)), else weights.
 __global__ void __launch_bounds__(RED_THREADS) k_reduce(const float *__restrict__ in, uint32_t n,
@@ -133,7 +138,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce(const float *__restrict_
     const float ref = ref_dev ? *ref_dev : ref_host;
     unsigned int *ticket = reinterpret_cast<unsigned int *>(ws);
     double *part = reinterpret_cast<double *>(ws + 16);
-    __shared__ double s_sum[RED_THREADS / 32], s_sum2[RED_THREADS / 32];
+    __shared__ double s_sum[RED_THREADS / 32], s_sum2[RED_THREADS / 32], s_mind[RED_THREADS / 32];
     __shared__ float s_min[RED_THREADS / 32];
     __shared__ bool s_last;
     double a = 0.0, b = 0.0;
@@ -177,14 +182,33 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce(const float *__restrict_
         s_last = (t == gridDim.x - 1);
     }
     __syncthreads();
-    if (s_last && threadIdx.x == 0) {
+    // the last CTA combines the partials: every thread loads its share from
+    // L2 (ld.global.cg: written by other CTAs, ordered by their fences and
+    // the ticket), then warp shuffles and a fixed pass over the warps -- a
+    // fixed order, so the sums are deterministic
+    if (s_last) {
         __threadfence();
-        volatile double *vp = part;
         double ta = 0.0, tb = 0.0, tm = 0.0;
-        for (uint32_t k = 0; k < gridDim.x; ++k) {
-            ta += vp[4 * k + 0];
-            tb += vp[4 * k + 1];
-            tm = fmin(tm, vp[4 * k + 2]);
+        for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+            ta += __ldcg(&part[4 * k + 0]);
+            tb += __ldcg(&part[4 * k + 1]);
+            tm = fmin(tm, __ldcg(&part[4 * k + 2]));
+        }
+        ta = warp_sum(ta);
+        tb = warp_sum(tb);
+        tm = warp_min_d(tm);
+        if (lane == 0) {
+            s_sum[warp] = ta;
+            s_sum2[warp] = tb;
+            s_mind[warp] = tm;
+        }
+        __syncthreads();
+        if (threadIdx.x != 0) return;
+        ta = 0.0, tb = 0.0, tm = 0.0;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+            ta += s_sum[w];
+            tb += s_sum2[w];
+            tm = fmin(tm, s_mind[w]);
         }
         if (mode & RM_STATS) {
             o.stats[0] = (float)ta;

@@ -68,11 +68,12 @@ def test_unpack_j_bitexact(cuda, L, q, N):
     np.testing.assert_array_equal(host(Ju), oracle.unpack_j(J, L, q))
 
 
-@pytest.mark.parametrize("L,q,N", SHAPES)
+@pytest.mark.parametrize("L,q,N", SHAPES + [(26, 32, 512), (30, 40, 512)])
 @pytest.mark.parametrize("nsteps", [1, 37, 300])
 def test_metropolis_trajectory_bitexact(cuda, L, q, N, nsteps):
     """Same walkers, same RNG streams, same site list: identical sequences and
-    RNG states after nsteps proposals."""
+    RNG states after nsteps proposals (shapes with 5-bit and byte residues in
+    shared memory, q=32 the largest 5-bit alphabet, q=40 above it)."""
     J = random_model(L, q, 2, sigma=0.5)
     seqs = _seqs(L, q, N, 3)
     mem = oracle.pack_seqs(seqs)
