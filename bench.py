@@ -876,7 +876,10 @@ def run_inference(args):
       chosen     J resident; walkers carried over between rounds (reseed
                  'none'): 128 sweeps in the first round, args.chosen_sweeps
                  after it
-      chosen_half  as chosen with half as many sweeps per round."""
+      chosen_half  as chosen with half as many sweeps per round
+      chosen_files as chosen, writing the reference's run directories
+                 (J.npy, seqs, info.txt, ... per round) into a temporary
+                 directory."""
     from mi3gpu_b200.inference import make_target, infer
     from mi3gpu_b200.autotune import Autotuner
     tuner = None if args.no_tune else Autotuner(ROOT / "_build" / "autotune.json")
@@ -887,7 +890,9 @@ def run_inference(args):
              ("plain_dev", dict(reseed="independent", sweeps=128, device_resident=True)),
              ("chosen", dict(reseed="none", sweeps=args.chosen_sweeps, sweeps_first=128, device_resident=True)),
              ("chosen_half", dict(reseed="none", sweeps=max(1, args.chosen_sweeps // 2), sweeps_first=128,
-                                  device_resident=True)))
+                                  device_resident=True)),
+             ("chosen_files", dict(reseed="none", sweeps=args.chosen_sweeps, sweeps_first=128,
+                                   device_resident=True, outdir="tmp")))
     if args.forms:
         keep = args.forms.split(",")
         forms = tuple(f for f in forms if f[0] in keep)
@@ -895,7 +900,9 @@ def run_inference(args):
     for name, kw in forms:
         logs = []
         w0 = time.time()
-        res = infer(target, args.L, args.q, args.walkers, args.rounds, log=logs.append, tuner=tuner, **kw)
+        with tempfile.TemporaryDirectory() as tmpdir:
+            run_kw = dict(kw, outdir=Path(tmpdir)) if kw.get("outdir") else kw
+            res = infer(target, args.L, args.q, args.walkers, args.rounds, log=logs.append, tuner=tuner, **run_kw)
         wall = time.time() - w0
         hist = res["history"]
         cum = np.cumsum([h["round_s"] for h in hist]).tolist()
