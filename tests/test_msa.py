@@ -129,3 +129,56 @@ def test_background_writes_and_atomic_files(tmp_path):
     with pytest.raises(FileNotFoundError):
         node.flushWrites()
     node.flushWrites()  # nothing pending any more
+
+
+from hypothesis import given, settings, strategies as st
+
+
+@st.composite
+def _msa_case(draw):
+    alpha = "".join(draw(st.permutations(list("ACDEFGHIKLMNPQRSTVWY-")))[:draw(st.integers(2, 21))])
+    n = draw(st.integers(1, 40))
+    L = draw(st.integers(1, 30))
+    seqs = np.array(draw(st.lists(st.lists(st.integers(0, len(alpha) - 1), min_size=L, max_size=L),
+                                  min_size=n, max_size=n)), dtype='u1').reshape(n, L)
+    ids = None
+    if draw(st.booleans()):
+        ids = [draw(st.text(alphabet="abcxyz0123456789_", min_size=1, max_size=8)) for _ in range(n)]
+    return alpha, seqs, ids
+
+
+@settings(max_examples=150, deadline=None)
+@given(_msa_case())
+def test_round_trip_and_oracle_agree(case):
+    """Any alphabet, size and id field: writer -> reader is the identity,
+    and the oracle's line parser reads the same residues."""
+    alpha, seqs, ids = case
+    raw = bytes(seqload.header_bytes(alpha, ["x"], True)) + bytes(seqload.format_lines(seqs, alpha, ids))
+    msa = seqload.parse(raw, alpha)
+    back, back_ids = seqload.check(msa)
+    np.testing.assert_array_equal(back, seqs)
+    if ids is not None:
+        assert [x.decode() for x in back_ids] == ids
+    mem, first = oracle.text_to_seqs(msa.body, msa.nseq, msa.line_len, msa.id_len, msa.L, alpha)
+    assert first is None
+    np.testing.assert_array_equal(oracle.unpack_seqs(mem, msa.L), seqs)
+
+
+@settings(max_examples=150, deadline=None)
+@given(_msa_case(), st.data())
+def test_one_corrupt_byte_is_flagged_on_its_line(case, data):
+    """One byte of one line replaced by a character outside the alphabet
+    (not a newline): the reader raises for that line and the oracle's
+    parser flags the same line."""
+    alpha, seqs, ids = case
+    body = bytearray(seqload.format_lines(seqs, alpha, ids))
+    line_len = len(body) // seqs.shape[0]
+    id_len = line_len - seqs.shape[1] - 1
+    line = data.draw(st.integers(0, seqs.shape[0] - 1))
+    col = data.draw(st.integers(id_len, line_len - 2))  # a residue position
+    body[line * line_len + col] = ord('#') if line or col else ord('!')
+    msa = seqload.parse(bytes(body), alpha)
+    with pytest.raises(ValueError, match=f"sequence {line + 1} position {col - id_len}"):
+        seqload.check(msa)
+    _, first = oracle.text_to_seqs(msa.body, msa.nseq, msa.line_len, msa.id_len, msa.L, alpha)
+    assert first == line
