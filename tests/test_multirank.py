@@ -4,6 +4,7 @@ sum of bimarginal counts / weighted bimarginals, the min of dE and the FP64
 weight sums -- reproduce the single-process results."""
 import os
 import socket
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -266,3 +267,53 @@ def test_two_rank_device_resident_rounds_agree():
     assert res[0]["ssr"] == res[1]["ssr"] and res[0]["steps"] == res[1]["steps"]
     assert all(np.isfinite(res[0]["ssr"]))
     np.testing.assert_array_equal(res[0]["J"], res[1]["J"])
+
+
+def _msa_worker(rank, world, port, out):
+    """RankNode's MSA files: writeSeqs gathers every rank's walkers and rank
+    0 writes them in rank order; loadSeqs hands each rank its share."""
+    import torch.distributed as dist
+    from mi3gpu_b200.distributed import RankNode
+    from tests.fake_device import FakeMCMCGPU
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    L, q, n_per = 7, 4, 512
+    seqs = np.random.default_rng(3).integers(0, q, size=(world * n_per, L)).astype('<u1')
+    g = FakeMCMCGPU(L, q, n_per, seed=1 + rank)
+    node = RankNode(g)
+    node.setSeqs('main', seqs[rank * n_per:(rank + 1) * n_per])
+    path = Path(os.environ["MSA_TEST_DIR"]) / "walkers"
+    node.writeSeqs(path, 'main', "ACGT", zipf=True)
+    dist.barrier()
+    g.bufs['seq main'][...] = 0
+    node.loadSeqs(path, 'main', "ACGT")
+    try:
+        node.head_node
+        refused = False
+    except Exception:
+        refused = True
+    out.put(dict(rank=rank, mine=g.getBuf('seq main').read(), refused=refused))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_msa_files(tmp_path, monkeypatch):
+    from mi3gpu_b200 import seqload
+    monkeypatch.setenv("MSA_TEST_DIR", str(tmp_path))
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_guarded, args=(_msa_worker, r, 2, port, out)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted([out.get(timeout=180) for _ in range(2)], key=lambda r: r["rank"])
+    assert not any("error" in r for r in res), res
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    seqs = np.random.default_rng(3).integers(0, 4, size=(1024, 7)).astype('<u1')
+    np.testing.assert_array_equal(seqload.loadSeqs(tmp_path / "walkers", "ACGT")[0], seqs)
+    for r in res:
+        np.testing.assert_array_equal(r["mine"], seqs[r["rank"] * 512:(r["rank"] + 1) * 512])
+        assert r["refused"]
