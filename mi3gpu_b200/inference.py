@@ -52,7 +52,7 @@ def make_target(L, q, n_msa, seed, sweeps=None, contact_sigma=0.5, device=0):
 
 def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e-4, damping=1e-3,
           reg=('l1z', (2e-4,)), seed=1234, device=0, log=print, fused=True, outdir=None, reseed='independent',
-          sweeps_first=None, device_resident=True, tuner=None, distribute_jstep='all'):
+          sweeps_first=None, device_resident=True, tuner=None, distribute_jstep='all', alpha=None):
     """Run `rounds` quasi-Newton iterations from the independent model;
     returns the per-round history (SSR, wall seconds of MCMC and Newton
     phases) as recorded by NewtonSteps.MCMCstep.
@@ -67,7 +67,9 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
     autotune.Autotuner whose sampler plan and count kernel are installed
     (results do not depend on them).  distribute_jstep: 'all' runs the
     Newton steps over the walkers where they are; 'head_gpu' first gathers
-    them into the device's large buffer, as the reference's option does."""
+    them into the device's large buffer, as the reference's option does.
+    alpha: the residue letters of the run directories' MSA files (default
+    seqload.default_alpha(q))."""
     potts.check_target(target)  # as the reference's set-up does (Mi3.py:1029-1034)
     unimarg = potts.getUnimarg(target)
     J0 = potts.independent_couplings(unimarg)
@@ -78,7 +80,7 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
                   distribute_jstep=distribute_jstep, L=L, q=q, couplings=J0, nsteps=nsteps,
                   equiltime=max(1, sweeps * L // nsteps), trackequil=0, outdir=outdir, mcmcsteps=rounds,
                   newton_delta=32, reseed=reseed, rngseed=seed + 1, unimarg=unimarg, fused=fused, init_indep=True,
-                  device_resident=device_resident,
+                  device_resident=device_resident, alpha=alpha,
                   equiltime_first=None if sweeps_first is None else max(1, sweeps_first * L // nsteps)))
     g = MCMCGPU((device, 0), L, q, nwalkers, 512, outdir, 1024, seed + 1)
     gpus = GPU_node([g])

@@ -50,10 +50,14 @@ _BZ2_BLOCK = 8 * 1024 * 1024  # bytes per independently compressed stream
 
 
 def default_alpha(q):
-    """The protein alphabet for q = 21, its first q letters for smaller q."""
-    if q > len(alpha21):
+    """The protein alphabet for q = 21, its first q letters for smaller q;
+    for larger q it continues with the other printable ASCII characters
+    except '#' (a header line marker) and '/' (the Stockholm terminator)."""
+    extra = "".join(chr(c) for c in range(33, 127) if chr(c) not in alpha21 + "#/")
+    full = alpha21 + extra
+    if q > len(full):
         raise ValueError(f"no default alphabet for q={q}; give alpha")
-    return alpha21[:q]
+    return full[:q]
 
 
 def _as_bytes(alpha):

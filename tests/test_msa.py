@@ -182,3 +182,11 @@ def test_one_corrupt_byte_is_flagged_on_its_line(case, data):
         seqload.check(msa)
     _, first = oracle.text_to_seqs(msa.body, msa.nseq, msa.line_len, msa.id_len, msa.L, alpha)
     assert first == line
+
+
+def test_default_alphabet_beyond_21_letters(tmp_path):
+    a = seqload.default_alpha(80)
+    assert a[:21] == seqload.alpha21 and len(set(a)) == 80 and not set(a) & set("#/ \n")
+    seqs = np.random.default_rng(0).integers(0, 80, size=(50, 11)).astype('u1')
+    seqload.writeSeqs(tmp_path / "s", seqs, a)
+    np.testing.assert_array_equal(seqload.loadSeqs(tmp_path / "s", a)[0], seqs)
