@@ -194,13 +194,20 @@ def track_main_bufs(param, gpus, savedir=None, step=None):
     bicounts, energies = gpus.collect(['bicount', 'E main'])
     bimarg_model = bicounts.astype('f4') / np.float32(np.sum(bicounts[0, :]))
     if savedir is not None:
-        if 'bim' in (param.tracked or ''):
+        if 'bim' in (param.tracked or '') and _writer(gpus):
             np.save(savedir / f'bimarg_{step}', bimarg_model)
-        if 'E' in (param.tracked or ''):
+        if 'E' in (param.tracked or '') and _writer(gpus):
             np.save(savedir / f'energies_{step}', energies)
         if 'seq' in (param.tracked or ''):
             gpus.writeSeqs(savedir / f'seqs_{step}', 'main', _alpha(param), zipf=True)
     return energies, bimarg_model
+
+
+def _writer(gpus):
+    """Whether this process writes the output files: always, except on the
+    ranks other than 0 of a RankNode (each rank runs the same round loop;
+    collectives run everywhere, files are written once)."""
+    return getattr(gpus, 'is_writer', True)
 
 
 def _alpha(param):
@@ -300,7 +307,7 @@ def NewtonSteps(runName, param, bimarg_model, gpus, log):
         Jsteps, newJ, bimarg_p = iterNewton(param, bimarg_model, gpus, log, fused=bool(param.fused))
         if outdir is not None and param.device_resident:
             (bimarg_p,), (newJ,) = gpus.head_gpu.readBufs(['bi', 'J'])
-        if outdir is not None:
+        if outdir is not None and _writer(gpus):
             np.save(outdir / runName / 'predictedBimarg', bimarg_p)
             np.save(outdir / runName / 'perturbedJ', newJ)
     else:
@@ -356,9 +363,10 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
     if outdir is not None:
         rundir = outdir / runName
         rundir.mkdir(parents=True, exist_ok=True)
-        np.save(rundir / 'J', couplings)
-        (rundir / 'newtonsteps').write_text(str(param.newtonSteps))
-        (rundir / 'jstep').write_text(str(Jstep))
+        if _writer(gpus):
+            np.save(rundir / 'J', couplings)
+            (rundir / 'newtonsteps').write_text(str(param.newtonSteps))
+            (rundir / 'jstep').write_text(str(Jstep))
 
     start_time = time.time()
     (bimarg_model, bicount, sampledenergies, e_rho, ptinfo,
@@ -381,7 +389,8 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
     if outdir is not None:
         # writeStatus (NewtonSteps.py:76-94): the statistics, and the walkers
         # as a bzip2 MSA in the reference's format, formatted on the devices
-        (outdir / runName / 'info.txt').write_text(line)
+        if _writer(gpus):
+            (outdir / runName / 'info.txt').write_text(line)
         # compressed and written while the devices run the Newton phase
         gpus.writeSeqs(outdir / runName / 'seqs', 'main', _alpha(param), zipf=True, background=True)
 
@@ -401,7 +410,8 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
     param.newtonSteps = min(2048, Jsteps + ns_delta)
     log(f"Increasing newtonsteps to {param.newtonSteps}")
     if outdir is not None:
-        (outdir / runName / 'nsteps').write_text(str(Jsteps))
+        if _writer(gpus):
+            (outdir / runName / 'nsteps').write_text(str(Jsteps))
     return Jstep + Jsteps, seqs, sampledenergies, newJ
 
 
@@ -456,7 +466,8 @@ def preOpt(param, gpus, log):
     if param.outdir is not None:
         d = Path(param.outdir) / 'preopt'
         d.mkdir(parents=True, exist_ok=True)
-        (d / 'info.txt').write_text(printstats('preopt', 0, param.bimarg, bimarg, J, es, None))
+        if _writer(gpus):
+            (d / 'info.txt').write_text(printstats('preopt', 0, param.bimarg, bimarg, J, es, None))
         gpus.writeSeqs(d / 'seqs', 'main', _alpha(param), zipf=True)
     Jsteps, newJ = NewtonSteps('preopt', param, bimarg, gpus, log)
     if newJ is None:  # device-resident: J + dJ stays on the devices
@@ -520,7 +531,8 @@ def newtonMCMC(param, gpus, start_run, Jstep, log, resume=None):
             if param.outdir is not None:
                 rundir = Path(param.outdir) / runname
                 rundir.mkdir(parents=True, exist_ok=True)
-                (rundir / 'seedseq').write_text("".join(_alpha(param)[c] for c in seed))
+                if _writer(gpus):
+                    (rundir / 'seedseq').write_text("".join(_alpha(param)[c] for c in seed))
             gpus.fillSeqs(seed)
         elif param.reseed == 'independent' or (param.reseed == 'none' and first and param.init_indep
                                                 and not param.preopt):

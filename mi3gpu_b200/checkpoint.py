@@ -24,6 +24,16 @@ FORMAT = 1
 _PARAM_KEYS = ('newtonSteps', 'max_newtonSteps', 'last_ssr', 'min_ssr', 'history', 'seedseq')
 
 
+def rank_path(path, gpus):
+    """The checkpoint file of this process: `path` itself, or, when the
+    devices are spread over ranks (distributed.RankNode, one device per
+    rank), `path` with '.rank<r>' appended -- each rank checkpoints its own
+    walkers and resumes from its own file."""
+    path = Path(path)
+    world = getattr(gpus, 'world', 1)
+    return path if world <= 1 else path.with_name(f"{path.name}.rank{gpus.rank}")
+
+
 def device_state(gpu):
     """Host copy of one device's sampling state."""
     get = getattr(gpu, 'state_dict', None)
@@ -50,7 +60,7 @@ def save(path, gpus, param, next_run, Jstep, J, rng, seqs=None, es=None):
         'devices': [device_state(g) for g in gpus.gpus],
         'shape': (int(param.L), int(param.q), int(gpus.nwalkers)),
     }
-    path = Path(path)
+    path = rank_path(path, gpus)
     path.parent.mkdir(parents=True, exist_ok=True)
     tmp = path.with_name(f"{path.name}.{os.getpid()}.tmp")
     with open(tmp, 'wb') as f:

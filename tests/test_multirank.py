@@ -214,9 +214,14 @@ def test_two_rank_head_gpu_newton_phase_equals_single_process():
     np.testing.assert_array_equal(res[0]["bi"], bt)
 
 
-def _rounds_worker(rank, world, port, out):
+def _rounds_worker_files(rank, world, port, out):
+    _rounds_worker(rank, world, port, out, files=True)
+
+
+def _rounds_worker(rank, world, port, out, files=False):
     """Two device-resident rounds (sampling on each rank's own walkers,
-    Newton phase reduced across ranks) through RankNode."""
+    Newton phase reduced across ranks) through RankNode; with files, the
+    run directories and per-rank checkpoints as well."""
     import torch.distributed as dist
     from mi3gpu_b200 import NewtonSteps, potts
     from mi3gpu_b200.distributed import RankNode
@@ -240,10 +245,19 @@ def _rounds_worker(rank, world, port, out):
                   couplings=np.zeros((L * (L - 1) // 2, q * q), '<f4'), nsteps=4 * L, equiltime=4, trackequil=0,
                   outdir=None, mcmcsteps=2, newton_delta=8, reseed='none', rngseed=3, init_indep=True,
                   device_resident=True, unimarg=potts.getUnimarg(target)))
+    if files:
+        d = Path(os.environ["MSA_TEST_DIR"])
+        p.update(outdir=d / "out", checkpoint=d / "ck", alpha="ABC")
     node.prepare_indep(p.unimarg)
     J = NewtonSteps.newtonMCMC(p, node, 0, 0, lambda *a: None)
-    out.put(dict(rank=rank, J=J, ssr=[h['ssr'] for h in p.history], steps=[h['newton_steps'] for h in p.history],
-                 N=node.nwalkers))
+    res = dict(rank=rank, J=J, ssr=[h['ssr'] for h in p.history], steps=[h['newton_steps'] for h in p.history],
+               N=node.nwalkers)
+    if files:
+        from mi3gpu_b200 import checkpoint
+        st = checkpoint.load(checkpoint.rank_path(p.checkpoint, node))
+        res['ck_walkers'] = st['devices'][0]['seq main']
+        res['walkers'] = g.bufs['seq main'].copy()
+    out.put(res)
     dist.barrier()
     dist.destroy_process_group()
 
@@ -317,3 +331,34 @@ def test_two_rank_msa_files(tmp_path, monkeypatch):
     for r in res:
         np.testing.assert_array_equal(r["mine"], seqs[r["rank"] * 512:(r["rank"] + 1) * 512])
         assert r["refused"]
+
+
+def test_two_rank_rounds_write_run_directories_once_and_checkpoint_per_rank(tmp_path, monkeypatch):
+    """With outdir and checkpoints over two ranks: the run directories hold
+    the reference's files (written by rank 0; the walker file gathers both
+    ranks' walkers in rank order), and each rank checkpoints its own
+    walkers in its own file."""
+    from mi3gpu_b200 import seqload
+    monkeypatch.setenv("MSA_TEST_DIR", str(tmp_path))
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_guarded, args=(_rounds_worker_files, r, 2, port, out)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted([out.get(timeout=180) for _ in range(2)], key=lambda r: r["rank"])
+    assert not any("error" in r for r in res), res
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for run in ("run_0", "run_1"):
+        for f in ("J.npy", "jstep", "newtonsteps", "info.txt", "seqs", "nsteps"):
+            assert (tmp_path / "out" / run / f).exists(), (run, f)
+    assert sorted(x.name for x in tmp_path.iterdir()) == ["ck.rank0", "ck.rank1", "out"]
+    from oracle import oracle
+    walkers = seqload.loadSeqs(tmp_path / "out" / "run_1" / "seqs", "ABC")[0]
+    both = np.concatenate([oracle.unpack_seqs(r["walkers"], 6) for r in res])
+    np.testing.assert_array_equal(walkers, both)
+    for r in res:
+        np.testing.assert_array_equal(r["ck_walkers"], r["walkers"])
+    assert not np.array_equal(res[0]["walkers"], res[1]["walkers"])
