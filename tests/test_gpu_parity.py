@@ -68,12 +68,14 @@ def test_unpack_j_bitexact(cuda, L, q, N):
     np.testing.assert_array_equal(host(Ju), oracle.unpack_j(J, L, q))
 
 
-@pytest.mark.parametrize("L,q,N", SHAPES + [(26, 32, 512), (30, 40, 512)])
+@pytest.mark.parametrize("L,q,N", SHAPES + [(26, 32, 512), (30, 40, 512), (2, 2, 128), (50, 21, 512)])
 @pytest.mark.parametrize("nsteps", [1, 37, 300])
 def test_metropolis_trajectory_bitexact(cuda, L, q, N, nsteps):
     """Same walkers, same RNG streams, same site list: identical sequences and
     RNG states after nsteps proposals (shapes with 5-bit and byte residues in
-    shared memory, q=32 the largest 5-bit alphabet, q=40 above it)."""
+    shared memory, q=32 the largest 5-bit alphabet, q=40 above it, the
+    smallest model L=2 q=2, and L=50 whose last 24-site chunk holds 2 sites,
+    less than one 5-bit word)."""
     J = random_model(L, q, 2, sigma=0.5)
     seqs = _seqs(L, q, N, 3)
     mem = oracle.pack_seqs(seqs)
