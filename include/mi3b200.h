@@ -157,9 +157,13 @@ int mi3_energies_tc(const float *J, const uint32_t *seqmem, uint32_t buflen, uin
  * reference: it is an addition of this library.  The accumulators live in
  * an array inside the library: 8 MiB on every GPU where the library's
  * kernels are loaded, held until the process exits.  nseq above
- * MI3_ENERGIES_NOALLOC_MAX_SEQ is rejected with MI3_ERR_ARG.  The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress)
- * with that device current; make that first call before any stream capture.
+ * MI3_ENERGIES_NOALLOC_MAX_SEQ is rejected with MI3_ERR_ARG.  Every call made
+ * outside stream capture looks up the array's device address
+ * (cudaGetSymbolAddress) for the current device, so a device reset leaves no
+ * stale address; a call made during capture reuses the address of the last
+ * call made outside capture on that device.  So make one call on each
+ * device (nseq = 0 is enough) before capturing, and again after a
+ * cudaDeviceReset; a first call under capture returns MI3_ERR_ARG.
  * The call allocates nothing.  All calls share the one array, so calls whose
  * executions overlap on the GPU (other streams, other threads) race and
  * must be serialised by the caller.  Results equal mi3_energies. */

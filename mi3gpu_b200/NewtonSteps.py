@@ -335,7 +335,17 @@ def _device_stats_line(name, jstep, gpus, energies, e_rho):
             f"{name}      J: {printsome(head.peekBuf('J'))} ...\n"
             f"{name} min(E) = {lowE:.4f}     mean(E) = {meanE:.4f}     std(E) = {stdE:.4f}\n"
             f"{name} E Autocorr vs time: {rhostr}")
-    return ssr, line
+    return ssr, line, dict(ferr=float(st[2]), maxd=float(st[1]), X=xm, Xo=xt)
+
+
+def _host_stats(bimarg_target, bimarg_model, couplings):
+    """The numbers of printstats' error line (NewtonSteps.py:43-57) for the
+    round history: Ferr (mean relative error of target entries > 0.01, as a
+    fraction), max |diff|, and X of the model and of the target."""
+    ferr, _, maxd = bimarg_stats(bimarg_target, bimarg_model)
+    X = float(np.sum(couplings * (bimarg_model - indepF(bimarg_model))))
+    Xo = float(np.sum(couplings * (bimarg_target - indepF(bimarg_target))))
+    return dict(ferr=float(ferr), maxd=float(maxd), X=X, Xo=Xo)
 
 
 def MCMCstep(runName, Jstep, couplings, param, gpus, log):
@@ -379,12 +389,13 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
     if not dev or param.reseed in ('single_random', 'single_best'):
         seqs = gpus.collect('seq main')
     if dev:
-        ssr, line = _device_stats_line(runName, Jstep, gpus, sampledenergies, e_rho)
+        ssr, line, extra = _device_stats_line(runName, Jstep, gpus, sampledenergies, e_rho)
         if outdir is not None:
             bimarg_model = gpus.head_gpu.collect('bi')
     else:
         line = printstats(runName, Jstep, bimarg_target, bimarg_model, couplings, sampledenergies, e_rho)
         ssr = np.sum((bimarg_target - bimarg_model) ** 2)
+        extra = _host_stats(bimarg_target, bimarg_model, couplings)
     log(line)
     if outdir is not None:
         # writeStatus (NewtonSteps.py:76-94): the statistics, and the walkers
@@ -401,7 +412,8 @@ def MCMCstep(runName, Jstep, couplings, param, gpus, log):
             log(f"SSR increased over min. Decreasing newtonsteps to {param.newtonSteps}")
     param.last_ssr = ssr
     param.min_ssr = min(ssr, param.min_ssr if param.min_ssr is not None else np.inf)
-    param.history = (param.history or []) + [dict(run=runName, ssr=float(ssr), mcmc_s=dt, mc_per_s=MC_s)]
+    param.history = (param.history or []) + [dict(run=runName, ssr=float(ssr), mcmc_s=dt, mc_per_s=MC_s,
+                                                  equil_calls=int(equilsteps), jstep=int(Jstep), **extra)]
 
     t_newton = time.time()
     Jsteps, newJ = NewtonSteps(runName, param, bimarg_model, gpus, log)

@@ -74,8 +74,19 @@ def build_lib(verbose=False, extra=()):
     return LIB
 
 
+def reference_tree():
+    """Where the reference checkout is: $MI3_REFERENCE, else a directory
+    named `reference` beside this repository; None when neither exists."""
+    env = os.environ.get("MI3_REFERENCE")
+    cand = Path(env) if env else ROOT.parent / "reference"
+    return cand if (cand / "mi3gpu").is_dir() else None
+
+
 def build_oracle(verbose=False):
     cmd = ["make", "-s", "-C", str(ROOT / "oracle")]
+    ref = reference_tree()
+    if ref is not None:
+        cmd.append("REF=" + str(ref))
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -309,20 +309,31 @@ namespace mi3 {
 
 static __device__ __align__(256) unsigned long long g_energies_noalloc_acc[MI3_ENERGIES_NOALLOC_MAX_SEQ];
 
-// Device address of the array, looked up once per device.  The name of the
-// array in host code is only a host-side handle, so it must not be passed to
-// a kernel; cudaGetSymbolAddress gives the real device address for the device
-// that is current when it runs.
+// Device address of the array, per device.  The name of the array in host
+// code is only a host-side handle, so it must not be passed to a kernel;
+// cudaGetSymbolAddress gives the real device address for the device that is
+// current when it runs.  The lookup is repeated on every call made outside
+// stream capture (it is cheap), so a device reset or a new primary context
+// never leaves a stale address behind; a call made during capture uses the
+// address found by the last call made outside capture on that device.
 static std::mutex g_noalloc_mutex;
 static unsigned long long *g_noalloc_ptr[256] = {nullptr};
 
-static int noalloc_scratch(unsigned long long **out) {
+static int noalloc_scratch(cudaStream_t st, unsigned long long **out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 256)
         return fail(MI3_ERR_CUDA, std::string("mi3_energies_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess)
+        return fail(MI3_ERR_CUDA, std::string("mi3_energies_noalloc: cudaStreamIsCapturing: ") +
+                                      cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone || !g_noalloc_ptr[dev]) {
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(MI3_ERR_ARG, "mi3_energies_noalloc: the first call on a device must not be made "
+                                     "during stream capture");
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_energies_noalloc_acc);
         if (e != cudaSuccess || p == nullptr)
@@ -346,11 +357,13 @@ extern "C" int mi3_energies_noalloc(const float *J, const uint32_t *seqmem, uint
                                      " exceeds the built-in scratch capacity of " +
                                      std::to_string((unsigned)MI3_ENERGIES_NOALLOC_MAX_SEQ) +
                                      " sequences; use mi3_energies with a workspace");
-    if (nseq == 0) return MI3_OK;
-    unsigned long long *acc = nullptr;
-    int rc = noalloc_scratch(&acc);
-    if (rc) return rc;
+    // the address lookup comes first, so that any call -- a zero-size
+    // warm-up included -- prepares the device for later calls under capture
     cudaStream_t st = as_stream(stream);
+    unsigned long long *acc = nullptr;
+    int rc = noalloc_scratch(st, &acc);
+    if (rc) return rc;
+    if (nseq == 0) return MI3_OK;
     // the accumulators keep the previous call's sums: clear the part used
     if (cudaMemsetAsync(acc, 0, (size_t)nseq * 8, st) != cudaSuccess)
         return check_launch("mi3_energies_noalloc: memset");

@@ -52,7 +52,8 @@ def make_target(L, q, n_msa, seed, sweeps=None, contact_sigma=0.5, device=0):
 
 def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e-4, damping=1e-3,
           reg=('l1z', (2e-4,)), seed=1234, device=0, log=print, fused=True, outdir=None, reseed='independent',
-          sweeps_first=None, device_resident=True, tuner=None, distribute_jstep='all', alpha=None):
+          sweeps_first=None, device_resident=True, tuner=None, distribute_jstep='all', alpha=None,
+          equiltime=None, nsteps=None, min_equil=64, max_equil=32768, J0=None):
     """Run `rounds` quasi-Newton iterations from the independent model;
     returns the per-round history (SSR, wall seconds of MCMC and Newton
     phases) as recorded by NewtonSteps.MCMCstep.
@@ -69,19 +70,32 @@ def infer(target, L, q, nwalkers, rounds, sweeps=128, newtonsteps=1024, gamma=4e
     Newton steps over the walkers where they are; 'head_gpu' first gathers
     them into the device's large buffer, as the reference's option does.
     alpha: the residue letters of the run directories' MSA files (default
-    seqload.default_alpha(q))."""
+    seqload.default_alpha(q)).
+
+    equiltime='auto' equilibrates as the reference's default does
+    (NewtonSteps.py:395-442: rank correlation of energies between
+    checkpoints, at least min_equil and at most max_equil sampler calls of
+    `nsteps` steps, default 2048 as Mi3.py's --nsteps); an integer fixes the
+    number of sampler calls; None derives it from `sweeps`.  sweeps_first
+    may also be 'auto' (the first round only).  J0: starting
+    couplings (default: the independent model of the target)."""
     potts.check_target(target)  # as the reference's set-up does (Mi3.py:1029-1034)
     unimarg = potts.getUnimarg(target)
-    J0 = potts.independent_couplings(unimarg)
-    nsteps = 8 * L
+    if J0 is None:
+        J0 = potts.independent_couplings(unimarg)
+    if nsteps is None:
+        nsteps = 2048 if equiltime == 'auto' else 8 * L
+    if equiltime is None:
+        equiltime = max(1, sweeps * L // nsteps)
     p = NewtonSteps.Param()
     p.update(dict(bimarg=target, gamma0=gamma, newtonSteps=newtonsteps, pcdamping=damping, fracNeff=0.9,
                   nwalkers=nwalkers, reg=reg[0] if reg else None, regarg=reg[1] if reg else None, beta=None,
                   distribute_jstep=distribute_jstep, L=L, q=q, couplings=J0, nsteps=nsteps,
-                  equiltime=max(1, sweeps * L // nsteps), trackequil=0, outdir=outdir, mcmcsteps=rounds,
+                  equiltime=equiltime, min_equil=min_equil, max_equil=max_equil, trackequil=0, outdir=outdir, mcmcsteps=rounds,
                   newton_delta=32, reseed=reseed, rngseed=seed + 1, unimarg=unimarg, fused=fused, init_indep=True,
                   device_resident=device_resident, alpha=alpha,
-                  equiltime_first=None if sweeps_first is None else max(1, sweeps_first * L // nsteps)))
+                  equiltime_first=(None if sweeps_first is None else 'auto' if sweeps_first == 'auto'
+                                   else max(1, sweeps_first * L // nsteps))))
     g = MCMCGPU((device, 0), L, q, nwalkers, 512, outdir, 1024, seed + 1)
     gpus = GPU_node([g])
     gpus.initMCMC(nsteps)

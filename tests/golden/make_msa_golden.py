@@ -24,8 +24,16 @@ HERE = Path(__file__).resolve().parent
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None,
+                    help="reference checkout (default: $MI3_REFERENCE, else ../reference beside the repository)")
     args = ap.parse_args()
+    if args.ref is None:
+        import os
+        env = os.environ.get("MI3_REFERENCE")
+        cand = Path(env) if env else Path(__file__).resolve().parents[3] / "reference"
+        if not (cand / "mi3gpu").is_dir():
+            ap.error("reference checkout not found: pass --ref or set MI3_REFERENCE")
+        args.ref = str(cand)
     sys.path.insert(0, args.ref)
     from mi3gpu.utils import seqload
     from mi3gpu.utils.potts_common import alpha21

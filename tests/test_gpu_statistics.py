@@ -97,3 +97,146 @@ def test_gpu_sampler_matches_exact_and_reference_cpu_sampler(cuda):
     assert ssr_cpu < 3.0 * exp_cpu, (ssr_cpu, exp_cpu)
     ssr_between = float(np.sum((f_gpu - f_cpu) ** 2))
     assert ssr_between < 3.0 * exp_cpu + 1.5 * exp_gpu, (ssr_between, exp_cpu, exp_gpu)
+
+
+# ------------------------------------------------- the benchmark's shapes
+# At L=48 and L=60 nothing can be enumerated, so the B200 sampler's
+# bimarginals are compared with the reference's CPU sampler on the same
+# model: two independent estimates of one distribution differ by
+# E[SSR] = sum f (1 - f) (1/N_gpu + 1/N_cpu) when both samples are
+# independent draws from it (f estimated from both samples pooled).
+
+def _reference_chains(J, L, q, nchains, burn_sweeps, spacing_sweeps, per_chain, seed):
+    """per_chain samples from each of `nchains` independent runs of the
+    reference's CPU sampler (extras/mcmcCPUgenThreaded.c), spaced by
+    spacing_sweeps sweeps after burn_sweeps of burn-in, run in parallel."""
+    from oracle import oracle
+    exe = oracle.ref_cpu_binary()
+    if exe is None:
+        pytest.skip("reference CPU sampler not built (oracle/_ref)")
+    alpha = "ABCDEFGHIJKLMNOPQRSTUVWXYZ"[:q]
+    rng = np.random.default_rng(seed)
+    burn = max(1, burn_sweeps // spacing_sweeps)
+    with tempfile.TemporaryDirectory() as td:
+        jf = Path(td) / "J.dat"
+        J.astype("<f4").tofile(jf)
+        procs = []
+        for _ in range(nchains):
+            start = "".join(alpha[k] for k in rng.integers(0, q, size=L))
+            procs.append(subprocess.Popen([str(exe), str(jf), str(spacing_sweeps * L), str(burn + per_chain), alpha,
+                                           start], stdout=subprocess.PIPE, text=True))
+        outs = []
+        for p in procs:
+            txt, _ = p.communicate()
+            assert p.returncode == 0
+            lines = txt.split()[burn:]
+            assert len(lines) == per_chain
+            outs.append(np.frombuffer("".join(lines).encode(), dtype=np.uint8).reshape(per_chain, L) - ord("A"))
+    return np.concatenate(outs).astype(np.int64)
+
+
+def _bimarg_lq(seqs, L, q):
+    i, j = np.triu_indices(L, k=1)
+    n = seqs.shape[0]
+    codes = seqs[:, i] * q + seqs[:, j]  # (n, npairs)
+    out = np.empty((len(i), q * q))
+    for p in range(len(i)):
+        out[p] = np.bincount(codes[:, p], minlength=q * q)
+    return out / n
+
+
+def _gpu_samples(J, L, q, N, sweeps, seed, J_then=None, sweeps_then=0):
+    """N walkers of the B200 sampler after `sweeps` sweeps from random
+    sequences at J; then, if J_then is given, `sweeps_then` more sweeps at
+    J_then with the walkers carried over (as the reseed 'none' schedule
+    does between rounds)."""
+    g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, seed)
+    node = GPU_node([g])
+    node.initMCMC(4 * L)
+    node.setBuf('J', J)
+    node.setSeqs('main', np.random.default_rng(seed).integers(0, q, size=(N, L)).astype('<u1'))
+    for _ in range(sweeps // 4):
+        node.runMCMC()
+    if J_then is not None:
+        node.setBuf('J', J_then)
+        for _ in range(sweeps_then // 4):
+            node.runMCMC()
+    return node.collect('seq main').astype(np.int64)
+
+
+def _ssr_ratio(f_a, n_a, f_b, n_b):
+    """SSR of the difference over its finite-sample expectation."""
+    f = (f_a * n_a + f_b * n_b) / (n_a + n_b)
+    expect = float(np.sum(f * (1 - f)) * (1.0 / n_a + 1.0 / n_b))
+    return float(np.sum((f_a - f_b) ** 2)) / expect
+
+
+def _chi2_mean(f_a, n_a, f_b, n_b, fmin=0.005):
+    """Mean over the entries with pooled f > fmin of (f_a - f_b)^2 divided
+    by that entry's finite-sample variance f (1 - f) (1/n_a + 1/n_b).  Its
+    expectation is 1 for independent samples of one distribution (slightly
+    above for samples of one chain taken a few sweeps apart).  Unlike the
+    plain SSR ratio, which a few high-variance entries dominate (for two
+    sets of reference chains it spread over 0.85-1.24 at L=48), every entry
+    weighs the same, so it spreads little (1.00-1.10 there)."""
+    f = (f_a * n_a + f_b * n_b) / (n_a + n_b)
+    m = f > fmin
+    v = f * (1 - f) * (1.0 / n_a + 1.0 / n_b)
+    return float(np.mean((f_a - f_b)[m] ** 2 / v[m]))
+
+
+def _compare(s_a, s_b, L, q):
+    fa, fb = _bimarg_lq(s_a, L, q), _bimarg_lq(s_b, L, q)
+    return _chi2_mean(fa, len(s_a), fb, len(s_b)), _ssr_ratio(fa, len(s_a), fb, len(s_b))
+
+
+def test_sampler_L48_q4_matches_reference_cpu_sampler(cuda):
+    """The benchmark's small model (L=48, q=4: fields N(0,1), couplings
+    N(0,0.05^2) plus 3L contacts N(0,0.5^2), fieldless-even gauge): 16384
+    B200 walkers after 512 sweeps against 16 reference chains x 2048
+    samples 20 sweeps apart."""
+    from mi3gpu_b200.potts import synthetic_ground_truth
+    L, q = 48, 4
+    J = synthetic_ground_truth(L, q, seed=1000)
+    s_gpu = _gpu_samples(J, L, q, 16384, 512, seed=21)
+    s_cpu = _reference_chains(J, L, q, 16, 200, 20, 2048, seed=22)
+    chi2, ratio = _compare(s_gpu, s_cpu, L, q)
+    print("L=48 q=4: B200 vs reference sampler: chi2 per entry", chi2, "SSR / expectation", ratio)
+    assert chi2 < 1.25 and ratio < 2.0, (chi2, ratio)
+
+
+def test_sampler_L60_q21_matches_reference_cpu_sampler(cuda):
+    """A q=21 model built the same way (L=60): 16384 B200 walkers after
+    512 sweeps against 16 reference chains x 1024 samples 20 sweeps
+    apart."""
+    from mi3gpu_b200.potts import synthetic_ground_truth
+    L, q = 60, 21
+    J = synthetic_ground_truth(L, q, seed=1060)
+    s_gpu = _gpu_samples(J, L, q, 16384, 512, seed=23)
+    s_cpu = _reference_chains(J, L, q, 16, 200, 20, 1024, seed=24)
+    chi2, ratio = _compare(s_gpu, s_cpu, L, q)
+    print("L=60 q=21: B200 vs reference sampler: chi2 per entry", chi2, "SSR / expectation", ratio)
+    assert chi2 < 1.25 and ratio < 2.0, (chi2, ratio)
+
+
+def test_carried_over_walkers_reequilibrate_in_16_sweeps(cuda):
+    """The carry-over round schedule: walkers equilibrated at J0, the
+    couplings then change by a step of the size one quasi-Newton round
+    makes, and the walkers run 16 more sweeps.  Their bimarginals must
+    match the reference sampler's at the new couplings within the
+    finite-sample error; the change itself is far larger than that error,
+    so walkers still at J0 would fail."""
+    from mi3gpu_b200.potts import synthetic_ground_truth
+    L, q = 48, 4
+    J0 = synthetic_ground_truth(L, q, seed=1000)
+    rng = np.random.default_rng(25)
+    J1 = (J0 + rng.normal(0, 0.03, size=J0.shape)).astype("<f4")
+    s_old = _gpu_samples(J0, L, q, 16384, 512, seed=26)
+    s_gpu = _gpu_samples(J0, L, q, 16384, 512, seed=26, J_then=J1, sweeps_then=16)
+    s_cpu = _reference_chains(J1, L, q, 16, 200, 20, 2048, seed=27)
+    moved, moved_ssr = _compare(s_old, s_cpu, L, q)
+    chi2, ratio = _compare(s_gpu, s_cpu, L, q)
+    print("carried over 16 sweeps: chi2 per entry", chi2, "SSR / expectation", ratio,
+          "(walkers left at J0:", moved, moved_ssr, ")")
+    assert moved > 5.0, moved
+    assert chi2 < 1.25 and ratio < 2.0, (chi2, ratio)
