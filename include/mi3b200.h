@@ -112,6 +112,35 @@ int mi3_metropolis_plan(const float *Jrows, uint32_t *rngstates, uint32_t positi
  * stages) triples into plans[3*max] (nullable); returns how many exist. */
 uint32_t mi3_metropolis_plans(uint32_t L, uint32_t q, uint32_t nseqs, uint32_t *plans, uint32_t max);
 
+/* Floats of the chunk-tiled coupling layout of mi3_metropolis_skew:
+ * L rows, each of ceil((L + 31) / 32) chunks of [q*q cells][32 sites]. */
+uint64_t mi3_jtiles_floats(uint32_t L, uint32_t q);
+
+/* unpackfV (mcmc.cl:42-65) as launched by MCMCGPU.unpackJ
+ * (mcmcGPU.py:393-408), into the chunk-tiled layout:
+ * Jtiles[pos][k][a*q + b][c] = J_{pos,m}(a, b) for site m = 32 k + c,
+ * zero for m == pos and for m >= L.  Jtiles: mi3_jtiles_floats(L, q)
+ * floats, 16-byte aligned. */
+int mi3_unpack_j_tiles(const float *J, float *Jtiles, uint32_t L, uint32_t q, void *stream);
+
+/* metropolis + DeltaEnergy (mcmc.cl:360-458) as launched by MCMCGPU.runMCMC
+ * (mcmcGPU.py:460-482), a second kernel design with identical results to
+ * mi3_metropolis (same trajectories and RNG states, bit for bit): each
+ * warp's walkers run skewed by one site per lane so that the coupling
+ * gathers of a warp hit 32 different shared-memory banks; walker
+ * sequences are held in registers.  Reads the chunk-tiled couplings of
+ * mi3_unpack_j_tiles.  2 <= q <= 21, L + 31 <= 288, nseqs a multiple of
+ * 32, walkers_per_cta 512 or 768 (0: 512; the last CTA may be partly
+ * filled).  Residues >= q in
+ * seqmem are clamped to q - 1.  replicas (0 = 1): Jtiles holds that many
+ * identical copies of the table, mi3_jtiles_floats(L, q) floats apart, and
+ * CTA b reads copy b % replicas (spreads the CTAs' simultaneous reads of
+ * one coupling row over more L2 slices).  status: as mi3_metropolis. */
+int mi3_metropolis_skew(const float *Jtiles, uint32_t *rngstates, uint32_t position_offset,
+                        const uint32_t *position_list, uint32_t nsteps, const float *betas, float beta,
+                        uint32_t *seqmem, uint32_t nseqs, uint32_t L, uint32_t q, uint32_t walkers_per_cta,
+                        uint32_t replicas, int32_t *status, void *stream);
+
 /* gen_indep (mcmc.cl:170-244) as launched by MCMCGPU.gen_indep
  * (mcmcGPU.py:380-390); cprob is (L, q-1) cumulative probabilities
  * (MCMCGPU.prepare_indep, mcmcGPU.py:375-378). */

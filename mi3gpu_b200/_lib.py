@@ -23,6 +23,10 @@ SIGNATURES = {
     "mi3_metropolis_plan": (c.c_int, [_vp, _vp, _u32, _vp, _u32, _vp, _f32, _vp, _u32, _u32, _u32, _u32, _u32,
                                       _u32, _vp, _vp]),
     "mi3_metropolis_plans": (_u32, [_u32, _u32, _u32, _vp, _u32]),
+    "mi3_jtiles_floats": (_u64, [_u32, _u32]),
+    "mi3_unpack_j_tiles": (c.c_int, [_vp, _vp, _u32, _u32, _vp]),
+    "mi3_metropolis_skew": (c.c_int, [_vp, _vp, _u32, _vp, _u32, _vp, _f32, _vp, _u32, _u32, _u32, _u32, _u32, _vp,
+                                      _vp]),
     "mi3_gen_indep": (c.c_int, [_vp, _u32, _u32, _vp, _vp, _u32, _u32, _vp]),
     "mi3_energies_workspace": (c.c_size_t, [_u32]),
     "mi3_energies": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u32, _u32, _vp, c.c_size_t, _vp]),

@@ -1,7 +1,9 @@
 """Autotuner for the shape-dependent choices of the B200 kernels.
 
-The sampler's tile plan (walkers per CTA, sites per streamed coupling chunk,
-ring stages; `mi3_metropolis_plans` lists the valid ones), the bimarginal
+The sampler's plan (the skewed-lane kernel with 512 or 768 walkers per CTA,
+or a tile plan of the row-streaming kernel: walkers per CTA, sites per
+streamed coupling chunk, ring stages, which `mi3_metropolis_plans` lists;
+all give the same trajectories), the bimarginal
 count kernel and the weighted-bimarginal kernel (shared-memory histogram or
 tcgen05 one-hot GEMM, which give the same integers) are picked per
 (L, q, walkers) by timing every candidate once on the device, from the caller's own walker state copied to scratch buffers
@@ -32,11 +34,24 @@ def _events_time(stream, fn, reps):
 
 
 def sampler_plans(L, q, nseq):
-    """All valid (walkers_per_cta, sites_per_chunk, stages) plans."""
+    """All valid plans: ('skew', walkers_per_cta) for the skewed-lane
+    kernel where it applies, then the (walkers_per_cta, sites_per_chunk,
+    stages) plans of the row-streaming kernel."""
+    plans = []
+    if 2 <= q <= 21 and L + 31 <= 288 and nseq % 32 == 0:
+        plans += [('skew', 512), ('skew', 768)]
     n = int(_lib.query('mi3_metropolis_plans', L, q, nseq, None, 0))
     buf = (ctypes.c_uint32 * (3 * max(n, 1)))()
     _lib.query('mi3_metropolis_plans', L, q, nseq, buf, n)
-    return [tuple(int(v) for v in buf[3 * k:3 * k + 3]) for k in range(n)]
+    return plans + [tuple(int(v) for v in buf[3 * k:3 * k + 3]) for k in range(n)]
+
+
+def _plan_key(plan):
+    return ",".join(map(str, plan))
+
+
+def _plan_from_json(v):
+    return tuple(v[:1] + [int(x) for x in v[1:]]) if v and v[0] == 'skew' else tuple(int(x) for x in v)
 
 
 class Autotuner:
@@ -71,9 +86,11 @@ class Autotuner:
         (plan, {plan: ms})."""
         key = self._key("metropolis", gpu)
         if key in self.table:
-            return tuple(self.table[key]["plan"]), self.table[key].get("ms", {})
+            return _plan_from_json(self.table[key]["plan"]), self.table[key].get("ms", {})
         gpu.require('MCMC')
-        gpu.unpackJ()
+        gpu.unpackJ(kind='rows')
+        if gpu.skew_supported():
+            gpu.unpackJ(kind='tiles')
         L, q, N = gpu.L, gpu.q, gpu.nseq['main']
         steps = int(probe_steps or min(gpu.nsteps, 2 * L))
         with torch.cuda.stream(gpu.stream):
@@ -87,15 +104,14 @@ class Autotuner:
         times = {}
         for plan in sampler_plans(L, q, N):
             def run(plan=plan):
-                _lib.call('mi3_metropolis_plan', gpu._ptr('Junpacked'), rng.data_ptr(), 0, pos.data_ptr(),
-                          steps, None, gpu.beta, seq.data_ptr(), N, L, q, plan[0], plan[1], plan[2],
-                          status.data_ptr(), s)
+                gpu.sampler_call(0, pos.data_ptr(), steps, seq.data_ptr(), rng.data_ptr(), status.data_ptr(), s,
+                                 plan=plan)
             run()
             times[plan] = _events_time(gpu.stream, run, reps)
         if int(status.item()) != 0:
             raise RuntimeError("sampler reported status {} while tuning".format(int(status.item())))
         best = min(times, key=times.get)
-        self.table[key] = {"plan": list(best), "ms": {",".join(map(str, k)): v for k, v in times.items()},
+        self.table[key] = {"plan": list(best), "ms": {_plan_key(k): v for k, v in times.items()},
                            "probe_steps": steps}
         self._save()
         return best, self.table[key]["ms"]

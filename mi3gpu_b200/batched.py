@@ -143,13 +143,12 @@ class BatchedRounds:
         call = _lib.call
         call('mi3_gauge_fieldless_even', _p(b['J']), _p(b['J']), L, q, *self._ws(g, 'ws gauge',
              'mi3_gauge_workspace', L, q), s)
-        call('mi3_unpack_j', _p(b['J']), _p(b['Junpacked']), L, q, s)
+        g.unpack_call(s)
         if self.reseed == 'independent':
             call('mi3_gen_indep', _p(b['seq main']), N, N, _p(b['rngstates']), _p(b['cprob']), L, q, s)
-        plan = getattr(g, 'metro_plan', None) or (0, 0, 0)
         for k in range(ncalls):
-            call('mi3_metropolis_plan', _p(b['Junpacked']), _p(b['rngstates']), k * pr.nsteps, _p(pr.randpos_round),
-                 pr.nsteps, None, g.beta, _p(b['seq main']), N, L, q, plan[0], plan[1], plan[2], _p(b['status']), s)
+            g.sampler_call(k * pr.nsteps, _p(pr.randpos_round), pr.nsteps, _p(b['seq main']), _p(b['rngstates']),
+                           _p(b['status']), s)
         tensor = (getattr(g, 'count_kernel', None) == 'tc') if getattr(g, 'count_kernel', None) else \
             q in g.TENSOR_COUNT_Q
         if tensor:

@@ -381,13 +381,102 @@ class MCMCGPU:
         self.repackedSeqT[bufname] = False
         return self.logevt('gen_indep', s)
 
-    def unpackJ(self, wait_for=None):
-        if self.unpackedJ:
-            return wait_for
-        s = self._begin()
-        _lib.call('mi3_unpack_j', self._ptr('J'), self._ptr('Junpacked'), self.L, self.q, self._s)
-        self.unpackedJ = True
+    # ------------------------------------------------------------ couplings
+    # Two unpacked layouts exist: the padded rows ('Junpacked') of the
+    # row-streaming sampler and the chunk tiles ('Jtiles') of the skewed-lane
+    # sampler; both are rebuilt lazily after J changes.
+    @property
+    def unpackedJ(self):
+        return self._unpacked_rows
+
+    @unpackedJ.setter
+    def unpackedJ(self, v):
+        self._unpacked_rows = v
+        if not v:
+            self._unpacked_tiles = False
+
+    def unpackJ(self, wait_for=None, kind=None):
+        kind = kind or ('tiles' if self.sampler_plan()[0] == 'skew' else 'rows')
+        if kind == 'rows':
+            if self._unpacked_rows:
+                return wait_for
+            s = self._begin()
+            _lib.call('mi3_unpack_j', self._ptr('J'), self._ptr('Junpacked'), self.L, self.q, self._s)
+            self._unpacked_rows = True
+        else:
+            if self._unpacked_tiles:
+                return wait_for
+            self._ensure_tiles()
+            s = self._begin()
+            self._unpack_tiles(self._s)
+            self._unpacked_tiles = True
         return self.logevt('unpackJ', s)
+
+    def _ensure_tiles(self):
+        n = int(_lib.query('mi3_jtiles_floats', self.L, self.q))
+        if 'Jtiles' not in self.bufs or self.bufs['Jtiles'].numel() != n * self.skew_replicas:
+            with torch.cuda.device(self.device):
+                self.bufs['Jtiles'] = torch.empty(n * self.skew_replicas, dtype=torch.float32, device=self.device)
+            self._unpacked_tiles = False
+
+    def _unpack_tiles(self, stream_ptr):
+        n = int(_lib.query('mi3_jtiles_floats', self.L, self.q))
+        for r in range(self.skew_replicas):
+            _lib.call('mi3_unpack_j_tiles', self._ptr('J'), self._ptr('Jtiles') + 4 * n * r, self.L, self.q,
+                      stream_ptr)
+
+    def unpack_call(self, stream_ptr):
+        """Launch the unpacking kernel of the current sampler plan on
+        stream_ptr (for callers that record it themselves, e.g. in a CUDA
+        graph, where J changes on the device)."""
+        if self.sampler_plan()[0] == 'skew':
+            self._ensure_tiles()
+            self._unpack_tiles(stream_ptr)
+        else:
+            _lib.call('mi3_unpack_j', self._ptr('J'), self._ptr('Junpacked'), self.L, self.q, stream_ptr)
+
+    # ------------------------------------------------------------ sampler plans
+    # The skewed-lane sampler (mi3_metropolis_skew) gives the same
+    # trajectories as the row-streaming one; it takes q <= 21 and
+    # L + 31 <= 288.  Untuned, it is used from SKEW_MIN_Q on with at least
+    # one CTA per SM (B200, 2048-step calls: 8.7e9 vs 6.1e9 site-updates/s at
+    # L=232, q=21, 2^20 walkers; even at L=60, q=21; slower at q=4, where
+    # the row kernel's gathers mostly hit the same address and broadcast).
+    SKEW_DEFAULT = True
+    SKEW_MIN_Q = 16
+    # copies of the tiled table; CTAs read different copies, so that their
+    # simultaneous reads of one coupling row spread over more L2 slices
+    skew_replicas = 1
+
+    def skew_supported(self):
+        return 2 <= self.q <= 21 and self.L + 31 <= 288 and self.nseq['main'] % 32 == 0
+
+    def sampler_plan(self):
+        """The plan runMCMC uses: ('skew', walkers_per_cta) or a
+        (walkers_per_cta, sites_per_chunk, stages) triple of the
+        row-streaming kernel ((0, 0, 0): its built-in choice).  Set by
+        autotune.Autotuner.tune as metro_plan; otherwise the skewed-lane
+        kernel where it applies."""
+        plan = getattr(self, 'metro_plan', None)
+        if plan:
+            return tuple(plan)
+        if (self.SKEW_DEFAULT and self.skew_supported() and self.q >= self.SKEW_MIN_Q
+                and self.nseq['main'] >= 148 * 512):
+            return ('skew', 512)
+        return (0, 0, 0)
+
+    def sampler_call(self, pos_offset, pos_ptr, nsteps, seq_ptr, rng_ptr, status_ptr, stream_ptr, betas=None,
+                     plan=None):
+        """One sampler launch with the given plan (default: sampler_plan())
+        on caller-chosen buffers; J must already be unpacked for it."""
+        plan = tuple(plan) if plan else self.sampler_plan()
+        N, L, q = self.nseq['main'], self.L, self.q
+        if plan[0] == 'skew':
+            _lib.call('mi3_metropolis_skew', self._ptr('Jtiles'), rng_ptr, int(pos_offset), pos_ptr, int(nsteps),
+                      betas, self.beta, seq_ptr, N, L, q, int(plan[1]), self.skew_replicas, status_ptr, stream_ptr)
+        else:
+            _lib.call('mi3_metropolis_plan', self._ptr('Junpacked'), rng_ptr, int(pos_offset), pos_ptr, int(nsteps),
+                      betas, self.beta, seq_ptr, N, L, q, plan[0], plan[1], plan[2], status_ptr, stream_ptr)
 
     # ------------------------------------------------------------ sampler
     def _initMCMC_RNG(self, rng_offset, rng_span, wait_for=None):
@@ -423,10 +512,8 @@ class MCMCGPU:
         self.repackedSeqT['main'] = False
         s = self._begin()
         betas = self._ptr('Bs') if getattr(self, 'tempering', False) else None
-        plan = getattr(self, 'metro_plan', None) or (0, 0, 0)  # set by autotune.Autotuner.tune
-        _lib.call('mi3_metropolis_plan', self._ptr('Junpacked'), self._ptr('rngstates'), int(rngoffset),
-                  self._ptr('randpos'), self.nsteps, betas, self.beta, self._ptr('seq main'),
-                  self.nseq['main'], self.L, self.q, plan[0], plan[1], plan[2], self._ptr('status'), self._s)
+        self.sampler_call(rngoffset, self._ptr('randpos'), self.nsteps, self._ptr('seq main'),
+                          self._ptr('rngstates'), self._ptr('status'), self._s, betas=betas)
         return self.logevt('mcmc', s)
 
     # ------------------------------------------------------------ statistics
@@ -717,6 +804,10 @@ class MCMCGPU:
     def getBuf(self, bufname, truncateLarge=True, wait_for=None):
         """Copy a device buffer to host; returns a FutureBuf
         (mcmcGPU.py:845-867)."""
+        if bufname == 'Junpacked' and self._unpacked_tiles and not self._unpacked_rows:
+            # the skewed-lane sampler unpacked J into the tiled layout only;
+            # build the rows a reader of 'Junpacked' expects from the same J
+            self.unpackJ(kind='rows')
         buftype, bufshape = self.buf_spec[bufname]
         dev = self.bufs[bufname]
         host = self._readback_buffer(bufname, dev)

@@ -164,6 +164,18 @@ def unpack_j(J, L, q):
     return Ju.reshape(L, stride)
 
 
+def unpack_j_tiles(J, L, q):
+    """The chunk-tiled coupling layout of the skewed sampler: for each site
+    pos, ceil((L + 31) / 32) chunks of [q*q cells][32 sites], holding
+    unpackfV's (mcmc.cl:42-65) J_{pos,m}(a, b) at [pos][m // 32][a*q+b][m % 32]
+    and zero for m == pos and m >= L.  Built from unpack_j's rows."""
+    rows = unpack_j(J, L, q)[:, :L * q * q].reshape(L, L, q * q)
+    nc = (L + 62) // 32
+    t = np.zeros((L, nc * 32, q * q), np.float32)
+    t[:, :L, :] = rows
+    return np.ascontiguousarray(t.reshape(L, nc, 32, q * q).transpose(0, 1, 3, 2))
+
+
 def metropolis(J, rngstates, position_list, position_offset, nsteps, seqmem, L, q,
                betas=None, beta=1.0, walkers=None):
     """Runs the sampler in place on (rngstates (N,4) u4, seqmem (SWORDS,N) u4)."""

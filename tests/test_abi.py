@@ -92,7 +92,11 @@ def test_metropolis_plans_host_query(L, q, N):
     from mi3gpu_b200.autotune import sampler_plans
     plans = sampler_plans(L, q, N)
     assert plans, "no plan for a supported shape"
-    for nw, m, st in plans:
+    skew = [p for p in plans if p[0] == 'skew']
+    assert bool(skew) == (q <= 21 and L + 31 <= 288 and N % 32 == 0)
+    for _, w in skew:  # the skewed-lane kernel: 512 or 768 walkers per CTA
+        assert w in (512, 768)
+    for nw, m, st in [p for p in plans if p[0] != 'skew']:
         assert nw % 32 == 0 and 64 <= nw <= 512 and N % nw == 0
         assert m % 4 == 0 and 4 <= m <= ((L + 3) // 4) * 4
         assert 2 <= st <= 8

@@ -127,7 +127,8 @@ def test_device_resident_rounds_on_gpu(cuda):
 
 
 def test_sampler_plans_same_trajectory_and_autotuner(cuda, tmp_path):
-    """Every tile plan of the sampler gives the same walkers and RNG states
+    """Every plan of the sampler -- the skewed-lane kernel's and every tile
+    plan of the row-streaming kernel -- gives the same walkers and RNG states
     (the plan changes only the schedule); the autotuner picks one of them,
     caches it and installs it on the device object."""
     import torch
@@ -139,15 +140,16 @@ def test_sampler_plans_same_trajectory_and_autotuner(cuda, tmp_path):
         node.initMCMC(2 * L)
         node.setBuf('J', potts.synthetic_ground_truth(L, q, seed=L, contact_sigma=0.4))
         node.setSeqs('main', np.random.default_rng(L).integers(0, q, size=(N, L)).astype('<u1'))
-        g.unpackJ()
+        g.unpackJ(kind='rows')
+        g.unpackJ(kind='tiles')
         pos = torch.from_numpy(np.random.default_rng(q).integers(0, L, size=3 * L).astype(np.int32)).to(g.device)
         seq0, rng0 = g.bufs['seq main'].clone(), g.bufs['rngstates'].clone()
         outs = []
         for plan in [(0, 0, 0)] + sampler_plans(L, q, N):
             seq, rng = seq0.clone(), rng0.clone()
             st = torch.zeros(1, dtype=torch.int32, device=g.device)
-            _lib.call('mi3_metropolis_plan', g._ptr('Junpacked'), rng.data_ptr(), 0, pos.data_ptr(), 3 * L,
-                      None, 1.0, seq.data_ptr(), N, L, q, *plan, st.data_ptr(), g.stream.cuda_stream)
+            g.sampler_call(0, pos.data_ptr(), 3 * L, seq.data_ptr(), rng.data_ptr(), st.data_ptr(),
+                           g.stream.cuda_stream, plan=plan)
             g.stream.synchronize()
             assert int(st.item()) == 0
             outs.append((plan, seq, rng))
