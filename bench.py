@@ -37,6 +37,14 @@ sys.path.insert(0, str(ROOT))
 
 L_, Q_, N_ = 232, 21, 1 << 20
 METRIC = "site-updates/s"
+
+# (kernel, L, q, walkers, proposals per call) -> (DRAM bytes read + written
+# per launch, where the figure comes from)
+TRAFFIC_CITED = {
+    ("k_metropolis", 232, 21, 1 << 20, 2048): (
+        4638818048.0, "ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum, one full launch "
+                      "(profiles/metropolis_L232_q21.md)"),
+}
 WORKLOAD = "metropolis L=232 q=21 walkers=2^20 (plain native sampler)"
 
 
@@ -238,15 +246,12 @@ def run_gpu(args):
         peaks = json.loads(pk.read_text())
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = upd_launch * hbm_bytes_per_update / (per_launch_ms / 1e3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "metropolis_L232_q21.md"
-    if tf.exists():
-        for line in tf.read_text().splitlines():
-            if line.startswith("dram_bytes_per_full_launch:"):
-                try:
-                    traffic = float(line.split(":")[1])
-                except ValueError:
-                    pass
+    plan = gpu.sampler_plan()
+    kernel = "k_metropolis_skew" if plan[0] == "skew" else "k_metropolis"
+    # DRAM bytes of one full-size launch (2^20 walkers x 2048 proposals),
+    # measured by a one-pass ncu capture of this command's own launch; a
+    # cited figure, not measured in this run
+    traffic, traffic_src = TRAFFIC_CITED.get((kernel, L, q, N, args.nsteps), (None, None))
     # shared-memory load roofline: 148 SMs x 128 B/clk at the sampled clock
     clocks = clk.summary()
     sm_mhz = clocks.get("sm_mhz") or 1965.0
@@ -270,8 +275,8 @@ def run_gpu(args):
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                     "path": "GPU_node.setBuf('J') + runMCMC() + MCMCGPU.getBuf('seq main') (pinned, packed words)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": traffic,
-                         "kernel": "k_metropolis",
+                         "frac": achieved / hbm_peak, "traffic": traffic, "traffic_source": traffic_src,
+                         "kernel": kernel, "plan": list(plan),
                          "algorithmic_bytes_per_update": hbm_bytes_per_update,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if pk.exists() else "fallback"},
             "roofline_onchip": {"bound": "smem", "achieved": onchip, "peak": smem_peak, "unit": "GB/s",
@@ -861,7 +866,7 @@ def headline_inference(args):
     carry = infer(target, args.L, args.q, args.walkers, 3, reseed="none", sweeps=args.chosen_sweeps,
                   sweeps_first=128, device_resident=True, log=lambda *a: None, tuner=tuner)["history"]
     r_s, c_s = ref[-1]["round_s"], carry[-1]["round_s"]
-    return {"unit": "s/iter", "sampler": "plain native sampler (k_metropolis) in both schedules",
+    return {"unit": "s/iter", "sampler": "the plain native sampler (same kernel and plan) in both schedules",
             "reference_schedule": r_s, "carry_over": c_s, "reference_over_carry_over": r_s / c_s,
             "ssr_round2": {"reference_schedule": ref[1]["ssr"], "carry_over": carry[1]["ssr"]},
             "reference_schedule_form": "reseed independent, 128 sweeps/round, host round work",
