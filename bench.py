@@ -41,6 +41,9 @@ METRIC = "site-updates/s"
 # (kernel, L, q, walkers, proposals per call) -> (DRAM bytes read + written
 # per launch, where the figure comes from)
 TRAFFIC_CITED = {
+    ("k_metropolis_skew", 232, 21, 1 << 20, 2048): (
+        106627657472.0, "ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum, one full launch "
+                        "(profiles/metropolis_skew_L232_q21.md)"),
     ("k_metropolis", 232, 21, 1 << 20, 2048): (
         4638818048.0, "ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum, one full launch "
                       "(profiles/metropolis_L232_q21.md)"),
