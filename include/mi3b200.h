@@ -215,6 +215,35 @@ int mi3_energies_cons(const float *J, const uint32_t *seqmem, uint32_t buflen, u
                       float *energies, uint32_t L, uint32_t q, const uint8_t *cons, void *workspace,
                       size_t ws_bytes, void *stream);
 
+/* ------------------------------------------------- equilibration test */
+
+/* The rank correlation test of runMCMC's automatic equilibration
+ * (NewtonSteps.py:395-442, scipy.stats.spearmanr on the energies of the
+ * latest checkpoint against one and two checkpoints before, p > 0.02) on
+ * the device.  Bytes of workspace mi3_rank_average needs (0 < n < 2^23). */
+size_t mi3_rank_workspace(uint32_t n);
+
+/* ranks[i] = the average rank (1-based) of x[i] among x[0..n-1], ties
+ * sharing the mean of their positions (scipy.stats.rankdata, method
+ * 'average').  x finite; workspace 16-byte aligned. */
+int mi3_rank_average(const float *x, uint32_t n, float *ranks, void *workspace, size_t ws_bytes, void *stream);
+
+/* Bytes of workspace mi3_rank_corr needs. */
+size_t mi3_rank_corr_workspace(void);
+
+/* *r (double, device) = the Pearson correlation of two rank vectors of
+ * mi3_rank_average (spearmanr's statistic), summed in FP64 in a fixed
+ * order; NaN when either vector is constant (as spearmanr). */
+int mi3_rank_corr(const float *ranks_a, const float *ranks_b, uint32_t n, double *r, void *workspace,
+                  size_t ws_bytes, void *stream);
+
+/* *flag (int32, device) = 1 when |*r1| < rcrit and |*r2| < rcrit, else 0
+ * (NaN gives 0).  With rcrit = t_c / sqrt(n - 2 + t_c^2), t_c the upper 1%
+ * point of Student's t with n - 2 degrees of freedom, this is the
+ * reference's "p1 > 0.02 and p2 > 0.02".  No counterpart in the reference
+ * (it decides on the host). */
+int mi3_equil_decide(const double *r1, const double *r2, double rcrit, int32_t *flag, void *stream);
+
 /* ------------------------------------------------------------ bimarginals */
 
 /* countBivariate (mcmc.cl:462-516) as launched by MCMCGPU.calcBicounts

@@ -17,6 +17,7 @@ from pathlib import Path
 
 import numpy as np
 from scipy.stats import spearmanr
+from scipy.stats import t as student_t
 
 from .potts import bimarg_stats, fieldlessGaugeEven, indepF, printsome
 
@@ -215,6 +216,56 @@ def _alpha(param):
     return param.alpha if param.alpha is not None else default_alpha(param.q)
 
 
+def _spearman_p(r, n):
+    """Two-sided p-value of a Spearman r over n samples, as
+    scipy.stats.spearmanr gives it (Student t, n - 2 degrees of freedom)."""
+    if not np.isfinite(r):
+        return float('nan')
+    r = np.float64(max(-1.0, min(1.0, float(r))))
+    with np.errstate(divide='ignore'):
+        t = r * np.sqrt(max(np.float64(0.0), np.float64(n - 2) / ((r + 1.0) * (1.0 - r))))  # |r| = 1: inf
+    return float(2 * student_t.sf(abs(t), n - 2))
+
+
+def _equilibrate_on_device(gpus, param, log):
+    """runMCMC's automatic equilibration (NewtonSteps.py:395-442) with the
+    rank correlation test on the device: the energies of each checkpoint are
+    ranked where they are (mi3_rank_average) and only the correlations come
+    back (16 bytes per checkpoint), instead of every walker's energy.  Same
+    schedule (8 calls, then doubling), same rule (p > 0.02 for the last two
+    lags and at least min_equil calls), same log lines."""
+    n = gpus.nwalkers
+    loops = 8
+    for _ in range(loops):
+        gpus.runMCMC()
+    step = loops
+    k = 0
+    while True:
+        for _ in range(loops):
+            gpus.runMCMC()
+        step += loops
+        gpus.calcEnergies('main')
+        gpus.rankEnergies(k)
+        k += 1
+        rstr = f"Step {step} <E>={gpus.energyMean():.2f}. "
+        if k >= 3:
+            r1, r2 = gpus.rankCorr([(k - 1, k - 2), (k - 1, k - 3)])
+            p1, p2 = _spearman_p(r1, n), _spearman_p(r2, n)
+            fmt = "({:.3f}, {:.2g}) ".format
+            rstr += f"r={fmt(r1, p1)} prev:{fmt(r2, p2)}"
+            if p1 > 0.02 and p2 > 0.02 and step >= (param.min_equil or 64):
+                log(rstr + "Equilibrated.")
+                break
+        if step >= (param.max_equil or 32768):
+            log(rstr + "Reached Max Steps. Stopping")
+            break
+        log(rstr + "Continuing.")
+        loops = loops * 2
+    rs = gpus.rankCorr([(i, k - 1) for i in range(k)])
+    gpus.dropRanks()
+    return step, [(float(r), _spearman_p(r, n)) for r in rs]
+
+
 def runMCMC(gpus, couplings, runName, param, log):
     """Equilibrate the walkers at `couplings` and measure their bimarginals
     (NewtonSteps.py:385-486)."""
@@ -224,7 +275,9 @@ def runMCMC(gpus, couplings, runName, param, log):
     if couplings is not None:  # None: J is already resident on the devices
         gpus.setBuf('J', couplings)
 
-    if nloop == 'auto':
+    if nloop == 'auto' and trackequil == 0 and getattr(gpus, 'deviceRanks', lambda: False)():
+        step, e_rho = _equilibrate_on_device(gpus, param, log)
+    elif nloop == 'auto':
         equil_dir = None
         if trackequil != 0 and outdir is not None:
             equil_dir = outdir / runName / 'equilibration'

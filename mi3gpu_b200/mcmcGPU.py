@@ -733,6 +733,65 @@ class MCMCGPU:
             host = dev[:n].to('cpu', non_blocking=False)
         return host.numpy().copy()
 
+    # ------------------------------------------------------------ equilibration
+    def rankEnergies(self, slot):
+        """Average ranks of the walkers' current energies ('E main', from
+        calcEnergies) into the device rank buffer `slot` -- the rank
+        transform of spearmanr in runMCMC's equilibration test
+        (NewtonSteps.py:419-428), done here instead of on the host."""
+        n = self.nseq['main']
+        name = f'Erank {slot}'
+        with torch.cuda.device(self.device):
+            if name not in self.bufs:
+                self.bufs[name] = torch.empty(n, dtype=torch.float32, device=self.device)
+            nb = int(_lib.query('mi3_rank_workspace', n))
+            if 'ws rank' not in self.bufs or self.bufs['ws rank'].numel() * 8 < nb:
+                self.bufs['ws rank'] = torch.empty(nb // 8 + 2, dtype=torch.int64, device=self.device)
+            if 'E sums' not in self.bufs:
+                self.bufs['E sums'] = torch.empty(4, dtype=torch.float64, device=self.device)
+                self.bufs['E sums32'] = torch.empty(4, dtype=torch.float32, device=self.device)
+        s = self._begin()
+        ws = self.bufs['ws rank']
+        _lib.call('mi3_rank_average', self._ptr('E main'), n, self._ptr(name), ws.data_ptr(), ws.numel() * 8,
+                  self._s)
+        # sum E (FP64) for the mean energy the log line reports
+        _lib.call('mi3_weight_stats', self._ptr('E main'), n, self._ptr('E sums32'), self._ptr('E sums'),
+                  self._ptr('ws reduce'), self._wsbytes('ws reduce'), self._s)
+        return self.logevt('rankEnergies', s)
+
+    def energyMean(self):
+        """Mean of 'E main' as summed by the last rankEnergies (FP64)."""
+        with torch.cuda.stream(self.stream):
+            v = self.bufs['E sums'][0].to('cpu', non_blocking=False)
+        return float(v) / self.nseq['main']
+
+    def rankCorr(self, pairs):
+        """Spearman r (FP64, on the device) of each (slot_a, slot_b) pair of
+        rank buffers; returns a FutureBuf of the r values in pair order."""
+        k = len(pairs)
+        with torch.cuda.device(self.device):
+            if 'rank r' not in self.bufs or self.bufs['rank r'].numel() < k:
+                self.bufs['rank r'] = torch.empty(max(k, 16), dtype=torch.float64, device=self.device)
+            if 'ws corr' not in self.bufs:
+                nb = int(_lib.query('mi3_rank_corr_workspace'))
+                self.bufs['ws corr'] = torch.empty(nb // 8 + 2, dtype=torch.float64, device=self.device)
+        n = self.nseq['main']
+        ws, r = self.bufs['ws corr'], self.bufs['rank r']
+        for i, (a, b) in enumerate(pairs):
+            _lib.call('mi3_rank_corr', self._ptr(f'Erank {a}'), self._ptr(f'Erank {b}'), n,
+                      r.data_ptr() + 8 * i, ws.data_ptr(), ws.numel() * 8, self._s)
+        host = torch.empty(k, dtype=torch.float64, pin_memory=True)
+        with torch.cuda.stream(self.stream):
+            host.copy_(r[:k], non_blocking=True)
+        evt = torch.cuda.Event()
+        evt.record(self.stream)
+        return FutureBuf(host, evt, lambda b: b.numpy().copy(), self)
+
+    def dropRanks(self):
+        """Free the rank buffers of an equilibration run."""
+        for name in [b for b in self.bufs if b.startswith('Erank ')]:
+            del self.bufs[name]
+
     # ------------------------------------------------------------ Newton step
     def updateJ(self, gamma, pc, Jbuf='dJ', wait_for=None):
         self.require('Jstep')

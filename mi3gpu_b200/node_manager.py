@@ -222,6 +222,23 @@ class GPU_node:
         for gpu in self.gpus:
             gpu.calcEnergies(seqbufname, Jbufname)
 
+    # the device-side equilibration test ranks each device's own walkers, so
+    # it stands for the reference's test over all walkers on one device only
+    def deviceRanks(self):
+        return self.ngpus == 1 and hasattr(self.gpus[0], 'rankEnergies')
+
+    def rankEnergies(self, slot):
+        self.gpus[0].rankEnergies(slot)
+
+    def rankCorr(self, pairs):
+        return self.gpus[0].rankCorr(pairs).read()
+
+    def energyMean(self):
+        return self.gpus[0].energyMean()
+
+    def dropRanks(self):
+        self.gpus[0].dropRanks()
+
     def calcBicounts(self, seqbufname):
         for gpu in self.gpus:
             gpu.calcBicounts(seqbufname)

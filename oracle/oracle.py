@@ -439,3 +439,52 @@ def subseq_log_frequencies(J, bseqs, sseqs, fixpos, iterbackgrounds, L, q):
             lmem = copy_subseq(smem, n, marks, lmem, L)
             logf[n] = logsumexp(origEs - energies_f64(J, lmem, L, q))
     return logf
+
+
+# ------------------------------------------------------ equilibration test
+# The reference decides equilibration with scipy.stats.spearmanr
+# (NewtonSteps.py:419-428; scipy 1.18.1 here, not part of the reference
+# tree).  Its published algorithm, restated: average ranks (rankdata,
+# method 'average'), the Pearson correlation of the rank vectors, and the
+# two-sided Student-t p-value of t = r sqrt((n-2)/((1+r)(1-r))), n-2
+# degrees of freedom; a constant input gives r = NaN.
+
+def rank_average(x):
+    """1-based ranks, ties sharing the mean of their sorted positions."""
+    x = np.asarray(x)
+    n = x.shape[0]
+    order = np.argsort(x, kind="stable")
+    xs = x[order]
+    start = np.ones(n, bool)
+    start[1:] = xs[1:] != xs[:-1]
+    end = np.ones(n, bool)
+    end[:-1] = xs[1:] != xs[:-1]
+    lo = np.maximum.accumulate(np.where(start, np.arange(n), 0))
+    hi = np.minimum.accumulate(np.where(end, np.arange(n), n)[::-1])[::-1]
+    r = np.empty(n, np.float64)
+    r[order] = 0.5 * (lo + hi) + 1.0
+    return r
+
+
+def spearman(a, b):
+    """(r, p) as scipy.stats.spearmanr(a, b) for two 1-D vectors."""
+    from scipy.stats import t as student_t
+    ra, rb = rank_average(a), rank_average(b)
+    n = ra.shape[0]
+    da, db = ra - ra.mean(), rb - rb.mean()
+    saa, sbb = np.dot(da, da), np.dot(db, db)
+    if saa == 0 or sbb == 0:
+        return float("nan"), float("nan")
+    r = float(np.dot(da, db) / np.sqrt(saa * sbb))
+    r = max(-1.0, min(1.0, r))
+    with np.errstate(divide="ignore"):
+        tt = r * np.sqrt(max(0.0, (n - 2) / ((r + 1.0) * (1.0 - r))))
+    p = float(2 * student_t.sf(abs(tt), n - 2))
+    return r, p
+
+
+def spearman_rcrit(n, pmin=0.02):
+    """|r| below which spearmanr's p exceeds pmin (two-sided), n samples."""
+    from scipy.stats import t as student_t
+    tc = float(student_t.isf(pmin / 2, n - 2))
+    return tc / np.sqrt(n - 2 + tc * tc)

@@ -135,6 +135,29 @@ class FakeMCMCGPU:
     def calcBicounts(self, seqbufname):
         self.bufs['bicount'] = oracle.bicounts(self._seqs(seqbufname), self.L, self.q)
 
+    # the device-side equilibration test (rank buffers and their correlations)
+    def rankEnergies(self, slot):
+        self.bufs[f'Erank {slot}'] = oracle.rank_average(self.bufs['E main']).astype('<f4')
+        self.bufs['E sums'] = np.array([np.sum(self.bufs['E main'], dtype=np.float64)])
+
+    def rankCorr(self, pairs):
+        out = []
+        for a, b in pairs:
+            ra = self.bufs[f'Erank {a}'].astype(np.float64)
+            rb = self.bufs[f'Erank {b}'].astype(np.float64)
+            m = 0.5 * (len(ra) + 1)
+            da, db = ra - m, rb - m
+            saa, sbb = np.dot(da, da), np.dot(db, db)
+            out.append(np.dot(da, db) / np.sqrt(saa * sbb) if saa > 0 and sbb > 0 else np.nan)
+        return _Fut(np.array(out))
+
+    def energyMean(self):
+        return float(self.bufs['E sums'][0]) / self.nseq['main']
+
+    def dropRanks(self):
+        for k in [b for b in self.bufs if b.startswith('Erank ')]:
+            del self.bufs[k]
+
     def bicounts_to_bimarg(self, seqbufname='main'):
         self.bufs['bi'] = oracle.bicounts_to_bimarg(self.bufs['bicount'], self._n(seqbufname))
 
