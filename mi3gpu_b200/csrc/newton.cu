@@ -101,6 +101,124 @@ __global__ void k_reg_lz(const float *__restrict__ bi, float gamma, float pc, fl
     }
 }
 
+// reg_l1z / reg_l2z for q*q <= 512 with the trees run per lane.  The
+// reference's zeroGauge (mcmc.cl:764-822) sums each row and each column of
+// the block with the same odd-aware tree (level m -> (m+1)/2: element b
+// gets b + m' for b < m' - odd) and the column sums with that tree again.
+// Here lane a owns row a (and, in a transposed copy, column a) and runs its
+// tree sequentially, level by level -- the same additions of the same
+// operands, so the sums are bit-identical -- instead of every level looping
+// over all q*q cells with an index modulo.  The block's values and dJ stay
+// in registers for the final pass.
+__device__ __forceinline__ void tree_level(float *__restrict__ w, const float *__restrict__ rd, uint32_t cnt,
+                                           uint32_t stride) {
+    // w[b] += rd[b] for b < cnt: the read half (from element m on) and the
+    // written half (below m) do not overlap, so the adds of a level are
+    // independent
+#pragma unroll 4
+    for (uint32_t b = 0; b < cnt; ++b) w[b * stride] = w[b * stride] + rd[b * stride];
+}
+
+__device__ __forceinline__ float lane_tree(float *r, uint32_t q, uint32_t stride) {
+    uint32_t m = q;
+    while (m > 1) {
+        const uint32_t odd = m & 1;
+        m = (m + 1) >> 1;
+        tree_level(r, r + m * stride, m - odd, stride);
+    }
+    return r[0];
+}
+
+// PER: cells per lane, ceil(q*q / 32) rounded up to a power of two.
+template <bool L2, uint32_t PER>
+__global__ void __launch_bounds__(256) k_reg_lz_rows(const float *__restrict__ bi, float gamma, float pc, float lJ,
+                                                     const float *__restrict__ J, float *__restrict__ dJ,
+                                                     uint64_t npairs, uint32_t q) {
+    extern __shared__ float sm[];
+    const uint32_t qq = q * q;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint32_t WS = 2 * qq + 2 * q + 1;
+    float *xs = sm + warp * WS;  // [q*q] rows
+    float *xt = xs + qq;         // [q*q] columns (transposed)
+    float *hi = xt + qq;
+    float *hj = hi + q;
+    float *mean_s = hj + q;
+    const float fq = (float)q;
+    // this lane's cells li = lane + 32 k, as (a, b) with li = a q + b
+    const uint32_t a0 = lane / q, b0 = lane - a0 * q, da = 32 / q, db = 32 - da * q;
+    for (uint64_t p = (uint64_t)blockIdx.x * wpb + warp; p < npairs; p += (uint64_t)gridDim.x * wpb) {
+        const float *Jb = J + p * qq;
+        float *dJb = dJ + p * qq;
+        const float *bb = bi + p * qq;
+        float xv[PER], dv[PER], bv[PER];
+        // every global load of the block first (all in flight together),
+        // then the shared-memory copies
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t li = lane + 32 * k;
+            if (li < qq) {
+                dv[k] = dJb[li];
+                xv[k] = Jb[li];
+                bv[k] = bb[li];
+            }
+        }
+        uint32_t a = a0, b = b0;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t li = lane + 32 * k;
+            if (li < qq) {
+                xv[k] = xv[k] + dv[k];
+                xs[li] = xv[k];
+                xt[b * q + a] = xv[k];
+            }
+            b += db;
+            a += da;
+            if (b >= q) {
+                b -= q;
+                ++a;
+            }
+        }
+        __syncwarp();
+        if (lane < q) {
+            hi[lane] = lane_tree(xs + lane * q, q, 1) / fq;
+            hj[lane] = lane_tree(xt + lane * q, q, 1) / fq;  // xt[lane*q] keeps column lane's sum
+        }
+        __syncwarp();
+        if (lane == 0) *mean_s = lane_tree(xt, q, q) / fq / fq;  // total of the column sums
+        __syncwarp();
+        const float mean = *mean_s;
+        if (lane < q) {
+            hi[lane] = hi[lane] - mean;
+            hj[lane] = hj[lane] - mean;
+        }
+        __syncwarp();
+        a = a0;
+        b = b0;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t li = lane + 32 * k;
+            if (li < qq) {
+                const float J0 = xv[k] - (hi[a] + hj[b]) - mean;
+                float R;
+                if (L2) R = -lJ * J0 * gamma / (bv[k] + pc);
+                else R = -lJ * ocl_sign(J0) * gamma / (bv[k] + pc);
+                float Jp = dv[k];
+                if (ocl_sign(J0) != ocl_sign(J0 + R)) Jp = Jp - J0;
+                else Jp = Jp + R;
+                dJb[li] = Jp;
+            }
+            b += db;
+            a += da;
+            if (b >= q) {
+                b -= q;
+                ++a;
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------ reductions
 // Workspace: [ticket counter (uint32, padded to 16 B)][partials: NBLK x 4 doubles]
 constexpr uint32_t RED_BLOCKS = 296;
@@ -289,6 +407,20 @@ static int reg_lz(bool l2, const float *bi, float gamma, float pc, float lJ, con
     if (L < 2 || q < 1 || q * q > 4096) return fail(MI3_ERR_ARG, std::string(name) + ": bad L/q");
     uint64_t np = npairs_of(L);
     uint32_t tb = 256;
+    if (q * q <= 512) {  // up to 16 cells per lane (q <= 22); larger blocks use the generic kernel
+        using K = void (*)(const float *, float, float, float, const float *, float *, uint64_t, uint32_t);
+        const uint32_t per = (q * q + 31) / 32;
+        K k = nullptr;
+        if (per <= 2) k = l2 ? (K)k_reg_lz_rows<true, 2> : (K)k_reg_lz_rows<false, 2>;
+        else if (per <= 4) k = l2 ? (K)k_reg_lz_rows<true, 4> : (K)k_reg_lz_rows<false, 4>;
+        else if (per <= 8) k = l2 ? (K)k_reg_lz_rows<true, 8> : (K)k_reg_lz_rows<false, 8>;
+        else k = l2 ? (K)k_reg_lz_rows<true, 16> : (K)k_reg_lz_rows<false, 16>;
+        const size_t sm2 = (size_t)(tb / 32) * (2 * q * q + 2 * q + 1) * 4;
+        const uint32_t grid2 = (uint32_t)std::min<uint64_t>((np + 7) / 8, 148 * 16);
+        if (sm2 > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        k<<<grid2, tb, sm2, as_stream(stream)>>>(bi, gamma, pc, lJ, J, dJ, np, q);
+        return check_launch(name);
+    }
     size_t smem = (size_t)(tb / 32) * (q * q + 2 * q + 2) * 4;
     uint32_t grid = (uint32_t)std::min<uint64_t>((np + 7) / 8, 148 * 16);
     if (smem > 48 * 1024) {

@@ -263,8 +263,10 @@ def test_update_j_bitexact(cuda):
 
 
 @pytest.mark.parametrize("l2", [False, True])
-@pytest.mark.parametrize("q", [2, 3, 4, 8, 21])
+@pytest.mark.parametrize("q", [2, 3, 4, 5, 8, 9, 11, 12, 16, 17, 21, 22, 23, 32])
 def test_reg_lz_bitexact(cuda, l2, q):
+    """Every cells-per-lane variant of the per-lane-tree kernel (q*q <= 512)
+    and the generic kernel above it (q = 23, 32)."""
     L = 15
     rng = np.random.default_rng(13 + q)
     n = (L * (L - 1) // 2, q * q)
