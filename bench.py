@@ -940,6 +940,7 @@ def run_inference(args):
       carry          J resident; walkers carried over between rounds
                      (reseed 'none'): 128 sweeps in the first round,
                      args.chosen_sweeps after it
+      carry_x4       as carry with four times as many sweeps per round
       carry_half     as carry with half as many sweeps per round
       carry_files    as carry, writing the reference's run directories
                      (J.npy, seqs, info.txt, ... per round) into a
@@ -953,6 +954,8 @@ def run_inference(args):
     forms = (("reference", dict(reseed="independent", sweeps=128, device_resident=False)),
              ("reference_dev", dict(reseed="independent", sweeps=128, device_resident=True)),
              ("carry", dict(reseed="none", sweeps=args.chosen_sweeps, sweeps_first=128, device_resident=True)),
+             ("carry_x4", dict(reseed="none", sweeps=4 * args.chosen_sweeps, sweeps_first=128,
+                               device_resident=True)),
              ("carry_half", dict(reseed="none", sweeps=max(1, args.chosen_sweeps // 2), sweeps_first=128,
                                   device_resident=True)),
              ("carry_files", dict(reseed="none", sweeps=args.chosen_sweeps, sweeps_first=128,
