@@ -103,6 +103,74 @@ __device__ __forceinline__ void energies_chunk(const float *js, const uint32_t *
     }
 }
 
+// Full slices with lanes over pairs (tiling.cuh): the table is [cell][P];
+// lane w visits pair (t + w) mod P at step t.  Each sequence's B*B terms are
+// summed as B float partial sums (step rows th, at most B terms each) added
+// in double, then in fixed point as above.
+template <int B>
+__device__ __forceinline__ double lane_energy(uint32_t jbase, const uint32_t (&row)[B], const uint32_t (&col)[B],
+                                              uint32_t wl) {
+    float part[B];
+#pragma unroll
+    for (int th = 0; th < B; ++th) part[th] = 0.0f;
+#pragma unroll
+    for (int tl = 0; tl < B; ++tl) {
+        const bool carry = tl + wl >= (uint32_t)B;
+        const uint32_t c = jbase + col[tl];
+#pragma unroll
+        for (int th = 0; th < B; ++th) {
+            const uint32_t r = carry ? row[(th + 1) & (B - 1)] : row[th];
+            float v;
+            asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(c + r));
+            part[th] += v;
+        }
+    }
+    double e = 0.0;
+#pragma unroll
+    for (int th = 0; th < B; ++th) e += (double)part[th];
+    return e;
+}
+
+template <int B>
+__device__ __forceinline__ void energies_chunk_lanes(const float *js, const uint32_t *__restrict__ seq, uint32_t buflen,
+                                                     uint32_t nbeg, uint32_t nend, unsigned long long *acc,
+                                                     uint32_t L, uint32_t q, uint32_t bi, uint32_t bj) {
+    const uint32_t swords = (L - 1) / 4 + 1;
+    const uint32_t lane = threadIdx.x & 31, wl = lane % B;
+    const uint32_t jbase = (uint32_t)__cvta_generic_to_shared(js);
+    if constexpr (B == 16) {
+        // 256 terms per sequence: one sequence per thread has loads enough
+        // in flight (16 independent partial sums) and fits the registers
+        for (uint32_t n = nbeg + threadIdx.x; n < nend; n += blockDim.x) {
+            uint32_t wI[B / 4], wJ[B / 4];
+            load_block_words<B>(seq, buflen, n, bi, swords, wI);
+            load_block_words<B>(seq, buflen, n, bj, swords, wJ);
+            uint32_t row[B], col[B];
+            lane_offsets<B>(wI, wJ, q, lane, row, col);
+            const double e1 = lane_energy<B>(jbase, row, col, wl);
+            atomicAdd(&acc[n], (unsigned long long)__double2ll_rn(e1 * FIX_SCALE));
+        }
+        return;
+    }
+    // two sequences per thread: two independent chains of loads in flight
+    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += 2 * blockDim.x) {
+        const uint32_t n2 = n + blockDim.x;
+        const bool two = n2 < nend;
+        uint32_t wI[B / 4], wJ[B / 4], vI[B / 4], vJ[B / 4];
+        load_block_words<B>(seq, buflen, n, bi, swords, wI);
+        load_block_words<B>(seq, buflen, n, bj, swords, wJ);
+        load_block_words<B>(seq, buflen, two ? n2 : n, bi, swords, vI);
+        load_block_words<B>(seq, buflen, two ? n2 : n, bj, swords, vJ);
+        uint32_t row[B], col[B];
+        lane_offsets<B>(wI, wJ, q, lane, row, col);
+        const double e1 = lane_energy<B>(jbase, row, col, wl);
+        lane_offsets<B>(vI, vJ, q, lane, row, col);
+        const double e2 = lane_energy<B>(jbase, row, col, wl);
+        atomicAdd(&acc[n], (unsigned long long)__double2ll_rn(e1 * FIX_SCALE));
+        if (two) atomicAdd(&acc[n2], (unsigned long long)__double2ll_rn(e2 * FIX_SCALE));
+    }
+}
+
 template <int B, bool CONS>
 __global__ void __launch_bounds__(512, 2) k_energies(const float *__restrict__ J,
                                                      const uint32_t *__restrict__ seq, uint32_t buflen,
@@ -115,6 +183,27 @@ __global__ void __launch_bounds__(512, 2) k_energies(const float *__restrict__ J
     uint32_t bi, bj;
     slice_coords(s, g.nb, bi, bj);
     const uint32_t i0 = bi * B, j0 = bj * B;
+    const int kind = slice_kind(bi, bj, j0, B, L);
+    const uint32_t nbeg = chunk * g.chunk;
+    const uint32_t nend = min(nseq, nbeg + g.chunk);
+
+    if constexpr (!CONS && B >= 8) {
+        if (kind == SLICE_FULL) {
+            // cell-major table [cell][P] for lanes over pairs: lane l
+            // stages cell c0 + l % 8 of pair p0 + l / 8 (global reads of 8
+            // consecutive cells of 4 pairs)
+            constexpr uint32_t P = B * B;
+            const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+            const uint32_t cgroups = (qq + 7) / 8;
+            for (uint32_t t = warp; t < cgroups * (P / 4); t += nwarps) {
+                const uint32_t c = (t % cgroups) * 8 + (lane & 7), p = (t / cgroups) * 4 + (lane >> 3);
+                if (c < qq) js[c * P + p] = __ldg(&J[pair_index(i0 + p / B, j0 + p % B, L) * qq + c]);
+            }
+            __syncthreads();
+            energies_chunk_lanes<B>(js, seq, buflen, nbeg, nend, acc, L, q, bi, bj);
+            return;
+        }
+    }
 
     // Stage the slice's couplings: for each i, pairs (i, jlo..jhi-1) are
     // contiguous in the packed table.
@@ -135,9 +224,7 @@ __global__ void __launch_bounds__(512, 2) k_energies(const float *__restrict__ J
     }
     __syncthreads();
 
-    const uint32_t nbeg = chunk * g.chunk;
-    const uint32_t nend = min(nseq, nbeg + g.chunk);
-    switch (slice_kind(bi, bj, j0, B, L)) {
+    switch (kind) {
         case SLICE_FULL:
             energies_chunk<B, SLICE_FULL, CONS>(js, seq, buflen, nbeg, nend, acc, L, q, bi, bj, cI, cJ);
             break;

@@ -121,6 +121,66 @@ __device__ __forceinline__ void hist_chunk(uint32_t *h, const uint32_t *__restri
     }
 }
 
+// Full slices with lanes over pairs (tiling.cuh): the histograms are
+// [cell][P]; lane w adds to pair (t + w) mod P at step t, so the 32 lanes of
+// a shared-memory reduction always hit 32 different banks and different
+// bins (no serialised same-bin adds either).
+template <int B>
+__device__ __forceinline__ void lane_hist(uint32_t hbase, const uint32_t (&row)[B], const uint32_t (&col)[B],
+                                          uint32_t wl, uint32_t inc) {
+#pragma unroll
+    for (int tl = 0; tl < B; ++tl) {
+        const bool carry = tl + wl >= (uint32_t)B;
+        const uint32_t c = hbase + col[tl];
+#pragma unroll
+        for (int th = 0; th < B; ++th) {
+            const uint32_t r = carry ? row[(th + 1) & (B - 1)] : row[th];
+            asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(c + r), "r"(inc));
+        }
+    }
+}
+
+template <int B, bool WEIGHTED>
+__device__ __forceinline__ void hist_chunk_lanes(uint32_t *h, const uint32_t *__restrict__ seq, uint32_t buflen,
+                                                 uint32_t nbeg, uint32_t nend, const float *__restrict__ weights,
+                                                 float scale, uint32_t L, uint32_t q, uint32_t bi, uint32_t bj) {
+    const uint32_t swords = (L - 1) / 4 + 1;
+    const uint32_t lane = threadIdx.x & 31, wl = lane % B;
+    const uint32_t hbase = (uint32_t)__cvta_generic_to_shared(h);
+    if constexpr (B == 16) {
+        for (uint32_t n = nbeg + threadIdx.x; n < nend; n += blockDim.x) {
+            uint32_t wI[B / 4], wJ[B / 4];
+            load_block_words<B>(seq, buflen, n, bi, swords, wI);
+            load_block_words<B>(seq, buflen, n, bj, swords, wJ);
+            uint32_t inc = 1u;
+            if constexpr (WEIGHTED) inc = __float2uint_rn(__ldg(&weights[n]) * scale);
+            uint32_t row[B], col[B];
+            lane_offsets<B>(wI, wJ, q, lane, row, col);
+            lane_hist<B>(hbase, row, col, wl, inc);
+        }
+        return;
+    }
+    for (uint32_t n = nbeg + threadIdx.x; n < nend; n += 2 * blockDim.x) {
+        const uint32_t n2 = n + blockDim.x;
+        const bool two = n2 < nend;
+        uint32_t wI[B / 4], wJ[B / 4], vI[B / 4], vJ[B / 4];
+        load_block_words<B>(seq, buflen, n, bi, swords, wI);
+        load_block_words<B>(seq, buflen, n, bj, swords, wJ);
+        load_block_words<B>(seq, buflen, two ? n2 : n, bi, swords, vI);
+        load_block_words<B>(seq, buflen, two ? n2 : n, bj, swords, vJ);
+        uint32_t inc1 = 1u, inc2 = 1u;
+        if constexpr (WEIGHTED) {
+            inc1 = __float2uint_rn(__ldg(&weights[n]) * scale);
+            inc2 = two ? __float2uint_rn(__ldg(&weights[n2]) * scale) : 0u;
+        }
+        uint32_t row[B], col[B];
+        lane_offsets<B>(wI, wJ, q, lane, row, col);
+        lane_hist<B>(hbase, row, col, wl, inc1);
+        lane_offsets<B>(vI, vJ, q, lane, row, col);
+        lane_hist<B>(hbase, row, col, wl, two ? inc2 : 0u);
+    }
+}
+
 template <int B, bool WEIGHTED, bool CONS>
 __global__ void __launch_bounds__(512, 2) k_pairhist(const uint32_t *__restrict__ seq, uint32_t buflen,
                                                      uint32_t nseq, const float *__restrict__ weights,
@@ -148,7 +208,33 @@ __global__ void __launch_bounds__(512, 2) k_pairhist(const uint32_t *__restrict_
 
     const uint32_t nbeg = chunk * g.chunk;
     const uint32_t nend = min(nseq, nbeg + g.chunk);
-    switch (slice_kind(bi, bj, j0, B, L)) {
+    const int kind = slice_kind(bi, bj, j0, B, L);
+    if constexpr (!CONS && B >= 8) {
+        if (kind == SLICE_FULL) {
+            hist_chunk_lanes<B, WEIGHTED>(h, seq, buflen, nbeg, nend, weights, scale, L, q, bi, bj);
+            __syncthreads();
+            // flush the [cell][P] table: lane l takes cell c0 + l % 8 of pair
+            // p0 + l / 8 -- global writes of 8 consecutive cells of 4 pairs
+            constexpr uint32_t P = B * B;
+            const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+            const uint32_t cgroups = (qq + 7) / 8;
+            for (uint32_t t = warp; t < cgroups * (P / 4); t += nwarps) {
+                const uint32_t c = (t % cgroups) * 8 + (lane & 7), p = (t / cgroups) * 4 + (lane >> 3);
+                if (c >= qq) continue;
+                const uint32_t v = h[c * P + p];
+                const uint64_t dst = pair_index(i0 + p / B, j0 + p % B, L) * qq + c;
+                if constexpr (WEIGHTED) {
+                    reinterpret_cast<uint32_t *>(out)[(uint64_t)chunk * nbins + dst] = v;
+                } else if (g.nchunks > 1) {
+                    if (v) atomicAdd(reinterpret_cast<uint32_t *>(out) + dst, v);
+                } else {
+                    reinterpret_cast<uint32_t *>(out)[dst] = v;
+                }
+            }
+            return;
+        }
+    }
+    switch (kind) {
         case SLICE_FULL:
             hist_chunk<B, SLICE_FULL, WEIGHTED, CONS>(h, seq, buflen, nbeg, nend, weights, scale, L, q, bi, bj,
                                                       cI, cJ);

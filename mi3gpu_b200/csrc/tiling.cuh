@@ -132,6 +132,58 @@ __device__ __forceinline__ uint32_t slice_row(const uint32_t (&wI)[B / 4], int i
     return (uint32_t)ii * B * qq + block_byte<B>(wI, ii, q - 1) * q;
 }
 
+// ------------------------------------------------ lanes over pairs (full slices)
+// In a slice table laid out pair-major, [p][cell], the 32 sequences of a warp
+// all visit pair p at the same time and gather 32 random cells: about 3.3
+// shared-memory wavefronts per warp instruction.  For full slices (every
+// pair valid) the pair kernels can instead lay the table out cell-major,
+// [cell][p] with P = B*B pairs (p = ii*B + jj), and let lane w visit pair
+// (t + w) mod P at step t: 32 consecutive pairs, 32 different banks, one
+// wavefront.  Lane w = B*wh + wl then meets pair (ii, jj) with
+// jj = (tl + wl) mod B and ii = (th + wh + carry) mod B for step
+// t = B*th + tl, carry = (tl + wl >= B).  Rotating the sequence's residue
+// bytes of block I by wh and of block J by wl (byte k of the rotated block
+// = byte (k + r) mod B) turns these into static register indices: the
+// column offset of step t is col[tl], the row offset row[th] or
+// row[th + 1] -- one select per pair.  P >= 32 needs B >= 8.
+
+// byte k of o = byte (k + r) mod B of w, for 0 <= r < B
+template <int B>
+__device__ __forceinline__ void rotate_block(const uint32_t (&w)[B / 4], uint32_t r, uint32_t (&o)[B / 4]) {
+    constexpr int W = B / 4;
+    const uint32_t rw = r >> 2, rb = 8 * (r & 3);
+    uint32_t t[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+        uint32_t v = w[0];
+#pragma unroll
+        for (int j = 1; j < W; ++j) v = ((k + rw) % W == (uint32_t)j) ? w[j] : v;
+        t[k] = v;
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k) o[k] = __funnelshift_r(t[k], t[(k + 1) % W], rb);
+}
+
+// Byte offsets, in a [cell][P] float table, of lane's row (site ii of block
+// I with residue a: a*q*P + ii*B) and column (site jj of block J with
+// residue b: b*P + jj) terms, in rotated order.
+template <int B>
+__device__ __forceinline__ void lane_offsets(const uint32_t (&wI)[B / 4], const uint32_t (&wJ)[B / 4], uint32_t q,
+                                             uint32_t lane, uint32_t (&row)[B], uint32_t (&col)[B]) {
+    constexpr uint32_t P = B * B;
+    const uint32_t wh = lane / B, wl = lane % B;
+    uint32_t rI[B / 4], rJ[B / 4];
+    rotate_block<B>(wI, wh, rI);
+    rotate_block<B>(wJ, wl, rJ);
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+        const uint32_t a = min((rI[k >> 2] >> (8 * (k & 3))) & 0xffu, q - 1);
+        const uint32_t b = min((rJ[k >> 2] >> (8 * (k & 3))) & 0xffu, q - 1);
+        row[k] = 4 * (a * q * P + ((k + wh) & (B - 1)) * B);
+        col[k] = 4 * (b * P + ((k + wl) & (B - 1)));
+    }
+}
+
 // ---------------------------------------------------------------- consensus
 // Consensus decomposition.  Every site i has a reference residue c_i (any
 // choice is exact; the most frequent residue makes it fastest).  A pair
