@@ -555,7 +555,14 @@ class MCMCGPU:
     # gain (its masked shared-memory reductions become divergent branches,
     # which costs what the saved bank conflicts give back), so it keeps the
     # direct kernel unless nearly all pairs are skipped.
+    # Since the direct pair kernels visit full slices with lanes over pairs
+    # (conflict-free, tiling.cuh), the direct energy pass is faster than the
+    # consensus one at every shape measured (energies of dJ on sampled
+    # walkers: 5.55 vs 8.46 ms at L=232, q=21, 2^20; 0.39 vs 0.51 ms at L=99,
+    # q=4, 2^18; 0.27 vs 0.28 ms at L=60, q=8, 2^18), so it is off: the
+    # consensus energies are used only for alphabets up to CONS_ENERGY_MAX_Q.
     CONS_ENERGY_MAX_ACTIVE = 0.75
+    CONS_ENERGY_MAX_Q = 0
     CONS_WMARG_MAX_ACTIVE = 0.2
 
     def updateConsensus(self, seqbufname='main'):
@@ -584,7 +591,7 @@ class MCMCGPU:
         off = 1.0 - counts.max(axis=1) / max(1, nseq)
         active = (off.sum() ** 2 - (off ** 2).sum()) / (L * (L - 1))
         self.consActive = float(active)
-        self.consEnergies = active <= self.CONS_ENERGY_MAX_ACTIVE
+        self.consEnergies = active <= self.CONS_ENERGY_MAX_ACTIVE and self.q <= self.CONS_ENERGY_MAX_Q
         self.consWmarg = active <= self.CONS_WMARG_MAX_ACTIVE
         return evt
 
