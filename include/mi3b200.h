@@ -129,9 +129,10 @@ int mi3_unpack_j_tiles(const float *J, float *Jtiles, uint32_t L, uint32_t q, vo
  * warp's walkers run skewed by one site per lane so that the coupling
  * gathers of a warp hit 32 different shared-memory banks; walker
  * sequences are held in registers.  Reads the chunk-tiled couplings of
- * mi3_unpack_j_tiles.  2 <= q <= 21, L + 31 <= 288, nseqs a multiple of
- * 32, walkers_per_cta 512 or 768 (0: 512; the last CTA may be partly
- * filled).  Residues >= q in
+ * mi3_unpack_j_tiles.  2 <= q <= 21, nseqs a multiple of 32,
+ * walkers_per_cta 256, 512 or 768 (the last CTA may be partly filled):
+ * L + 31 <= 288 with 512 or 768, L + 31 <= 576 with 256; 0 picks 512 when
+ * L allows it, else 256.  Residues >= q in
  * seqmem are clamped to q - 1.  replicas (0 = 1): Jtiles holds that many
  * identical copies of the table, mi3_jtiles_floats(L, q) floats apart, and
  * CTA b reads copy b % replicas (spreads the CTAs' simultaneous reads of

@@ -38,8 +38,8 @@ def sampler_plans(L, q, nseq):
     kernel where it applies, then the (walkers_per_cta, sites_per_chunk,
     stages) plans of the row-streaming kernel."""
     plans = []
-    if 2 <= q <= 21 and L + 31 <= 288 and nseq % 32 == 0:
-        plans += [('skew', 512), ('skew', 768)]
+    if 2 <= q <= 21 and L + 31 <= 576 and nseq % 32 == 0:
+        plans += ([('skew', 512), ('skew', 768)] if L + 31 <= 288 else []) + [('skew', 256)]
     n = int(_lib.query('mi3_metropolis_plans', L, q, nseq, None, 0))
     buf = (ctypes.c_uint32 * (3 * max(n, 1)))()
     _lib.query('mi3_metropolis_plans', L, q, nseq, buf, n)

@@ -215,10 +215,11 @@ __device__ __forceinline__ bool skew_bodies(const SkewStep &st, const uint32_t (
 // NW: sequence registers per lane (6 * NW >= L + 31); WARPS: consumer warps.
 // Register cap: each of the SM's 4 schedulers owns a quarter of the register
 // file (16384 registers) and holds every fourth warp, so with WARPS + 1 = 17
-// warps one scheduler holds 5 (5 x 32 x 96 <= 16384) and with 25 warps one
-// holds 7 (7 x 32 x 72 <= 16384).
+// warps one scheduler holds 5 (5 x 32 x 96 <= 16384), with 25 warps 7
+// (7 x 32 x 72 <= 16384) and with 9 warps 3 (3 x 32 x 168 <= 16384) -- the
+// 8-warp kernel has room for the 91 sequence registers of L = 512.
 template <uint32_t NW, uint32_t WARPS>
-__global__ void __maxnreg__(WARPS == 16 ? 96 : 72) k_metropolis_skew(const SkewParams p) {
+__global__ void __maxnreg__(WARPS == 8 ? 168 : (WARPS == 16 ? 96 : 72)) k_metropolis_skew(const SkewParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
     uint64_t *empty = full + SKEW_SLOTS;
@@ -380,11 +381,25 @@ static SkewKernel skew_kernel_for(uint32_t nw) {
     }
 }
 
-// Sequence registers for L: the smallest instantiated NW with 6 NW >= L + 31.
-static uint32_t skew_nw(uint32_t L) {
-    const uint32_t nws[7] = {8, 16, 24, 32, 40, 44, 48};
+// Longer sequences: the 8-warp kernel only.
+static SkewKernel skew_kernel_long(uint32_t nw) {
+    switch (nw) {
+        case 56: return k_metropolis_skew<56, 8>;
+        case 64: return k_metropolis_skew<64, 8>;
+        case 72: return k_metropolis_skew<72, 8>;
+        case 80: return k_metropolis_skew<80, 8>;
+        case 88: return k_metropolis_skew<88, 8>;
+        case 96: return k_metropolis_skew<96, 8>;
+        default: return skew_kernel_for<8>(nw);
+    }
+}
+
+// Sequence registers for L: the smallest instantiated NW with 6 NW >= L + 31
+// (at most 48 with 512 or 768 walkers per CTA, 96 with 256).
+static uint32_t skew_nw(uint32_t L, uint32_t max_nw) {
+    const uint32_t nws[13] = {8, 16, 24, 32, 40, 44, 48, 56, 64, 72, 80, 88, 96};
     for (uint32_t nw : nws)
-        if (6 * nw >= L + 31) return nw;
+        if (nw <= max_nw && 6 * nw >= L + 31) return nw;
     return 0;
 }
 
@@ -422,18 +437,19 @@ extern "C" int mi3_metropolis_skew(const float *Jtiles, uint32_t *rngstates, uin
     if (!Jtiles || !rngstates || !position_list || !seqmem || !status)
         return fail(MI3_ERR_ARG, "mi3_metropolis_skew: null pointer");
     if (L < 2 || q < 2 || q > 21) return fail(MI3_ERR_ARG, "mi3_metropolis_skew: needs 2 <= q <= 21");
-    const uint32_t nw = skew_nw(L);
-    if (!nw) return fail(MI3_ERR_ARG, "mi3_metropolis_skew: L too large (L + 31 <= 288)");
-    if (walkers_per_cta == 0) walkers_per_cta = 512;
-    if (walkers_per_cta != 512 && walkers_per_cta != 768)
-        return fail(MI3_ERR_ARG, "mi3_metropolis_skew: walkers per CTA must be 512 or 768");
+    if (walkers_per_cta == 0) walkers_per_cta = L + 31 <= 6 * 48 ? 512 : 256;
+    if (walkers_per_cta != 256 && walkers_per_cta != 512 && walkers_per_cta != 768)
+        return fail(MI3_ERR_ARG, "mi3_metropolis_skew: walkers per CTA must be 256, 512 or 768");
+    const uint32_t nw = skew_nw(L, walkers_per_cta == 256 ? 96 : 48);
+    if (!nw)
+        return fail(MI3_ERR_ARG, "mi3_metropolis_skew: L too large (L + 31 <= 288, or <= 576 with 256 walkers per CTA)");
     if (nseqs == 0 || nseqs % 32)
         return fail(MI3_ERR_ARG, "mi3_metropolis_skew: nseqs must be a positive multiple of 32");
     if (!aligned(Jtiles, 16) || !aligned(rngstates, 16))
         return fail(MI3_ERR_ALIGN, "mi3_metropolis_skew: Jtiles/rngstates must be 16B aligned");
     if (nsteps == 0) return MI3_OK;
     const uint32_t warps = walkers_per_cta / 32;
-    SkewKernel kernel = warps == 16 ? skew_kernel_for<16>(nw) : skew_kernel_for<24>(nw);
+    SkewKernel kernel = warps == 8 ? skew_kernel_long(nw) : warps == 16 ? skew_kernel_for<16>(nw) : skew_kernel_for<24>(nw);
     const size_t smem = skew_smem(q, nw, warps);
     if (!kernel || smem > 227 * 1024) return fail(MI3_ERR_ARG, "mi3_metropolis_skew: shape exceeds the kernel's limits");
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -449,7 +449,9 @@ class MCMCGPU:
     skew_replicas = 1
 
     def skew_supported(self):
-        return 2 <= self.q <= 21 and self.L + 31 <= 288 and self.nseq['main'] % 32 == 0
+        """The skewed-lane kernel takes 2 <= q <= 21 and L + 31 <= 576
+        (L + 31 <= 288 with 512 or 768 walkers per CTA, else 256)."""
+        return 2 <= self.q <= 21 and self.L + 31 <= 576 and self.nseq['main'] % 32 == 0
 
     def sampler_plan(self):
         """The plan runMCMC uses: ('skew', walkers_per_cta) or a
@@ -462,7 +464,7 @@ class MCMCGPU:
             return tuple(plan)
         if (self.SKEW_DEFAULT and self.skew_supported() and self.q >= self.SKEW_MIN_Q
                 and self.nseq['main'] >= 148 * 512):
-            return ('skew', 512)
+            return ('skew', 512 if self.L + 31 <= 288 else 256)
         return (0, 0, 0)
 
     def sampler_call(self, pos_offset, pos_ptr, nsteps, seq_ptr, rng_ptr, status_ptr, stream_ptr, betas=None,

@@ -93,9 +93,9 @@ def test_metropolis_plans_host_query(L, q, N):
     plans = sampler_plans(L, q, N)
     assert plans, "no plan for a supported shape"
     skew = [p for p in plans if p[0] == 'skew']
-    assert bool(skew) == (q <= 21 and L + 31 <= 288 and N % 32 == 0)
-    for _, w in skew:  # the skewed-lane kernel: 512 or 768 walkers per CTA
-        assert w in (512, 768)
+    assert bool(skew) == (q <= 21 and L + 31 <= 576 and N % 32 == 0)
+    for _, w in skew:  # the skewed-lane kernel: 256, 512 or 768 walkers per CTA
+        assert w in (256, 512, 768) and (w == 256 or L + 31 <= 288)
     for nw, m, st in [p for p in plans if p[0] != 'skew']:
         assert nw % 32 == 0 and 64 <= nw <= 512 and N % nw == 0
         assert m % 4 == 0 and 4 <= m <= ((L + 3) // 4) * 4

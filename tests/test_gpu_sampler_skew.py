@@ -51,12 +51,16 @@ def test_unpack_j_tiles_bitexact(cuda, L, q):
 
 @pytest.mark.parametrize("L,q,N", [(10, 5, 512), (48, 4, 1536), (37, 21, 512), (93, 4, 1536), (64, 8, 512),
                                    (2, 2, 512), (31, 7, 512), (32, 3, 512), (33, 21, 512), (257, 4, 512),
-                                   (99, 21, 1536), (60, 21, 1024), (40, 6, 96)])
+                                   (99, 21, 1536), (60, 21, 1024), (40, 6, 96), (300, 4, 512), (512, 21, 256),
+                                   (545, 3, 512)])
 @pytest.mark.parametrize("nsteps", [1, 37, 300])
-@pytest.mark.parametrize("wpc", [512, 768])
+@pytest.mark.parametrize("wpc", [256, 512, 768])
 def test_skew_trajectory_bitexact(cuda, L, q, N, nsteps, wpc):
     """N need not be a multiple of the walkers per CTA: the last CTA is then
-    partly filled (1024 = 768 + 256, 96 < 512)."""
+    partly filled (1024 = 768 + 256, 96 < 512).  Rows longer than
+    L + 31 = 288 take 256 walkers per CTA only."""
+    if L + 31 > 288 and wpc != 256:
+        pytest.skip("512 or 768 walkers per CTA hold rows up to L + 31 = 288")
     J = random_model(L, q, 2, sigma=0.5)
     seqs = _seqs(L, q, N, 3)
     mem = oracle.pack_seqs(seqs)
@@ -92,6 +96,31 @@ def test_skew_betas(cuda):
     oracle.metropolis(J, st, pos, 0, nsteps, mem, L, q, betas=betas)
     np.testing.assert_array_equal(host(dmem, np.uint32), mem)
     np.testing.assert_array_equal(host(dst, np.uint32), st)
+
+
+def test_skew_long_rows_equal_row_kernel(cuda):
+    """L=512, q=21 (the large workload's shape), 256 walkers per CTA, 300
+    proposals: the same walkers and RNG states as mi3_metropolis."""
+    L, q, N, nsteps = 512, 21, 1024, 300
+    from mi3gpu_b200.potts import synthetic_ground_truth
+    J = synthetic_ground_truth(L, q, seed=1004)
+    mem = oracle.pack_seqs(_seqs(L, q, N, 19))
+    st = oracle.init_rng(N, 9, 2 ** 63 // (2 * N))
+    pos = np.random.RandomState(4).randint(0, L, size=nsteps).astype("<u4")
+    stride = int(_lib.query("mi3_jrows_stride", L, q))
+    Ju = empty((L, stride), np.float32)
+    _lib.call("mi3_unpack_j", dev(J).data_ptr(), Ju.data_ptr(), L, q, stream())
+    T = _tiles(J, L, q)
+    status = empty((1,), np.int32)
+    a_mem, a_st = dev(mem), dev(st)
+    _lib.call("mi3_metropolis", Ju.data_ptr(), a_st.data_ptr(), 0, dev(pos).data_ptr(), nsteps, None, 1.0,
+              a_mem.data_ptr(), N, L, q, status.data_ptr(), stream())
+    b_mem, b_st = dev(mem), dev(st)
+    _lib.call("mi3_metropolis_skew", T.data_ptr(), b_st.data_ptr(), 0, dev(pos).data_ptr(), nsteps, None, 1.0,
+              b_mem.data_ptr(), N, L, q, 0, 1, status.data_ptr(), stream())
+    np.testing.assert_array_equal(host(b_mem, np.uint32), host(a_mem, np.uint32))
+    np.testing.assert_array_equal(host(b_st, np.uint32), host(a_st, np.uint32))
+    assert int(host(status)[0]) == 0
 
 
 def test_skew_equals_row_kernel_reference_shape(cuda):
@@ -137,7 +166,8 @@ def test_skew_bad_site_reported(cuda):
 def test_skew_rejects_unsupported_shapes(cuda):
     status = empty((1,), np.int32)
     buf = empty((16,), np.float32)
-    for L, q, N, wpc in [(20, 22, 512, 0), (258, 4, 512, 0), (20, 4, 500, 0), (20, 4, 1024, 640)]:
+    for L, q, N, wpc in [(20, 22, 512, 0), (258, 4, 512, 512), (546, 4, 512, 0), (20, 4, 500, 0),
+                         (20, 4, 1024, 640)]:
         with pytest.raises(_lib.Mi3Error):
             _lib.call("mi3_metropolis_skew", buf.data_ptr(), buf.data_ptr(), 0, buf.data_ptr(), 1, None, 1.0,
                       buf.data_ptr(), N, L, q, wpc, 1, status.data_ptr(), stream())
