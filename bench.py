@@ -38,6 +38,16 @@ sys.path.insert(0, str(ROOT))
 L_, Q_, N_ = 232, 21, 1 << 20
 METRIC = "site-updates/s"
 
+# (kernel, L, q) -> what bounds the kernel, from its ncu capture (cited)
+BINDING_CITED = {
+    ("k_metropolis_skew", 232, 21): {
+        "resource": "instruction issue", "issue_active": 0.768, "l1tex_throughput": 0.476,
+        "shared_wavefronts_per_update": 18.4, "source": "ncu --set full (profiles/metropolis_skew_L232_q21.md)"},
+    ("k_metropolis", 232, 21): {
+        "resource": "shared-memory pipe", "issue_active": 0.576, "l1tex_throughput": 0.914,
+        "shared_wavefronts_per_update": 49.7, "source": "ncu --set full (profiles/metropolis_L232_q21.md)"},
+}
+
 # (kernel, L, q, walkers, proposals per call) -> (DRAM bytes read + written
 # per launch, where the figure comes from)
 TRAFFIC_CITED = {
@@ -255,6 +265,7 @@ def run_gpu(args):
     # measured by a one-pass ncu capture of this command's own launch; a
     # cited figure, not measured in this run
     traffic, traffic_src = TRAFFIC_CITED.get((kernel, L, q, N, args.nsteps), (None, None))
+    binding = BINDING_CITED.get((kernel, L, q))
     # shared-memory load roofline: 148 SMs x 128 B/clk at the sampled clock
     clocks = clk.summary()
     sm_mhz = clocks.get("sm_mhz") or 1965.0
@@ -285,6 +296,7 @@ def run_gpu(args):
             "roofline_onchip": {"bound": "smem", "achieved": onchip, "peak": smem_peak, "unit": "GB/s",
                                 "frac": onchip / smem_peak, "bytes_per_update": onchip_bytes_per_update,
                                 "peak_basis": "148 SM x 128 B/clk x sampled SM clock"},
+            "binding_resource": binding,
             "kernel_ms_per_launch": per_launch_ms,
             "newton": newton,
             "gpu_launches": args.steps,
