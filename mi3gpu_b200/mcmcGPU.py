@@ -521,13 +521,15 @@ class MCMCGPU:
     # ------------------------------------------------------------ statistics
     # alphabet sizes for which the tcgen05 one-hot GEMM counts beat the
     # shared-memory histogram when nothing was tuned (measured on B200 at
-    # 2^18 walkers: 1.3x at q=4, even at q=8, 3x slower at q=21); both give
-    # identical integers.
+    # 2^18 walkers against the lanes-over-pairs histogram: 1.4x at q=4-6,
+    # slower from q=8 on and at 2^14 walkers); both give identical integers.
     TENSOR_COUNT_Q = range(4, 7)
     # the same for the weighted bimarginals (three byte-plane integer GEMMs
     # against the shared-memory fixed-point histogram, identical results):
-    # 2.1x at q=4, 1.2x at q=5, slower from q=6 on
-    TENSOR_WMARG_Q = range(4, 6)
+    # since the histogram visits pairs with lanes over pairs it is as fast at
+    # q=4 (0.40 vs 0.40 ms at L=99, 2^18) and faster from q=5 on, so the
+    # tensor-core form is left to the autotuner's per-shape timing
+    TENSOR_WMARG_Q = range(0)
 
     def calcBicounts(self, seqbufname, wait_for=None, tensor=None):
         nseq, buflen = self._span(seqbufname)
