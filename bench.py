@@ -805,6 +805,7 @@ def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, 
     from mi3gpu_b200 import MCMCGPU, GPU_node
     from mi3gpu_b200.potts import synthetic_ground_truth
     from mi3gpu_b200.learned import MadeProposal, LearnedSampler
+    from mi3gpu_b200._lib import call as _lib_call, query as _lib_query
     J = synthetic_ground_truth(L, q, seed=1003, contact_sigma=0.8)
     g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, args.seed + 1)
     gpus = GPU_node([g])
@@ -824,6 +825,43 @@ def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, 
     t_train = time.time() - t0
     start = g.bufs['seq main'].clone()
     start_rng = g.bufs['rngstates'].clone()
+    # the proposal step's parts, timed with CUDA events on the sampler's stream
+    parts = {}
+    with torch.cuda.stream(g.stream):
+        prop = torch.zeros_like(start)
+        lqp = torch.zeros(N, dtype=torch.float32, device=start.device)
+        ws = torch.zeros(int(_lib_query('mi3_energies_workspace', N)) // 8 + 2, dtype=torch.int64,
+                         device=start.device)
+
+        def timed(fn, reps=5):
+            fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(g.stream)
+            for _ in range(reps):
+                fn()
+            e1.record(g.stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        kind = made.sampler
+        for smp in ((kind, "simt") if kind != "simt" else ("simt",)):
+            made.sampler = smp
+            parts[f"made_sample_{smp}_ms"] = timed(lambda: made.sample(prop, N, lqp, seed=5))
+            parts[f"made_logq_{smp}_ms"] = timed(lambda: made.sample(start, N, lqp, seed=0, given=True))
+        made.sampler = kind
+        parts["energies_ms"] = timed(lambda: _lib_call('mi3_energies', g._ptr('J'), prop.data_ptr(), N, N,
+                                                       lqp.data_ptr(), L, q, ws.data_ptr(), ws.numel() * 8,
+                                                       g.stream.cuda_stream))
+        made.check_status()
+        g.bufs['seq main'].copy_(start)
+        ls_t = LearnedSampler(g, made, every=every, min_accept=0.0, seed=3)
+        ls_t.propose()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(5):
+            ls_t.propose()
+        parts["proposal_step_ms"] = (time.perf_counter() - t1) / 5 * 1e3
+        parts["sampler"] = kind
     res = {}
     for mode in ("plain", "learned"):
         g.bufs['seq main'].copy_(start)
@@ -852,6 +890,7 @@ def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, 
                                                     "equil_sweeps": equil_sweeps, "every": every,
                                                     "train_epochs": epochs},
                       "train_nll": hist, "t_equil_s": t_equil, "t_train_s": t_train, "results": res,
+                      "proposal_step": parts,
                       "tau_gain_per_sweep": gain,
                       "tau_gain_per_second": res["plain"]["tau_int_s"] / res["learned"]["tau_int_s"]}))
 

@@ -468,6 +468,32 @@ int mi3_made_sample(uint32_t L, uint32_t q, uint32_t H, const void *W1T_bf16, co
                     uint32_t buflen, uint32_t nseq, float *logq, uint64_t seed, int32_t given,
                     void *stream);
 
+/* Tensor-core MADE sampler (tcgen05).  Hidden degrees m1, m2 (host arrays
+ * of H int32, sorted, in [1, L-1]) grouped in blocks of G sites: block b
+ * owns the units of degree in (bG, bG+G], 0, 16, 32 or 48 per layer;
+ * q in {4, 8}, H <= 512 a multiple of 16, G a multiple of 4 with G q <= 64
+ * and ceil(L/G) * roundup(G q, 16) + 48 <= 512.  The activations entering
+ * layers 2 and 3 are rounded to bf16.
+ * mi3_made_tc_workspace: device bytes for the plan's tables and weight
+ * tiles (0 if the degrees or sizes are not supported). */
+uint64_t mi3_made_tc_workspace(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const int32_t *m1,
+                               const int32_t *m2);
+
+/* Build the plan from float weights holding bf16 values (the layouts
+ * above) into workspace (256-byte aligned); plan_out (host, 24 uint64)
+ * receives the launch parameters.  Call again after the weights change. */
+int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const int32_t *m1,
+                        const int32_t *m2, const float *W1T, const float *b1, const float *W2,
+                        const float *b2, const float *W3, const float *b3, void *workspace,
+                        uint64_t ws_bytes, uint64_t *plan_out, void *stream);
+
+/* Draw nseq sequences into seq (given = 0; residue i of walker n from the
+ * uniform (seed, n, i) of mi3_made_sample), or log q of the sequences in
+ * seq (given = 1); log q of a drawn sequence is reproduced exactly.  A
+ * timed-out wait sets *status (int32, device). */
+int mi3_made_tc_sample(const uint64_t *plan, uint32_t *seq, uint32_t buflen, uint32_t nseq,
+                       float *logq, uint64_t seed, int32_t given, int32_t *status, void *stream);
+
 /* Independence Metropolis-Hastings: walker n takes proposal n with
  * probability min(1, exp(-(Ep-E)) exp(logq - logq_prop)); accepted walkers
  * copy sequence, energy and log q; *naccept (uint64) += acceptances. */

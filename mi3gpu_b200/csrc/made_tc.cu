@@ -1,0 +1,785 @@
+// made_tc.cu -- autoregressive sampling (and teacher-forced log q) of the
+// MADE proposal with the bulk of the network on the tcgen05 tensor cores.
+//
+// Network (as in made.cu): h1 = b1 + sum_j W1T[(j, s_j)], a1 = bf16(relu(h1)),
+// h2 = b2 + W2 a1, a2 = bf16(relu(h2)), logits = b3 + W3 a2, with MADE masks
+// (hidden-1 unit v sees sites j < m1[v], hidden-2 unit u sees hidden-1 units
+// with m1 <= m2[u], output site i sees hidden-2 units with m2 <= i).  The
+// activations entering layers 2 and 3 are rounded to bf16, as the tensor
+// cores read them; weights are bf16 values, sums are FP32.
+//
+// Degree blocks.  The hidden degrees are grouped in blocks of G sites:
+// block b owns the units of degree in (bG, bG + G], unit indices sorted by
+// degree, 16, 32 or 48 units per block and layer.  Walking the sites in
+// order, when block b starts (sites < s0 = bG drawn):
+//   * every hidden-1 unit of an earlier block is final, so the hidden-2
+//     units of block b get their share from them as one GEMM,
+//       D2 = A1[:, 0:c1] . W2[U2_b, 0:c1]^T      (tcgen05, D2 in TMEM)
+//     where A1 (128 walkers x H, bf16, shared memory) holds the final a1;
+//   * the logits of every site of block b already hold the share of all
+//     hidden-2 units of earlier blocks: after each block the new units'
+//     a2 (128 x n2_b, bf16) are multiplied into a TMEM accumulator of the
+//     logits of all later sites (tcgen05, acc3 += A2 . W3[later, U2_b]^T).
+// What remains inside a block -- the block's own hidden-1 units (their
+// inputs from earlier sites gathered once, then one weight row per drawn
+// site), its hidden-2 units (one dot product over the block's hidden-1
+// units each, as they become final) and the in-block share of each site's
+// logits -- runs on the CUDA cores, one walker per thread.  Masked weights
+// are zero, so each in-block loop runs over all of the block's units.
+//
+// CTA: 128 walkers (TMEM lanes); warps 0-3 compute, warp 4 issues the MMAs,
+// warp 5 streams the weight tiles (pre-swizzled K-major images, one 1-D bulk
+// copy each) through a 3-stage ring.  All waits are bounded (status word).
+// The kernel draws walker n's residue i from the same counter-based uniform
+// as made.cu (seed, n, i); with given = 1 it reads the residues instead and
+// returns log q: the same arithmetic, so log q of a drawn sequence is
+// reproduced bit for bit.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "made.cuh"
+#include "tc.cuh"
+
+namespace mi3 {
+
+constexpr uint32_t MT_M = 128;        // walkers per tile
+constexpr uint32_t MT_NU = 48;        // largest unit count per block and layer
+constexpr uint32_t MT_HMAX = 512;     // hidden units (A1 holds 8 K-chunks of 64)
+constexpr uint32_t MT_GQMAX = 64;     // sites x residues per block
+constexpr uint32_t MT_STAGES = 3;
+constexpr uint32_t MT_STAGE_BYTES = 128 * 128;  // up to 128 rows x 64 K bf16
+constexpr uint32_t MT_A1_BYTES = (MT_HMAX / 64) * MT_M * 128;
+constexpr uint32_t MT_A2_BYTES = MT_M * 128;
+constexpr uint32_t MT_D2S_BYTES = MT_NU * MT_M * 4;
+constexpr uint32_t MT_THREADS = 192;
+constexpr uint32_t MT_TMEM_COLS = 512;
+constexpr uint32_t MT_SMEM = 1024 + MT_A1_BYTES + MT_A2_BYTES + MT_STAGES * MT_STAGE_BYTES + MT_D2S_BYTES + 256;
+
+// One weight tile of the ring and the MMAs that consume it.
+struct MtOp {
+    uint32_t off;     // byte offset of the tile image
+    uint32_t rows;    // N of the MMA (tile rows, 128 B each)
+    uint32_t kc;      // A1 K-chunk (layer-2 tiles)
+    uint32_t ksteps;  // K / 16 in this tile
+    uint32_t dcol;    // TMEM column of the accumulator
+    uint32_t first;   // 1: the first tile of a layer-2 product (overwrite D2)
+    uint32_t kind;    // 0: layer-2 prefix, 1: logits accumulator update
+    uint32_t blk;
+};
+
+// per block: c1 (hidden-1 units before the block), n1, c2, n2, first op of
+// the layer-2 tiles, first op of the logits tiles, end, D2 valid
+constexpr uint32_t MT_BLK = 8;
+
+struct MtPlan {
+    uint32_t L, q, H, G, nb, N3, d2col, nops;
+    uint64_t img_bytes;
+    const MtOp *ops;
+    const uint32_t *blk;
+    const int32_t *deg2_start;  // [L + 1]: first hidden-2 unit of degree >= d
+    const unsigned char *img;
+    const float *W1b;  // [nb][L q][NU]   W1T[(j, a)][c1 + v]
+    const float *W2b;  // [nb][NU][NU]    W2[c2 + u][c1 + v]
+    const float *W3b;  // [nb][GQMAX][NU] W3[(s0 q + c)][c2 + u]
+    const float *b1b;  // [nb][NU]
+    const float *b2b;  // [nb][NU]
+    const float *b3;   // [L q]
+};
+static_assert(sizeof(MtPlan) <= 24 * 8, "plan blob");
+
+__device__ __forceinline__ uint32_t mt_idesc(uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((MT_M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mt_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// byte offset of (row, k) in a 128-row K-major 128B-swizzled tile of 64 K
+__device__ __forceinline__ uint32_t mt_sw(uint32_t row, uint32_t k) {
+    return row * 128 + ((((k >> 3) ^ (row & 7)) & 7) << 4) + ((k & 7) << 1);
+}
+
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
+           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+}
+
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float (&v)[4]) {
+    uint32_t r0, r1, r2, r3;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    v[0] = __uint_as_float(r0);
+    v[1] = __uint_as_float(r1);
+    v[2] = __uint_as_float(r2);
+    v[3] = __uint_as_float(r3);
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ void tmem_zero16(uint32_t taddr) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(
+            taddr),
+        "r"(0u)
+        : "memory");
+}
+
+template <uint32_t Q>
+__device__ __forceinline__ void tmem_ldq(uint32_t taddr, float (&v)[Q]);
+template <>
+__device__ __forceinline__ void tmem_ldq<4>(uint32_t taddr, float (&v)[4]) {
+    tmem_ld4(taddr, v);
+}
+template <>
+__device__ __forceinline__ void tmem_ldq<8>(uint32_t taddr, float (&v)[8]) {
+    tmem_ld8(taddr, v);
+}
+
+template <uint32_t Q>
+__global__ void __launch_bounds__(MT_THREADS, 1)
+    k_made_tc(const MtPlan p, uint32_t *seq, uint32_t buflen, uint32_t nseq, float *logq, uint64_t seed,
+              int given, int32_t *status) {
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t base_addr = smem_addr(smem_raw);
+    unsigned char *sm = smem_raw + ((1024u - (base_addr & 1023u)) & 1023u);
+    unsigned char *A1 = sm;
+    unsigned char *A2 = A1 + MT_A1_BYTES;
+    unsigned char *ring = A2 + MT_A2_BYTES;
+    float *d2s = reinterpret_cast<float *>(ring + MT_STAGES * MT_STAGE_BYTES);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(d2s + MT_NU * MT_M);
+    uint64_t *full = bars, *empty = bars + MT_STAGES;
+    uint64_t *bar_a1 = bars + 2 * MT_STAGES, *bar_a2 = bar_a1 + 1, *bar_mma = bar_a1 + 2, *bar_fin = bar_a1 + 3;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_a1 + 4);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t L = p.L, q = p.q, G = p.G, nb = p.nb, Lq = L * q;
+    const uint32_t ntiles = (nseq + MT_M - 1) / MT_M;
+
+    if (tid == 0) {
+        for (uint32_t s = 0; s < MT_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(bar_a1, MT_M);
+        mbar_init(bar_a2, MT_M);
+        mbar_init(bar_mma, 1);
+        mbar_init(bar_fin, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 4) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(MT_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 5) {
+        // ---------------------------------------------------- producer
+        if ((tid & 31) == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                for (uint32_t o = 0; o < p.nops; ++o) {
+                    const uint32_t s = it % MT_STAGES, round = it / MT_STAGES;
+                    if (round > 0 && !mbar_wait_bounded(&empty[s], (round - 1) & 1, abort_flag, WAIT_LIMIT_NS)) {
+                        report(status, ST_TIMEOUT_EMPTY);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    const MtOp op = p.ops[o];
+                    const uint32_t bytes = op.rows * 128;
+                    mbar_arrive_expect_tx(&full[s], bytes);
+                    bulk_g2s(ring + s * MT_STAGE_BYTES, p.img + op.off, bytes, &full[s]);
+                    ++it;
+                }
+            }
+            // the copies still in flight land before the CTA exits
+            for (uint32_t k = 0; k < MT_STAGES && k < it; ++k) {
+                const uint32_t j = it - 1 - k;
+                mbar_wait_bounded(&full[j % MT_STAGES], (j / MT_STAGES) & 1, nullptr, WAIT_LIMIT_NS);
+            }
+        }
+    } else if (warp == 4) {
+        // ---------------------------------------------------- MMA issue
+        if ((tid & 31) == 0) {
+            uint32_t it = 0, na1 = 0, na2 = 0;
+            bool ok = true;
+            const uint32_t a1base = smem_addr(A1), a2base = smem_addr(A2), rbase = smem_addr(ring);
+            for (uint32_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                for (uint32_t b = 0; b < nb && ok; ++b) {
+                    const uint32_t *bk = p.blk + b * MT_BLK;
+                    if (!mbar_wait_bounded(bar_a1, na1++ & 1, abort_flag, WAIT_LIMIT_NS)) {
+                        report(status, ST_TIMEOUT_FULL);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    for (uint32_t pass = 0; pass < 2 && ok; ++pass) {
+                        if (pass == 1) {
+                            // block 0 has no layer-2 product and every MMA of the
+                            // previous tile completed before its last block began
+                            if (b == 0)
+                                mbar_arrive(bar_mma);
+                            else
+                                tc_commit(bar_mma);
+                            if (!mbar_wait_bounded(bar_a2, na2++ & 1, abort_flag, WAIT_LIMIT_NS)) {
+                                report(status, ST_TIMEOUT_FULL);
+                                *abort_flag = 1;
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                        }
+                        const uint32_t lo = bk[4 + pass], hi = bk[5 + pass];
+                        for (uint32_t o = lo; o < hi; ++o) {
+                            const uint32_t s = it % MT_STAGES;
+                            if (!mbar_wait_bounded(&full[s], (it / MT_STAGES) & 1, abort_flag, WAIT_LIMIT_NS)) {
+                                report(status, ST_TIMEOUT_FULL);
+                                *abort_flag = 1;
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                            const MtOp op = p.ops[o];
+                            const uint32_t idesc = mt_idesc(op.rows);
+                            const uint32_t bb = rbase + s * MT_STAGE_BYTES;
+                            const uint32_t ab = op.kind == 0 ? a1base + op.kc * (MT_M * 128) : a2base;
+                            for (uint32_t kk = 0; kk < op.ksteps; ++kk)
+                                mt_mma(tmem + op.dcol, umma_desc_sw128(ab + kk * 32), umma_desc_sw128(bb + kk * 32),
+                                       idesc, (op.kind == 0 && op.first && kk == 0) ? 0u : 1u);
+                            tc_commit(&empty[s]);
+                            ++it;
+                        }
+                    }
+                }
+            }
+            // every MMA issued has completed before the accumulators are freed
+            tc_commit(bar_fin);
+            mbar_wait_bounded(bar_fin, 0, nullptr, WAIT_LIMIT_NS);
+        }
+    } else {
+        // ---------------------------------------------------- walkers
+        const uint32_t m = tid;
+        const uint32_t lane_base = (32 * warp) << 16;
+        uint32_t nmma = 0;
+        bool ok = true;
+        for (uint32_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            const uint32_t n = t * MT_M + m;
+            const bool valid = n < nseq;
+            float lq = 0.0f;
+            uint32_t cw = 0;  // residues of the current sequence word
+            for (uint32_t b = 0; b < nb; ++b) {
+                const uint32_t *bk = p.blk + b * MT_BLK;
+                const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], d2ok = bk[7];
+                const uint32_t s0 = b * G, s1 = min(L, s0 + G);
+                if (b == 0) {
+                    // the logits accumulator of this tile starts at zero
+                    for (uint32_t c = 0; c < nb * p.N3; c += 16) tmem_zero16(tmem + lane_base + c);
+                    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                }
+                tc_fence_before();
+                mbar_arrive(bar_a1);
+
+                // hidden-1 units of the block: bias + inputs from sites < s0
+                float h1[MT_NU];
+                {
+                    const float *bb1 = p.b1b + b * MT_NU;
+#pragma unroll
+                    for (uint32_t v = 0; v < MT_NU; ++v) h1[v] = __ldg(&bb1[v]);
+                    const float *w1 = p.W1b + (size_t)b * Lq * MT_NU;
+                    uint32_t word = 0;
+                    for (uint32_t j = 0; j < s0; ++j) {
+                        if ((j & 3) == 0) word = valid ? seq[(size_t)(j >> 2) * buflen + n] : 0u;
+                        const uint32_t x = min((word >> (8 * (j & 3))) & 0xffu, q - 1);
+                        const float4 *row = reinterpret_cast<const float4 *>(w1 + (size_t)(j * q + x) * MT_NU);
+#pragma unroll
+                        for (uint32_t g = 0; g < MT_NU / 4; ++g) {
+                            const float4 w = __ldg(&row[g]);
+                            h1[4 * g] += w.x;
+                            h1[4 * g + 1] += w.y;
+                            h1[4 * g + 2] += w.z;
+                            h1[4 * g + 3] += w.w;
+                        }
+                    }
+                }
+                // hidden-2 pre-activations of the block from earlier blocks (the
+                // warp decides together: tcgen05.ld needs all 32 lanes)
+                {
+                    const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(bar_mma, nmma++ & 1, abort_flag,
+                                                                                 WAIT_LIMIT_NS));
+                    if (!got) {
+                        report(status, ST_TIMEOUT_FULL);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                }
+                {
+                    const float *bb2 = p.b2b + b * MT_NU;
+#pragma unroll
+                    for (uint32_t c = 0; c < MT_NU; c += 16) {
+                        uint32_t r[16];
+                        if (d2ok) tmem_ld16(tmem + lane_base + p.d2col + c, r);
+#pragma unroll
+                        for (uint32_t k = 0; k < 16; ++k)
+                            d2s[(c + k) * MT_M + m] = (d2ok ? __uint_as_float(r[k]) : 0.0f) + __ldg(&bb2[c + k]);
+                    }
+                }
+#pragma unroll
+                for (uint32_t g = 0; g < 8; ++g)
+                    *reinterpret_cast<uint4 *>(A2 + m * 128 + (g << 4)) = make_uint4(0, 0, 0, 0);
+
+                const float *w3 = p.W3b + (size_t)b * MT_GQMAX * MT_NU;
+                const float *w2 = p.W2b + (size_t)b * MT_NU * MT_NU;
+                const float *w1 = p.W1b + (size_t)b * Lq * MT_NU;
+                uint32_t gword = 0;
+                for (uint32_t i = s0; i < s1; ++i) {
+                    const uint32_t il = i - s0;
+                    // logits of site i
+                    float lg[Q];
+                    if (b >= 1) {
+                        tmem_ldq<Q>(tmem + lane_base + b * p.N3 + il * Q, lg);
+                    } else {
+#pragma unroll
+                        for (uint32_t a = 0; a < Q; ++a) lg[a] = 0.0f;
+                    }
+                    {
+                        float act2[MT_NU];
+#pragma unroll
+                        for (uint32_t g = 0; g < MT_NU / 8; ++g) {
+                            const uint4 w = *reinterpret_cast<const uint4 *>(A2 + m * 128 + (((g ^ (m & 7)) & 7) << 4));
+                            const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                            for (uint32_t h = 0; h < 4; ++h) {
+                                act2[8 * g + 2 * h] = __uint_as_float(ww[h] << 16);
+                                act2[8 * g + 2 * h + 1] = __uint_as_float(ww[h] & 0xffff0000u);
+                            }
+                        }
+#pragma unroll
+                        for (uint32_t a = 0; a < Q; ++a) {
+                            const float4 *row = reinterpret_cast<const float4 *>(w3 + (il * Q + a) * MT_NU);
+                            float s = 0.0f;
+#pragma unroll
+                            for (uint32_t g = 0; g < MT_NU / 4; ++g) {
+                                const float4 w = __ldg(&row[g]);
+                                s = __fmaf_rn(w.x, act2[4 * g], s);
+                                s = __fmaf_rn(w.y, act2[4 * g + 1], s);
+                                s = __fmaf_rn(w.z, act2[4 * g + 2], s);
+                                s = __fmaf_rn(w.w, act2[4 * g + 3], s);
+                            }
+                            lg[a] += __ldg(&p.b3[i * Q + a]) + s;
+                        }
+                    }
+                    // draw (or read) residue i
+                    float mx = lg[0];
+#pragma unroll
+                    for (uint32_t a = 1; a < Q; ++a) mx = fmaxf(mx, lg[a]);
+                    float ex[Q], se = 0.0f;
+#pragma unroll
+                    for (uint32_t a = 0; a < Q; ++a) {
+                        ex[a] = expf(lg[a] - mx);
+                        se += ex[a];
+                    }
+                    const float lse = mx + logf(se);
+                    uint32_t r;
+                    if (given) {
+                        if ((i & 3) == 0) gword = valid ? seq[(size_t)(i >> 2) * buflen + n] : 0u;
+                        r = min((gword >> (8 * (i & 3))) & 0xffu, Q - 1);
+                    } else {
+                        const float u = hash_uniform(seed, n, i) * se;
+                        float c = 0.0f;
+                        r = Q - 1;
+                        bool found = false;
+#pragma unroll
+                        for (uint32_t a = 0; a < Q; ++a) {
+                            c += ex[a];
+                            if (!found && u < c) {
+                                r = a;
+                                found = true;
+                            }
+                        }
+                    }
+                    float lr = lg[0];
+#pragma unroll
+                    for (uint32_t a = 1; a < Q; ++a) lr = (r == a) ? lg[a] : lr;
+                    lq += lr - lse;
+                    if (!given) {
+                        cw |= r << (8 * (i & 3));
+                        if ((i & 3) == 3 || i == L - 1) {
+                            if (valid) seq[(size_t)(i >> 2) * buflen + n] = cw;
+                            cw = 0;
+                        }
+                    }
+                    // its input to the block's hidden-1 units
+                    {
+                        const float4 *row = reinterpret_cast<const float4 *>(w1 + (size_t)(i * Q + r) * MT_NU);
+#pragma unroll
+                        for (uint32_t g = 0; g < MT_NU / 4; ++g) {
+                            const float4 w = __ldg(&row[g]);
+                            h1[4 * g] += w.x;
+                            h1[4 * g + 1] += w.y;
+                            h1[4 * g + 2] += w.z;
+                            h1[4 * g + 3] += w.w;
+                        }
+                    }
+                    // hidden-2 units of degree i + 1
+                    if (i + 1 < L) {
+                        const int32_t ulo = __ldg(&p.deg2_start[i + 1]) - (int32_t)c2;
+                        const int32_t uhi = __ldg(&p.deg2_start[i + 2]) - (int32_t)c2;
+                        if (ulo < uhi) {
+                            float act1[MT_NU];
+#pragma unroll
+                            for (uint32_t v = 0; v < MT_NU; ++v) act1[v] = bf16r(fmaxf(h1[v], 0.0f));
+                            for (int32_t u = ulo; u < uhi; ++u) {
+                                const float4 *row = reinterpret_cast<const float4 *>(w2 + u * MT_NU);
+                                float s = 0.0f;
+#pragma unroll
+                                for (uint32_t g = 0; g < MT_NU / 4; ++g) {
+                                    const float4 w = __ldg(&row[g]);
+                                    s = __fmaf_rn(w.x, act1[4 * g], s);
+                                    s = __fmaf_rn(w.y, act1[4 * g + 1], s);
+                                    s = __fmaf_rn(w.z, act1[4 * g + 2], s);
+                                    s = __fmaf_rn(w.w, act1[4 * g + 3], s);
+                                }
+                                const float z = d2s[u * MT_M + m] + s;
+                                *reinterpret_cast<unsigned short *>(A2 + mt_sw(m, (uint32_t)u)) =
+                                    __bfloat16_as_ushort(__float2bfloat16_rn(fmaxf(z, 0.0f)));
+                            }
+                        }
+                    }
+                }
+                // the block's hidden-1 units are final: into A1 for later blocks
+#pragma unroll
+                for (uint32_t g = 0; g < MT_NU / 8; ++g) {
+                    if (8 * g < n1) {
+                        const uint32_t k = c1 + 8 * g;
+                        uint4 w;
+                        w.x = pack_bf16x2(fmaxf(h1[8 * g], 0.0f), fmaxf(h1[8 * g + 1], 0.0f));
+                        w.y = pack_bf16x2(fmaxf(h1[8 * g + 2], 0.0f), fmaxf(h1[8 * g + 3], 0.0f));
+                        w.z = pack_bf16x2(fmaxf(h1[8 * g + 4], 0.0f), fmaxf(h1[8 * g + 5], 0.0f));
+                        w.w = pack_bf16x2(fmaxf(h1[8 * g + 6], 0.0f), fmaxf(h1[8 * g + 7], 0.0f));
+                        *reinterpret_cast<uint4 *>(A1 + (k >> 6) * (MT_M * 128) + mt_sw(m, k & 63)) = w;
+                    }
+                }
+                fence_proxy_async_smem();
+                tc_fence_before();
+                mbar_arrive(bar_a2);
+            }
+            if (ok && valid) logq[n] = lq;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 4) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(MT_TMEM_COLS));
+    }
+}
+
+// Weight images and per-block arrays from the (bf16-valued) float weights.
+__global__ void k_made_tc_images(const MtPlan p, unsigned char *img, const float *__restrict__ W2,
+                                 const float *__restrict__ W3) {
+    const MtOp op = p.ops[blockIdx.x];
+    const uint32_t *bk = p.blk + op.blk * MT_BLK;
+    const uint32_t c1 = bk[0], c2 = bk[2], n2 = bk[3];
+    const uint32_t H = p.H, q = p.q, G = p.G, N3 = p.N3, L = p.L;
+    for (uint32_t e = threadIdx.x; e < op.rows * 64; e += blockDim.x) {
+        const uint32_t r = e / 64, k = e % 64;
+        float v = 0.0f;
+        if (op.kind == 0) {
+            const uint32_t u = c2 + r, hv = op.kc * 64 + k;
+            if (hv < c1) v = W2[(size_t)u * H + hv];
+        } else {
+            const uint32_t col = op.dcol + r;  // logits column of a later block
+            const uint32_t beta = col / N3, c = col % N3;
+            const uint32_t i = beta * G + c / q, a = c % q;
+            if (c < G * q && i < L && k < n2) v = W3[(size_t)(i * q + a) * H + c2 + k];
+        }
+        *reinterpret_cast<unsigned short *>(img + op.off + mt_sw(r, k)) =
+            __bfloat16_as_ushort(__float2bfloat16_rn(v));
+    }
+}
+
+__global__ void k_made_tc_blocks(const MtPlan p, float *W1b, float *W2b, float *W3b, float *b1b, float *b2b,
+                                 float *b3c, const float *__restrict__ W1T, const float *__restrict__ b1,
+                                 const float *__restrict__ W2, const float *__restrict__ b2,
+                                 const float *__restrict__ W3, const float *__restrict__ b3) {
+    const uint32_t H = p.H, q = p.q, G = p.G, L = p.L, Lq = L * q, NU = MT_NU;
+    const size_t n1tot = (size_t)p.nb * Lq * NU, n2tot = (size_t)p.nb * NU * NU, n3tot = (size_t)p.nb * MT_GQMAX * NU;
+    const size_t nbias = (size_t)p.nb * NU;
+    const size_t total = n1tot + n2tot + n3tot + 2 * nbias + Lq;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        size_t x = e;
+        if (x < n1tot) {
+            const uint32_t b = (uint32_t)(x / ((size_t)Lq * NU)), rem = (uint32_t)(x % ((size_t)Lq * NU));
+            const uint32_t row = rem / NU, v = rem % NU;
+            const uint32_t *bk = p.blk + b * MT_BLK;
+            W1b[x] = v < bk[1] ? W1T[(size_t)row * H + bk[0] + v] : 0.0f;
+            continue;
+        }
+        x -= n1tot;
+        if (x < n2tot) {
+            const uint32_t b = (uint32_t)(x / (NU * NU)), rem = (uint32_t)(x % (NU * NU));
+            const uint32_t u = rem / NU, v = rem % NU;
+            const uint32_t *bk = p.blk + b * MT_BLK;
+            W2b[x] = (u < bk[3] && v < bk[1]) ? W2[(size_t)(bk[2] + u) * H + bk[0] + v] : 0.0f;
+            continue;
+        }
+        x -= n2tot;
+        if (x < n3tot) {
+            const uint32_t b = (uint32_t)(x / (MT_GQMAX * NU)), rem = (uint32_t)(x % (MT_GQMAX * NU));
+            const uint32_t c = rem / NU, u = rem % NU;
+            const uint32_t *bk = p.blk + b * MT_BLK;
+            const uint32_t i = b * G + c / q;
+            W3b[x] = (c < G * q && i < L && u < bk[3]) ? W3[(size_t)(b * G * q + c) * H + bk[2] + u] : 0.0f;
+            continue;
+        }
+        x -= n3tot;
+        if (x < nbias) {
+            const uint32_t b = (uint32_t)(x / NU), v = (uint32_t)(x % NU);
+            const uint32_t *bk = p.blk + b * MT_BLK;
+            b1b[x] = v < bk[1] ? b1[bk[0] + v] : 0.0f;
+            continue;
+        }
+        x -= nbias;
+        if (x < nbias) {
+            const uint32_t b = (uint32_t)(x / NU), u = (uint32_t)(x % NU);
+            const uint32_t *bk = p.blk + b * MT_BLK;
+            b2b[x] = u < bk[3] ? b2[bk[2] + u] : 0.0f;
+            continue;
+        }
+        x -= nbias;
+        b3c[x] = b3[x];
+    }
+}
+
+struct MtLayout {
+    size_t ops, blk, deg, img, W1b, W2b, W3b, b1b, b2b, b3, total;
+};
+
+static size_t mt_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static MtLayout mt_layout(uint32_t L, uint32_t q, uint32_t H, uint32_t nb, size_t nops, size_t img_bytes) {
+    MtLayout o;
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        const size_t here = at;
+        at = mt_align(at + bytes);
+        return here;
+    };
+    o.ops = take(nops * sizeof(MtOp));
+    o.blk = take((size_t)nb * MT_BLK * 4);
+    o.deg = take((size_t)(L + 1) * 4);
+    o.img = take(img_bytes);
+    o.W1b = take((size_t)nb * L * q * MT_NU * 4);
+    o.W2b = take((size_t)nb * MT_NU * MT_NU * 4);
+    o.W3b = take((size_t)nb * MT_GQMAX * MT_NU * 4);
+    o.b1b = take((size_t)nb * MT_NU * 4);
+    o.b2b = take((size_t)nb * MT_NU * 4);
+    o.b3 = take((size_t)L * q * 4);
+    o.total = at;
+    (void)H;
+    return o;
+}
+
+// The host-side plan: block table, op list and image size, or an error text.
+struct MtHostPlan {
+    uint32_t nb = 0, N3 = 0, d2col = 0;
+    std::vector<uint32_t> blk;
+    std::vector<MtOp> ops;
+    std::vector<int32_t> deg2;
+    size_t img_bytes = 0;
+    const char *err = nullptr;
+};
+
+static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const int32_t *m1, const int32_t *m2) {
+    MtHostPlan h;
+    if (L < 2 || (q != 4 && q != 8) || H == 0 || H > MT_HMAX || H % 16 || G == 0 || G % 4 || G * q > MT_GQMAX) {
+        h.err = "mi3_made_tc: needs q in {4, 8}, H <= 512 a multiple of 16, G a multiple of 4 with G q <= 64";
+        return h;
+    }
+    h.nb = (L + G - 1) / G;
+    h.N3 = (G * q + 15) / 16 * 16;
+    h.d2col = h.nb * h.N3;
+    if (h.d2col + MT_NU > MT_TMEM_COLS) {
+        h.err = "mi3_made_tc: logits of all blocks do not fit tensor memory (nb * roundup(G q, 16) + 48 > 512)";
+        return h;
+    }
+    std::vector<uint32_t> n1(h.nb, 0), n2(h.nb, 0);
+    for (uint32_t k = 0; k < H; ++k) {
+        if (m1[k] < 1 || m1[k] > (int32_t)L - 1 || m2[k] < 1 || m2[k] > (int32_t)L - 1 ||
+            (k > 0 && (m1[k] < m1[k - 1] || m2[k] < m2[k - 1]))) {
+            h.err = "mi3_made_tc: hidden degrees must be sorted and in [1, L-1]";
+            return h;
+        }
+        ++n1[(m1[k] - 1) / G];
+        ++n2[(m2[k] - 1) / G];
+    }
+    h.blk.assign((size_t)h.nb * MT_BLK, 0);
+    uint32_t c1 = 0, c2 = 0, off = 0;
+    for (uint32_t b = 0; b < h.nb; ++b) {
+        if (n1[b] % 16 || n2[b] % 16 || n1[b] > MT_NU || n2[b] > MT_NU) {
+            h.err = "mi3_made_tc: each degree block needs 0, 16, 32 or 48 units per layer";
+            return h;
+        }
+        uint32_t *bk = &h.blk[(size_t)b * MT_BLK];
+        bk[0] = c1;
+        bk[1] = n1[b];
+        bk[2] = c2;
+        bk[3] = n2[b];
+        bk[4] = (uint32_t)h.ops.size();
+        if (b >= 1 && n2[b] > 0 && c1 > 0) {
+            for (uint32_t kc = 0; kc * 64 < c1; ++kc) {
+                MtOp op{off, n2[b], kc, std::min<uint32_t>(64, c1 - 64 * kc) / 16, h.d2col, kc == 0 ? 1u : 0u, 0, b};
+                h.ops.push_back(op);
+                off += n2[b] * 128;
+            }
+        }
+        bk[5] = (uint32_t)h.ops.size();
+        if (b + 1 < h.nb && n2[b] > 0) {
+            const uint32_t R = (h.nb - 1 - b) * h.N3;
+            for (uint32_t r0 = 0; r0 < R; r0 += 128) {
+                const uint32_t rows = std::min<uint32_t>(128, R - r0);
+                MtOp op{off, rows, 0, n2[b] / 16, (b + 1) * h.N3 + r0, 0, 1, b};
+                h.ops.push_back(op);
+                off += rows * 128;
+            }
+        }
+        bk[6] = (uint32_t)h.ops.size();
+        bk[7] = bk[5] > bk[4] ? 1u : 0u;
+        c1 += n1[b];
+        c2 += n2[b];
+    }
+    h.img_bytes = off;
+    h.deg2.assign(L + 1, (int32_t)H);
+    for (uint32_t d = 0; d <= L; ++d) {
+        uint32_t k = 0;
+        while (k < H && m2[k] < (int32_t)d) ++k;
+        h.deg2[d] = (int32_t)k;
+    }
+    return h;
+}
+
+}  // namespace mi3
+
+using namespace mi3;
+
+extern "C" uint64_t mi3_made_tc_workspace(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const int32_t *m1,
+                                          const int32_t *m2) {
+    if (!m1 || !m2) return 0;
+    MtHostPlan h = mt_plan(L, q, H, G, m1, m2);
+    if (h.err) return 0;
+    return mt_layout(L, q, H, h.nb, h.ops.size(), h.img_bytes).total;
+}
+
+extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const int32_t *m1,
+                                   const int32_t *m2, const float *W1T, const float *b1, const float *W2,
+                                   const float *b2, const float *W3, const float *b3, void *workspace,
+                                   uint64_t ws_bytes, uint64_t *plan_out, void *stream) {
+    if (!m1 || !m2 || !W1T || !b1 || !W2 || !b2 || !W3 || !b3 || !workspace || !plan_out)
+        return fail(MI3_ERR_ARG, "mi3_made_tc_prepare: null pointer");
+    MtHostPlan h = mt_plan(L, q, H, G, m1, m2);
+    if (h.err) return fail(MI3_ERR_ARG, h.err);
+    const MtLayout lay = mt_layout(L, q, H, h.nb, h.ops.size(), h.img_bytes);
+    if (ws_bytes < lay.total) return fail(MI3_ERR_WORKSPACE, "mi3_made_tc_prepare: workspace too small");
+    if (!aligned(workspace, 256)) return fail(MI3_ERR_ALIGN, "mi3_made_tc_prepare: workspace alignment");
+    cudaStream_t st = as_stream(stream);
+    unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
+    if (cudaMemcpyAsync(ws + lay.ops, h.ops.data(), h.ops.size() * sizeof(MtOp), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(ws + lay.blk, h.blk.data(), h.blk.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(ws + lay.deg, h.deg2.data(), h.deg2.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return check_launch("mi3_made_tc_prepare: tables");
+    MtPlan p;
+    std::memset(&p, 0, sizeof(p));
+    p.L = L;
+    p.q = q;
+    p.H = H;
+    p.G = G;
+    p.nb = h.nb;
+    p.N3 = h.N3;
+    p.d2col = h.d2col;
+    p.nops = (uint32_t)h.ops.size();
+    p.img_bytes = h.img_bytes;
+    p.ops = reinterpret_cast<const MtOp *>(ws + lay.ops);
+    p.blk = reinterpret_cast<const uint32_t *>(ws + lay.blk);
+    p.deg2_start = reinterpret_cast<const int32_t *>(ws + lay.deg);
+    p.img = ws + lay.img;
+    p.W1b = reinterpret_cast<const float *>(ws + lay.W1b);
+    p.W2b = reinterpret_cast<const float *>(ws + lay.W2b);
+    p.W3b = reinterpret_cast<const float *>(ws + lay.W3b);
+    p.b1b = reinterpret_cast<const float *>(ws + lay.b1b);
+    p.b2b = reinterpret_cast<const float *>(ws + lay.b2b);
+    p.b3 = reinterpret_cast<const float *>(ws + lay.b3);
+    if (p.nops > 0) {
+        k_made_tc_images<<<p.nops, 256, 0, st>>>(p, ws + lay.img, W2, W3);
+        int rc = check_launch("mi3_made_tc_prepare: images");
+        if (rc) return rc;
+    }
+    k_made_tc_blocks<<<592, 256, 0, st>>>(p, reinterpret_cast<float *>(ws + lay.W1b),
+                                          reinterpret_cast<float *>(ws + lay.W2b),
+                                          reinterpret_cast<float *>(ws + lay.W3b),
+                                          reinterpret_cast<float *>(ws + lay.b1b),
+                                          reinterpret_cast<float *>(ws + lay.b2b),
+                                          reinterpret_cast<float *>(ws + lay.b3), W1T, b1, W2, b2, W3, b3);
+    int rc = check_launch("mi3_made_tc_prepare: blocks");
+    if (rc) return rc;
+    std::memset(plan_out, 0, 24 * 8);
+    std::memcpy(plan_out, &p, sizeof(p));
+    return MI3_OK;
+}
+
+extern "C" int mi3_made_tc_sample(const uint64_t *plan, uint32_t *seq, uint32_t buflen, uint32_t nseq, float *logq,
+                                  uint64_t seed, int32_t given, int32_t *status, void *stream) {
+    if (!plan || !seq || !logq || !status) return fail(MI3_ERR_ARG, "mi3_made_tc_sample: null pointer");
+    MtPlan p;
+    std::memcpy(&p, plan, sizeof(p));
+    if (!p.ops || !p.blk || p.nb == 0 || (p.q != 4 && p.q != 8))
+        return fail(MI3_ERR_ARG, "mi3_made_tc_sample: plan not prepared");
+    if (nseq > buflen) return fail(MI3_ERR_ARG, "mi3_made_tc_sample: nseq > buflen");
+    if (nseq == 0) return MI3_OK;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t ntiles = (nseq + MT_M - 1) / MT_M;
+    const uint32_t grid = std::min<uint32_t>(ntiles, (uint32_t)nsm);
+    cudaStream_t st = as_stream(stream);
+    if (p.q == 4) {
+        cudaFuncSetAttribute(k_made_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MT_SMEM);
+        k_made_tc<4><<<grid, MT_THREADS, MT_SMEM, st>>>(p, seq, buflen, nseq, logq, seed, given, status);
+    } else {
+        cudaFuncSetAttribute(k_made_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MT_SMEM);
+        k_made_tc<8><<<grid, MT_THREADS, MT_SMEM, st>>>(p, seq, buflen, nseq, logq, seed, given, status);
+    }
+    return check_launch("mi3_made_tc_sample");
+}

@@ -13,10 +13,13 @@ the sampler stays exact whatever the quality of q.  Proposal steps are
 interleaved with ordinary single-site sweeps; when the acceptance rate falls
 below a threshold the plain sampler carries on alone.
 
-All arithmetic runs in libmi3b200 (csrc/made.cu): the forward, backward and
-Adam kernels for training, a degree-ordered sampling kernel (one forward
-pass per sample), and the MH accept kernel.  PyTorch tensors hold the
-parameters as device memory only.
+All arithmetic runs in libmi3b200: the forward, backward and Adam kernels
+for training, the MH accept kernel and two samplers.  The tensor-core
+sampler (csrc/made_tc.cu) groups the hidden units in blocks of G sites
+("blocked" degrees) and runs the products between blocks as tcgen05 GEMMs,
+the rest on the CUDA cores; the SIMT sampler (csrc/made.cu) walks the sites
+with one forward pass per sample and takes any degrees.  PyTorch tensors
+hold the parameters as device memory only.
 """
 import math
 
@@ -36,12 +39,64 @@ def made_degrees(L, H, seed=0):
     return m1, m2
 
 
-def made_masks(L, q, H, seed=0):
+def blocked_degrees(L, H, G):
+    """Hidden degrees for the tensor-core sampler: block b of G sites owns
+    the units of degree in (bG, bG+G]; every block gets 0, 16, 32 or 48
+    units (about in proportion to its number of degrees), each cycling
+    through its degrees, and the units are sorted by degree.  Raises
+    ValueError when H cannot be split that way."""
+    if H % 16 or G < 1:
+        raise ValueError("blocked degrees need H a multiple of 16")
+    nb = -(-L // G)
+    degs = [list(range(b * G + 1, min(b * G + G, L - 1) + 1)) for b in range(nb)]
+    nd = np.array([len(d) for d in degs], dtype=np.float64)
+    groups = H // 16
+    share = groups * nd / nd.sum()
+    cnt = np.floor(share).astype(np.int64)
+    order = np.argsort(-(share - cnt), kind="stable")
+    cnt[order[:groups - int(cnt.sum())]] += 1
+    if cnt.max() > 3 or np.any((cnt > 0) & (nd == 0)):
+        raise ValueError(f"cannot place {H} units in blocks of {G} sites (at most 48 per block)")
+    m = []
+    for b in range(nb):
+        m += sorted(degs[b][r % len(degs[b])] for r in range(16 * int(cnt[b])))
+    return np.array(m, dtype=np.int64)
+
+
+TC_TMEM_COLS, TC_MAX_UNITS = 512, 48
+
+
+def tc_block_size(L, q, H):
+    """The largest block size G (a multiple of 4, G q <= 64) with which the
+    tensor-core sampler can run this network, or None: the logits of all
+    blocks (ceil(L/G) x roundup(G q, 16) columns) and one block's layer-2
+    accumulator must fit the 512 tensor-memory columns."""
+    if q not in (4, 8) or H % 16 or H > 512 or L < 2:
+        return None
+    for G in range(64 // q // 4 * 4, 0, -4):
+        nb = -(-L // G)
+        n3 = -(-G * q // 16) * 16
+        if nb * n3 + TC_MAX_UNITS > TC_TMEM_COLS:
+            continue
+        try:
+            blocked_degrees(L, H, G)
+        except ValueError:
+            continue
+        return G
+    return None
+
+
+def made_masks(L, q, H, seed=0, G=None):
     """MADE connectivity: input (site i) -> hidden-1 k iff m1[k] >= i+1;
     hidden-1 k -> hidden-2 k' iff m2[k'] >= m1[k]; hidden-2 k' -> output
-    site i iff i+1 > m2[k'].  Returned in the kernels' layouts:
+    site i iff i+1 > m2[k'].  Degrees cycled and shuffled, or blocked in
+    blocks of G sites when G is given.  Returned in the kernels' layouts:
     mW1T [Lq][H], mW2 [H][H] (row k'), mW3 [Lq][H]."""
-    m1, m2 = made_degrees(L, H, seed)
+    if G:
+        m1 = blocked_degrees(L, H, G)
+        m2 = m1.copy()
+    else:
+        m1, m2 = made_degrees(L, H, seed)
     din = np.repeat(np.arange(1, L + 1), q)          # degree of input / output (i, a)
     mW1T = (m1[None, :] >= din[:, None]).astype(np.float32)
     mW2 = (m2[:, None] >= m1[None, :]).astype(np.float32)
@@ -52,13 +107,25 @@ def made_masks(L, q, H, seed=0):
 class MadeProposal:
     PARAMS = ("W1T", "b1", "W2", "b2", "W3", "b3")
 
-    def __init__(self, L, q, H=512, device=0, seed=0, lr=1e-3):
+    def __init__(self, L, q, H=512, device=0, seed=0, lr=1e-3, sampler="auto", G=None):
+        """sampler: "tc" (tensor-core sampler, blocked degrees), "simt"
+        (cycled degrees, the SIMT sampler) or "auto" (tc where it runs);
+        G: the tensor-core sampler's block size (default: tc_block_size)."""
         self.L, self.q, self.H = L, q, H
         self.Lq = L * q
         self.device = torch.device("cuda", device) if isinstance(device, int) else device
         self.lr = lr
         self.step = 0
-        mW1T, mW2, mW3, m1, m2 = made_masks(L, q, H, seed)
+        G = G or tc_block_size(L, q, H)
+        if sampler == "auto":
+            sampler = "tc" if G else "simt"
+        if sampler == "tc" and not G:
+            raise ValueError(f"no tensor-core sampler plan for L={L}, q={q}, H={H}")
+        if sampler not in ("tc", "simt"):
+            raise ValueError(f"unknown sampler {sampler!r}")
+        self.sampler = sampler
+        self.G = G if sampler == "tc" else None
+        mW1T, mW2, mW3, m1, m2 = made_masks(L, q, H, seed, G=self.G)
         rng = np.random.default_rng(seed + 1)
         init = {
             "W1T": rng.normal(0, 1.0 / math.sqrt(L), size=(self.Lq, H)) * mW1T,
@@ -85,6 +152,10 @@ class MadeProposal:
         self.deg2_start = t(starts, torch.int32)
         self.m1, self.m2 = m1, m2
         self._ws = {}
+        self._tc_ws = None
+        self._tc_plan = np.zeros(24, dtype=np.uint64)
+        self._tc_dirty = True
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.round_params()
 
     # ----------------------------------------------------------- plumbing
@@ -97,6 +168,7 @@ class MadeProposal:
         for k, v in self.p.items():
             _lib.call("mi3_made_round_bf16", v.data_ptr(), self.pc[k].data_ptr(),
                       self.ph[k].data_ptr() if k in self.ph else None, v.numel(), self.stream)
+        self._tc_dirty = True
 
     def _buf(self, name, shape):
         b = self._ws.get(name)
@@ -138,6 +210,7 @@ class MadeProposal:
 
     def adam_step(self, beta1=0.9, beta2=0.999, eps=1e-8):
         self.step += 1
+        self._tc_dirty = True
         for k, v in self.p.items():
             _lib.call("mi3_made_adam", v.data_ptr(), self.pc[k].data_ptr(),
                       self.ph[k].data_ptr() if k in self.ph else None, self.g[k].data_ptr(), self.m[k].data_ptr(),
@@ -166,9 +239,40 @@ class MadeProposal:
         return hist
 
     # ----------------------------------------------------------- sampling
+    def _tc_prepare(self):
+        """Weight tiles and per-block arrays of the tensor-core sampler from
+        the current bf16-rounded parameters."""
+        m1 = np.ascontiguousarray(self.m1, dtype=np.int32)
+        m2 = np.ascontiguousarray(self.m2, dtype=np.int32)
+        L, q, H, G = self.L, self.q, self.H, self.G
+        nbytes = int(_lib.query("mi3_made_tc_workspace", L, q, H, G, m1.ctypes.data, m2.ctypes.data))
+        if nbytes == 0:
+            raise ValueError(f"no tensor-core sampler plan for L={L}, q={q}, H={H}, G={G}")
+        if self._tc_ws is None or self._tc_ws.numel() < nbytes:
+            self._tc_ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        pc = self.pc
+        _lib.call("mi3_made_tc_prepare", L, q, H, G, m1.ctypes.data, m2.ctypes.data, pc["W1T"].data_ptr(),
+                  pc["b1"].data_ptr(), pc["W2"].data_ptr(), pc["b2"].data_ptr(), pc["W3"].data_ptr(),
+                  pc["b3"].data_ptr(), self._tc_ws.data_ptr(), nbytes, self._tc_plan.ctypes.data, self.stream)
+        self._tc_dirty = False
+
+    def check_status(self):
+        """Raise if a sampler kernel gave up waiting (status word set)."""
+        st = int(self.status.item())
+        if st:
+            self.status.zero_()
+            raise RuntimeError(f"MADE tensor-core sampler: wait timed out (status {st})")
+
     def sample(self, seq_out, nseq, logq_out, seed, buflen=None, given=False):
         """Draw nseq sequences into a packed buffer (given=False), or compute
         log q of the sequences already there (given=True)."""
+        if self.sampler == "tc":
+            if self._tc_dirty:
+                self._tc_prepare()
+            _lib.call("mi3_made_tc_sample", self._tc_plan.ctypes.data, seq_out.data_ptr(), buflen or nseq, nseq,
+                      logq_out.data_ptr(), int(seed) & ((1 << 64) - 1), 1 if given else 0, self.status.data_ptr(),
+                      self.stream)
+            return
         ph, pc = self.ph, self.pc
         _lib.call("mi3_made_sample", self.L, self.q, self.H, ph["W1T"].data_ptr(), pc["b1"].data_ptr(),
                   ph["W2"].data_ptr(), pc["b2"].data_ptr(), ph["W3"].data_ptr(), pc["b3"].data_ptr(),
@@ -217,6 +321,7 @@ class LearnedSampler:
                       self.Ep.data_ptr(), self.lq.data_ptr(), self.lqp.data_ptr(),
                       self.seed * 7919 + self.rounds, self.nacc.data_ptr(), s)
             acc = int(self.nacc.item())
+        m.check_status()
         self.accepted += acc
         self.proposed += N
         rate = acc / N

@@ -1,5 +1,7 @@
 """Learned proposal (MADE) kernels against a PyTorch-CPU oracle of the same
-network (float64 autograd), and exactness of the independence MH step."""
+network (float64 autograd), and exactness of the independence MH step.  The
+sampler tests here run the SIMT sampler (FP32 activations); the tensor-core
+sampler has its own tests (test_gpu_made_tc.py)."""
 import itertools
 
 import numpy as np
@@ -28,7 +30,7 @@ def _cpu_made(made, seqs):
 
 
 def _made(L, q, H, seed=0, lr=1e-2):
-    m = MadeProposal(L, q, H=H, device=0, seed=seed, lr=lr)
+    m = MadeProposal(L, q, H=H, device=0, seed=seed, lr=lr, sampler="simt")
     rng = np.random.default_rng(seed + 7)
     for k in ("b1", "b2", "b3"):
         m.p[k].copy_(torch.as_tensor(rng.normal(0, 0.3, size=m.p[k].shape), dtype=torch.float32))
