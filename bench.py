@@ -895,6 +895,46 @@ def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, 
                       "tau_gain_per_second": res["plain"]["tau_int_s"] / res["learned"]["tau_int_s"]}))
 
 
+def run_made(args, H=512):
+    """The MADE proposal's two sampler kernels alone at --L/--q/--walkers
+    (default here L=99, q=4, 2^18: the learned-proposal workload): a
+    network with random weights and biases, 2 + --steps draws and
+    teacher-forced passes each, timed with CUDA events; the tensor-core
+    sampler also repeats its own log q (same arithmetic, compared)."""
+    import torch
+    from mi3gpu_b200.learned import MadeProposal
+    L, q, N = args.L, args.q, args.walkers
+    made = MadeProposal(L, q, H=H, device=0, seed=3)
+    rng = np.random.default_rng(7)
+    for k in ("b1", "b2", "b3"):
+        made.p[k].copy_(torch.as_tensor(rng.normal(0, 0.3, size=made.p[k].shape), dtype=torch.float32))
+    made.round_params()
+    sw = (L - 1) // 4 + 1
+    seq = torch.zeros(sw * N, dtype=torch.int32, device="cuda")
+    lq_s, lq_t = torch.zeros(N, device="cuda"), torch.zeros(N, device="cuda")
+    out = {"mode": "made", "config": {"L": L, "q": q, "walkers": N, "H": H, "G": made.G}}
+    kinds = ("tc", "simt") if made.sampler == "tc" else ("simt",)
+    for kind in kinds:
+        made.sampler = kind
+        times = {}
+        for given in (False, True):
+            lq = lq_t if given else lq_s
+            for _ in range(args.warmup):
+                made.sample(seq, N, lq, seed=11, given=given)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                made.sample(seq, N, lq, seed=11, given=given)
+            e1.record()
+            e1.synchronize()
+            times["logq_ms" if given else "sample_ms"] = e0.elapsed_time(e1) / args.steps
+        made.check_status()
+        times["logq_reproduced"] = bool(torch.equal(lq_s, lq_t))
+        out[kind] = times
+    made.sampler = kinds[0]
+    print(json.dumps(out))
+
+
 def headline_inference(args):
     """Seconds per quasi-Newton iteration of the plain native sampler under
     two round schedules, compact enough for the default run, on one
@@ -1064,7 +1104,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--newton-steps", type=int, default=10, help="quasi-Newton steps to time (0: skip)")
     ap.add_argument("--mode", default="sampler", choices=["sampler", "inference", "kernels", "learned", "batched", "graph_small",
-                                                           "msa", "streams", "hiv"],
+                                                           "msa", "streams", "hiv", "made"],
                     help="inference: run full quasi-Newton rounds and report s/iter and SSR")
     ap.add_argument("--rounds", type=int, default=4, help="inference rounds (--mode inference)")
     ap.add_argument("--msa", type=int, default=1 << 16, help="synthetic MSA size (--mode inference)")
@@ -1127,6 +1167,9 @@ def main():
         return
     if args.mode == "hiv":
         run_hiv(args)
+        return
+    if args.mode == "made":
+        run_made(args)
         return
     out, J = run_gpu(args)
     if rank == 0 and world == 1 and not args.no_inference:

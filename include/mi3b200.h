@@ -448,6 +448,34 @@ int mi3_made_backward(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_
                       float *gW2, float *gb2, float *gW3, float *gb3, const float *mW1T,
                       const float *mW2, const float *mW3, float *loss_per_seq, void *stream);
 
+/* The same forward and backward with their dense products as BF16
+ * tensor-core GEMMs (mi3_gemm_bf16: operands rounded to bf16, FP32
+ * accumulation); workspace of mi3_made_gemm_workspace(B, L, q, H) bytes,
+ * 1024-byte aligned; a timed-out wait sets *status. */
+uint64_t mi3_made_gemm_workspace(uint32_t B, uint32_t L, uint32_t q, uint32_t H);
+int mi3_made_forward_tc(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+                        uint32_t q, uint32_t H, const float *W1T, const float *b1, const float *W2,
+                        const float *b2, const float *W3, const float *b3, float *h1, float *a1, float *h2,
+                        float *a2, float *logits, float *logq, void *workspace, uint64_t ws_bytes,
+                        int32_t *status, void *stream);
+int mi3_made_backward_tc(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+                         uint32_t q, uint32_t H, const float *W2, const float *W3, const float *h1,
+                         const float *a1, const float *h2, const float *a2, const float *logits,
+                         float *dlogits, float *X, float *dh1, float *dh2, float *gW1T, float *gb1,
+                         float *gW2, float *gb2, float *gW3, float *gb3, const float *mW1T,
+                         const float *mW2, const float *mW3, float *loss_per_seq, void *workspace,
+                         uint64_t ws_bytes, int32_t *status, void *stream);
+
+/* C (M x N, row stride ldc, FP32) = alpha A B^T + beta C on the tcgen05
+ * tensor cores, A(m, k) = A[m sam + k sak], B^T(k, n) = B[k sbk + n sbn]
+ * given in FP32 and rounded to bf16, FP32 accumulation.  The operands are
+ * packed into workspace (mi3_gemm_bf16_workspace bytes, 1024-byte
+ * aligned) first; a timed-out wait sets *status. */
+uint64_t mi3_gemm_bf16_workspace(uint32_t M, uint32_t N, uint32_t K);
+int mi3_gemm_bf16(uint32_t M, uint32_t N, uint32_t K, const float *A, int64_t sam, int64_t sak,
+                  const float *B, int64_t sbk, int64_t sbn, float *C, int64_t ldc, float alpha, float beta,
+                  void *workspace, uint64_t ws_bytes, int32_t *status, void *stream);
+
 /* Adam step (bias-corrected, step >= 1) on n parameters p with gradient g
  * and moments m, v; refreshes the bf16-rounded float copy pc and the bf16
  * copy ph (nullable); entries with mask 0 (mask nullable) stay 0. */
@@ -471,8 +499,8 @@ int mi3_made_sample(uint32_t L, uint32_t q, uint32_t H, const void *W1T_bf16, co
 /* Tensor-core MADE sampler (tcgen05).  Hidden degrees m1, m2 (host arrays
  * of H int32, sorted, in [1, L-1]) grouped in blocks of G sites: block b
  * owns the units of degree in (bG, bG+G], 0, 16, 32 or 48 per layer;
- * q in {4, 8}, H <= 512 a multiple of 16, G a multiple of 4 with G q <= 64
- * and ceil(L/G) * roundup(G q, 16) + 48 <= 512.  The activations entering
+ * q in {4, 8}, H <= 512 a multiple of 16, G in {4, 8, 16} with G q <= 64
+ * and ceil(L/G) * roundup(G q, 16) + 48 + ceil(L/4) <= 512.  The activations entering
  * layers 2 and 3 are rounded to bf16.
  * mi3_made_tc_workspace: device bytes for the plan's tables and weight
  * tiles (0 if the degrees or sizes are not supported). */

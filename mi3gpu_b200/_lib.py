@@ -93,6 +93,12 @@ SIGNATURES = {
     "mi3_made_round_bf16": (c.c_int, [_vp, _vp, _vp, _u64, _vp]),
     "mi3_made_sample": (c.c_int, [_u32, _u32, _u32] + [_vp] * 8 + [_vp, _u32, _u32, _vp, _u64, c.c_int32, _vp]),
     "mi3_mh_independence": (c.c_int, [_vp, _vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp, _u64, _vp, _vp]),
+    "mi3_made_gemm_workspace": (_u64, [_u32, _u32, _u32, _u32]),
+    "mi3_made_forward_tc": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _u32, _u32] + [_vp] * 12 + [_vp, _u64, _vp, _vp]),
+    "mi3_made_backward_tc": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _u32, _u32] + [_vp] * 21 + [_vp, _u64, _vp, _vp]),
+    "mi3_gemm_bf16_workspace": (_u64, [_u32, _u32, _u32]),
+    "mi3_gemm_bf16": (c.c_int, [_u32, _u32, _u32, _vp, c.c_int64, c.c_int64, _vp, c.c_int64, c.c_int64, _vp,
+                                c.c_int64, _f32, _f32, _vp, _u64, _vp, _vp]),
     "mi3_made_tc_workspace": (_u64, [_u32, _u32, _u32, _u32, _vp, _vp]),
     "mi3_made_tc_prepare": (c.c_int, [_u32, _u32, _u32, _u32] + [_vp] * 8 + [_vp, _u64, _vp, _vp]),
     "mi3_made_tc_sample": (c.c_int, [_vp, _vp, _u32, _u32, _vp, _u64, c.c_int32, _vp, _vp]),

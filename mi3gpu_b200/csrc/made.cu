@@ -17,6 +17,8 @@
 // output site i depends on sites < i only.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "made.cuh"
 
 namespace mi3 {
@@ -72,8 +74,19 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const float *
     }
 }
 
-static int gemm(int M, int N, int K, const float *A, long sam, long sak, const float *B, long sbk, long sbn, float *C,
-                long ldc, float alpha, float beta, cudaStream_t st) {
+// Where the dense products run: the FP32 SIMT kernel above (ws null), or
+// the BF16 tensor-core GEMM (mi3_gemm_bf16) with its workspace.
+struct GemmPath {
+    void *ws = nullptr;
+    uint64_t ws_bytes = 0;
+    int32_t *status = nullptr;
+};
+
+static int gemm(const GemmPath &gp, int M, int N, int K, const float *A, long sam, long sak, const float *B, long sbk,
+                long sbn, float *C, long ldc, float alpha, float beta, cudaStream_t st) {
+    if (gp.ws)
+        return mi3_gemm_bf16(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, alpha, beta, gp.ws, gp.ws_bytes, gp.status,
+                             st);
     dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
     k_gemm<<<grid, 256, 0, st>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, alpha, beta);
     return check_launch("made gemm");
@@ -367,7 +380,7 @@ static inline unsigned nb(size_t n, unsigned t = 256) { return (unsigned)((n + t
 using namespace mi3;
 
 // --------------------------------------------------------------- C ABI
-extern "C" int mi3_made_forward(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+static int made_forward(const GemmPath &gp, const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
                                 uint32_t q, uint32_t H, const float *W1T, const float *b1, const float *W2,
                                 const float *b2, const float *W3, const float *b3, float *h1, float *a1, float *h2,
                                 float *a2, float *logits, float *logq, void *stream) {
@@ -381,18 +394,18 @@ extern "C" int mi3_made_forward(const uint32_t *seq, uint32_t buflen, uint32_t n
     k_made_h1<<<g1, 256, 0, st>>>(seq, buflen, n0, B, L, q, H, W1T, b1, h1);
     k_relu<<<nb((size_t)B * H), 256, 0, st>>>(h1, a1, (size_t)B * H);
     // h2 = a1 W2^T + b2
-    int rc = gemm(B, H, H, a1, H, 1, W2, 1, H, h2, H, 1.0f, 0.0f, st);
+    int rc = gemm(gp, B, H, H, a1, H, 1, W2, 1, H, h2, H, 1.0f, 0.0f, st);
     if (rc) return rc;
     k_add_bias<<<nb((size_t)B * H), 256, 0, st>>>(h2, b2, B, H);
     k_relu<<<nb((size_t)B * H), 256, 0, st>>>(h2, a2, (size_t)B * H);
-    rc = gemm(B, Lq, H, a2, H, 1, W3, 1, H, logits, Lq, 1.0f, 0.0f, st);
+    rc = gemm(gp, B, Lq, H, a2, H, 1, W3, 1, H, logits, Lq, 1.0f, 0.0f, st);
     if (rc) return rc;
     k_add_bias<<<nb((size_t)B * Lq), 256, 0, st>>>(logits, b3, B, Lq);
     if (logq) k_made_loss<<<nb(B, 128), 128, 0, st>>>(seq, buflen, n0, B, L, q, logits, logq, nullptr, 0.0f);
     return check_launch("mi3_made_forward");
 }
 
-extern "C" int mi3_made_backward(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+static int made_backward(const GemmPath &gp, const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
                                  uint32_t q, uint32_t H, const float *W2, const float *W3, const float *h1,
                                  const float *a1, const float *h2, const float *a2, const float *logits,
                                  float *dlogits, float *X, float *dh1, float *dh2, float *gW1T, float *gb1, float *gW2,
@@ -408,25 +421,75 @@ extern "C" int mi3_made_backward(const uint32_t *seq, uint32_t buflen, uint32_t 
     k_made_loss<<<nb(B, 128), 128, 0, st>>>(seq, buflen, n0, B, L, q, logits, loss_per_seq, dlogits, 1.0f / B);
     int rc;
     // gW3[o][k'] = sum_b dlogits[b][o] a2[b][k']
-    if ((rc = gemm(Lq, H, B, dlogits, 1, Lq, a2, H, 1, gW3, H, 1.0f, 0.0f, st))) return rc;
+    if ((rc = gemm(gp, Lq, H, B, dlogits, 1, Lq, a2, H, 1, gW3, H, 1.0f, 0.0f, st))) return rc;
     k_colsum<<<nb(Lq), 256, 0, st>>>(dlogits, B, Lq, gb3, 0.0f);
     // dh2 = dlogits W3 * relu'(h2)
-    if ((rc = gemm(B, H, Lq, dlogits, Lq, 1, W3, H, 1, dh2, H, 1.0f, 0.0f, st))) return rc;
+    if ((rc = gemm(gp, B, H, Lq, dlogits, Lq, 1, W3, H, 1, dh2, H, 1.0f, 0.0f, st))) return rc;
     k_relu_grad<<<nb((size_t)B * H), 256, 0, st>>>(h2, dh2, (size_t)B * H);
     // gW2[k'][k] = sum_b dh2[b][k'] a1[b][k]
-    if ((rc = gemm(H, H, B, dh2, 1, H, a1, H, 1, gW2, H, 1.0f, 0.0f, st))) return rc;
+    if ((rc = gemm(gp, H, H, B, dh2, 1, H, a1, H, 1, gW2, H, 1.0f, 0.0f, st))) return rc;
     k_colsum<<<nb(H), 256, 0, st>>>(dh2, B, H, gb2, 0.0f);
     // dh1 = dh2 W2 * relu'(h1)
-    if ((rc = gemm(B, H, H, dh2, H, 1, W2, H, 1, dh1, H, 1.0f, 0.0f, st))) return rc;
+    if ((rc = gemm(gp, B, H, H, dh2, H, 1, W2, H, 1, dh1, H, 1.0f, 0.0f, st))) return rc;
     k_relu_grad<<<nb((size_t)B * H), 256, 0, st>>>(h1, dh1, (size_t)B * H);
     // gW1T[(i,a)][k] = sum_b X[b][(i,a)] dh1[b][k]
     k_onehot<<<nb((size_t)B * Lq), 256, 0, st>>>(seq, buflen, n0, B, L, q, X);
-    if ((rc = gemm(Lq, H, B, X, 1, Lq, dh1, H, 1, gW1T, H, 1.0f, 0.0f, st))) return rc;
+    if ((rc = gemm(gp, Lq, H, B, X, 1, Lq, dh1, H, 1, gW1T, H, 1.0f, 0.0f, st))) return rc;
     k_colsum<<<nb(H), 256, 0, st>>>(dh1, B, H, gb1, 0.0f);
     k_mask_mul<<<nb((size_t)Lq * H), 256, 0, st>>>(gW1T, mW1T, (size_t)Lq * H);
     k_mask_mul<<<nb((size_t)H * H), 256, 0, st>>>(gW2, mW2, (size_t)H * H);
     k_mask_mul<<<nb((size_t)Lq * H), 256, 0, st>>>(gW3, mW3, (size_t)Lq * H);
     return check_launch("mi3_made_backward");
+}
+
+extern "C" int mi3_made_forward(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+                                uint32_t q, uint32_t H, const float *W1T, const float *b1, const float *W2,
+                                const float *b2, const float *W3, const float *b3, float *h1, float *a1, float *h2,
+                                float *a2, float *logits, float *logq, void *stream) {
+    return made_forward(GemmPath{}, seq, buflen, n0, B, L, q, H, W1T, b1, W2, b2, W3, b3, h1, a1, h2, a2, logits, logq,
+                        stream);
+}
+
+extern "C" int mi3_made_backward(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+                                 uint32_t q, uint32_t H, const float *W2, const float *W3, const float *h1,
+                                 const float *a1, const float *h2, const float *a2, const float *logits,
+                                 float *dlogits, float *X, float *dh1, float *dh2, float *gW1T, float *gb1, float *gW2,
+                                 float *gb2, float *gW3, float *gb3, const float *mW1T, const float *mW2,
+                                 const float *mW3, float *loss_per_seq, void *stream) {
+    return made_backward(GemmPath{}, seq, buflen, n0, B, L, q, H, W2, W3, h1, a1, h2, a2, logits, dlogits, X, dh1,
+                         dh2, gW1T, gb1, gW2, gb2, gW3, gb3, mW1T, mW2, mW3, loss_per_seq, stream);
+}
+
+extern "C" uint64_t mi3_made_gemm_workspace(uint32_t B, uint32_t L, uint32_t q, uint32_t H) {
+    const uint32_t Lq = L * q;
+    uint64_t w = 0;
+    const uint32_t shapes[7][3] = {{B, H, H}, {B, Lq, H}, {Lq, H, B}, {B, H, Lq}, {H, H, B}, {B, H, H}, {Lq, H, B}};
+    for (const auto &sh : shapes) w = std::max<uint64_t>(w, mi3_gemm_bf16_workspace(sh[0], sh[1], sh[2]));
+    return w;
+}
+
+extern "C" int mi3_made_forward_tc(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+                                   uint32_t q, uint32_t H, const float *W1T, const float *b1, const float *W2,
+                                   const float *b2, const float *W3, const float *b3, float *h1, float *a1, float *h2,
+                                   float *a2, float *logits, float *logq, void *workspace, uint64_t ws_bytes,
+                                   int32_t *status, void *stream) {
+    if (!workspace || !status) return fail(MI3_ERR_ARG, "mi3_made_forward_tc: null workspace or status");
+    GemmPath gp{workspace, ws_bytes, status};
+    return made_forward(gp, seq, buflen, n0, B, L, q, H, W1T, b1, W2, b2, W3, b3, h1, a1, h2, a2, logits, logq,
+                        stream);
+}
+
+extern "C" int mi3_made_backward_tc(const uint32_t *seq, uint32_t buflen, uint32_t n0, uint32_t B, uint32_t L,
+                                    uint32_t q, uint32_t H, const float *W2, const float *W3, const float *h1,
+                                    const float *a1, const float *h2, const float *a2, const float *logits,
+                                    float *dlogits, float *X, float *dh1, float *dh2, float *gW1T, float *gb1,
+                                    float *gW2, float *gb2, float *gW3, float *gb3, const float *mW1T,
+                                    const float *mW2, const float *mW3, float *loss_per_seq, void *workspace,
+                                    uint64_t ws_bytes, int32_t *status, void *stream) {
+    if (!workspace || !status) return fail(MI3_ERR_ARG, "mi3_made_backward_tc: null workspace or status");
+    GemmPath gp{workspace, ws_bytes, status};
+    return made_backward(gp, seq, buflen, n0, B, L, q, H, W2, W3, h1, a1, h2, a2, logits, dlogits, X, dh1, dh2, gW1T,
+                         gb1, gW2, gb2, gW3, gb3, mW1T, mW2, mW3, loss_per_seq, stream);
 }
 
 extern "C" int mi3_made_adam(float *p, float *pc, void *ph_bf16, const float *g, float *m, float *v, const float *mask,

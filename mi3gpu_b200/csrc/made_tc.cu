@@ -8,10 +8,10 @@
 // activations entering layers 2 and 3 are rounded to bf16, as the tensor
 // cores read them; weights are bf16 values, sums are FP32.
 //
-// Degree blocks.  The hidden degrees are grouped in blocks of G sites:
-// block b owns the units of degree in (bG, bG + G], unit indices sorted by
-// degree, 16, 32 or 48 units per block and layer.  Walking the sites in
-// order, when block b starts (sites < s0 = bG drawn):
+// Degree blocks.  The hidden degrees are grouped in blocks of G sites
+// (G = 4, 8 or 16): block b owns the units of degree in (bG, bG + G], unit
+// indices sorted by degree, 16, 32 or 48 units per block and layer.
+// Walking the sites in order, when block b starts (sites < s0 = bG drawn):
 //   * every hidden-1 unit of an earlier block is final, so the hidden-2
 //     units of block b get their share from them as one GEMM,
 //       D2 = A1[:, 0:c1] . W2[U2_b, 0:c1]^T      (tcgen05, D2 in TMEM)
@@ -24,16 +24,20 @@
 // inputs from earlier sites gathered once, then one weight row per drawn
 // site), its hidden-2 units (one dot product over the block's hidden-1
 // units each, as they become final) and the in-block share of each site's
-// logits -- runs on the CUDA cores, one walker per thread.  Masked weights
-// are zero, so each in-block loop runs over all of the block's units.
+// logits -- runs on the CUDA cores, one walker per thread, from weights
+// staged in shared memory.  Masked weights are zero, so each in-block loop
+// runs over all of the block's units.
 //
-// CTA: 128 walkers (TMEM lanes); warps 0-3 compute, warp 4 issues the MMAs,
-// warp 5 streams the weight tiles (pre-swizzled K-major images, one 1-D bulk
-// copy each) through a 3-stage ring.  All waits are bounded (status word).
-// The kernel draws walker n's residue i from the same counter-based uniform
-// as made.cu (seed, n, i); with given = 1 it reads the residues instead and
-// returns log q: the same arithmetic, so log q of a drawn sequence is
-// reproduced bit for bit.
+// CTA: 128 walkers (TMEM lanes).  Warps 0-3 run the walkers; warp 4 issues
+// the MMAs; warp 5 streams their weight tiles (pre-swizzled K-major images,
+// one 1-D bulk copy each) through a 3-stage ring; warp 6 streams the
+// CUDA-core weights (the block's layer-1 rows in chunks of 16 sites, then
+// its layer-2/3 slice, bf16) through a 4-stage ring.  Each walker's
+// sequence words are kept in spare TMEM columns for the layer-1 gathers.
+// All waits are bounded (status word).  The kernel draws walker n's
+// residue i from the same counter-based uniform as made.cu (seed, n, i);
+// with given = 1 it reads the residues instead and returns log q: the same
+// arithmetic, so log q of a drawn sequence is reproduced bit for bit.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -49,16 +53,25 @@ constexpr uint32_t MT_M = 128;        // walkers per tile
 constexpr uint32_t MT_NU = 48;        // largest unit count per block and layer
 constexpr uint32_t MT_HMAX = 512;     // hidden units (A1 holds 8 K-chunks of 64)
 constexpr uint32_t MT_GQMAX = 64;     // sites x residues per block
-constexpr uint32_t MT_STAGES = 3;
-constexpr uint32_t MT_STAGE_BYTES = 128 * 128;  // up to 128 rows x 64 K bf16
+constexpr uint32_t MT_CS = 16;        // sites per layer-1 chunk
+constexpr uint32_t MT_STAGES = 3;     // MMA weight-tile ring
+constexpr uint32_t MT_STAGE_ROWS = 64;
+constexpr uint32_t MT_STAGE_BYTES = MT_STAGE_ROWS * 128;
+constexpr uint32_t MT_WSTAGES = 4;    // CUDA-core weight ring
+constexpr uint32_t MT_WSTAGE_BYTES = 12288;
+constexpr uint32_t MT_ROW_BYTES = MT_NU * 2;  // one bf16 weight row over a block's units
+constexpr uint32_t MT_W2_BYTES = MT_NU * MT_ROW_BYTES;
+constexpr uint32_t MT_W23_BYTES = MT_W2_BYTES + MT_GQMAX * MT_ROW_BYTES;
 constexpr uint32_t MT_A1_BYTES = (MT_HMAX / 64) * MT_M * 128;
 constexpr uint32_t MT_A2_BYTES = MT_M * 128;
-constexpr uint32_t MT_D2S_BYTES = MT_NU * MT_M * 4;
-constexpr uint32_t MT_THREADS = 192;
+constexpr uint32_t MT_THREADS = 224;
 constexpr uint32_t MT_TMEM_COLS = 512;
-constexpr uint32_t MT_SMEM = 1024 + MT_A1_BYTES + MT_A2_BYTES + MT_STAGES * MT_STAGE_BYTES + MT_D2S_BYTES + 256;
+constexpr uint32_t MT_SMEM = 1024 + MT_A1_BYTES + MT_A2_BYTES + MT_STAGES * MT_STAGE_BYTES +
+                             MT_WSTAGES * MT_WSTAGE_BYTES + 256;
+static_assert(MT_SMEM <= 232448, "shared memory");
+static_assert(MT_W23_BYTES <= MT_WSTAGE_BYTES && MT_CS * 8 * MT_ROW_BYTES <= MT_WSTAGE_BYTES, "weight stage");
 
-// One weight tile of the ring and the MMAs that consume it.
+// One weight tile of the MMA ring and the MMAs that consume it.
 struct MtOp {
     uint32_t off;     // byte offset of the tile image
     uint32_t rows;    // N of the MMA (tile rows, 128 B each)
@@ -70,23 +83,32 @@ struct MtOp {
     uint32_t blk;
 };
 
+// One stage of the CUDA-core weight ring: a layer-1 chunk (rows (j, a) of
+// 16 sites x the block's hidden-1 units) or the block's layer-2/3 slice.
+struct MtWOp {
+    uint32_t off, bytes, kind, blk, chunk, pad0, pad1, pad2;
+};
+
+__host__ __device__ __forceinline__ uint32_t op_bytes(const MtOp &o) { return o.rows * 128; }
+__host__ __device__ __forceinline__ uint32_t op_bytes(const MtWOp &o) { return o.bytes; }
+
 // per block: c1 (hidden-1 units before the block), n1, c2, n2, first op of
-// the layer-2 tiles, first op of the logits tiles, end, D2 valid
-constexpr uint32_t MT_BLK = 8;
+// the layer-2 tiles, first op of the logits tiles, end, D2 valid, first
+// weight-ring op, layer-1 chunks
+constexpr uint32_t MT_BLK = 12;
 
 struct MtPlan {
-    uint32_t L, q, H, G, nb, N3, d2col, nops;
-    uint64_t img_bytes;
+    uint32_t L, q, H, G, nb, N3, d2col, wcol, nops, nwops;
+    uint64_t img_bytes, wimg_bytes;
     const MtOp *ops;
+    const MtWOp *wops;
     const uint32_t *blk;
     const int32_t *deg2_start;  // [L + 1]: first hidden-2 unit of degree >= d
-    const unsigned char *img;
-    const float *W1b;  // [nb][L q][NU]   W1T[(j, a)][c1 + v]
-    const float *W2b;  // [nb][NU][NU]    W2[c2 + u][c1 + v]
-    const float *W3b;  // [nb][GQMAX][NU] W3[(s0 q + c)][c2 + u]
-    const float *b1b;  // [nb][NU]
-    const float *b2b;  // [nb][NU]
-    const float *b3;   // [L q]
+    const unsigned char *img;   // MMA weight tiles
+    const unsigned char *wimg;  // CUDA-core weight stages
+    const float *b1b;           // [nb][NU]
+    const float *b2b;           // [nb][NU]
+    const float *b3;            // [L q]
 };
 static_assert(sizeof(MtPlan) <= 24 * 8, "plan blob");
 
@@ -103,7 +125,7 @@ __device__ __forceinline__ void mt_mma(uint32_t tmem_d, uint64_t adesc, uint64_t
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
-// byte offset of (row, k) in a 128-row K-major 128B-swizzled tile of 64 K
+// byte offset of (row, k) in a K-major 128B-swizzled tile of 64 K
 __device__ __forceinline__ uint32_t mt_sw(uint32_t row, uint32_t k) {
     return row * 128 + ((((k >> 3) ^ (row & 7)) & 7) << 4) + ((k & 7) << 1);
 }
@@ -113,6 +135,53 @@ __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__floa
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
     return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
            ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+}
+
+// 8 bf16 (one 16-byte word) -> floats
+__device__ __forceinline__ void unpack8(const uint4 w, float *f) {
+    f[0] = __uint_as_float(w.x << 16);
+    f[1] = __uint_as_float(w.x & 0xffff0000u);
+    f[2] = __uint_as_float(w.y << 16);
+    f[3] = __uint_as_float(w.y & 0xffff0000u);
+    f[4] = __uint_as_float(w.z << 16);
+    f[5] = __uint_as_float(w.z & 0xffff0000u);
+    f[6] = __uint_as_float(w.w << 16);
+    f[7] = __uint_as_float(w.w & 0xffff0000u);
+}
+
+// sum_u row[u] x[u] over the 48 units of a bf16 row in shared memory, in unit order
+__device__ __forceinline__ float dot48(const unsigned char *row, const float *x) {
+    float s = 0.0f;
+#pragma unroll
+    for (uint32_t g = 0; g < MT_NU / 8; ++g) {
+        float w[8];
+        unpack8(*reinterpret_cast<const uint4 *>(row + 16 * g), w);
+#pragma unroll
+        for (uint32_t e = 0; e < 8; ++e) s = __fmaf_rn(w[e], x[8 * g + e], s);
+    }
+    return s;
+}
+
+__device__ __forceinline__ void add48(const unsigned char *row, float *h) {
+#pragma unroll
+    for (uint32_t g = 0; g < MT_NU / 8; ++g) {
+        float w[8];
+        unpack8(*reinterpret_cast<const uint4 *>(row + 16 * g), w);
+#pragma unroll
+        for (uint32_t e = 0; e < 8; ++e) h[8 * g + e] += w[e];
+    }
+}
+
+__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    return r;
+}
+
+__device__ __forceinline__ void tmem_st1(uint32_t taddr, uint32_t v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(v) : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float (&v)[4]) {
@@ -157,6 +226,36 @@ __device__ __forceinline__ void tmem_ldq<8>(uint32_t taddr, float (&v)[8]) {
     tmem_ld8(taddr, v);
 }
 
+// One producer thread: stream a list of records into a ring, once per tile
+// this CTA owns; on exit wait for the copies still in flight.
+template <typename Op, uint32_t NS, uint32_t SB>
+__device__ __forceinline__ void mt_produce(const Op *ops, uint32_t nops, const unsigned char *src, unsigned char *ring,
+                                           uint64_t *full, uint64_t *empty, uint32_t ntiles,
+                                           volatile int *abort_flag, int32_t *status) {
+    uint32_t it = 0;
+    bool ok = true;
+    for (uint32_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        for (uint32_t o = 0; o < nops; ++o) {
+            const uint32_t s = it % NS, round = it / NS;
+            if (round > 0 && !mbar_wait_bounded(&empty[s], (round - 1) & 1, abort_flag, WAIT_LIMIT_NS)) {
+                report(status, ST_TIMEOUT_EMPTY);
+                *abort_flag = 1;
+                ok = false;
+                break;
+            }
+            const Op op = ops[o];
+            const uint32_t bytes = op_bytes(op);
+            mbar_arrive_expect_tx(&full[s], bytes);
+            bulk_g2s(ring + s * SB, src + op.off, bytes, &full[s]);
+            ++it;
+        }
+    }
+    for (uint32_t k = 0; k < NS && k < it; ++k) {
+        const uint32_t j = it - 1 - k;
+        mbar_wait_bounded(&full[j % NS], (j / NS) & 1, nullptr, WAIT_LIMIT_NS);
+    }
+}
+
 template <uint32_t Q>
 __global__ void __launch_bounds__(MT_THREADS, 1)
     k_made_tc(const MtPlan p, uint32_t *seq, uint32_t buflen, uint32_t nseq, float *logq, uint64_t seed,
@@ -167,21 +266,26 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
     unsigned char *A1 = sm;
     unsigned char *A2 = A1 + MT_A1_BYTES;
     unsigned char *ring = A2 + MT_A2_BYTES;
-    float *d2s = reinterpret_cast<float *>(ring + MT_STAGES * MT_STAGE_BYTES);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(d2s + MT_NU * MT_M);
+    unsigned char *wring = ring + MT_STAGES * MT_STAGE_BYTES;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(wring + MT_WSTAGES * MT_WSTAGE_BYTES);
     uint64_t *full = bars, *empty = bars + MT_STAGES;
-    uint64_t *bar_a1 = bars + 2 * MT_STAGES, *bar_a2 = bar_a1 + 1, *bar_mma = bar_a1 + 2, *bar_fin = bar_a1 + 3;
+    uint64_t *wfull = bars + 2 * MT_STAGES, *wempty = wfull + MT_WSTAGES;
+    uint64_t *bar_a1 = wempty + MT_WSTAGES, *bar_a2 = bar_a1 + 1, *bar_mma = bar_a1 + 2, *bar_fin = bar_a1 + 3;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_a1 + 4);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t L = p.L, q = p.q, G = p.G, nb = p.nb, Lq = L * q;
+    const uint32_t L = p.L, G = p.G, nb = p.nb;
     const uint32_t ntiles = (nseq + MT_M - 1) / MT_M;
 
     if (tid == 0) {
         for (uint32_t s = 0; s < MT_STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
+        }
+        for (uint32_t s = 0; s < MT_WSTAGES; ++s) {
+            mbar_init(&wfull[s], 1);
+            mbar_init(&wempty[s], MT_M);
         }
         mbar_init(bar_a1, MT_M);
         mbar_init(bar_a2, MT_M);
@@ -201,32 +305,15 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 5) {
-        // ---------------------------------------------------- producer
-        if ((tid & 31) == 0) {
-            uint32_t it = 0;
-            bool ok = true;
-            for (uint32_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                for (uint32_t o = 0; o < p.nops; ++o) {
-                    const uint32_t s = it % MT_STAGES, round = it / MT_STAGES;
-                    if (round > 0 && !mbar_wait_bounded(&empty[s], (round - 1) & 1, abort_flag, WAIT_LIMIT_NS)) {
-                        report(status, ST_TIMEOUT_EMPTY);
-                        *abort_flag = 1;
-                        ok = false;
-                        break;
-                    }
-                    const MtOp op = p.ops[o];
-                    const uint32_t bytes = op.rows * 128;
-                    mbar_arrive_expect_tx(&full[s], bytes);
-                    bulk_g2s(ring + s * MT_STAGE_BYTES, p.img + op.off, bytes, &full[s]);
-                    ++it;
-                }
-            }
-            // the copies still in flight land before the CTA exits
-            for (uint32_t k = 0; k < MT_STAGES && k < it; ++k) {
-                const uint32_t j = it - 1 - k;
-                mbar_wait_bounded(&full[j % MT_STAGES], (j / MT_STAGES) & 1, nullptr, WAIT_LIMIT_NS);
-            }
-        }
+        // ------------------------------------------ MMA weight-tile producer
+        if ((tid & 31) == 0)
+            mt_produce<MtOp, MT_STAGES, MT_STAGE_BYTES>(p.ops, p.nops, p.img, ring, full, empty, ntiles, abort_flag,
+                                                        status);
+    } else if (warp == 6) {
+        // ------------------------------------------ CUDA-core weight producer
+        if ((tid & 31) == 0)
+            mt_produce<MtWOp, MT_WSTAGES, MT_WSTAGE_BYTES>(p.wops, p.nwops, p.wimg, wring, wfull, wempty, ntiles,
+                                                           abort_flag, status);
     } else if (warp == 4) {
         // ---------------------------------------------------- MMA issue
         if ((tid & 31) == 0) {
@@ -290,16 +377,26 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
         // ---------------------------------------------------- walkers
         const uint32_t m = tid;
         const uint32_t lane_base = (32 * warp) << 16;
-        uint32_t nmma = 0;
+        uint32_t nmma = 0, wit = 0;
         bool ok = true;
+        // a warp-wide bounded wait: the lanes decide together (tcgen05.ld/st
+        // need all 32 of them)
+        auto wait_all = [&](uint64_t *bar, uint32_t parity) {
+            const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity, abort_flag, WAIT_LIMIT_NS));
+            if (!got) {
+                report(status, ST_TIMEOUT_FULL);
+                *abort_flag = 1;
+            }
+            return got;
+        };
         for (uint32_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
             const uint32_t n = t * MT_M + m;
             const bool valid = n < nseq;
             float lq = 0.0f;
             uint32_t cw = 0;  // residues of the current sequence word
-            for (uint32_t b = 0; b < nb; ++b) {
+            for (uint32_t b = 0; b < nb && ok; ++b) {
                 const uint32_t *bk = p.blk + b * MT_BLK;
-                const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], d2ok = bk[7];
+                const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], d2ok = bk[7], nch = bk[9];
                 const uint32_t s0 = b * G, s1 = min(L, s0 + G);
                 if (b == 0) {
                     // the logits accumulator of this tile starts at zero
@@ -309,59 +406,54 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                 tc_fence_before();
                 mbar_arrive(bar_a1);
 
-                // hidden-1 units of the block: bias + inputs from sites < s0
+                // the block's hidden-1 units: bias + inputs from sites < s0,
+                // weight rows streamed 16 sites at a time
                 float h1[MT_NU];
-                {
-                    const float *bb1 = p.b1b + b * MT_NU;
 #pragma unroll
-                    for (uint32_t v = 0; v < MT_NU; ++v) h1[v] = __ldg(&bb1[v]);
-                    const float *w1 = p.W1b + (size_t)b * Lq * MT_NU;
-                    uint32_t word = 0;
-                    for (uint32_t j = 0; j < s0; ++j) {
-                        if ((j & 3) == 0) word = valid ? seq[(size_t)(j >> 2) * buflen + n] : 0u;
-                        const uint32_t x = min((word >> (8 * (j & 3))) & 0xffu, q - 1);
-                        const float4 *row = reinterpret_cast<const float4 *>(w1 + (size_t)(j * q + x) * MT_NU);
-#pragma unroll
-                        for (uint32_t g = 0; g < MT_NU / 4; ++g) {
-                            const float4 w = __ldg(&row[g]);
-                            h1[4 * g] += w.x;
-                            h1[4 * g + 1] += w.y;
-                            h1[4 * g + 2] += w.z;
-                            h1[4 * g + 3] += w.w;
-                        }
-                    }
-                }
-                // hidden-2 pre-activations of the block from earlier blocks (the
-                // warp decides together: tcgen05.ld needs all 32 lanes)
-                {
-                    const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(bar_mma, nmma++ & 1, abort_flag,
-                                                                                 WAIT_LIMIT_NS));
-                    if (!got) {
-                        report(status, ST_TIMEOUT_FULL);
-                        *abort_flag = 1;
+                for (uint32_t v = 0; v < MT_NU; ++v) h1[v] = __ldg(&p.b1b[b * MT_NU + v]);
+                uint32_t s_last = 0;
+                for (uint32_t c = 0; c < nch; ++c) {
+                    const uint32_t s = wit % MT_WSTAGES;
+                    if (!wait_all(&wfull[s], (wit / MT_WSTAGES) & 1)) {
                         ok = false;
                         break;
                     }
-                    tc_fence_after();
-                }
-                {
-                    const float *bb2 = p.b2b + b * MT_NU;
-#pragma unroll
-                    for (uint32_t c = 0; c < MT_NU; c += 16) {
-                        uint32_t r[16];
-                        if (d2ok) tmem_ld16(tmem + lane_base + p.d2col + c, r);
-#pragma unroll
-                        for (uint32_t k = 0; k < 16; ++k)
-                            d2s[(c + k) * MT_M + m] = (d2ok ? __uint_as_float(r[k]) : 0.0f) + __ldg(&bb2[c + k]);
+                    ++wit;
+                    const unsigned char *chunk = wring + s * MT_WSTAGE_BYTES;
+                    const uint32_t jend = min(s0, MT_CS * (c + 1));
+                    uint32_t word = 0;
+                    for (uint32_t j = MT_CS * c; j < jend; ++j) {
+                        if ((j & 3) == 0) word = tmem_ld1(tmem + lane_base + p.wcol + (j >> 2));
+                        const uint32_t x = min((word >> (8 * (j & 3))) & 0xffu, Q - 1);
+                        add48(chunk + ((j - MT_CS * c) * Q + x) * MT_ROW_BYTES, h1);
                     }
+                    if (c + 1 < nch)
+                        mbar_arrive(&wempty[s]);
+                    else
+                        s_last = s;  // holds the rows of this block's own sites
                 }
+                if (!ok) break;
+                const uint32_t s23 = wit % MT_WSTAGES;
+                if (!wait_all(&wfull[s23], (wit / MT_WSTAGES) & 1)) {
+                    ok = false;
+                    break;
+                }
+                ++wit;
+                const unsigned char *w1c = wring + s_last * MT_WSTAGE_BYTES;
+                const uint32_t jc0 = MT_CS * (nch - 1);
+                const unsigned char *w2s = wring + s23 * MT_WSTAGE_BYTES;
+                const unsigned char *w3s = w2s + MT_W2_BYTES;
+
+                // layer-2 prefix of the block (and the logits accumulator)
+                if (!wait_all(bar_mma, nmma++ & 1)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
 #pragma unroll
                 for (uint32_t g = 0; g < 8; ++g)
                     *reinterpret_cast<uint4 *>(A2 + m * 128 + (g << 4)) = make_uint4(0, 0, 0, 0);
 
-                const float *w3 = p.W3b + (size_t)b * MT_GQMAX * MT_NU;
-                const float *w2 = p.W2b + (size_t)b * MT_NU * MT_NU;
-                const float *w1 = p.W1b + (size_t)b * Lq * MT_NU;
                 uint32_t gword = 0;
                 for (uint32_t i = s0; i < s1; ++i) {
                     const uint32_t il = i - s0;
@@ -376,29 +468,12 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                     {
                         float act2[MT_NU];
 #pragma unroll
-                        for (uint32_t g = 0; g < MT_NU / 8; ++g) {
-                            const uint4 w = *reinterpret_cast<const uint4 *>(A2 + m * 128 + (((g ^ (m & 7)) & 7) << 4));
-                            const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
+                        for (uint32_t g = 0; g < MT_NU / 8; ++g)
+                            unpack8(*reinterpret_cast<const uint4 *>(A2 + m * 128 + (((g ^ (m & 7)) & 7) << 4)),
+                                    &act2[8 * g]);
 #pragma unroll
-                            for (uint32_t h = 0; h < 4; ++h) {
-                                act2[8 * g + 2 * h] = __uint_as_float(ww[h] << 16);
-                                act2[8 * g + 2 * h + 1] = __uint_as_float(ww[h] & 0xffff0000u);
-                            }
-                        }
-#pragma unroll
-                        for (uint32_t a = 0; a < Q; ++a) {
-                            const float4 *row = reinterpret_cast<const float4 *>(w3 + (il * Q + a) * MT_NU);
-                            float s = 0.0f;
-#pragma unroll
-                            for (uint32_t g = 0; g < MT_NU / 4; ++g) {
-                                const float4 w = __ldg(&row[g]);
-                                s = __fmaf_rn(w.x, act2[4 * g], s);
-                                s = __fmaf_rn(w.y, act2[4 * g + 1], s);
-                                s = __fmaf_rn(w.z, act2[4 * g + 2], s);
-                                s = __fmaf_rn(w.w, act2[4 * g + 3], s);
-                            }
-                            lg[a] += __ldg(&p.b3[i * Q + a]) + s;
-                        }
+                        for (uint32_t a = 0; a < Q; ++a)
+                            lg[a] += __ldg(&p.b3[i * Q + a]) + dot48(w3s + (il * Q + a) * MT_ROW_BYTES, act2);
                     }
                     // draw (or read) residue i
                     float mx = lg[0];
@@ -413,7 +488,10 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                     const float lse = mx + logf(se);
                     uint32_t r;
                     if (given) {
-                        if ((i & 3) == 0) gword = valid ? seq[(size_t)(i >> 2) * buflen + n] : 0u;
+                        if ((i & 3) == 0) {
+                            gword = valid ? seq[(size_t)(i >> 2) * buflen + n] : 0u;
+                            tmem_st1(tmem + lane_base + p.wcol + (i >> 2), gword);
+                        }
                         r = min((gword >> (8 * (i & 3))) & 0xffu, Q - 1);
                     } else {
                         const float u = hash_uniform(seed, n, i) * se;
@@ -437,21 +515,12 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                         cw |= r << (8 * (i & 3));
                         if ((i & 3) == 3 || i == L - 1) {
                             if (valid) seq[(size_t)(i >> 2) * buflen + n] = cw;
+                            tmem_st1(tmem + lane_base + p.wcol + (i >> 2), cw);
                             cw = 0;
                         }
                     }
                     // its input to the block's hidden-1 units
-                    {
-                        const float4 *row = reinterpret_cast<const float4 *>(w1 + (size_t)(i * Q + r) * MT_NU);
-#pragma unroll
-                        for (uint32_t g = 0; g < MT_NU / 4; ++g) {
-                            const float4 w = __ldg(&row[g]);
-                            h1[4 * g] += w.x;
-                            h1[4 * g + 1] += w.y;
-                            h1[4 * g + 2] += w.z;
-                            h1[4 * g + 3] += w.w;
-                        }
-                    }
+                    add48(w1c + ((i - jc0) * Q + r) * MT_ROW_BYTES, h1);
                     // hidden-2 units of degree i + 1
                     if (i + 1 < L) {
                         const int32_t ulo = __ldg(&p.deg2_start[i + 1]) - (int32_t)c2;
@@ -461,23 +530,18 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
 #pragma unroll
                             for (uint32_t v = 0; v < MT_NU; ++v) act1[v] = bf16r(fmaxf(h1[v], 0.0f));
                             for (int32_t u = ulo; u < uhi; ++u) {
-                                const float4 *row = reinterpret_cast<const float4 *>(w2 + u * MT_NU);
-                                float s = 0.0f;
-#pragma unroll
-                                for (uint32_t g = 0; g < MT_NU / 4; ++g) {
-                                    const float4 w = __ldg(&row[g]);
-                                    s = __fmaf_rn(w.x, act1[4 * g], s);
-                                    s = __fmaf_rn(w.y, act1[4 * g + 1], s);
-                                    s = __fmaf_rn(w.z, act1[4 * g + 2], s);
-                                    s = __fmaf_rn(w.w, act1[4 * g + 3], s);
-                                }
-                                const float z = d2s[u * MT_M + m] + s;
+                                const float d2 =
+                                    d2ok ? __uint_as_float(tmem_ld1(tmem + lane_base + p.d2col + (uint32_t)u)) : 0.0f;
+                                const float z =
+                                    (d2 + __ldg(&p.b2b[b * MT_NU + u])) + dot48(w2s + u * MT_ROW_BYTES, act1);
                                 *reinterpret_cast<unsigned short *>(A2 + mt_sw(m, (uint32_t)u)) =
                                     __bfloat16_as_ushort(__float2bfloat16_rn(fmaxf(z, 0.0f)));
                             }
                         }
                     }
                 }
+                mbar_arrive(&wempty[s_last]);
+                mbar_arrive(&wempty[s23]);
                 // the block's hidden-1 units are final: into A1 for later blocks
 #pragma unroll
                 for (uint32_t g = 0; g < MT_NU / 8; ++g) {
@@ -506,7 +570,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
     }
 }
 
-// Weight images and per-block arrays from the (bf16-valued) float weights.
+// MMA weight tiles from the (bf16-valued) float weights.
 __global__ void k_made_tc_images(const MtPlan p, unsigned char *img, const float *__restrict__ W2,
                                  const float *__restrict__ W3) {
     const MtOp op = p.ops[blockIdx.x];
@@ -530,66 +594,56 @@ __global__ void k_made_tc_images(const MtPlan p, unsigned char *img, const float
     }
 }
 
-__global__ void k_made_tc_blocks(const MtPlan p, float *W1b, float *W2b, float *W3b, float *b1b, float *b2b,
-                                 float *b3c, const float *__restrict__ W1T, const float *__restrict__ b1,
-                                 const float *__restrict__ W2, const float *__restrict__ b2,
-                                 const float *__restrict__ W3, const float *__restrict__ b3) {
-    const uint32_t H = p.H, q = p.q, G = p.G, L = p.L, Lq = L * q, NU = MT_NU;
-    const size_t n1tot = (size_t)p.nb * Lq * NU, n2tot = (size_t)p.nb * NU * NU, n3tot = (size_t)p.nb * MT_GQMAX * NU;
-    const size_t nbias = (size_t)p.nb * NU;
-    const size_t total = n1tot + n2tot + n3tot + 2 * nbias + Lq;
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        size_t x = e;
-        if (x < n1tot) {
-            const uint32_t b = (uint32_t)(x / ((size_t)Lq * NU)), rem = (uint32_t)(x % ((size_t)Lq * NU));
-            const uint32_t row = rem / NU, v = rem % NU;
-            const uint32_t *bk = p.blk + b * MT_BLK;
-            W1b[x] = v < bk[1] ? W1T[(size_t)row * H + bk[0] + v] : 0.0f;
-            continue;
+// CUDA-core weight stages (bf16): layer-1 chunks [16 q rows][48 units] and
+// the layer-2/3 slice [48][48] + [64][48] of each block.
+__global__ void k_made_tc_wimages(const MtPlan p, unsigned char *wimg, const float *__restrict__ W1T,
+                                  const float *__restrict__ W2, const float *__restrict__ W3) {
+    const MtWOp op = p.wops[blockIdx.x];
+    const uint32_t *bk = p.blk + op.blk * MT_BLK;
+    const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], n2 = bk[3];
+    const uint32_t H = p.H, q = p.q, G = p.G, L = p.L;
+    unsigned short *out = reinterpret_cast<unsigned short *>(wimg + op.off);
+    for (uint32_t e = threadIdx.x; e < op.bytes / 2; e += blockDim.x) {
+        const uint32_t r = e / MT_NU, x = e % MT_NU;
+        float v = 0.0f;
+        if (op.kind == 0) {
+            const uint32_t j = MT_CS * op.chunk + r / q, a = r % q;
+            if (j < L && x < n1) v = W1T[(size_t)(j * q + a) * H + c1 + x];
+        } else if (r < MT_NU) {
+            if (r < n2 && x < n1) v = W2[(size_t)(c2 + r) * H + c1 + x];
+        } else {
+            const uint32_t c = r - MT_NU, i = op.blk * G + c / q;
+            if (c < G * q && i < L && x < n2) v = W3[(size_t)(op.blk * G * q + c) * H + c2 + x];
         }
-        x -= n1tot;
-        if (x < n2tot) {
-            const uint32_t b = (uint32_t)(x / (NU * NU)), rem = (uint32_t)(x % (NU * NU));
-            const uint32_t u = rem / NU, v = rem % NU;
+        out[e] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+    }
+}
+
+__global__ void k_made_tc_bias(const MtPlan p, float *b1b, float *b2b, float *b3c, const float *__restrict__ b1,
+                               const float *__restrict__ b2, const float *__restrict__ b3) {
+    const uint32_t nbias = p.nb * MT_NU, Lq = p.L * p.q;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * nbias + Lq; e += gridDim.x * blockDim.x) {
+        if (e < 2 * nbias) {
+            const uint32_t x = e % nbias, b = x / MT_NU, v = x % MT_NU;
             const uint32_t *bk = p.blk + b * MT_BLK;
-            W2b[x] = (u < bk[3] && v < bk[1]) ? W2[(size_t)(bk[2] + u) * H + bk[0] + v] : 0.0f;
-            continue;
+            if (e < nbias)
+                b1b[x] = v < bk[1] ? b1[bk[0] + v] : 0.0f;
+            else
+                b2b[x] = v < bk[3] ? b2[bk[2] + v] : 0.0f;
+        } else {
+            b3c[e - 2 * nbias] = b3[e - 2 * nbias];
         }
-        x -= n2tot;
-        if (x < n3tot) {
-            const uint32_t b = (uint32_t)(x / (MT_GQMAX * NU)), rem = (uint32_t)(x % (MT_GQMAX * NU));
-            const uint32_t c = rem / NU, u = rem % NU;
-            const uint32_t *bk = p.blk + b * MT_BLK;
-            const uint32_t i = b * G + c / q;
-            W3b[x] = (c < G * q && i < L && u < bk[3]) ? W3[(size_t)(b * G * q + c) * H + bk[2] + u] : 0.0f;
-            continue;
-        }
-        x -= n3tot;
-        if (x < nbias) {
-            const uint32_t b = (uint32_t)(x / NU), v = (uint32_t)(x % NU);
-            const uint32_t *bk = p.blk + b * MT_BLK;
-            b1b[x] = v < bk[1] ? b1[bk[0] + v] : 0.0f;
-            continue;
-        }
-        x -= nbias;
-        if (x < nbias) {
-            const uint32_t b = (uint32_t)(x / NU), u = (uint32_t)(x % NU);
-            const uint32_t *bk = p.blk + b * MT_BLK;
-            b2b[x] = u < bk[3] ? b2[bk[2] + u] : 0.0f;
-            continue;
-        }
-        x -= nbias;
-        b3c[x] = b3[x];
     }
 }
 
 struct MtLayout {
-    size_t ops, blk, deg, img, W1b, W2b, W3b, b1b, b2b, b3, total;
+    size_t ops, wops, blk, deg, img, wimg, b1b, b2b, b3, total;
 };
 
 static size_t mt_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static MtLayout mt_layout(uint32_t L, uint32_t q, uint32_t H, uint32_t nb, size_t nops, size_t img_bytes) {
+static MtLayout mt_layout(uint32_t L, uint32_t q, uint32_t nb, size_t nops, size_t nwops, size_t img_bytes,
+                          size_t wimg_bytes) {
     MtLayout o;
     size_t at = 0;
     auto take = [&](size_t bytes) {
@@ -598,41 +652,42 @@ static MtLayout mt_layout(uint32_t L, uint32_t q, uint32_t H, uint32_t nb, size_
         return here;
     };
     o.ops = take(nops * sizeof(MtOp));
+    o.wops = take(nwops * sizeof(MtWOp));
     o.blk = take((size_t)nb * MT_BLK * 4);
     o.deg = take((size_t)(L + 1) * 4);
     o.img = take(img_bytes);
-    o.W1b = take((size_t)nb * L * q * MT_NU * 4);
-    o.W2b = take((size_t)nb * MT_NU * MT_NU * 4);
-    o.W3b = take((size_t)nb * MT_GQMAX * MT_NU * 4);
+    o.wimg = take(wimg_bytes);
     o.b1b = take((size_t)nb * MT_NU * 4);
     o.b2b = take((size_t)nb * MT_NU * 4);
     o.b3 = take((size_t)L * q * 4);
     o.total = at;
-    (void)H;
     return o;
 }
 
-// The host-side plan: block table, op list and image size, or an error text.
+// The host-side plan: block table, op lists and image sizes, or an error text.
 struct MtHostPlan {
-    uint32_t nb = 0, N3 = 0, d2col = 0;
+    uint32_t nb = 0, N3 = 0, d2col = 0, wcol = 0;
     std::vector<uint32_t> blk;
     std::vector<MtOp> ops;
+    std::vector<MtWOp> wops;
     std::vector<int32_t> deg2;
-    size_t img_bytes = 0;
+    size_t img_bytes = 0, wimg_bytes = 0;
     const char *err = nullptr;
 };
 
 static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const int32_t *m1, const int32_t *m2) {
     MtHostPlan h;
-    if (L < 2 || (q != 4 && q != 8) || H == 0 || H > MT_HMAX || H % 16 || G == 0 || G % 4 || G * q > MT_GQMAX) {
-        h.err = "mi3_made_tc: needs q in {4, 8}, H <= 512 a multiple of 16, G a multiple of 4 with G q <= 64";
+    if (L < 2 || (q != 4 && q != 8) || H == 0 || H > MT_HMAX || H % 16 || (G != 4 && G != 8 && G != 16) ||
+        G * q > MT_GQMAX) {
+        h.err = "mi3_made_tc: needs q in {4, 8}, H <= 512 a multiple of 16, G in {4, 8, 16} with G q <= 64";
         return h;
     }
     h.nb = (L + G - 1) / G;
     h.N3 = (G * q + 15) / 16 * 16;
     h.d2col = h.nb * h.N3;
-    if (h.d2col + MT_NU > MT_TMEM_COLS) {
-        h.err = "mi3_made_tc: logits of all blocks do not fit tensor memory (nb * roundup(G q, 16) + 48 > 512)";
+    h.wcol = h.d2col + MT_NU;
+    if (h.wcol + (L + 3) / 4 > MT_TMEM_COLS) {
+        h.err = "mi3_made_tc: tensor memory too small (nb * roundup(G q, 16) + 48 + ceil(L/4) > 512)";
         return h;
     }
     std::vector<uint32_t> n1(h.nb, 0), n2(h.nb, 0);
@@ -646,7 +701,7 @@ static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const 
         ++n2[(m2[k] - 1) / G];
     }
     h.blk.assign((size_t)h.nb * MT_BLK, 0);
-    uint32_t c1 = 0, c2 = 0, off = 0;
+    uint32_t c1 = 0, c2 = 0, off = 0, woff = 0;
     for (uint32_t b = 0; b < h.nb; ++b) {
         if (n1[b] % 16 || n2[b] % 16 || n1[b] > MT_NU || n2[b] > MT_NU) {
             h.err = "mi3_made_tc: each degree block needs 0, 16, 32 or 48 units per layer";
@@ -668,8 +723,8 @@ static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const 
         bk[5] = (uint32_t)h.ops.size();
         if (b + 1 < h.nb && n2[b] > 0) {
             const uint32_t R = (h.nb - 1 - b) * h.N3;
-            for (uint32_t r0 = 0; r0 < R; r0 += 128) {
-                const uint32_t rows = std::min<uint32_t>(128, R - r0);
+            for (uint32_t r0 = 0; r0 < R; r0 += MT_STAGE_ROWS) {
+                const uint32_t rows = std::min<uint32_t>(MT_STAGE_ROWS, R - r0);
                 MtOp op{off, rows, 0, n2[b] / 16, (b + 1) * h.N3 + r0, 0, 1, b};
                 h.ops.push_back(op);
                 off += rows * 128;
@@ -677,10 +732,26 @@ static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const 
         }
         bk[6] = (uint32_t)h.ops.size();
         bk[7] = bk[5] > bk[4] ? 1u : 0u;
+        // the CUDA-core weights: layer-1 chunks of the sites < min(L, s0 + G)
+        // (the block's own sites fall in the last one, as G divides 16), then
+        // the layer-2/3 slice
+        const uint32_t s1 = std::min(L, b * G + G);
+        const uint32_t nch = (s1 + MT_CS - 1) / MT_CS;
+        bk[8] = (uint32_t)h.wops.size();
+        bk[9] = nch;
+        for (uint32_t c = 0; c < nch; ++c) {
+            MtWOp w{woff, MT_CS * q * MT_ROW_BYTES, 0, b, c, 0, 0, 0};
+            h.wops.push_back(w);
+            woff += w.bytes;
+        }
+        MtWOp w{woff, MT_W23_BYTES, 1, b, 0, 0, 0, 0};
+        h.wops.push_back(w);
+        woff += w.bytes;
         c1 += n1[b];
         c2 += n2[b];
     }
     h.img_bytes = off;
+    h.wimg_bytes = woff;
     h.deg2.assign(L + 1, (int32_t)H);
     for (uint32_t d = 0; d <= L; ++d) {
         uint32_t k = 0;
@@ -699,7 +770,7 @@ extern "C" uint64_t mi3_made_tc_workspace(uint32_t L, uint32_t q, uint32_t H, ui
     if (!m1 || !m2) return 0;
     MtHostPlan h = mt_plan(L, q, H, G, m1, m2);
     if (h.err) return 0;
-    return mt_layout(L, q, H, h.nb, h.ops.size(), h.img_bytes).total;
+    return mt_layout(L, q, h.nb, h.ops.size(), h.wops.size(), h.img_bytes, h.wimg_bytes).total;
 }
 
 extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const int32_t *m1,
@@ -710,12 +781,15 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
         return fail(MI3_ERR_ARG, "mi3_made_tc_prepare: null pointer");
     MtHostPlan h = mt_plan(L, q, H, G, m1, m2);
     if (h.err) return fail(MI3_ERR_ARG, h.err);
-    const MtLayout lay = mt_layout(L, q, H, h.nb, h.ops.size(), h.img_bytes);
+    const MtLayout lay = mt_layout(L, q, h.nb, h.ops.size(), h.wops.size(), h.img_bytes, h.wimg_bytes);
     if (ws_bytes < lay.total) return fail(MI3_ERR_WORKSPACE, "mi3_made_tc_prepare: workspace too small");
     if (!aligned(workspace, 256)) return fail(MI3_ERR_ALIGN, "mi3_made_tc_prepare: workspace alignment");
     cudaStream_t st = as_stream(stream);
     unsigned char *ws = reinterpret_cast<unsigned char *>(workspace);
-    if (cudaMemcpyAsync(ws + lay.ops, h.ops.data(), h.ops.size() * sizeof(MtOp), cudaMemcpyHostToDevice, st) !=
+    if ((!h.ops.empty() &&
+         cudaMemcpyAsync(ws + lay.ops, h.ops.data(), h.ops.size() * sizeof(MtOp), cudaMemcpyHostToDevice, st) !=
+             cudaSuccess) ||
+        cudaMemcpyAsync(ws + lay.wops, h.wops.data(), h.wops.size() * sizeof(MtWOp), cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
         cudaMemcpyAsync(ws + lay.blk, h.blk.data(), h.blk.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(ws + lay.deg, h.deg2.data(), h.deg2.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
@@ -729,31 +803,31 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
     p.nb = h.nb;
     p.N3 = h.N3;
     p.d2col = h.d2col;
+    p.wcol = h.wcol;
     p.nops = (uint32_t)h.ops.size();
+    p.nwops = (uint32_t)h.wops.size();
     p.img_bytes = h.img_bytes;
+    p.wimg_bytes = h.wimg_bytes;
     p.ops = reinterpret_cast<const MtOp *>(ws + lay.ops);
+    p.wops = reinterpret_cast<const MtWOp *>(ws + lay.wops);
     p.blk = reinterpret_cast<const uint32_t *>(ws + lay.blk);
     p.deg2_start = reinterpret_cast<const int32_t *>(ws + lay.deg);
     p.img = ws + lay.img;
-    p.W1b = reinterpret_cast<const float *>(ws + lay.W1b);
-    p.W2b = reinterpret_cast<const float *>(ws + lay.W2b);
-    p.W3b = reinterpret_cast<const float *>(ws + lay.W3b);
+    p.wimg = ws + lay.wimg;
     p.b1b = reinterpret_cast<const float *>(ws + lay.b1b);
     p.b2b = reinterpret_cast<const float *>(ws + lay.b2b);
     p.b3 = reinterpret_cast<const float *>(ws + lay.b3);
+    int rc;
     if (p.nops > 0) {
         k_made_tc_images<<<p.nops, 256, 0, st>>>(p, ws + lay.img, W2, W3);
-        int rc = check_launch("mi3_made_tc_prepare: images");
-        if (rc) return rc;
+        if ((rc = check_launch("mi3_made_tc_prepare: images"))) return rc;
     }
-    k_made_tc_blocks<<<592, 256, 0, st>>>(p, reinterpret_cast<float *>(ws + lay.W1b),
-                                          reinterpret_cast<float *>(ws + lay.W2b),
-                                          reinterpret_cast<float *>(ws + lay.W3b),
-                                          reinterpret_cast<float *>(ws + lay.b1b),
-                                          reinterpret_cast<float *>(ws + lay.b2b),
-                                          reinterpret_cast<float *>(ws + lay.b3), W1T, b1, W2, b2, W3, b3);
-    int rc = check_launch("mi3_made_tc_prepare: blocks");
-    if (rc) return rc;
+    k_made_tc_wimages<<<p.nwops, 256, 0, st>>>(p, ws + lay.wimg, W1T, W2, W3);
+    if ((rc = check_launch("mi3_made_tc_prepare: weight stages"))) return rc;
+    k_made_tc_bias<<<32, 256, 0, st>>>(p, reinterpret_cast<float *>(ws + lay.b1b),
+                                       reinterpret_cast<float *>(ws + lay.b2b), reinterpret_cast<float *>(ws + lay.b3),
+                                       b1, b2, b3);
+    if ((rc = check_launch("mi3_made_tc_prepare: biases"))) return rc;
     std::memset(plan_out, 0, 24 * 8);
     std::memcpy(plan_out, &p, sizeof(p));
     return MI3_OK;
@@ -764,7 +838,7 @@ extern "C" int mi3_made_tc_sample(const uint64_t *plan, uint32_t *seq, uint32_t 
     if (!plan || !seq || !logq || !status) return fail(MI3_ERR_ARG, "mi3_made_tc_sample: null pointer");
     MtPlan p;
     std::memcpy(&p, plan, sizeof(p));
-    if (!p.ops || !p.blk || p.nb == 0 || (p.q != 4 && p.q != 8))
+    if (!p.wops || !p.blk || p.nb == 0 || (p.q != 4 && p.q != 8))
         return fail(MI3_ERR_ARG, "mi3_made_tc_sample: plan not prepared");
     if (nseq > buflen) return fail(MI3_ERR_ARG, "mi3_made_tc_sample: nseq > buflen");
     if (nseq == 0) return MI3_OK;

@@ -67,16 +67,19 @@ TC_TMEM_COLS, TC_MAX_UNITS = 512, 48
 
 
 def tc_block_size(L, q, H):
-    """The largest block size G (a multiple of 4, G q <= 64) with which the
+    """The largest block size G (4, 8 or 16, G q <= 64) with which the
     tensor-core sampler can run this network, or None: the logits of all
-    blocks (ceil(L/G) x roundup(G q, 16) columns) and one block's layer-2
-    accumulator must fit the 512 tensor-memory columns."""
+    blocks (ceil(L/G) x roundup(G q, 16) columns), one block's layer-2
+    accumulator and the walkers' sequence words (ceil(L/4) columns) must
+    fit the 512 tensor-memory columns."""
     if q not in (4, 8) or H % 16 or H > 512 or L < 2:
         return None
-    for G in range(64 // q // 4 * 4, 0, -4):
+    for G in (16, 8, 4):
+        if G * q > 64:
+            continue
         nb = -(-L // G)
         n3 = -(-G * q // 16) * 16
-        if nb * n3 + TC_MAX_UNITS > TC_TMEM_COLS:
+        if nb * n3 + TC_MAX_UNITS + -(-L // 4) > TC_TMEM_COLS:
             continue
         try:
             blocked_degrees(L, H, G)
@@ -107,10 +110,15 @@ def made_masks(L, q, H, seed=0, G=None):
 class MadeProposal:
     PARAMS = ("W1T", "b1", "W2", "b2", "W3", "b3")
 
-    def __init__(self, L, q, H=512, device=0, seed=0, lr=1e-3, sampler="auto", G=None):
+    def __init__(self, L, q, H=512, device=0, seed=0, lr=1e-3, sampler="auto", G=None, gemm="tc"):
         """sampler: "tc" (tensor-core sampler, blocked degrees), "simt"
         (cycled degrees, the SIMT sampler) or "auto" (tc where it runs);
-        G: the tensor-core sampler's block size (default: tc_block_size)."""
+        G: the tensor-core sampler's block size (default: tc_block_size);
+        gemm: the training pass's dense products as BF16 tensor-core GEMMs
+        ("tc") or FP32 SIMT loops ("simt")."""
+        if gemm not in ("tc", "simt"):
+            raise ValueError(f"unknown gemm {gemm!r}")
+        self.gemm = gemm
         self.L, self.q, self.H = L, q, H
         self.Lq = L * q
         self.device = torch.device("cuda", device) if isinstance(device, int) else device
@@ -186,11 +194,24 @@ class MadeProposal:
         a["logits"] = self._buf("logits", (B, Lq))
         a["logq"] = self._buf("logq", (B,))
         pc = self.pc
-        _lib.call("mi3_made_forward", seq.data_ptr(), buflen, n0, B, self.L, self.q, H, pc["W1T"].data_ptr(),
-                  pc["b1"].data_ptr(), pc["W2"].data_ptr(), pc["b2"].data_ptr(), pc["W3"].data_ptr(),
-                  pc["b3"].data_ptr(), a["h1"].data_ptr(), a["a1"].data_ptr(), a["h2"].data_ptr(),
-                  a["a2"].data_ptr(), a["logits"].data_ptr(), a["logq"].data_ptr(), self.stream)
+        args = (seq.data_ptr(), buflen, n0, B, self.L, self.q, H, pc["W1T"].data_ptr(), pc["b1"].data_ptr(),
+                pc["W2"].data_ptr(), pc["b2"].data_ptr(), pc["W3"].data_ptr(), pc["b3"].data_ptr(),
+                a["h1"].data_ptr(), a["a1"].data_ptr(), a["h2"].data_ptr(), a["a2"].data_ptr(),
+                a["logits"].data_ptr(), a["logq"].data_ptr())
+        if self.gemm == "tc":
+            ws, nbytes = self._gemm_ws(B)
+            _lib.call("mi3_made_forward_tc", *args, ws.data_ptr(), nbytes, self.status.data_ptr(), self.stream)
+        else:
+            _lib.call("mi3_made_forward", *args, self.stream)
         return a
+
+    def _gemm_ws(self, B):
+        nbytes = int(_lib.query("mi3_made_gemm_workspace", B, self.L, self.q, self.H))
+        ws = self._ws.get("gemm")
+        if ws is None or ws.numel() < nbytes + 1024:
+            ws = self._ws["gemm"] = torch.empty(nbytes + 1024, dtype=torch.uint8, device=self.device)
+        off = (-ws.data_ptr()) % 1024
+        return ws[off:], nbytes
 
     def backward(self, seq, buflen, n0, B, act):
         """Gradients of the batch-mean NLL into self.g; returns log q per sequence."""
@@ -200,12 +221,16 @@ class MadeProposal:
         dh1, dh2 = self._buf("dh1", (B, H)), self._buf("dh2", (B, H))
         lq = self._buf("lq_bwd", (B,))
         g, pc, m = self.g, self.pc, self.mask
-        _lib.call("mi3_made_backward", seq.data_ptr(), buflen, n0, B, self.L, self.q, H, pc["W2"].data_ptr(),
-                  pc["W3"].data_ptr(), act["h1"].data_ptr(), act["a1"].data_ptr(), act["h2"].data_ptr(),
-                  act["a2"].data_ptr(), act["logits"].data_ptr(), dlog.data_ptr(), X.data_ptr(), dh1.data_ptr(),
-                  dh2.data_ptr(), g["W1T"].data_ptr(), g["b1"].data_ptr(), g["W2"].data_ptr(), g["b2"].data_ptr(),
-                  g["W3"].data_ptr(), g["b3"].data_ptr(), m["W1T"].data_ptr(), m["W2"].data_ptr(),
-                  m["W3"].data_ptr(), lq.data_ptr(), self.stream)
+        args = (seq.data_ptr(), buflen, n0, B, self.L, self.q, H, pc["W2"].data_ptr(), pc["W3"].data_ptr(),
+                act["h1"].data_ptr(), act["a1"].data_ptr(), act["h2"].data_ptr(), act["a2"].data_ptr(),
+                act["logits"].data_ptr(), dlog.data_ptr(), X.data_ptr(), dh1.data_ptr(), dh2.data_ptr(),
+                g["W1T"].data_ptr(), g["b1"].data_ptr(), g["W2"].data_ptr(), g["b2"].data_ptr(), g["W3"].data_ptr(),
+                g["b3"].data_ptr(), m["W1T"].data_ptr(), m["W2"].data_ptr(), m["W3"].data_ptr(), lq.data_ptr())
+        if self.gemm == "tc":
+            ws, nbytes = self._gemm_ws(B)
+            _lib.call("mi3_made_backward_tc", *args, ws.data_ptr(), nbytes, self.status.data_ptr(), self.stream)
+        else:
+            _lib.call("mi3_made_backward", *args, self.stream)
         return lq
 
     def adam_step(self, beta1=0.9, beta2=0.999, eps=1e-8):
@@ -233,6 +258,7 @@ class MadeProposal:
                 tot += lq.double().sum()
                 nb += 1
             nll = -float(tot.item()) / max(1, nb * batch)
+            self.check_status()
             hist.append(nll)
             if log:
                 log(f"MADE epoch {ep}: mean NLL {nll:.4f} nats ({nll / self.L:.4f} per site)")
@@ -257,11 +283,11 @@ class MadeProposal:
         self._tc_dirty = False
 
     def check_status(self):
-        """Raise if a sampler kernel gave up waiting (status word set)."""
+        """Raise if a tensor-core kernel (sampler or GEMM) gave up waiting."""
         st = int(self.status.item())
         if st:
             self.status.zero_()
-            raise RuntimeError(f"MADE tensor-core sampler: wait timed out (status {st})")
+            raise RuntimeError(f"MADE tensor-core kernel: wait timed out (status {st})")
 
     def sample(self, seq_out, nseq, logq_out, seed, buflen=None, given=False):
         """Draw nseq sequences into a packed buffer (given=False), or compute

@@ -30,7 +30,7 @@ def _cpu_made(made, seqs):
 
 
 def _made(L, q, H, seed=0, lr=1e-2):
-    m = MadeProposal(L, q, H=H, device=0, seed=seed, lr=lr, sampler="simt")
+    m = MadeProposal(L, q, H=H, device=0, seed=seed, lr=lr, sampler="simt", gemm="simt")
     rng = np.random.default_rng(seed + 7)
     for k in ("b1", "b2", "b3"):
         m.p[k].copy_(torch.as_tensor(rng.normal(0, 0.3, size=m.p[k].shape), dtype=torch.float32))

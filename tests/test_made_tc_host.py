@@ -11,14 +11,14 @@ from mi3gpu_b200.learned import blocked_degrees, made_masks, tc_block_size
                                    (5, 4, 32), (8, 4, 64)])
 def test_blocked_degrees(L, q, H):
     G = tc_block_size(L, q, H)
-    assert G and G % 4 == 0 and G * q <= 64
+    assert G in (4, 8, 16) and G * q <= 64
     m = blocked_degrees(L, H, G)
     assert len(m) == H and m.min() >= 1 and m.max() <= L - 1
     assert np.all(np.diff(m) >= 0)
     nb = -(-L // G)
     cnt = np.bincount((m - 1) // G, minlength=nb)
     assert np.all(cnt % 16 == 0) and cnt.max() <= 48
-    assert nb * (-(-G * q // 16) * 16) + 48 <= 512
+    assert nb * (-(-G * q // 16) * 16) + 48 + -(-L // 4) <= 512
     m32 = np.ascontiguousarray(m, dtype=np.int32)
     assert _lib.query("mi3_made_tc_workspace", L, q, H, G, m32.ctypes.data, m32.ctypes.data) > 0
 
