@@ -796,7 +796,7 @@ def energy_autocorr(Es):
     return rho, tau
 
 
-def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, epochs=16, every=4):
+def run_learned(args, L=99, q=4, N=1 << 18, equil_sweeps=1024, track=64, epochs=16, every=4):
     """Learned independence proposal at L=99, q=4 with strong contacts
     (sigma 0.8): train the MADE on 2^18 equilibrated walkers, then track
     the energy autocorrelation over `track` sampler calls of one sweep each,
@@ -806,6 +806,7 @@ def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, 
     from mi3gpu_b200.potts import synthetic_ground_truth
     from mi3gpu_b200.learned import MadeProposal, LearnedSampler
     from mi3gpu_b200._lib import call as _lib_call, query as _lib_query
+    H = args.hidden
     J = synthetic_ground_truth(L, q, seed=1003, contact_sigma=0.8)
     g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, args.seed + 1)
     gpus = GPU_node([g])
@@ -895,7 +896,7 @@ def run_learned(args, L=99, q=4, N=1 << 18, H=512, equil_sweeps=1024, track=64, 
                       "tau_gain_per_second": res["plain"]["tau_int_s"] / res["learned"]["tau_int_s"]}))
 
 
-def run_made(args, H=512):
+def run_made(args):
     """The MADE proposal's two sampler kernels alone at --L/--q/--walkers
     (default here L=99, q=4, 2^18: the learned-proposal workload): a
     network with random weights and biases, 2 + --steps draws and
@@ -903,7 +904,7 @@ def run_made(args, H=512):
     sampler also repeats its own log q (same arithmetic, compared)."""
     import torch
     from mi3gpu_b200.learned import MadeProposal
-    L, q, N = args.L, args.q, args.walkers
+    L, q, N, H = args.L, args.q, args.walkers, args.hidden
     made = MadeProposal(L, q, H=H, device=0, seed=3)
     rng = np.random.default_rng(7)
     for k in ("b1", "b2", "b3"):
@@ -1115,6 +1116,7 @@ def main():
     ap.add_argument("--no-inference", action="store_true", help="skip the s/iter comparison of the default run")
     ap.add_argument("--forms", default="", help="comma list of forms for --mode inference (default: all)")
     ap.add_argument("--shape", default="", help="L,q,N: one shape for --mode kernels")
+    ap.add_argument("--hidden", type=int, default=512, help="MADE hidden units (--mode learned / made)")
     args = ap.parse_args()
     rank, world, _ = env_rank()
 

@@ -499,7 +499,7 @@ int mi3_made_sample(uint32_t L, uint32_t q, uint32_t H, const void *W1T_bf16, co
 /* Tensor-core MADE sampler (tcgen05).  Hidden degrees m1, m2 (host arrays
  * of H int32, sorted, in [1, L-1]) grouped in blocks of G sites: block b
  * owns the units of degree in (bG, bG+G], 0, 16, 32 or 48 per layer;
- * q in {4, 8}, H <= 512 a multiple of 16, G in {4, 8, 16} with G q <= 64
+ * q in {4, 8}, H <= 512 a multiple of 16, G in {4, 8} with G q <= 32
  * and ceil(L/G) * roundup(G q, 16) + 48 + ceil(L/4) <= 512.  The activations entering
  * layers 2 and 3 are rounded to bf16.
  * mi3_made_tc_workspace: device bytes for the plan's tables and weight

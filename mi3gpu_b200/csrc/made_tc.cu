@@ -9,8 +9,9 @@
 // cores read them; weights are bf16 values, sums are FP32.
 //
 // Degree blocks.  The hidden degrees are grouped in blocks of G sites
-// (G = 4, 8 or 16): block b owns the units of degree in (bG, bG + G], unit
-// indices sorted by degree, 16, 32 or 48 units per block and layer.
+// (G = 4 or 8, G q <= 32): block b owns the units of degree in
+// (bG, bG + G], unit indices sorted by degree, 16, 32 or 48 units per
+// block and layer.
 // Walking the sites in order, when block b starts (sites < s0 = bG drawn):
 //   * every hidden-1 unit of an earlier block is final, so the hidden-2
 //     units of block b get their share from them as one GEMM,
@@ -31,8 +32,9 @@
 // CTA: 128 walkers (TMEM lanes).  Warps 0-3 run the walkers; warp 4 issues
 // the MMAs; warp 5 streams their weight tiles (pre-swizzled K-major images,
 // one 1-D bulk copy each) through a 3-stage ring; warp 6 streams the
-// CUDA-core weights (the block's layer-1 rows in chunks of 16 sites, then
-// its layer-2/3 slice, bf16) through a 4-stage ring.  Each walker's
+// CUDA-core weights (the layer-1 rows of the earlier sites in FP32 chunks
+// of 64 / q sites, then the block's layer-2 and layer-3 weights and the
+// layer-1 rows of its own sites in bf16) through a 4-stage ring.  Each walker's
 // sequence words are kept in spare TMEM columns for the layer-1 gathers.
 // All waits are bounded (status word).  The kernel draws walker n's
 // residue i from the same counter-based uniform as made.cu (seed, n, i);
@@ -52,8 +54,8 @@ namespace mi3 {
 constexpr uint32_t MT_M = 128;        // walkers per tile
 constexpr uint32_t MT_NU = 48;        // largest unit count per block and layer
 constexpr uint32_t MT_HMAX = 512;     // hidden units (A1 holds 8 K-chunks of 64)
-constexpr uint32_t MT_GQMAX = 64;     // sites x residues per block
-constexpr uint32_t MT_CS = 16;        // sites per layer-1 chunk
+constexpr uint32_t MT_GQMAX = 32;     // sites x residues per block
+constexpr uint32_t MT_CROWS = 64;     // layer-1 rows (site, residue) per chunk: 64 / q sites
 constexpr uint32_t MT_STAGES = 3;     // MMA weight-tile ring
 constexpr uint32_t MT_STAGE_ROWS = 64;
 constexpr uint32_t MT_STAGE_BYTES = MT_STAGE_ROWS * 128;
@@ -61,7 +63,10 @@ constexpr uint32_t MT_WSTAGES = 4;    // CUDA-core weight ring
 constexpr uint32_t MT_WSTAGE_BYTES = 12288;
 constexpr uint32_t MT_ROW_BYTES = MT_NU * 2;  // one bf16 weight row over a block's units
 constexpr uint32_t MT_W2_BYTES = MT_NU * MT_ROW_BYTES;
-constexpr uint32_t MT_W23_BYTES = MT_W2_BYTES + MT_GQMAX * MT_ROW_BYTES;
+constexpr uint32_t MT_W3_BYTES = MT_GQMAX * MT_ROW_BYTES;
+// a block's CUDA-core weights besides the layer-1 prefix: W2 [48][48], W3
+// [G q][48] and the layer-1 rows of its own sites [G q][48], bf16
+constexpr uint32_t MT_W123_BYTES = MT_W2_BYTES + 2 * MT_W3_BYTES;
 constexpr uint32_t MT_A1_BYTES = (MT_HMAX / 64) * MT_M * 128;
 constexpr uint32_t MT_A2_BYTES = MT_M * 128;
 constexpr uint32_t MT_THREADS = 224;
@@ -69,7 +74,7 @@ constexpr uint32_t MT_TMEM_COLS = 512;
 constexpr uint32_t MT_SMEM = 1024 + MT_A1_BYTES + MT_A2_BYTES + MT_STAGES * MT_STAGE_BYTES +
                              MT_WSTAGES * MT_WSTAGE_BYTES + 256;
 static_assert(MT_SMEM <= 232448, "shared memory");
-static_assert(MT_W23_BYTES <= MT_WSTAGE_BYTES && MT_CS * 8 * MT_ROW_BYTES <= MT_WSTAGE_BYTES, "weight stage");
+static_assert(MT_W123_BYTES <= MT_WSTAGE_BYTES && MT_CROWS * MT_NU * 4 <= MT_WSTAGE_BYTES, "weight stage");
 
 // One weight tile of the MMA ring and the MMAs that consume it.
 struct MtOp {
@@ -83,8 +88,9 @@ struct MtOp {
     uint32_t blk;
 };
 
-// One stage of the CUDA-core weight ring: a layer-1 chunk (rows (j, a) of
-// 16 sites x the block's hidden-1 units) or the block's layer-2/3 slice.
+// One stage of the CUDA-core weight ring: a layer-1 chunk (FP32 rows (j, a)
+// of 64 / q sites x the block's hidden-1 units) or the block's in-block
+// weights (bf16).
 struct MtWOp {
     uint32_t off, bytes, kind, blk, chunk, pad0, pad1, pad2;
 };
@@ -98,12 +104,13 @@ __host__ __device__ __forceinline__ uint32_t op_bytes(const MtWOp &o) { return o
 constexpr uint32_t MT_BLK = 12;
 
 struct MtPlan {
-    uint32_t L, q, H, G, nb, N3, d2col, wcol, nops, nwops;
+    uint32_t L, q, H, G, nb, N3, d2col, wcol, nops, nwops, nu, pad;
     uint64_t img_bytes, wimg_bytes;
     const MtOp *ops;
     const MtWOp *wops;
     const uint32_t *blk;
     const int32_t *deg2_start;  // [L + 1]: first hidden-2 unit of degree >= d
+    const int32_t *deg1_start;  // [L + 1]: first hidden-1 unit of degree >= d
     const unsigned char *img;   // MMA weight tiles
     const unsigned char *wimg;  // CUDA-core weight stages
     const float *b1b;           // [nb][NU]
@@ -149,27 +156,71 @@ __device__ __forceinline__ void unpack8(const uint4 w, float *f) {
     f[7] = __uint_as_float(w.w & 0xffff0000u);
 }
 
-// sum_u row[u] x[u] over the 48 units of a bf16 row in shared memory, in unit order
-__device__ __forceinline__ float dot48(const unsigned char *row, const float *x) {
-    float s = 0.0f;
+// sum_u row[u] x[u] over the first NU units of a bf16 row in shared
+// memory, as four interleaved partial sums (units u = 4k + e in sum e)
+template <uint32_t NU>
+__device__ __forceinline__ float dotn(const unsigned char *row, const float *x) {
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    uint4 w[NU / 8];
 #pragma unroll
-    for (uint32_t g = 0; g < MT_NU / 8; ++g) {
-        float w[8];
-        unpack8(*reinterpret_cast<const uint4 *>(row + 16 * g), w);
+    for (uint32_t g = 0; g < NU / 8; ++g) w[g] = *reinterpret_cast<const uint4 *>(row + 16 * g);
 #pragma unroll
-        for (uint32_t e = 0; e < 8; ++e) s = __fmaf_rn(w[e], x[8 * g + e], s);
+    for (uint32_t g = 0; g < NU / 8; ++g) {
+        float f[8];
+        unpack8(w[g], f);
+#pragma unroll
+        for (uint32_t e = 0; e < 8; ++e) s[e & 3] = __fmaf_rn(f[e], x[8 * g + e], s[e & 3]);
     }
-    return s;
+    return (s[0] + s[1]) + (s[2] + s[3]);
 }
 
-__device__ __forceinline__ void add48(const unsigned char *row, float *h) {
+// The FP32 layer-1 rows of a chunk hold their 16-byte groups in the order
+// g ^ mt_rsw(row): the 4 (q=4) or 8 (q=8) rows a warp reads for one site
+// then fall in different bank groups.
+__host__ __device__ __forceinline__ uint32_t mt_rsw(uint32_t row) { return (row >> 1) & 3; }
+
+// h[v] += row[v] over the first NU units of a swizzled FP32 chunk row
+template <uint32_t NU>
+__device__ __forceinline__ void add_f(const float *chunk, uint32_t rr, float *h) {
+    const float *row = chunk + rr * MT_NU;
+    const uint32_t sw = mt_rsw(rr);
 #pragma unroll
-    for (uint32_t g = 0; g < MT_NU / 8; ++g) {
-        float w[8];
-        unpack8(*reinterpret_cast<const uint4 *>(row + 16 * g), w);
-#pragma unroll
-        for (uint32_t e = 0; e < 8; ++e) h[8 * g + e] += w[e];
+    for (uint32_t g = 0; g < NU / 4; ++g) {
+        const float4 w = *reinterpret_cast<const float4 *>(row + 4 * (g ^ sw));
+        h[4 * g] += w.x;
+        h[4 * g + 1] += w.y;
+        h[4 * g + 2] += w.z;
+        h[4 * g + 3] += w.w;
     }
+}
+
+// h[v] += row[v] over the first NU units of a bf16 row in shared memory
+template <uint32_t NU>
+__device__ __forceinline__ void add_h(const unsigned char *row, float *h) {
+    uint4 w[NU / 8];
+#pragma unroll
+    for (uint32_t g = 0; g < NU / 8; ++g) w[g] = *reinterpret_cast<const uint4 *>(row + 16 * g);
+#pragma unroll
+    for (uint32_t g = 0; g < NU / 8; ++g) {
+        float f[8];
+        unpack8(w[g], f);
+#pragma unroll
+        for (uint32_t e = 0; e < 8; ++e) h[8 * g + e] += f[e];
+    }
+}
+
+// four single-column TMEM loads in flight together, one wait
+__device__ __forceinline__ void tmem_ld1x4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, float (&v)[4]) {
+    uint32_t r0, r1, r2, r3;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r0) : "r"(a0));
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r1) : "r"(a1));
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r2) : "r"(a2));
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r3) : "r"(a3));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    v[0] = __uint_as_float(r0);
+    v[1] = __uint_as_float(r1);
+    v[2] = __uint_as_float(r2);
+    v[3] = __uint_as_float(r3);
 }
 
 __device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
@@ -256,7 +307,7 @@ __device__ __forceinline__ void mt_produce(const Op *ops, uint32_t nops, const u
     }
 }
 
-template <uint32_t Q>
+template <uint32_t Q, uint32_t NU>
 __global__ void __launch_bounds__(MT_THREADS, 1)
     k_made_tc(const MtPlan p, uint32_t *seq, uint32_t buflen, uint32_t nseq, float *logq, uint64_t seed,
               int given, int32_t *status) {
@@ -407,11 +458,11 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                 mbar_arrive(bar_a1);
 
                 // the block's hidden-1 units: bias + inputs from sites < s0,
-                // weight rows streamed 16 sites at a time
-                float h1[MT_NU];
+                // FP32 weight rows streamed 64 / q sites at a time
+                float h1[NU];
 #pragma unroll
-                for (uint32_t v = 0; v < MT_NU; ++v) h1[v] = __ldg(&p.b1b[b * MT_NU + v]);
-                uint32_t s_last = 0;
+                for (uint32_t v = 0; v < NU; ++v) h1[v] = __ldg(&p.b1b[b * MT_NU + v]);
+                constexpr uint32_t CS = MT_CROWS / Q;  // sites per layer-1 chunk
                 for (uint32_t c = 0; c < nch; ++c) {
                     const uint32_t s = wit % MT_WSTAGES;
                     if (!wait_all(&wfull[s], (wit / MT_WSTAGES) & 1)) {
@@ -419,30 +470,27 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                         break;
                     }
                     ++wit;
-                    const unsigned char *chunk = wring + s * MT_WSTAGE_BYTES;
-                    const uint32_t jend = min(s0, MT_CS * (c + 1));
+                    const float *chunk = reinterpret_cast<const float *>(wring + s * MT_WSTAGE_BYTES);
+                    const uint32_t jend = min(s0, CS * (c + 1));
                     uint32_t word = 0;
-                    for (uint32_t j = MT_CS * c; j < jend; ++j) {
+                    for (uint32_t j = CS * c; j < jend; ++j) {
                         if ((j & 3) == 0) word = tmem_ld1(tmem + lane_base + p.wcol + (j >> 2));
                         const uint32_t x = min((word >> (8 * (j & 3))) & 0xffu, Q - 1);
-                        add48(chunk + ((j - MT_CS * c) * Q + x) * MT_ROW_BYTES, h1);
+                        add_f<NU>(chunk, (j - CS * c) * Q + x, h1);
                     }
-                    if (c + 1 < nch)
-                        mbar_arrive(&wempty[s]);
-                    else
-                        s_last = s;  // holds the rows of this block's own sites
+                    mbar_arrive(&wempty[s]);
                 }
                 if (!ok) break;
+                // the block's in-block weights, held for its sites
                 const uint32_t s23 = wit % MT_WSTAGES;
                 if (!wait_all(&wfull[s23], (wit / MT_WSTAGES) & 1)) {
                     ok = false;
                     break;
                 }
                 ++wit;
-                const unsigned char *w1c = wring + s_last * MT_WSTAGE_BYTES;
-                const uint32_t jc0 = MT_CS * (nch - 1);
                 const unsigned char *w2s = wring + s23 * MT_WSTAGE_BYTES;
                 const unsigned char *w3s = w2s + MT_W2_BYTES;
+                const unsigned char *w1s = w3s + MT_W3_BYTES;
 
                 // layer-2 prefix of the block (and the logits accumulator)
                 if (!wait_all(bar_mma, nmma++ & 1)) {
@@ -466,14 +514,14 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                         for (uint32_t a = 0; a < Q; ++a) lg[a] = 0.0f;
                     }
                     {
-                        float act2[MT_NU];
+                        float act2[NU];
 #pragma unroll
-                        for (uint32_t g = 0; g < MT_NU / 8; ++g)
+                        for (uint32_t g = 0; g < NU / 8; ++g)
                             unpack8(*reinterpret_cast<const uint4 *>(A2 + m * 128 + (((g ^ (m & 7)) & 7) << 4)),
                                     &act2[8 * g]);
 #pragma unroll
                         for (uint32_t a = 0; a < Q; ++a)
-                            lg[a] += __ldg(&p.b3[i * Q + a]) + dot48(w3s + (il * Q + a) * MT_ROW_BYTES, act2);
+                            lg[a] += __ldg(&p.b3[i * Q + a]) + dotn<NU>(w3s + (il * Q + a) * MT_ROW_BYTES, act2);
                     }
                     // draw (or read) residue i
                     float mx = lg[0];
@@ -520,31 +568,40 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                         }
                     }
                     // its input to the block's hidden-1 units
-                    add48(w1c + ((i - jc0) * Q + r) * MT_ROW_BYTES, h1);
-                    // hidden-2 units of degree i + 1
+                    add_h<NU>(w1s + (il * Q + r) * MT_ROW_BYTES, h1);
+                    // hidden-2 units of degree i + 1, four at a time
                     if (i + 1 < L) {
                         const int32_t ulo = __ldg(&p.deg2_start[i + 1]) - (int32_t)c2;
                         const int32_t uhi = __ldg(&p.deg2_start[i + 2]) - (int32_t)c2;
                         if (ulo < uhi) {
-                            float act1[MT_NU];
+                            float act1[NU];
 #pragma unroll
-                            for (uint32_t v = 0; v < MT_NU; ++v) act1[v] = bf16r(fmaxf(h1[v], 0.0f));
-                            for (int32_t u = ulo; u < uhi; ++u) {
-                                const float d2 =
-                                    d2ok ? __uint_as_float(tmem_ld1(tmem + lane_base + p.d2col + (uint32_t)u)) : 0.0f;
-                                const float z =
-                                    (d2 + __ldg(&p.b2b[b * MT_NU + u])) + dot48(w2s + u * MT_ROW_BYTES, act1);
-                                *reinterpret_cast<unsigned short *>(A2 + mt_sw(m, (uint32_t)u)) =
-                                    __bfloat16_as_ushort(__float2bfloat16_rn(fmaxf(z, 0.0f)));
+                            for (uint32_t v = 0; v < NU; ++v) act1[v] = bf16r(fmaxf(h1[v], 0.0f));
+                            for (int32_t u0 = ulo; u0 < uhi; u0 += 4) {
+                                uint32_t uk[4];
+#pragma unroll
+                                for (uint32_t k = 0; k < 4; ++k) uk[k] = (uint32_t)min(u0 + (int32_t)k, uhi - 1);
+                                float d2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                                if (d2ok) {
+                                    const uint32_t tb = tmem + lane_base + p.d2col;
+                                    tmem_ld1x4(tb + uk[0], tb + uk[1], tb + uk[2], tb + uk[3], d2);
+                                }
+#pragma unroll
+                                for (uint32_t k = 0; k < 4; ++k) {
+                                    const float z = (d2[k] + __ldg(&p.b2b[b * MT_NU + uk[k]])) +
+                                                    dotn<NU>(w2s + uk[k] * MT_ROW_BYTES, act1);
+                                    if (u0 + (int32_t)k < uhi)
+                                        *reinterpret_cast<unsigned short *>(A2 + mt_sw(m, uk[k])) =
+                                            __bfloat16_as_ushort(__float2bfloat16_rn(fmaxf(z, 0.0f)));
+                                }
                             }
                         }
                     }
                 }
-                mbar_arrive(&wempty[s_last]);
                 mbar_arrive(&wempty[s23]);
                 // the block's hidden-1 units are final: into A1 for later blocks
 #pragma unroll
-                for (uint32_t g = 0; g < MT_NU / 8; ++g) {
+                for (uint32_t g = 0; g < NU / 8; ++g) {
                     if (8 * g < n1) {
                         const uint32_t k = c1 + 8 * g;
                         uint4 w;
@@ -594,26 +651,38 @@ __global__ void k_made_tc_images(const MtPlan p, unsigned char *img, const float
     }
 }
 
-// CUDA-core weight stages (bf16): layer-1 chunks [16 q rows][48 units] and
-// the layer-2/3 slice [48][48] + [64][48] of each block.
+// CUDA-core weight stages: layer-1 chunks [64 rows (j, a)][48 units] in
+// FP32, and per block W2 [48][48], W3 [G q][48] and the layer-1 rows of the
+// block's own sites [G q][48] in bf16.
 __global__ void k_made_tc_wimages(const MtPlan p, unsigned char *wimg, const float *__restrict__ W1T,
                                   const float *__restrict__ W2, const float *__restrict__ W3) {
     const MtWOp op = p.wops[blockIdx.x];
     const uint32_t *bk = p.blk + op.blk * MT_BLK;
     const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], n2 = bk[3];
     const uint32_t H = p.H, q = p.q, G = p.G, L = p.L;
+    if (op.kind == 0) {
+        float *out = reinterpret_cast<float *>(wimg + op.off);
+        for (uint32_t e = threadIdx.x; e < MT_CROWS * MT_NU; e += blockDim.x) {
+            const uint32_t r = e / MT_NU, x = e % MT_NU;
+            const uint32_t j = (MT_CROWS / q) * op.chunk + r / q, a = r % q;
+            out[r * MT_NU + 4 * ((x / 4) ^ mt_rsw(r)) + x % 4] =
+                (j < L && x < n1) ? W1T[(size_t)(j * q + a) * H + c1 + x] : 0.0f;
+        }
+        return;
+    }
     unsigned short *out = reinterpret_cast<unsigned short *>(wimg + op.off);
+    const uint32_t s0 = op.blk * G;
     for (uint32_t e = threadIdx.x; e < op.bytes / 2; e += blockDim.x) {
         const uint32_t r = e / MT_NU, x = e % MT_NU;
         float v = 0.0f;
-        if (op.kind == 0) {
-            const uint32_t j = MT_CS * op.chunk + r / q, a = r % q;
-            if (j < L && x < n1) v = W1T[(size_t)(j * q + a) * H + c1 + x];
-        } else if (r < MT_NU) {
+        if (r < MT_NU) {
             if (r < n2 && x < n1) v = W2[(size_t)(c2 + r) * H + c1 + x];
+        } else if (r < MT_NU + MT_GQMAX) {
+            const uint32_t c = r - MT_NU, i = s0 + c / q;
+            if (c < G * q && i < L && x < n2) v = W3[(size_t)(s0 * q + c) * H + c2 + x];
         } else {
-            const uint32_t c = r - MT_NU, i = op.blk * G + c / q;
-            if (c < G * q && i < L && x < n2) v = W3[(size_t)(op.blk * G * q + c) * H + c2 + x];
+            const uint32_t c = r - MT_NU - MT_GQMAX, i = s0 + c / q;
+            if (c < G * q && i < L && x < n1) v = W1T[(size_t)(s0 * q + c) * H + c1 + x];
         }
         out[e] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
     }
@@ -637,7 +706,7 @@ __global__ void k_made_tc_bias(const MtPlan p, float *b1b, float *b2b, float *b3
 }
 
 struct MtLayout {
-    size_t ops, wops, blk, deg, img, wimg, b1b, b2b, b3, total;
+    size_t ops, wops, blk, deg, deg1, img, wimg, b1b, b2b, b3, total;
 };
 
 static size_t mt_align(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -655,6 +724,7 @@ static MtLayout mt_layout(uint32_t L, uint32_t q, uint32_t nb, size_t nops, size
     o.wops = take(nwops * sizeof(MtWOp));
     o.blk = take((size_t)nb * MT_BLK * 4);
     o.deg = take((size_t)(L + 1) * 4);
+    o.deg1 = take((size_t)(L + 1) * 4);
     o.img = take(img_bytes);
     o.wimg = take(wimg_bytes);
     o.b1b = take((size_t)nb * MT_NU * 4);
@@ -666,20 +736,20 @@ static MtLayout mt_layout(uint32_t L, uint32_t q, uint32_t nb, size_t nops, size
 
 // The host-side plan: block table, op lists and image sizes, or an error text.
 struct MtHostPlan {
-    uint32_t nb = 0, N3 = 0, d2col = 0, wcol = 0;
+    uint32_t nb = 0, N3 = 0, d2col = 0, wcol = 0, nu = 32;
     std::vector<uint32_t> blk;
     std::vector<MtOp> ops;
     std::vector<MtWOp> wops;
-    std::vector<int32_t> deg2;
+    std::vector<int32_t> deg1, deg2;
     size_t img_bytes = 0, wimg_bytes = 0;
     const char *err = nullptr;
 };
 
 static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const int32_t *m1, const int32_t *m2) {
     MtHostPlan h;
-    if (L < 2 || (q != 4 && q != 8) || H == 0 || H > MT_HMAX || H % 16 || (G != 4 && G != 8 && G != 16) ||
+    if (L < 2 || (q != 4 && q != 8) || H == 0 || H > MT_HMAX || H % 16 || (G != 4 && G != 8) ||
         G * q > MT_GQMAX) {
-        h.err = "mi3_made_tc: needs q in {4, 8}, H <= 512 a multiple of 16, G in {4, 8, 16} with G q <= 64";
+        h.err = "mi3_made_tc: needs q in {4, 8}, H <= 512 a multiple of 16, G in {4, 8} with G q <= 32";
         return h;
     }
     h.nb = (L + G - 1) / G;
@@ -707,6 +777,7 @@ static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const 
             h.err = "mi3_made_tc: each degree block needs 0, 16, 32 or 48 units per layer";
             return h;
         }
+        h.nu = std::max(h.nu, std::max(n1[b], n2[b]));
         uint32_t *bk = &h.blk[(size_t)b * MT_BLK];
         bk[0] = c1;
         bk[1] = n1[b];
@@ -732,19 +803,18 @@ static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const 
         }
         bk[6] = (uint32_t)h.ops.size();
         bk[7] = bk[5] > bk[4] ? 1u : 0u;
-        // the CUDA-core weights: layer-1 chunks of the sites < min(L, s0 + G)
-        // (the block's own sites fall in the last one, as G divides 16), then
-        // the layer-2/3 slice
-        const uint32_t s1 = std::min(L, b * G + G);
-        const uint32_t nch = (s1 + MT_CS - 1) / MT_CS;
+        // the CUDA-core weights: layer-1 chunks of the sites < s0, then the
+        // block's in-block weights
+        const uint32_t cs = MT_CROWS / q;
+        const uint32_t nch = (b * G + cs - 1) / cs;
         bk[8] = (uint32_t)h.wops.size();
         bk[9] = nch;
         for (uint32_t c = 0; c < nch; ++c) {
-            MtWOp w{woff, MT_CS * q * MT_ROW_BYTES, 0, b, c, 0, 0, 0};
+            MtWOp w{woff, MT_CROWS * MT_NU * 4, 0, b, c, 0, 0, 0};
             h.wops.push_back(w);
             woff += w.bytes;
         }
-        MtWOp w{woff, MT_W23_BYTES, 1, b, 0, 0, 0, 0};
+        MtWOp w{woff, MT_W123_BYTES, 1, b, 0, 0, 0, 0};
         h.wops.push_back(w);
         woff += w.bytes;
         c1 += n1[b];
@@ -752,11 +822,15 @@ static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const 
     }
     h.img_bytes = off;
     h.wimg_bytes = woff;
+    h.deg1.assign(L + 1, (int32_t)H);
     h.deg2.assign(L + 1, (int32_t)H);
     for (uint32_t d = 0; d <= L; ++d) {
         uint32_t k = 0;
         while (k < H && m2[k] < (int32_t)d) ++k;
         h.deg2[d] = (int32_t)k;
+        k = 0;
+        while (k < H && m1[k] < (int32_t)d) ++k;
+        h.deg1[d] = (int32_t)k;
     }
     return h;
 }
@@ -792,7 +866,8 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
         cudaMemcpyAsync(ws + lay.wops, h.wops.data(), h.wops.size() * sizeof(MtWOp), cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
         cudaMemcpyAsync(ws + lay.blk, h.blk.data(), h.blk.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(ws + lay.deg, h.deg2.data(), h.deg2.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        cudaMemcpyAsync(ws + lay.deg, h.deg2.data(), h.deg2.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(ws + lay.deg1, h.deg1.data(), h.deg1.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return check_launch("mi3_made_tc_prepare: tables");
     MtPlan p;
     std::memset(&p, 0, sizeof(p));
@@ -804,6 +879,7 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
     p.N3 = h.N3;
     p.d2col = h.d2col;
     p.wcol = h.wcol;
+    p.nu = h.nu;
     p.nops = (uint32_t)h.ops.size();
     p.nwops = (uint32_t)h.wops.size();
     p.img_bytes = h.img_bytes;
@@ -812,6 +888,7 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
     p.wops = reinterpret_cast<const MtWOp *>(ws + lay.wops);
     p.blk = reinterpret_cast<const uint32_t *>(ws + lay.blk);
     p.deg2_start = reinterpret_cast<const int32_t *>(ws + lay.deg);
+    p.deg1_start = reinterpret_cast<const int32_t *>(ws + lay.deg1);
     p.img = ws + lay.img;
     p.wimg = ws + lay.wimg;
     p.b1b = reinterpret_cast<const float *>(ws + lay.b1b);
@@ -848,12 +925,14 @@ extern "C" int mi3_made_tc_sample(const uint64_t *plan, uint32_t *seq, uint32_t 
     const uint32_t ntiles = (nseq + MT_M - 1) / MT_M;
     const uint32_t grid = std::min<uint32_t>(ntiles, (uint32_t)nsm);
     cudaStream_t st = as_stream(stream);
-    if (p.q == 4) {
-        cudaFuncSetAttribute(k_made_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MT_SMEM);
-        k_made_tc<4><<<grid, MT_THREADS, MT_SMEM, st>>>(p, seq, buflen, nseq, logq, seed, given, status);
-    } else {
-        cudaFuncSetAttribute(k_made_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MT_SMEM);
-        k_made_tc<8><<<grid, MT_THREADS, MT_SMEM, st>>>(p, seq, buflen, nseq, logq, seed, given, status);
-    }
+    // the kernel holds 32 or 48 units per block and layer in registers
+    auto launch = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MT_SMEM);
+        kern<<<grid, MT_THREADS, MT_SMEM, st>>>(p, seq, buflen, nseq, logq, seed, given, status);
+    };
+    if (p.q == 4)
+        p.nu <= 32 ? launch(k_made_tc<4, 32>) : launch(k_made_tc<4, 48>);
+    else
+        p.nu <= 32 ? launch(k_made_tc<8, 32>) : launch(k_made_tc<8, 48>);
     return check_launch("mi3_made_tc_sample");
 }

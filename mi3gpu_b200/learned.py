@@ -67,15 +67,15 @@ TC_TMEM_COLS, TC_MAX_UNITS = 512, 48
 
 
 def tc_block_size(L, q, H):
-    """The largest block size G (4, 8 or 16, G q <= 64) with which the
+    """The largest block size G (4 or 8, G q <= 32) with which the
     tensor-core sampler can run this network, or None: the logits of all
     blocks (ceil(L/G) x roundup(G q, 16) columns), one block's layer-2
     accumulator and the walkers' sequence words (ceil(L/4) columns) must
     fit the 512 tensor-memory columns."""
     if q not in (4, 8) or H % 16 or H > 512 or L < 2:
         return None
-    for G in (16, 8, 4):
-        if G * q > 64:
+    for G in (8, 4):
+        if G * q > 32:
             continue
         nb = -(-L // G)
         n3 = -(-G * q // 16) * 16

@@ -11,7 +11,7 @@ from mi3gpu_b200.learned import blocked_degrees, made_masks, tc_block_size
                                    (5, 4, 32), (8, 4, 64)])
 def test_blocked_degrees(L, q, H):
     G = tc_block_size(L, q, H)
-    assert G in (4, 8, 16) and G * q <= 64
+    assert G in (4, 8) and G * q <= 32
     m = blocked_degrees(L, H, G)
     assert len(m) == H and m.min() >= 1 and m.max() <= L - 1
     assert np.all(np.diff(m) >= 0)
