@@ -25,16 +25,16 @@
 // inputs from earlier sites gathered once, then one weight row per drawn
 // site), its hidden-2 units (one dot product over the block's hidden-1
 // units each, as they become final) and the in-block share of each site's
-// logits -- runs on the CUDA cores, one walker per thread, from weights
-// staged in shared memory.  Masked weights are zero, so each in-block loop
+// logits -- runs on the CUDA cores, two or three threads per walker (one
+// per 16 units), from weights staged in shared memory.  Masked weights are zero, so each in-block loop
 // runs over all of the block's units.
 //
-// CTA: 128 walkers (TMEM lanes).  Warps 0-3 run the walkers; warp 4 issues
-// the MMAs; warp 5 streams their weight tiles (pre-swizzled K-major images,
-// one 1-D bulk copy each) through a 3-stage ring; warp 6 streams the
+// CTA: 128 walkers (TMEM lanes).  8 or 12 warps run the walkers; the next
+// warp issues the MMAs; one streams their weight tiles (pre-swizzled K-major
+// images, one 1-D bulk copy each) through a 2-stage ring; one streams the
 // CUDA-core weights (the layer-1 rows of the earlier sites in FP32 chunks
 // of 64 / q sites, then the block's layer-2 and layer-3 weights and the
-// layer-1 rows of its own sites in bf16) through a 4-stage ring.  Each walker's
+// layer-1 rows of its own sites in bf16) through a 2- or 3-stage ring.  Each walker's
 // sequence words are kept in spare TMEM columns for the layer-1 gathers.
 // All waits are bounded (status word).  The kernel draws walker n's
 // residue i from the same counter-based uniform as made.cu (seed, n, i);
@@ -56,24 +56,23 @@ constexpr uint32_t MT_NU = 48;        // largest unit count per block and layer
 constexpr uint32_t MT_HMAX = 512;     // hidden units (A1 holds 8 K-chunks of 64)
 constexpr uint32_t MT_GQMAX = 32;     // sites x residues per block
 constexpr uint32_t MT_CROWS = 64;     // layer-1 rows (site, residue) per chunk: 64 / q sites
-constexpr uint32_t MT_STAGES = 3;     // MMA weight-tile ring
 constexpr uint32_t MT_STAGE_ROWS = 64;
 constexpr uint32_t MT_STAGE_BYTES = MT_STAGE_ROWS * 128;
-constexpr uint32_t MT_WSTAGES = 4;    // CUDA-core weight ring
 constexpr uint32_t MT_WSTAGE_BYTES = 12288;
 constexpr uint32_t MT_ROW_BYTES = MT_NU * 2;  // one bf16 weight row over a block's units
 constexpr uint32_t MT_W2_BYTES = MT_NU * MT_ROW_BYTES;
 constexpr uint32_t MT_W3_BYTES = MT_GQMAX * MT_ROW_BYTES;
 // a block's CUDA-core weights besides the layer-1 prefix: W2 [48][48], W3
 // [G q][48] and the layer-1 rows of its own sites [G q][48], bf16
-constexpr uint32_t MT_W123_BYTES = MT_W2_BYTES + 2 * MT_W3_BYTES;
+// then the block's small parameters (FP32 b3 [G q], b2 [48], b1 [48], and
+// int32 cnt [16]: block-local index of the first hidden-2 unit of degree
+// >= s0 + 1 + k), so that no global load sits on a site's critical path
+constexpr uint32_t MT_PAR_OFF = MT_W2_BYTES + 2 * MT_W3_BYTES;
+constexpr uint32_t MT_PAR_B3 = 0, MT_PAR_B2 = MT_GQMAX, MT_PAR_B1 = MT_PAR_B2 + MT_NU, MT_PAR_CNT = MT_PAR_B1 + MT_NU;
+constexpr uint32_t MT_W123_BYTES = MT_PAR_OFF + (MT_PAR_CNT + 16) * 4;
 constexpr uint32_t MT_A1_BYTES = (MT_HMAX / 64) * MT_M * 128;
 constexpr uint32_t MT_A2_BYTES = MT_M * 128;
-constexpr uint32_t MT_THREADS = 224;
 constexpr uint32_t MT_TMEM_COLS = 512;
-constexpr uint32_t MT_SMEM = 1024 + MT_A1_BYTES + MT_A2_BYTES + MT_STAGES * MT_STAGE_BYTES +
-                             MT_WSTAGES * MT_WSTAGE_BYTES + 256;
-static_assert(MT_SMEM <= 232448, "shared memory");
 static_assert(MT_W123_BYTES <= MT_WSTAGE_BYTES && MT_CROWS * MT_NU * 4 <= MT_WSTAGE_BYTES, "weight stage");
 
 // One weight tile of the MMA ring and the MMAs that consume it.
@@ -156,58 +155,13 @@ __device__ __forceinline__ void unpack8(const uint4 w, float *f) {
     f[7] = __uint_as_float(w.w & 0xffff0000u);
 }
 
-// sum_u row[u] x[u] over the first NU units of a bf16 row in shared
-// memory, as four interleaved partial sums (units u = 4k + e in sum e)
-template <uint32_t NU>
-__device__ __forceinline__ float dotn(const unsigned char *row, const float *x) {
-    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    uint4 w[NU / 8];
-#pragma unroll
-    for (uint32_t g = 0; g < NU / 8; ++g) w[g] = *reinterpret_cast<const uint4 *>(row + 16 * g);
-#pragma unroll
-    for (uint32_t g = 0; g < NU / 8; ++g) {
-        float f[8];
-        unpack8(w[g], f);
-#pragma unroll
-        for (uint32_t e = 0; e < 8; ++e) s[e & 3] = __fmaf_rn(f[e], x[8 * g + e], s[e & 3]);
-    }
-    return (s[0] + s[1]) + (s[2] + s[3]);
-}
 
 // The FP32 layer-1 rows of a chunk hold their 16-byte groups in the order
 // g ^ mt_rsw(row): the 4 (q=4) or 8 (q=8) rows a warp reads for one site
 // then fall in different bank groups.
 __host__ __device__ __forceinline__ uint32_t mt_rsw(uint32_t row) { return (row >> 1) & 3; }
 
-// h[v] += row[v] over the first NU units of a swizzled FP32 chunk row
-template <uint32_t NU>
-__device__ __forceinline__ void add_f(const float *chunk, uint32_t rr, float *h) {
-    const float *row = chunk + rr * MT_NU;
-    const uint32_t sw = mt_rsw(rr);
-#pragma unroll
-    for (uint32_t g = 0; g < NU / 4; ++g) {
-        const float4 w = *reinterpret_cast<const float4 *>(row + 4 * (g ^ sw));
-        h[4 * g] += w.x;
-        h[4 * g + 1] += w.y;
-        h[4 * g + 2] += w.z;
-        h[4 * g + 3] += w.w;
-    }
-}
 
-// h[v] += row[v] over the first NU units of a bf16 row in shared memory
-template <uint32_t NU>
-__device__ __forceinline__ void add_h(const unsigned char *row, float *h) {
-    uint4 w[NU / 8];
-#pragma unroll
-    for (uint32_t g = 0; g < NU / 8; ++g) w[g] = *reinterpret_cast<const uint4 *>(row + 16 * g);
-#pragma unroll
-    for (uint32_t g = 0; g < NU / 8; ++g) {
-        float f[8];
-        unpack8(w[g], f);
-#pragma unroll
-        for (uint32_t e = 0; e < 8; ++e) h[8 * g + e] += f[e];
-    }
-}
 
 // four single-column TMEM loads in flight together, one wait
 __device__ __forceinline__ void tmem_ld1x4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, float (&v)[4]) {
@@ -230,9 +184,10 @@ __device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
     return r;
 }
 
+// single-column TMEM store; the writer waits (tcgen05.wait::st) before it
+// reads the column back
 __device__ __forceinline__ void tmem_st1(uint32_t taddr, uint32_t v) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(v) : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float (&v)[4]) {
@@ -307,45 +262,126 @@ __device__ __forceinline__ void mt_produce(const Op *ops, uint32_t nops, const u
     }
 }
 
+// Compute threads: NU / 16 warps per TMEM lane quadrant (32 walkers), warp w
+// owning walker 32 (w % 4) + lane and unit slice w / 4 (16 of a block's
+// units).  Sums over a block's units are taken per slice and added across
+// the slices through shared memory in slice order, so the threads of a
+// walker hold identical logits and draw the same residue.
 template <uint32_t Q, uint32_t NU>
-__global__ void __launch_bounds__(MT_THREADS, 1)
+struct MtShape {
+    static constexpr uint32_t SL = NU / 16;           // unit slices
+    static constexpr uint32_t CT = SL * MT_M;         // compute threads
+    static constexpr uint32_t THREADS = CT + 96;      // + MMA issue, MMA-tile and weight producer warps
+    static constexpr uint32_t ST = 2;                 // MMA weight-tile ring stages
+    static constexpr uint32_t WST = Q == 4 ? 3 : 2;   // CUDA-core weight ring stages
+    static constexpr uint32_t HG = 4;                 // hidden-2 units reduced per barrier
+    static constexpr uint32_t RED_LG = 2 * Q * SL * MT_M * 4;
+    static constexpr uint32_t RED_H2 = 2 * HG * SL * MT_M * 4;
+    static constexpr uint32_t SMEM =
+        1024 + MT_A1_BYTES + MT_A2_BYTES + ST * MT_STAGE_BYTES + WST * MT_WSTAGE_BYTES + RED_LG + RED_H2 + 256;
+    static_assert(SMEM <= 232448, "shared memory");
+};
+
+// sum of a 16-unit slice of a bf16 row in shared memory times x, four partial sums
+__device__ __forceinline__ float dot16(const unsigned char *row, const float *x) {
+    const uint4 w0 = *reinterpret_cast<const uint4 *>(row), w1 = *reinterpret_cast<const uint4 *>(row + 16);
+    float f[16];
+    unpack8(w0, f);
+    unpack8(w1, f + 8);
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (uint32_t e = 0; e < 16; ++e) s[e & 3] = __fmaf_rn(f[e], x[e], s[e & 3]);
+    return (s[0] + s[1]) + (s[2] + s[3]);
+}
+
+// h[k] += row[v0 + k], k < 16, for a swizzled FP32 chunk row
+__device__ __forceinline__ void add16f(const float *chunk, uint32_t rr, uint32_t v0, float *h) {
+    const float *row = chunk + rr * MT_NU;
+    const uint32_t sw = mt_rsw(rr);
+#pragma unroll
+    for (uint32_t gg = 0; gg < 4; ++gg) {
+        const float4 w = *reinterpret_cast<const float4 *>(row + 4 * ((v0 / 4 + gg) ^ sw));
+        h[4 * gg] += w.x;
+        h[4 * gg + 1] += w.y;
+        h[4 * gg + 2] += w.z;
+        h[4 * gg + 3] += w.w;
+    }
+}
+
+// h[k] += row[k], k < 16, for a 16-unit slice of a bf16 row
+__device__ __forceinline__ void add16h(const unsigned char *row, float *h) {
+    const uint4 w0 = *reinterpret_cast<const uint4 *>(row), w1 = *reinterpret_cast<const uint4 *>(row + 16);
+    float f[16];
+    unpack8(w0, f);
+    unpack8(w1, f + 8);
+#pragma unroll
+    for (uint32_t e = 0; e < 16; ++e) h[e] += f[e];
+}
+
+// named barrier 1 over the CT compute threads; returns the AND of `pred`
+template <uint32_t CT>
+__device__ __forceinline__ bool compute_all(bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "n"(CT)
+        : "memory");
+    return r != 0;
+}
+
+template <uint32_t CT>
+__device__ __forceinline__ void compute_sync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(CT) : "memory");
+}
+
+template <uint32_t Q, uint32_t NU>
+__global__ void __launch_bounds__(MtShape<Q, NU>::THREADS, 1)
     k_made_tc(const MtPlan p, uint32_t *seq, uint32_t buflen, uint32_t nseq, float *logq, uint64_t seed,
               int given, int32_t *status) {
+    using S = MtShape<Q, NU>;
+    constexpr uint32_t SL = S::SL, CT = S::CT, ST = S::ST, WST = S::WST, HG = S::HG;
     extern __shared__ unsigned char smem_raw[];
     const uint32_t base_addr = smem_addr(smem_raw);
     unsigned char *sm = smem_raw + ((1024u - (base_addr & 1023u)) & 1023u);
     unsigned char *A1 = sm;
     unsigned char *A2 = A1 + MT_A1_BYTES;
     unsigned char *ring = A2 + MT_A2_BYTES;
-    unsigned char *wring = ring + MT_STAGES * MT_STAGE_BYTES;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(wring + MT_WSTAGES * MT_WSTAGE_BYTES);
-    uint64_t *full = bars, *empty = bars + MT_STAGES;
-    uint64_t *wfull = bars + 2 * MT_STAGES, *wempty = wfull + MT_WSTAGES;
-    uint64_t *bar_a1 = wempty + MT_WSTAGES, *bar_a2 = bar_a1 + 1, *bar_mma = bar_a1 + 2, *bar_fin = bar_a1 + 3;
+    unsigned char *wring = ring + ST * MT_STAGE_BYTES;
+    float *red_lg = reinterpret_cast<float *>(wring + WST * MT_WSTAGE_BYTES);  // [2][Q][SL][128]
+    float *red_h2 = red_lg + S::RED_LG / 4;                                    // [2][HG][SL][128]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(red_h2 + S::RED_H2 / 4);
+    uint64_t *full = bars, *empty = bars + ST;
+    uint64_t *wfull = bars + 2 * ST, *wempty = wfull + WST;
+    uint64_t *bar_a1 = wempty + WST, *bar_a2 = bar_a1 + 1, *bar_mma = bar_a1 + 2, *bar_fin = bar_a1 + 3;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_a1 + 4);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t L = p.L, G = p.G, nb = p.nb;
     const uint32_t ntiles = (nseq + MT_M - 1) / MT_M;
+    constexpr uint32_t W_MMA = CT / 32, W_PROD = W_MMA + 1, W_WPROD = W_MMA + 2;
 
     if (tid == 0) {
-        for (uint32_t s = 0; s < MT_STAGES; ++s) {
+        for (uint32_t s = 0; s < ST; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        for (uint32_t s = 0; s < MT_WSTAGES; ++s) {
+        for (uint32_t s = 0; s < WST; ++s) {
             mbar_init(&wfull[s], 1);
-            mbar_init(&wempty[s], MT_M);
+            mbar_init(&wempty[s], CT);
         }
-        mbar_init(bar_a1, MT_M);
-        mbar_init(bar_a2, MT_M);
+        mbar_init(bar_a1, CT);
+        mbar_init(bar_a2, CT);
         mbar_init(bar_mma, 1);
         mbar_init(bar_fin, 1);
         *abort_flag = 0;
         fence_mbar_init();
     }
-    if (warp == 4) {
+    if (warp == W_MMA) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
                      "r"(MT_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -355,17 +391,16 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 5) {
+    if (warp == W_PROD) {
         // ------------------------------------------ MMA weight-tile producer
         if ((tid & 31) == 0)
-            mt_produce<MtOp, MT_STAGES, MT_STAGE_BYTES>(p.ops, p.nops, p.img, ring, full, empty, ntiles, abort_flag,
-                                                        status);
-    } else if (warp == 6) {
+            mt_produce<MtOp, ST, MT_STAGE_BYTES>(p.ops, p.nops, p.img, ring, full, empty, ntiles, abort_flag, status);
+    } else if (warp == W_WPROD) {
         // ------------------------------------------ CUDA-core weight producer
         if ((tid & 31) == 0)
-            mt_produce<MtWOp, MT_WSTAGES, MT_WSTAGE_BYTES>(p.wops, p.nwops, p.wimg, wring, wfull, wempty, ntiles,
-                                                           abort_flag, status);
-    } else if (warp == 4) {
+            mt_produce<MtWOp, WST, MT_WSTAGE_BYTES>(p.wops, p.nwops, p.wimg, wring, wfull, wempty, ntiles, abort_flag,
+                                                    status);
+    } else if (warp == W_MMA) {
         // ---------------------------------------------------- MMA issue
         if ((tid & 31) == 0) {
             uint32_t it = 0, na1 = 0, na2 = 0;
@@ -399,8 +434,8 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                         }
                         const uint32_t lo = bk[4 + pass], hi = bk[5 + pass];
                         for (uint32_t o = lo; o < hi; ++o) {
-                            const uint32_t s = it % MT_STAGES;
-                            if (!mbar_wait_bounded(&full[s], (it / MT_STAGES) & 1, abort_flag, WAIT_LIMIT_NS)) {
+                            const uint32_t s = it % ST;
+                            if (!mbar_wait_bounded(&full[s], (it / ST) & 1, abort_flag, WAIT_LIMIT_NS)) {
                                 report(status, ST_TIMEOUT_FULL);
                                 *abort_flag = 1;
                                 ok = false;
@@ -426,14 +461,16 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
         }
     } else {
         // ---------------------------------------------------- walkers
-        const uint32_t m = tid;
-        const uint32_t lane_base = (32 * warp) << 16;
-        uint32_t nmma = 0, wit = 0;
+        const uint32_t lane = tid & 31, qd = warp & 3, sl = warp >> 2;
+        const uint32_t m = 32 * qd + lane;
+        const uint32_t lane_base = (32 * qd) << 16;
+        const uint32_t v0 = 16 * sl;  // this thread's first unit of a block
+        uint32_t nmma = 0, wit = 0, ph_lg = 0, ph_h2 = 0;
         bool ok = true;
-        // a warp-wide bounded wait: the lanes decide together (tcgen05.ld/st
-        // need all 32 of them)
-        auto wait_all = [&](uint64_t *bar, uint32_t parity) {
-            const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity, abort_flag, WAIT_LIMIT_NS));
+        // a bounded wait all compute threads decide together: named-barrier
+        // steps follow, and tcgen05.ld/st need whole warps
+        auto wait_cta = [&](uint64_t *bar, uint32_t parity) {
+            const bool got = compute_all<CT>(mbar_wait_bounded(bar, parity, abort_flag, WAIT_LIMIT_NS));
             if (!got) {
                 report(status, ST_TIMEOUT_FULL);
                 *abort_flag = 1;
@@ -449,7 +486,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                 const uint32_t *bk = p.blk + b * MT_BLK;
                 const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], d2ok = bk[7], nch = bk[9];
                 const uint32_t s0 = b * G, s1 = min(L, s0 + G);
-                if (b == 0) {
+                if (b == 0 && sl == 0) {
                     // the logits accumulator of this tile starts at zero
                     for (uint32_t c = 0; c < nb * p.N3; c += 16) tmem_zero16(tmem + lane_base + c);
                     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
@@ -457,33 +494,52 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                 tc_fence_before();
                 mbar_arrive(bar_a1);
 
-                // the block's hidden-1 units: bias + inputs from sites < s0,
+                // this slice's hidden-1 units: bias + inputs from sites < s0,
                 // FP32 weight rows streamed 64 / q sites at a time
-                float h1[NU];
+                float h1[16];
 #pragma unroll
-                for (uint32_t v = 0; v < NU; ++v) h1[v] = __ldg(&p.b1b[b * MT_NU + v]);
+                for (uint32_t k = 0; k < 16; ++k) h1[k] = __ldg(&p.b1b[b * MT_NU + v0 + k]);
                 constexpr uint32_t CS = MT_CROWS / Q;  // sites per layer-1 chunk
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");  // the words stored so far
                 for (uint32_t c = 0; c < nch; ++c) {
-                    const uint32_t s = wit % MT_WSTAGES;
-                    if (!wait_all(&wfull[s], (wit / MT_WSTAGES) & 1)) {
+                    const uint32_t s = wit % WST;
+                    if (!wait_cta(&wfull[s], (wit / WST) & 1)) {
                         ok = false;
                         break;
                     }
                     ++wit;
                     const float *chunk = reinterpret_cast<const float *>(wring + s * MT_WSTAGE_BYTES);
                     const uint32_t jend = min(s0, CS * (c + 1));
-                    uint32_t word = 0;
-                    for (uint32_t j = CS * c; j < jend; ++j) {
-                        if ((j & 3) == 0) word = tmem_ld1(tmem + lane_base + p.wcol + (j >> 2));
-                        const uint32_t x = min((word >> (8 * (j & 3))) & 0xffu, Q - 1);
-                        add_f<NU>(chunk, (j - CS * c) * Q + x, h1);
+                    // four sites (one sequence word) per step, their 16 loads together
+                    for (uint32_t j = CS * c; j < jend; j += 4) {
+                        const uint32_t word = tmem_ld1(tmem + lane_base + p.wcol + (j >> 2));
+                        float4 w[4][4];
+#pragma unroll
+                        for (uint32_t jj = 0; jj < 4; ++jj) {
+                            const uint32_t x = min((word >> (8 * jj)) & 0xffu, Q - 1);
+                            const uint32_t rr = (j + jj - CS * c) * Q + x;
+                            const float *row = chunk + rr * MT_NU;
+                            const uint32_t sw = mt_rsw(rr);
+#pragma unroll
+                            for (uint32_t gg = 0; gg < 4; ++gg)
+                                w[jj][gg] = *reinterpret_cast<const float4 *>(row + 4 * ((v0 / 4 + gg) ^ sw));
+                        }
+#pragma unroll
+                        for (uint32_t jj = 0; jj < 4; ++jj)
+#pragma unroll
+                            for (uint32_t gg = 0; gg < 4; ++gg) {
+                                h1[4 * gg] += w[jj][gg].x;
+                                h1[4 * gg + 1] += w[jj][gg].y;
+                                h1[4 * gg + 2] += w[jj][gg].z;
+                                h1[4 * gg + 3] += w[jj][gg].w;
+                            }
                     }
                     mbar_arrive(&wempty[s]);
                 }
                 if (!ok) break;
                 // the block's in-block weights, held for its sites
-                const uint32_t s23 = wit % MT_WSTAGES;
-                if (!wait_all(&wfull[s23], (wit / MT_WSTAGES) & 1)) {
+                const uint32_t s23 = wit % WST;
+                if (!wait_cta(&wfull[s23], (wit / WST) & 1)) {
                     ok = false;
                     break;
                 }
@@ -491,21 +547,46 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                 const unsigned char *w2s = wring + s23 * MT_WSTAGE_BYTES;
                 const unsigned char *w3s = w2s + MT_W2_BYTES;
                 const unsigned char *w1s = w3s + MT_W3_BYTES;
-
+                const float *par = reinterpret_cast<const float *>(w2s + MT_PAR_OFF);
+                const int32_t *cnt = reinterpret_cast<const int32_t *>(par + MT_PAR_CNT);
                 // layer-2 prefix of the block (and the logits accumulator)
-                if (!wait_all(bar_mma, nmma++ & 1)) {
+                if (!wait_cta(bar_mma, nmma++ & 1)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
+                // this slice's layer-2 prefix values, once per block
+                float d2r[16];
+                {
+                    uint32_t r16[16];
+                    if (d2ok) tmem_ld16(tmem + lane_base + p.d2col + v0, r16);
 #pragma unroll
-                for (uint32_t g = 0; g < 8; ++g)
-                    *reinterpret_cast<uint4 *>(A2 + m * 128 + (g << 4)) = make_uint4(0, 0, 0, 0);
+                    for (uint32_t k = 0; k < 16; ++k) d2r[k] = (d2ok ? __uint_as_float(r16[k]) : 0.0f) + par[MT_PAR_B2 + v0 + k];
+                }
+                // the block's sequence words when they are given
+                uint32_t gw[2] = {0u, 0u};
+                if (given && valid) {
+                    gw[0] = seq[(size_t)(s0 >> 2) * buflen + n];
+                    if (s1 > s0 + 4) gw[1] = seq[(size_t)((s0 >> 2) + 1) * buflen + n];
+                }
+                *reinterpret_cast<uint4 *>(A2 + m * 128 + ((((2 * sl) ^ (m & 7)) & 7) << 4)) = make_uint4(0, 0, 0, 0);
+                *reinterpret_cast<uint4 *>(A2 + m * 128 + ((((2 * sl + 1) ^ (m & 7)) & 7) << 4)) =
+                    make_uint4(0, 0, 0, 0);
 
-                uint32_t gword = 0;
                 for (uint32_t i = s0; i < s1; ++i) {
                     const uint32_t il = i - s0;
-                    // logits of site i
+                    // this slice's share of the logits of site i
+                    {
+                        float act2[16];
+                        unpack8(*reinterpret_cast<const uint4 *>(A2 + m * 128 + ((((2 * sl) ^ (m & 7)) & 7) << 4)),
+                                act2);
+                        unpack8(*reinterpret_cast<const uint4 *>(A2 + m * 128 + ((((2 * sl + 1) ^ (m & 7)) & 7) << 4)),
+                                act2 + 8);
+                        float *rl = red_lg + (ph_lg & 1) * (Q * CT);
+#pragma unroll
+                        for (uint32_t a = 0; a < Q; ++a)
+                            rl[(a * SL + sl) * MT_M + m] = dot16(w3s + (il * Q + a) * MT_ROW_BYTES + 2 * v0, act2);
+                    }
                     float lg[Q];
                     if (b >= 1) {
                         tmem_ldq<Q>(tmem + lane_base + b * p.N3 + il * Q, lg);
@@ -513,17 +594,19 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
 #pragma unroll
                         for (uint32_t a = 0; a < Q; ++a) lg[a] = 0.0f;
                     }
+                    compute_sync<CT>();
                     {
-                        float act2[NU];
+                        const float *rl = red_lg + (ph_lg & 1) * (Q * CT);
 #pragma unroll
-                        for (uint32_t g = 0; g < NU / 8; ++g)
-                            unpack8(*reinterpret_cast<const uint4 *>(A2 + m * 128 + (((g ^ (m & 7)) & 7) << 4)),
-                                    &act2[8 * g]);
+                        for (uint32_t a = 0; a < Q; ++a) {
+                            float s = rl[(a * SL) * MT_M + m];
 #pragma unroll
-                        for (uint32_t a = 0; a < Q; ++a)
-                            lg[a] += __ldg(&p.b3[i * Q + a]) + dotn<NU>(w3s + (il * Q + a) * MT_ROW_BYTES, act2);
+                            for (uint32_t k = 1; k < SL; ++k) s += rl[(a * SL + k) * MT_M + m];
+                            lg[a] += par[MT_PAR_B3 + il * Q + a] + s;
+                        }
                     }
-                    // draw (or read) residue i
+                    ++ph_lg;
+                    // draw (or read) residue i: the same in every slice
                     float mx = lg[0];
 #pragma unroll
                     for (uint32_t a = 1; a < Q; ++a) mx = fmaxf(mx, lg[a]);
@@ -536,10 +619,8 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                     const float lse = mx + logf(se);
                     uint32_t r;
                     if (given) {
-                        if ((i & 3) == 0) {
-                            gword = valid ? seq[(size_t)(i >> 2) * buflen + n] : 0u;
-                            tmem_st1(tmem + lane_base + p.wcol + (i >> 2), gword);
-                        }
+                        const uint32_t gword = il < 4 ? gw[0] : gw[1];
+                        if ((i & 3) == 0) tmem_st1(tmem + lane_base + p.wcol + (i >> 2), gword);
                         r = min((gword >> (8 * (i & 3))) & 0xffu, Q - 1);
                     } else {
                         const float u = hash_uniform(seed, n, i) * se;
@@ -562,48 +643,57 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                     if (!given) {
                         cw |= r << (8 * (i & 3));
                         if ((i & 3) == 3 || i == L - 1) {
-                            if (valid) seq[(size_t)(i >> 2) * buflen + n] = cw;
+                            if (valid && sl == 0) seq[(size_t)(i >> 2) * buflen + n] = cw;
+                            // every slice writes the same word: each reads back its own
                             tmem_st1(tmem + lane_base + p.wcol + (i >> 2), cw);
                             cw = 0;
                         }
                     }
-                    // its input to the block's hidden-1 units
-                    add_h<NU>(w1s + (il * Q + r) * MT_ROW_BYTES, h1);
-                    // hidden-2 units of degree i + 1, four at a time
+                    // its input to this slice's hidden-1 units
+                    add16h(w1s + (il * Q + r) * MT_ROW_BYTES + 2 * v0, h1);
+                    // hidden-2 units of degree i + 1, HG per barrier
                     if (i + 1 < L) {
-                        const int32_t ulo = __ldg(&p.deg2_start[i + 1]) - (int32_t)c2;
-                        const int32_t uhi = __ldg(&p.deg2_start[i + 2]) - (int32_t)c2;
+                        const int32_t ulo = cnt[il], uhi = cnt[il + 1];
                         if (ulo < uhi) {
-                            float act1[NU];
+                            float act1[16];
 #pragma unroll
-                            for (uint32_t v = 0; v < NU; ++v) act1[v] = bf16r(fmaxf(h1[v], 0.0f));
-                            for (int32_t u0 = ulo; u0 < uhi; u0 += 4) {
-                                uint32_t uk[4];
+                            for (uint32_t k = 0; k < 16; ++k) act1[k] = bf16r(fmaxf(h1[k], 0.0f));
+                            for (int32_t u0 = ulo; u0 < uhi; u0 += HG) {
+                                float *rh = red_h2 + (ph_h2 & 1) * (HG * CT);
 #pragma unroll
-                                for (uint32_t k = 0; k < 4; ++k) uk[k] = (uint32_t)min(u0 + (int32_t)k, uhi - 1);
-                                float d2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                                if (d2ok) {
-                                    const uint32_t tb = tmem + lane_base + p.d2col;
-                                    tmem_ld1x4(tb + uk[0], tb + uk[1], tb + uk[2], tb + uk[3], d2);
+                                for (uint32_t k = 0; k < HG; ++k) {
+                                    const uint32_t uk = (uint32_t)min(u0 + (int32_t)k, uhi - 1);
+                                    rh[(k * SL + sl) * MT_M + m] = dot16(w2s + uk * MT_ROW_BYTES + 2 * v0, act1);
                                 }
+                                compute_sync<CT>();
 #pragma unroll
-                                for (uint32_t k = 0; k < 4; ++k) {
-                                    const float z = (d2[k] + __ldg(&p.b2b[b * MT_NU + uk[k]])) +
-                                                    dotn<NU>(w2s + uk[k] * MT_ROW_BYTES, act1);
-                                    if (u0 + (int32_t)k < uhi)
-                                        *reinterpret_cast<unsigned short *>(A2 + mt_sw(m, uk[k])) =
+                                for (uint32_t k = 0; k < HG; ++k) {
+                                    const int32_t u = u0 + (int32_t)k;
+                                    // the slice that owns unit u finishes it
+                                    if (u < uhi && (uint32_t)u / 16 == sl) {
+                                        const uint32_t ul = (uint32_t)u - v0;
+                                        float d2 = d2r[0];
+#pragma unroll
+                                        for (uint32_t e = 1; e < 16; ++e) d2 = (ul == e) ? d2r[e] : d2;
+                                        float s = rh[(k * SL) * MT_M + m];
+#pragma unroll
+                                        for (uint32_t e = 1; e < SL; ++e) s += rh[(k * SL + e) * MT_M + m];
+                                        const float z = d2 + s;
+                                        *reinterpret_cast<unsigned short *>(A2 + mt_sw(m, (uint32_t)u)) =
                                             __bfloat16_as_ushort(__float2bfloat16_rn(fmaxf(z, 0.0f)));
+                                    }
                                 }
+                                ++ph_h2;
                             }
                         }
                     }
                 }
                 mbar_arrive(&wempty[s23]);
-                // the block's hidden-1 units are final: into A1 for later blocks
+                // this slice's hidden-1 units are final: into A1 for later blocks
+                if (v0 < n1) {
 #pragma unroll
-                for (uint32_t g = 0; g < NU / 8; ++g) {
-                    if (8 * g < n1) {
-                        const uint32_t k = c1 + 8 * g;
+                    for (uint32_t g = 0; g < 2; ++g) {
+                        const uint32_t k = c1 + v0 + 8 * g;
                         uint4 w;
                         w.x = pack_bf16x2(fmaxf(h1[8 * g], 0.0f), fmaxf(h1[8 * g + 1], 0.0f));
                         w.y = pack_bf16x2(fmaxf(h1[8 * g + 2], 0.0f), fmaxf(h1[8 * g + 3], 0.0f));
@@ -616,12 +706,12 @@ __global__ void __launch_bounds__(MT_THREADS, 1)
                 tc_fence_before();
                 mbar_arrive(bar_a2);
             }
-            if (ok && valid) logq[n] = lq;
+            if (ok && valid && sl == 0) logq[n] = lq;
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 4) {
+    if (warp == W_MMA) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(MT_TMEM_COLS));
     }
@@ -655,7 +745,9 @@ __global__ void k_made_tc_images(const MtPlan p, unsigned char *img, const float
 // FP32, and per block W2 [48][48], W3 [G q][48] and the layer-1 rows of the
 // block's own sites [G q][48] in bf16.
 __global__ void k_made_tc_wimages(const MtPlan p, unsigned char *wimg, const float *__restrict__ W1T,
-                                  const float *__restrict__ W2, const float *__restrict__ W3) {
+                                  const float *__restrict__ W2, const float *__restrict__ W3,
+                                  const float *__restrict__ b1, const float *__restrict__ b2,
+                                  const float *__restrict__ b3) {
     const MtWOp op = p.wops[blockIdx.x];
     const uint32_t *bk = p.blk + op.blk * MT_BLK;
     const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], n2 = bk[3];
@@ -672,7 +764,23 @@ __global__ void k_made_tc_wimages(const MtPlan p, unsigned char *wimg, const flo
     }
     unsigned short *out = reinterpret_cast<unsigned short *>(wimg + op.off);
     const uint32_t s0 = op.blk * G;
-    for (uint32_t e = threadIdx.x; e < op.bytes / 2; e += blockDim.x) {
+    float *par = reinterpret_cast<float *>(wimg + op.off + MT_PAR_OFF);
+    for (uint32_t e = threadIdx.x; e < MT_PAR_CNT + 16; e += blockDim.x) {
+        if (e < MT_PAR_B2) {  // b3 of the block's sites
+            const uint32_t i = s0 + e / q;
+            par[e] = (e < G * q && i < L) ? b3[s0 * q + e] : 0.0f;
+        } else if (e < MT_PAR_B1) {
+            const uint32_t u = e - MT_PAR_B2;
+            par[e] = u < n2 ? b2[c2 + u] : 0.0f;
+        } else if (e < MT_PAR_CNT) {
+            const uint32_t v = e - MT_PAR_B1;
+            par[e] = v < n1 ? b1[c1 + v] : 0.0f;
+        } else {
+            const uint32_t d = min(L, s0 + 1 + (e - MT_PAR_CNT));
+            reinterpret_cast<int32_t *>(par)[e] = p.deg2_start[d] - (int32_t)c2;
+        }
+    }
+    for (uint32_t e = threadIdx.x; e < MT_PAR_OFF / 2; e += blockDim.x) {
         const uint32_t r = e / MT_NU, x = e % MT_NU;
         float v = 0.0f;
         if (r < MT_NU) {
@@ -736,7 +844,7 @@ static MtLayout mt_layout(uint32_t L, uint32_t q, uint32_t nb, size_t nops, size
 
 // The host-side plan: block table, op lists and image sizes, or an error text.
 struct MtHostPlan {
-    uint32_t nb = 0, N3 = 0, d2col = 0, wcol = 0, nu = 32;
+    uint32_t nb = 0, N3 = 0, d2col = 0, wcol = 0, nu = 16;
     std::vector<uint32_t> blk;
     std::vector<MtOp> ops;
     std::vector<MtWOp> wops;
@@ -899,7 +1007,7 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
         k_made_tc_images<<<p.nops, 256, 0, st>>>(p, ws + lay.img, W2, W3);
         if ((rc = check_launch("mi3_made_tc_prepare: images"))) return rc;
     }
-    k_made_tc_wimages<<<p.nwops, 256, 0, st>>>(p, ws + lay.wimg, W1T, W2, W3);
+    k_made_tc_wimages<<<p.nwops, 256, 0, st>>>(p, ws + lay.wimg, W1T, W2, W3, b1, b2, b3);
     if ((rc = check_launch("mi3_made_tc_prepare: weight stages"))) return rc;
     k_made_tc_bias<<<32, 256, 0, st>>>(p, reinterpret_cast<float *>(ws + lay.b1b),
                                        reinterpret_cast<float *>(ws + lay.b2b), reinterpret_cast<float *>(ws + lay.b3),
@@ -925,14 +1033,25 @@ extern "C" int mi3_made_tc_sample(const uint64_t *plan, uint32_t *seq, uint32_t 
     const uint32_t ntiles = (nseq + MT_M - 1) / MT_M;
     const uint32_t grid = std::min<uint32_t>(ntiles, (uint32_t)nsm);
     cudaStream_t st = as_stream(stream);
-    // the kernel holds 32 or 48 units per block and layer in registers
-    auto launch = [&](auto kern) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MT_SMEM);
-        kern<<<grid, MT_THREADS, MT_SMEM, st>>>(p, seq, buflen, nseq, logq, seed, given, status);
+    // 1, 2 or 3 unit slices per walker for 16, 32 or 48 units per block and layer
+    auto launch = [&](auto kern, uint32_t threads, uint32_t smem) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, threads, smem, st>>>(p, seq, buflen, nseq, logq, seed, given, status);
     };
-    if (p.q == 4)
-        p.nu <= 32 ? launch(k_made_tc<4, 32>) : launch(k_made_tc<4, 48>);
-    else
-        p.nu <= 32 ? launch(k_made_tc<8, 32>) : launch(k_made_tc<8, 48>);
+    if (p.q == 4) {
+        if (p.nu <= 16)
+            launch(k_made_tc<4, 16>, MtShape<4, 16>::THREADS, MtShape<4, 16>::SMEM);
+        else if (p.nu <= 32)
+            launch(k_made_tc<4, 32>, MtShape<4, 32>::THREADS, MtShape<4, 32>::SMEM);
+        else
+            launch(k_made_tc<4, 48>, MtShape<4, 48>::THREADS, MtShape<4, 48>::SMEM);
+    } else {
+        if (p.nu <= 16)
+            launch(k_made_tc<8, 16>, MtShape<8, 16>::THREADS, MtShape<8, 16>::SMEM);
+        else if (p.nu <= 32)
+            launch(k_made_tc<8, 32>, MtShape<8, 32>::THREADS, MtShape<8, 32>::SMEM);
+        else
+            launch(k_made_tc<8, 48>, MtShape<8, 48>::THREADS, MtShape<8, 48>::SMEM);
+    }
     return check_launch("mi3_made_tc_sample");
 }

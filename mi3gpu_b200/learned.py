@@ -67,11 +67,14 @@ TC_TMEM_COLS, TC_MAX_UNITS = 512, 48
 
 
 def tc_block_size(L, q, H):
-    """The largest block size G (4 or 8, G q <= 32) with which the
-    tensor-core sampler can run this network, or None: the logits of all
-    blocks (ceil(L/G) x roundup(G q, 16) columns), one block's layer-2
+    """The block size G (4 or 8, G q <= 32) with which the tensor-core
+    sampler runs this network, or None.  The logits of all blocks
+    (ceil(L/G) x roundup(G q, 16) columns), one block's layer-2
     accumulator and the walkers' sequence words (ceil(L/4) columns) must
-    fit the 512 tensor-memory columns."""
+    fit the 512 tensor-memory columns.  The larger block is preferred: at
+    L=99, q=4 both run equally fast (4 sites: 32-unit blocks, twice as many
+    block boundaries), and the 8-site blocking trained the better proposal
+    at H=256."""
     if q not in (4, 8) or H % 16 or H > 512 or L < 2:
         return None
     for G in (8, 4):
