@@ -796,7 +796,7 @@ def energy_autocorr(Es):
     return rho, tau
 
 
-def run_learned(args, L=99, q=4, N=1 << 18, equil_sweeps=1024, track=64, epochs=16, every=4):
+def run_learned(args, L=99, q=4, N=1 << 18, equil_sweeps=1024, track=64):
     """Learned independence proposal at L=99, q=4 with strong contacts
     (sigma 0.8): train the MADE on 2^18 equilibrated walkers, then track
     the energy autocorrelation over `track` sampler calls of one sweep each,
@@ -806,7 +806,7 @@ def run_learned(args, L=99, q=4, N=1 << 18, equil_sweeps=1024, track=64, epochs=
     from mi3gpu_b200.potts import synthetic_ground_truth
     from mi3gpu_b200.learned import MadeProposal, LearnedSampler
     from mi3gpu_b200._lib import call as _lib_call, query as _lib_query
-    H = args.hidden
+    H, epochs, every = args.hidden, args.made_epochs, args.made_every
     J = synthetic_ground_truth(L, q, seed=1003, contact_sigma=0.8)
     g = MCMCGPU((0, 0), L, q, N, 512, None, 1024, args.seed + 1)
     gpus = GPU_node([g])
@@ -1117,6 +1117,8 @@ def main():
     ap.add_argument("--forms", default="", help="comma list of forms for --mode inference (default: all)")
     ap.add_argument("--shape", default="", help="L,q,N: one shape for --mode kernels")
     ap.add_argument("--hidden", type=int, default=512, help="MADE hidden units (--mode learned / made)")
+    ap.add_argument("--made-epochs", type=int, default=16, help="MADE training epochs (--mode learned)")
+    ap.add_argument("--made-every", type=int, default=4, help="sweeps per proposal step (--mode learned)")
     args = ap.parse_args()
     rank, world, _ = env_rank()
 
