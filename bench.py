@@ -1117,7 +1117,7 @@ def main():
     ap.add_argument("--forms", default="", help="comma list of forms for --mode inference (default: all)")
     ap.add_argument("--shape", default="", help="L,q,N: one shape for --mode kernels")
     ap.add_argument("--hidden", type=int, default=512, help="MADE hidden units (--mode learned / made)")
-    ap.add_argument("--made-epochs", type=int, default=16, help="MADE training epochs (--mode learned)")
+    ap.add_argument("--made-epochs", type=int, default=48, help="MADE training epochs (--mode learned)")
     ap.add_argument("--made-every", type=int, default=4, help="sweeps per proposal step (--mode learned)")
     args = ap.parse_args()
     rank, world, _ = env_rank()
