@@ -219,6 +219,97 @@ __global__ void __launch_bounds__(256) k_reg_lz_rows(const float *__restrict__ b
     }
 }
 
+// reg_l1z / reg_l2z with q known at compile time: lane a holds row a and
+// column a of the block in registers and runs the odd-aware tree of
+// zeroGauge on them (level m -> (m+1)/2: element b gets b + m' for
+// b < m' - odd), fully unrolled -- the same additions of the same operands
+// as k_reg_lz / k_reg_lz_rows, so the sums are bit-identical; the mean is
+// the same tree over the column sums, gathered by shuffles.  The block
+// (J + dJ) and dJ are staged in shared memory by coalesced loads.
+template <uint32_t Q>
+__device__ __forceinline__ float tree_reg(float (&w)[Q]) {
+    uint32_t m = Q;
+#pragma unroll
+    for (int lev = 0; lev < 8; ++lev) {
+        if (m > 1) {
+            const uint32_t odd = m & 1;
+            m = (m + 1) >> 1;
+#pragma unroll
+            for (uint32_t b = 0; b < Q; ++b)
+                if (b + odd < m && b + m < Q) w[b] = w[b] + w[b + m];
+        }
+    }
+    return w[0];
+}
+
+template <bool L2, uint32_t Q>
+__global__ void __launch_bounds__(256) k_reg_lz_q(const float *__restrict__ bi, float gamma, float pc, float lJ,
+                                                  const float *__restrict__ J, float *__restrict__ dJ,
+                                                  uint64_t npairs) {
+    constexpr uint32_t QQ = Q * Q, PER = (QQ + 31) / 32;
+    __shared__ float xs[8][QQ + 1], ds[8][QQ + 1];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const float fq = (float)Q;
+    float *x = xs[warp], *d = ds[warp];
+    for (uint64_t p = (uint64_t)blockIdx.x * 8 + warp; p < npairs; p += (uint64_t)gridDim.x * 8) {
+        const float *Jb = J + p * QQ;
+        float *dJb = dJ + p * QQ;
+        const float *bb = bi + p * QQ;
+        float jv[PER], dv[PER];
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t li = lane + 32 * k;
+            if (li < QQ) {
+                dv[k] = dJb[li];
+                jv[k] = Jb[li];
+            }
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t li = lane + 32 * k;
+            if (li < QQ) {
+                x[li] = jv[k] + dv[k];
+                d[li] = dv[k];
+            }
+        }
+        __syncwarp();
+        float rsum = 0.0f, csum = 0.0f;
+        if (lane < Q) {
+            float w[Q];
+#pragma unroll
+            for (uint32_t b = 0; b < Q; ++b) w[b] = x[lane * Q + b];
+            rsum = tree_reg<Q>(w);
+#pragma unroll
+            for (uint32_t a = 0; a < Q; ++a) w[a] = x[a * Q + lane];
+            csum = tree_reg<Q>(w);
+        }
+        float cs[Q];
+#pragma unroll
+        for (uint32_t b = 0; b < Q; ++b) cs[b] = __shfl_sync(0xffffffffu, csum, b);
+        const float mean = tree_reg<Q>(cs) / fq / fq;
+        const float hi = rsum / fq - mean, hj = csum / fq - mean;
+#pragma unroll
+        for (uint32_t k = 0; k < PER; ++k) {
+            const uint32_t li = lane + 32 * k;
+            const uint32_t lc = li < QQ ? li : QQ - 1;
+            const uint32_t a = lc / Q, b = lc - a * Q;
+            const float ha = __shfl_sync(0xffffffffu, hi, a), hb = __shfl_sync(0xffffffffu, hj, b);
+            if (li < QQ) {
+                const float J0 = x[li] - (ha + hb) - mean;
+                const float bv = bb[li];
+                float R;
+                if (L2) R = -lJ * J0 * gamma / (bv + pc);
+                else R = -lJ * ocl_sign(J0) * gamma / (bv + pc);
+                float Jp = d[li];
+                if (ocl_sign(J0) != ocl_sign(J0 + R)) Jp = Jp - J0;
+                else Jp = Jp + R;
+                dJb[li] = Jp;
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------ reductions
 // Workspace: [ticket counter (uint32, padded to 16 B)][partials: NBLK x 4 doubles]
 constexpr uint32_t RED_BLOCKS = 296;
@@ -407,6 +498,15 @@ static int reg_lz(bool l2, const float *bi, float gamma, float pc, float lJ, con
     if (L < 2 || q < 1 || q * q > 4096) return fail(MI3_ERR_ARG, std::string(name) + ": bad L/q");
     uint64_t np = npairs_of(L);
     uint32_t tb = 256;
+    if (q == 21 || q == 4) {  // the protein and nucleotide alphabets, q fixed at compile time
+        using K = void (*)(const float *, float, float, float, const float *, float *, uint64_t);
+        K k;
+        if (q == 21) k = l2 ? (K)k_reg_lz_q<true, 21> : (K)k_reg_lz_q<false, 21>;
+        else k = l2 ? (K)k_reg_lz_q<true, 4> : (K)k_reg_lz_q<false, 4>;
+        const uint32_t grid = (uint32_t)std::min<uint64_t>((np + 7) / 8, 148 * 32);
+        k<<<grid, tb, 0, as_stream(stream)>>>(bi, gamma, pc, lJ, J, dJ, np);
+        return check_launch(name);
+    }
     if (q * q <= 512) {  // up to 16 cells per lane (q <= 22); larger blocks use the generic kernel
         using K = void (*)(const float *, float, float, float, const float *, float *, uint64_t, uint32_t);
         const uint32_t per = (q * q + 31) / 32;
