@@ -581,6 +581,27 @@ int mi3_capture_while_begin(void *stream, void *body_stream, unsigned long long 
 /* End the body capture begun by mi3_capture_while_begin. */
 int mi3_capture_while_end(void *body_stream);
 
+/* A conditional handle of the graph `stream` is capturing into, reset to
+ * `value` (0 or 1) at every launch.  No counterpart in the reference. */
+int mi3_cond_handle_create(void *stream, uint32_t value, unsigned long long *handle_out);
+
+/* At the current capture position of `stream`, a conditional IF node on
+ * `handle`: its body (captured on body_stream until mi3_capture_if_end)
+ * runs once when the handle is non-zero at that point of the launch. */
+int mi3_capture_if_begin(void *stream, void *body_stream, unsigned long long handle);
+int mi3_capture_if_end(void *body_stream);
+
+/* One checkpoint of runMCMC's automatic equilibration (NewtonSteps.py:
+ * 395-442) inside a graph: with test set, equilibrated when |*r1| and
+ * |*r2| (Spearman r against one and two checkpoints back, from
+ * mi3_rank_corr) are below rcrit (p > 0.02) and calls >= min_equil; the
+ * next checkpoint's IF handle (has_next) is set to 1 unless equilibrated
+ * or calls >= max_equil.  out (uint32 x 2, device) = {calls, verdict: 1
+ * equilibrated, 2 stopped at max_equil, 0 going on}. */
+int mi3_equil_control(unsigned long long next, int32_t has_next, const double *r1, const double *r2,
+                      double rcrit, int32_t test, uint32_t calls, uint32_t min_equil, uint32_t max_equil,
+                      uint32_t *out, void *stream);
+
 /* End-of-step control of a captured Newton loop (NewtonSteps.py:234-246):
  * ++*count; *ref = *minout (the next step's reference energy); the loop
  * continues while Neff = s^2/s2 (wstats64 = {s, s2}) >= neff_min and

@@ -93,6 +93,11 @@ SIGNATURES = {
     "mi3_made_round_bf16": (c.c_int, [_vp, _vp, _vp, _u64, _vp]),
     "mi3_made_sample": (c.c_int, [_u32, _u32, _u32] + [_vp] * 8 + [_vp, _u32, _u32, _vp, _u64, c.c_int32, _vp]),
     "mi3_mh_independence": (c.c_int, [_vp, _vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp, _u64, _vp, _vp]),
+    "mi3_cond_handle_create": (c.c_int, [_vp, _u32, c.POINTER(c.c_ulonglong)]),
+    "mi3_capture_if_begin": (c.c_int, [_vp, _vp, c.c_ulonglong]),
+    "mi3_capture_if_end": (c.c_int, [_vp]),
+    "mi3_equil_control": (c.c_int, [c.c_ulonglong, c.c_int32, _vp, _vp, c.c_double, c.c_int32, _u32, _u32, _u32,
+                                    _vp, _vp]),
     "mi3_made_gemm_workspace": (_u64, [_u32, _u32, _u32, _u32]),
     "mi3_made_forward_tc": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _u32, _u32] + [_vp] * 12 + [_vp, _u64, _vp, _vp]),
     "mi3_made_backward_tc": (c.c_int, [_vp, _u32, _u32, _u32, _u32, _u32, _u32] + [_vp] * 21 + [_vp, _u64, _vp, _vp]),

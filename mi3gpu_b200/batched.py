@@ -10,6 +10,15 @@ kernel sets from the FP64 weight sums after each step (the host loop's stop
 rule, NewtonSteps.py:217-246).  A round is then one graph launch plus one
 small read of the per-problem statistics.
 
+With equil=dict(min_equil=..., max_equil=...) the sampling phase
+equilibrates by itself, as runMCMC's equiltime='auto' does
+(NewtonSteps.py:395-442): 8 sampler calls, then checkpoints after 8, 16,
+32, ... more; at each one the walkers' energies are ranked and correlated
+with the two previous checkpoints on the device (mi3_rank_average,
+mi3_rank_corr), and each later checkpoint is a conditional IF node that
+the previous one opens unless both correlations have p > 0.02 (after at
+least min_equil calls) or max_equil calls have run (mi3_equil_control).
+
 Kernel schedules are autotuned per shape (autotune.Autotuner): the sampler's
 tile plan and the count kernel.  With the same seeds a problem follows the
 same trajectory as the host-driven device-resident loop
@@ -29,6 +38,19 @@ import torch
 
 from . import _lib, potts
 from .mcmcGPU import MCMCGPU, rng_buf_mul
+
+
+def equil_schedule(max_equil):
+    """(first call, calls) of each checkpoint of runMCMC's equilibration
+    (NewtonSteps.py:395-442) after its first 8 calls: 8, 16, 32, ... more,
+    until max_equil calls are reached."""
+    out, calls, loops = [], 8, 8
+    while True:
+        out.append((calls, loops))
+        calls += loops
+        if calls >= max_equil:
+            return out
+        loops *= 2
 
 
 class Problem:
@@ -66,6 +88,16 @@ class Problem:
         self.cap_stream = _new_stream(dev)
         self.body_stream = _new_stream(dev)
         self.history = []
+
+    def position_state(self):
+        """The state of the position-list stream (for rewinding it)."""
+        buf = getattr(self, '_posbuf', None)
+        return (self.gpu.rngstate.get_state(), self.gpu.randpos_offset, None if buf is None else buf.copy())
+
+    def set_position_state(self, state):
+        self.gpu.rngstate.set_state(state[0])
+        self.gpu.randpos_offset = state[1]
+        self._posbuf = state[2]
 
     def round_positions(self, ncalls):
         """The sites of the next `ncalls` sampler calls, drawn exactly as
@@ -106,9 +138,17 @@ class BatchedRounds:
     sweeps / sweeps_first: sweeps per round after / in the first round."""
 
     def __init__(self, problems, gamma=4e-4, damping=1e-3, lJ=2e-4, newton_max=1024, frac_neff=0.9,
-                 sweeps=16, sweeps_first=128, reseed='none', tuner=None, device=0, ns_delta=32):
+                 sweeps=16, sweeps_first=128, reseed='none', tuner=None, device=0, ns_delta=32, equil=None):
+        """equil: None (fixed sweeps per round) or dict(min_equil=64,
+        max_equil=...) -- sampler calls of each problem's nsteps steps --
+        for the equilibration test inside the graph."""
         if reseed not in ('none', 'independent'):
             raise ValueError("reseed must be 'none' or 'independent'")
+        self.equil = None
+        if equil is not None:
+            self.equil = dict(min_equil=int(equil.get('min_equil', 64)), max_equil=int(equil.get('max_equil', 1024)))
+            if self.equil['max_equil'] < 16:
+                raise ValueError("max_equil must allow the first checkpoint (16 calls)")
         self.problems = list(problems)
         self.gamma, self.damping, self.lJ = float(gamma), float(damping), float(lJ)
         self.newton_max, self.frac, self.ns_delta = int(newton_max), float(frac_neff), int(ns_delta)
@@ -125,8 +165,10 @@ class BatchedRounds:
             pr.ctl['budget'].fill_(self.newton_max)
             # the round's site list, sized for the longer round: graphs keep
             # its address, so it is never reallocated
-            n = max(self._ncalls(pr, self.sweeps), self._ncalls(pr, self.sweeps_first)) * pr.nsteps
+            n = max(self._ncalls(pr, self.sweeps), self._ncalls(pr, self.sweeps_first), self._max_calls()) * pr.nsteps
             pr.randpos_round = torch.zeros(n, dtype=torch.int32, device=pr.gpu.device)
+            if self.equil:
+                self._equil_buffers(pr)
         torch.cuda.synchronize(self.device)
         self.graphs = {}
         self.rounds_done = 0
@@ -134,6 +176,69 @@ class BatchedRounds:
     # ------------------------------------------------------------ capture
     def _ncalls(self, pr, sweeps):
         return max(1, sweeps * pr.L // pr.nsteps)
+
+    def _schedule(self):
+        return equil_schedule(self.equil['max_equil'])
+
+    def _max_calls(self):
+        if not self.equil:
+            return 0
+        c0, n = self._schedule()[-1]
+        return c0 + n
+
+    def _equil_buffers(self, pr):
+        from scipy.stats import t as student_t
+        g, N = pr.gpu, pr.N
+        J = len(self._schedule())
+        dev = g.device
+        pr.ctl['ranks'] = torch.zeros((J, N), dtype=torch.float32, device=dev)
+        pr.ctl['rank r'] = torch.zeros((J, 2), dtype=torch.float64, device=dev)
+        pr.ctl['equil out'] = torch.zeros(2, dtype=torch.int32, device=dev)
+        self._ws(g, 'ws rank', 'mi3_rank_workspace', N)
+        self._ws(g, 'ws corr', 'mi3_rank_corr_workspace')
+        tc = float(student_t.isf(0.02 / 2, N - 2))
+        pr.rcrit = tc / np.sqrt(N - 2 + tc * tc)  # |r| < rcrit  <=>  p > 0.02
+
+    def _capture_sampling(self, pr, s, bs):
+        """The equilibrating sampling phase of one problem (see the module
+        docstring); `s` is the problem's capture stream, `bs` the stream its
+        IF bodies are captured on."""
+        g, b, c, N, L, q = pr.gpu, pr.gpu.bufs, pr.ctl, pr.N, pr.L, pr.q
+        call = _lib.call
+        sched = self._schedule()
+        for k in range(8):
+            g.sampler_call(k * pr.nsteps, _p(pr.randpos_round), pr.nsteps, _p(b['seq main']), _p(b['rngstates']),
+                           _p(b['status']), s)
+        handles = [None]
+        for _ in range(1, len(sched)):
+            h = ctypes.c_ulonglong(0)
+            call('mi3_cond_handle_create', s, 0, ctypes.byref(h))
+            handles.append(h.value)
+        ranks, rr = c['ranks'], c['rank r']
+        wr, wc = self._ws(g, 'ws rank', 'mi3_rank_workspace', N), self._ws(g, 'ws corr', 'mi3_rank_corr_workspace')
+        for j, (c0, loops) in enumerate(sched):
+            st = s
+            if j > 0:
+                call('mi3_capture_if_begin', s, bs, handles[j])
+                st = bs
+            for k in range(loops):
+                g.sampler_call((c0 + k) * pr.nsteps, _p(pr.randpos_round), pr.nsteps, _p(b['seq main']),
+                               _p(b['rngstates']), _p(b['status']), st)
+            call('mi3_energies', _p(b['J']), _p(b['seq main']), N, N, _p(b['E main']), L, q, _p(b['ws energies']),
+                 g._wsbytes('ws energies'), st)
+            call('mi3_rank_average', _p(b['E main']), N, ranks[j].data_ptr(), *wr, st)
+            test = j >= 2
+            if test:
+                call('mi3_rank_corr', ranks[j].data_ptr(), ranks[j - 1].data_ptr(), N, rr[j].data_ptr(), *wc, st)
+                call('mi3_rank_corr', ranks[j].data_ptr(), ranks[j - 2].data_ptr(), N, rr[j].data_ptr() + 8, *wc,
+                     st)
+            has_next = j + 1 < len(sched)
+            call('mi3_equil_control', handles[j + 1] if has_next else 0, 1 if has_next else 0,
+                 rr[j].data_ptr() if test else None, rr[j].data_ptr() + 8 if test else None, pr.rcrit,
+                 1 if test else 0, c0 + loops, self.equil['min_equil'], self.equil['max_equil'],
+                 _p(c['equil out']), st)
+            if j > 0:
+                call('mi3_capture_if_end', bs)
 
     def _capture_problem(self, pr, ncalls):
         g, s, L, q, N = pr.gpu, pr.cap_stream.cuda_stream, pr.L, pr.q, pr.N
@@ -146,9 +251,12 @@ class BatchedRounds:
         g.unpack_call(s)
         if self.reseed == 'independent':
             call('mi3_gen_indep', _p(b['seq main']), N, N, _p(b['rngstates']), _p(b['cprob']), L, q, s)
-        for k in range(ncalls):
-            g.sampler_call(k * pr.nsteps, _p(pr.randpos_round), pr.nsteps, _p(b['seq main']), _p(b['rngstates']),
-                           _p(b['status']), s)
+        if self.equil:
+            self._capture_sampling(pr, s, pr.body_stream.cuda_stream)
+        else:
+            for k in range(ncalls):
+                g.sampler_call(k * pr.nsteps, _p(pr.randpos_round), pr.nsteps, _p(b['seq main']), _p(b['rngstates']),
+                               _p(b['status']), s)
         tensor = (getattr(g, 'count_kernel', None) == 'tc') if getattr(g, 'count_kernel', None) else \
             q in g.TENSOR_COUNT_Q
         if tensor:
@@ -235,11 +343,18 @@ class BatchedRounds:
     def run_round(self):
         """One round of every problem; returns the per-problem records."""
         first = self.rounds_done == 0
-        key = 'first' if first else 'next'
+        key = 'equil' if self.equil else ('first' if first else 'next')
         sweeps = self.sweeps_first if first else self.sweeps
         exec_ = self.graphs[key][1] if key in self.graphs else self._build(key, sweeps)
+        states = {}
         for pr in self.problems:
-            pos = pr.round_positions(self._ncalls(pr, sweeps))
+            if self.equil:
+                # positions for the longest equilibration; the stream is
+                # rewound to the calls actually made after the round
+                states[id(pr)] = pr.position_state()
+                pos = pr.round_positions(self._max_calls())
+            else:
+                pos = pr.round_positions(self._ncalls(pr, sweeps))
             pr.randpos_round[:pos.size].copy_(torch.from_numpy(pos.view(np.int32)))
         torch.cuda.synchronize(self.device)
         t0 = time.perf_counter()
@@ -259,14 +374,23 @@ class BatchedRounds:
             pr.gpu._check_status()
             if stopped == 2:
                 raise RuntimeError("Error: Divergence. Decrease gamma or increase pc-damping")
+            calls = self._ncalls(pr, sweeps)
             rec = dict(run=f"run_{self.rounds_done:02d}", ssr=float(pre[0]), predicted_ssr=float(post[0]),
-                       newton_steps=count - 1, mcmc_calls=self._ncalls(pr, sweeps))
+                       newton_steps=count - 1, mcmc_calls=calls)
+            if self.equil:
+                used, verdict = (int(x) for x in pr.ctl['equil out'].cpu().numpy())
+                rec.update(mcmc_calls=used, equilibrated=verdict == 1)
+                pr.set_position_state(states[id(pr)])
+                pr.round_positions(used)
             pr.history.append(rec)
             recs.append(rec)
         self.rounds_done += 1
         return dict(gpu_ms=gpu_ms, wall_s=wall, problems=recs)
 
     def site_updates_per_round(self, first=False):
+        """Site updates of a round (with equil: of the last round run)."""
+        if self.equil:
+            return sum(pr.history[-1]['mcmc_calls'] * pr.nsteps * pr.N for pr in self.problems if pr.history)
         sweeps = self.sweeps_first if first else self.sweeps
         return sum(self._ncalls(pr, sweeps) * pr.nsteps * pr.N for pr in self.problems)
 

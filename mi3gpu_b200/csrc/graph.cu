@@ -8,7 +8,10 @@
 // from the FP64 weight sums, with the same stop rule as the host loop of
 // NewtonSteps.iterNewton (NewtonSteps.py:217-246): stop after the step whose
 // effective sample size falls below frac * N0, or after max_steps steps.
-// The step counter bounds the loop, so a body always terminates.
+// The step counter bounds the loop, so a body always terminates.  The
+// sampling phase can equilibrate on the device too: each checkpoint of the
+// doubling schedule is a conditional IF node opened by the previous
+// checkpoint's rank-correlation test (k_equil_control).
 #include "common.cuh"
 
 namespace mi3 {
@@ -49,6 +52,27 @@ __global__ void k_newton_adapt(uint32_t after, const double *__restrict__ stats,
         const uint32_t steps = *count > 0 ? *count - 1 : 0;  // the reference's returned step index
         *budget = min(2048u, steps + delta);
     }
+}
+
+// After a checkpoint of the sampling phase (runMCMC's automatic
+// equilibration, NewtonSteps.py:395-442, in the device's rank form):
+// equilibrated when both rank correlations (last checkpoint against one
+// and two checkpoints back) have p > 0.02, i.e. |r| < rcrit, and at least
+// min_equil calls ran; stop at max_equil calls.  Opens the next checkpoint's
+// IF node when neither holds (has_next), and records {calls, verdict}:
+// verdict 1 equilibrated, 2 stopped at max_equil, 0 going on.  One thread.
+__global__ void k_equil_control(cudaGraphConditionalHandle next, int has_next, const double *__restrict__ r1,
+                                const double *__restrict__ r2, double rcrit, int test, uint32_t calls,
+                                uint32_t min_equil, uint32_t max_equil, uint32_t *out) {
+    bool eq = false;
+    if (test) {
+        const double a = fabs(*r1), b = fabs(*r2);
+        eq = a < rcrit && b < rcrit && calls >= min_equil;  // false for NaN
+    }
+    const bool more = !eq && calls < max_equil;
+    out[0] = calls;
+    out[1] = eq ? 1u : (more ? 0u : 2u);
+    if (has_next) cudaGraphSetConditional(next, more ? 1u : 0u);
 }
 
 }  // namespace mi3
@@ -93,12 +117,10 @@ extern "C" int mi3_graph_destroy(void *graph, void *exec) {
     return check_launch("mi3_graph_destroy");
 }
 
-// At the current capture position of `stream`, add a conditional WHILE node
-// (condition 1 at every graph launch) and begin capturing its body on
-// `body_stream`; everything issued on body_stream until mi3_capture_while_end
-// forms one iteration.  `stream` continues after the node.
-extern "C" int mi3_capture_while_begin(void *stream, void *body_stream, unsigned long long *handle_out) {
-    if (!handle_out || stream == body_stream) return fail(MI3_ERR_ARG, "mi3_capture_while_begin: bad arguments");
+// At the current capture position of `stream`, add a conditional node of
+// `type` driven by handle h and begin capturing its body on `body_stream`.
+static int capture_cond_begin(void *stream, void *body_stream, cudaGraphConditionalNodeType type,
+                              cudaGraphConditionalHandle h, const char *name) {
     cudaStream_t st = as_stream(stream);
     cudaStreamCaptureStatus cs;
     cudaGraph_t graph = nullptr;
@@ -106,30 +128,78 @@ extern "C" int mi3_capture_while_begin(void *stream, void *body_stream, unsigned
     size_t ndeps = 0;
     cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
     if (e != cudaSuccess || cs != cudaStreamCaptureStatusActive)
-        return fail(MI3_ERR_CUDA, "mi3_capture_while_begin: stream is not capturing");
-    cudaGraphConditionalHandle h;
-    e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
-    if (e != cudaSuccess)
-        return fail(MI3_ERR_CUDA, std::string("mi3_capture_while_begin: handle: ") + cudaGetErrorString(e));
+        return fail(MI3_ERR_CUDA, std::string(name) + ": stream is not capturing");
     cudaGraphNodeParams params = {};
     params.type = cudaGraphNodeTypeConditional;
     params.conditional.handle = h;
-    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.type = type;
     params.conditional.size = 1;
     cudaGraphNode_t node;
     e = cudaGraphAddNode(&node, graph, deps, ndeps, &params);
-    if (e != cudaSuccess)
-        return fail(MI3_ERR_CUDA, std::string("mi3_capture_while_begin: node: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(MI3_ERR_CUDA, std::string(name) + ": node: " + cudaGetErrorString(e));
     e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
-    if (e != cudaSuccess)
-        return fail(MI3_ERR_CUDA, std::string("mi3_capture_while_begin: deps: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(MI3_ERR_CUDA, std::string(name) + ": deps: " + cudaGetErrorString(e));
     cudaGraph_t body = params.conditional.phGraph_out[0];
     e = cudaStreamBeginCaptureToGraph(as_stream(body_stream), body, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeRelaxed);
-    if (e != cudaSuccess)
-        return fail(MI3_ERR_CUDA, std::string("mi3_capture_while_begin: body: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(MI3_ERR_CUDA, std::string(name) + ": body: " + cudaGetErrorString(e));
+    return MI3_OK;
+}
+
+// A conditional handle of the graph `stream` is capturing into, reset to
+// `value` at every launch of the graph.
+extern "C" int mi3_cond_handle_create(void *stream, uint32_t value, unsigned long long *handle_out) {
+    if (!handle_out) return fail(MI3_ERR_ARG, "mi3_cond_handle_create: null pointer");
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamGetCaptureInfo(as_stream(stream), &cs, nullptr, &graph, nullptr, nullptr);
+    if (e != cudaSuccess || cs != cudaStreamCaptureStatusActive)
+        return fail(MI3_ERR_CUDA, "mi3_cond_handle_create: stream is not capturing");
+    cudaGraphConditionalHandle h;
+    e = cudaGraphConditionalHandleCreate(&h, graph, value, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return fail(MI3_ERR_CUDA, std::string("mi3_cond_handle_create: ") + cudaGetErrorString(e));
     *handle_out = (unsigned long long)h;
     return MI3_OK;
+}
+
+// At the current capture position of `stream`, add a conditional WHILE node
+// (condition 1 at every graph launch) and begin capturing its body on
+// `body_stream`; everything issued on body_stream until mi3_capture_while_end
+// forms one iteration.  `stream` continues after the node.
+extern "C" int mi3_capture_while_begin(void *stream, void *body_stream, unsigned long long *handle_out) {
+    if (!handle_out || stream == body_stream) return fail(MI3_ERR_ARG, "mi3_capture_while_begin: bad arguments");
+    unsigned long long h = 0;
+    int rc = mi3_cond_handle_create(stream, 1, &h);
+    if (rc) return rc;
+    rc = capture_cond_begin(stream, body_stream, cudaGraphCondTypeWhile, (cudaGraphConditionalHandle)h,
+                            "mi3_capture_while_begin");
+    if (rc) return rc;
+    *handle_out = h;
+    return MI3_OK;
+}
+
+// The same for a conditional IF node on an existing handle (from
+// mi3_cond_handle_create): its body runs once when the handle is non-zero.
+extern "C" int mi3_capture_if_begin(void *stream, void *body_stream, unsigned long long handle) {
+    if (stream == body_stream) return fail(MI3_ERR_ARG, "mi3_capture_if_begin: bad arguments");
+    return capture_cond_begin(stream, body_stream, cudaGraphCondTypeIf, (cudaGraphConditionalHandle)handle,
+                              "mi3_capture_if_begin");
+}
+
+extern "C" int mi3_capture_if_end(void *body_stream) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(as_stream(body_stream), &g);
+    if (e != cudaSuccess) return fail(MI3_ERR_CUDA, std::string("mi3_capture_if_end: ") + cudaGetErrorString(e));
+    return MI3_OK;
+}
+
+extern "C" int mi3_equil_control(unsigned long long next, int32_t has_next, const double *r1, const double *r2,
+                                 double rcrit, int32_t test, uint32_t calls, uint32_t min_equil, uint32_t max_equil,
+                                 uint32_t *out, void *stream) {
+    if (!out || (test && (!r1 || !r2))) return fail(MI3_ERR_ARG, "mi3_equil_control: null pointer");
+    k_equil_control<<<1, 1, 0, as_stream(stream)>>>((cudaGraphConditionalHandle)next, has_next, r1, r2, rcrit, test,
+                                                    calls, min_equil, max_equil, out);
+    return check_launch("mi3_equil_control");
 }
 
 extern "C" int mi3_capture_while_end(void *body_stream) {

@@ -56,3 +56,32 @@ def test_batched_tuned_many_shapes(cuda, tmp_path):
         assert ssr[-1] < ssr[0], (k, ssr)
     assert all(r['gpu_ms'] > 0 for r in recs)
     br.close()
+
+
+def test_batched_graph_equilibrates_like_host_loop(cuda, monkeypatch):
+    """Equilibration inside the graph (IF node per checkpoint, rank test on
+    the device): for two problems in one graph, the sampler calls each
+    round settles on, its SSR, the Newton step counts and J after three
+    rounds equal those of inference.infer with equiltime='auto' (the
+    host-driven loop running the same rank test on the device)."""
+    from mi3gpu_b200.batched import BatchedRounds, Problem
+    from mi3gpu_b200.inference import infer
+    monkeypatch.setattr(MCMCGPU, 'CONS_ENERGY_MAX_ACTIVE', -1.0)
+    shapes = [(20, 4, 2048, 11), (13, 21, 2048, 12)]
+    targets = [_target(L, q, s) for L, q, N, s in shapes]
+    kw = dict(gamma=4e-3, damping=1e-2)
+    eq = dict(min_equil=64, max_equil=512)
+    probs = [Problem(t, L, q, N, seed=s) for t, (L, q, N, s) in zip(targets, shapes)]
+    br = BatchedRounds(probs, lJ=1e-3, newton_max=256, reseed='none', equil=eq, **kw)
+    for _ in range(3):
+        br.run_round()
+    for pr, t, (L, q, N, s) in zip(probs, targets, shapes):
+        res = infer(t, L, q, N, 3, equiltime='auto', nsteps=8 * L, newtonsteps=256, reg=('l1z', (1e-3,)), seed=s,
+                    log=lambda *a: None, reseed='none', device_resident=True, **eq, **kw)
+        assert [h['mcmc_calls'] for h in pr.history] == [h['equil_calls'] for h in res['history']]
+        assert all(64 <= h['mcmc_calls'] <= 512 for h in pr.history)
+        assert [h['ssr'] for h in pr.history] == [h['ssr'] for h in res['history']]
+        assert [h['newton_steps'] for h in pr.history] == [h['newton_steps'] for h in res['history']]
+        Jb = pr.gpu.bufs['J'].cpu().numpy()[:L * (L - 1) // 2 * q * q].reshape(-1, q * q)
+        np.testing.assert_array_equal(Jb, res['J'])
+    br.close()

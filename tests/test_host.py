@@ -513,3 +513,22 @@ def test_reseed_msa_restarts_every_round_from_the_seed_msa():
     for s in seen:
         np.testing.assert_array_equal(s, oracle.pack_seqs(seedmsa))
     assert not np.array_equal(g.bufs['seq main'], oracle.pack_seqs(seedmsa))  # the walkers did move
+
+
+@pytest.mark.parametrize("max_equil", [16, 64, 100, 512, 32768])
+def test_equil_schedule_matches_host_loop(max_equil):
+    """The checkpoints the round graph captures (batched.equil_schedule) are
+    those runMCMC's loop reaches: 8 calls, then 8, 16, 32, ... more, the
+    last one the first at or past max_equil."""
+    from mi3gpu_b200.batched import equil_schedule
+    host, step, loops = [], 8, 8
+    while True:
+        host.append((step, loops))
+        step += loops
+        if step >= max_equil:
+            break
+        loops *= 2
+    sched = equil_schedule(max_equil)
+    assert sched == host
+    c0, n = sched[-1]
+    assert c0 + n >= max_equil and (len(sched) == 1 or sched[-2][0] + sched[-2][1] < max_equil)
