@@ -64,11 +64,11 @@ constexpr uint32_t MT_W2_BYTES = MT_NU * MT_ROW_BYTES;
 constexpr uint32_t MT_W3_BYTES = MT_GQMAX * MT_ROW_BYTES;
 // a block's CUDA-core weights besides the layer-1 prefix: W2 [48][48], W3
 // [G q][48] and the layer-1 rows of its own sites [G q][48], bf16
-// then the block's small parameters (FP32 b3 [G q], b2 [48], b1 [48], and
-// int32 cnt [16]: block-local index of the first hidden-2 unit of degree
+// then the block's small parameters (FP32 b3 [G q], b2 [48], and int32
+// cnt [16]: block-local index of the first hidden-2 unit of degree
 // >= s0 + 1 + k), so that no global load sits on a site's critical path
 constexpr uint32_t MT_PAR_OFF = MT_W2_BYTES + 2 * MT_W3_BYTES;
-constexpr uint32_t MT_PAR_B3 = 0, MT_PAR_B2 = MT_GQMAX, MT_PAR_B1 = MT_PAR_B2 + MT_NU, MT_PAR_CNT = MT_PAR_B1 + MT_NU;
+constexpr uint32_t MT_PAR_B3 = 0, MT_PAR_B2 = MT_GQMAX, MT_PAR_CNT = MT_PAR_B2 + MT_NU;
 constexpr uint32_t MT_W123_BYTES = MT_PAR_OFF + (MT_PAR_CNT + 16) * 4;
 constexpr uint32_t MT_A1_BYTES = (MT_HMAX / 64) * MT_M * 128;
 constexpr uint32_t MT_A2_BYTES = MT_M * 128;
@@ -109,7 +109,6 @@ struct MtPlan {
     const MtWOp *wops;
     const uint32_t *blk;
     const int32_t *deg2_start;  // [L + 1]: first hidden-2 unit of degree >= d
-    const int32_t *deg1_start;  // [L + 1]: first hidden-1 unit of degree >= d
     const unsigned char *img;   // MMA weight tiles
     const unsigned char *wimg;  // CUDA-core weight stages
     const float *b1b;           // [nb][NU]
@@ -484,7 +483,7 @@ __global__ void __launch_bounds__(MtShape<Q, NU>::THREADS, 1)
             uint32_t cw = 0;  // residues of the current sequence word
             for (uint32_t b = 0; b < nb && ok; ++b) {
                 const uint32_t *bk = p.blk + b * MT_BLK;
-                const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], d2ok = bk[7], nch = bk[9];
+                const uint32_t c1 = bk[0], n1 = bk[1], d2ok = bk[7], nch = bk[9];
                 const uint32_t s0 = b * G, s1 = min(L, s0 + G);
                 if (b == 0 && sl == 0) {
                     // the logits accumulator of this tile starts at zero
@@ -746,8 +745,7 @@ __global__ void k_made_tc_images(const MtPlan p, unsigned char *img, const float
 // block's own sites [G q][48] in bf16.
 __global__ void k_made_tc_wimages(const MtPlan p, unsigned char *wimg, const float *__restrict__ W1T,
                                   const float *__restrict__ W2, const float *__restrict__ W3,
-                                  const float *__restrict__ b1, const float *__restrict__ b2,
-                                  const float *__restrict__ b3) {
+                                  const float *__restrict__ b2, const float *__restrict__ b3) {
     const MtWOp op = p.wops[blockIdx.x];
     const uint32_t *bk = p.blk + op.blk * MT_BLK;
     const uint32_t c1 = bk[0], n1 = bk[1], c2 = bk[2], n2 = bk[3];
@@ -769,12 +767,9 @@ __global__ void k_made_tc_wimages(const MtPlan p, unsigned char *wimg, const flo
         if (e < MT_PAR_B2) {  // b3 of the block's sites
             const uint32_t i = s0 + e / q;
             par[e] = (e < G * q && i < L) ? b3[s0 * q + e] : 0.0f;
-        } else if (e < MT_PAR_B1) {
+        } else if (e < MT_PAR_CNT) {
             const uint32_t u = e - MT_PAR_B2;
             par[e] = u < n2 ? b2[c2 + u] : 0.0f;
-        } else if (e < MT_PAR_CNT) {
-            const uint32_t v = e - MT_PAR_B1;
-            par[e] = v < n1 ? b1[c1 + v] : 0.0f;
         } else {
             const uint32_t d = min(L, s0 + 1 + (e - MT_PAR_CNT));
             reinterpret_cast<int32_t *>(par)[e] = p.deg2_start[d] - (int32_t)c2;
@@ -814,7 +809,7 @@ __global__ void k_made_tc_bias(const MtPlan p, float *b1b, float *b2b, float *b3
 }
 
 struct MtLayout {
-    size_t ops, wops, blk, deg, deg1, img, wimg, b1b, b2b, b3, total;
+    size_t ops, wops, blk, deg, img, wimg, b1b, b2b, b3, total;
 };
 
 static size_t mt_align(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -832,7 +827,6 @@ static MtLayout mt_layout(uint32_t L, uint32_t q, uint32_t nb, size_t nops, size
     o.wops = take(nwops * sizeof(MtWOp));
     o.blk = take((size_t)nb * MT_BLK * 4);
     o.deg = take((size_t)(L + 1) * 4);
-    o.deg1 = take((size_t)(L + 1) * 4);
     o.img = take(img_bytes);
     o.wimg = take(wimg_bytes);
     o.b1b = take((size_t)nb * MT_NU * 4);
@@ -848,7 +842,7 @@ struct MtHostPlan {
     std::vector<uint32_t> blk;
     std::vector<MtOp> ops;
     std::vector<MtWOp> wops;
-    std::vector<int32_t> deg1, deg2;
+    std::vector<int32_t> deg2;
     size_t img_bytes = 0, wimg_bytes = 0;
     const char *err = nullptr;
 };
@@ -930,15 +924,11 @@ static MtHostPlan mt_plan(uint32_t L, uint32_t q, uint32_t H, uint32_t G, const 
     }
     h.img_bytes = off;
     h.wimg_bytes = woff;
-    h.deg1.assign(L + 1, (int32_t)H);
     h.deg2.assign(L + 1, (int32_t)H);
     for (uint32_t d = 0; d <= L; ++d) {
         uint32_t k = 0;
         while (k < H && m2[k] < (int32_t)d) ++k;
         h.deg2[d] = (int32_t)k;
-        k = 0;
-        while (k < H && m1[k] < (int32_t)d) ++k;
-        h.deg1[d] = (int32_t)k;
     }
     return h;
 }
@@ -974,8 +964,7 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
         cudaMemcpyAsync(ws + lay.wops, h.wops.data(), h.wops.size() * sizeof(MtWOp), cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
         cudaMemcpyAsync(ws + lay.blk, h.blk.data(), h.blk.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(ws + lay.deg, h.deg2.data(), h.deg2.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(ws + lay.deg1, h.deg1.data(), h.deg1.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        cudaMemcpyAsync(ws + lay.deg, h.deg2.data(), h.deg2.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return check_launch("mi3_made_tc_prepare: tables");
     MtPlan p;
     std::memset(&p, 0, sizeof(p));
@@ -996,7 +985,6 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
     p.wops = reinterpret_cast<const MtWOp *>(ws + lay.wops);
     p.blk = reinterpret_cast<const uint32_t *>(ws + lay.blk);
     p.deg2_start = reinterpret_cast<const int32_t *>(ws + lay.deg);
-    p.deg1_start = reinterpret_cast<const int32_t *>(ws + lay.deg1);
     p.img = ws + lay.img;
     p.wimg = ws + lay.wimg;
     p.b1b = reinterpret_cast<const float *>(ws + lay.b1b);
@@ -1007,7 +995,7 @@ extern "C" int mi3_made_tc_prepare(uint32_t L, uint32_t q, uint32_t H, uint32_t 
         k_made_tc_images<<<p.nops, 256, 0, st>>>(p, ws + lay.img, W2, W3);
         if ((rc = check_launch("mi3_made_tc_prepare: images"))) return rc;
     }
-    k_made_tc_wimages<<<p.nwops, 256, 0, st>>>(p, ws + lay.wimg, W1T, W2, W3, b1, b2, b3);
+    k_made_tc_wimages<<<p.nwops, 256, 0, st>>>(p, ws + lay.wimg, W1T, W2, W3, b2, b3);
     if ((rc = check_launch("mi3_made_tc_prepare: weight stages"))) return rc;
     k_made_tc_bias<<<32, 256, 0, st>>>(p, reinterpret_cast<float *>(ws + lay.b1b),
                                        reinterpret_cast<float *>(ws + lay.b2b), reinterpret_cast<float *>(ws + lay.b3),
