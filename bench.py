@@ -689,8 +689,9 @@ def run_batched(args):
     t_targets = time.time() - t0
     shapes = [(p.L, p.q, p.N) for p in probs]
     t0 = time.time()
+    equil = dict(min_equil=64, max_equil=args.equil) if args.equil else None
     br = BatchedRounds(probs, sweeps=args.chosen_sweeps, sweeps_first=args.first_sweeps, reseed='none',
-                       tuner=Autotuner(ROOT / "_build" / "autotune.json") if not args.no_tune else None)
+                       tuner=Autotuner(ROOT / "_build" / "autotune.json") if not args.no_tune else None, equil=equil)
     t_tune = time.time() - t0
     rounds = []
     for r in range(args.rounds):
@@ -701,6 +702,7 @@ def run_batched(args):
         rounds.append(rec)
     upd_first = br.site_updates_per_round(first=True)
     upd = br.site_updates_per_round(first=False)
+    calls_b = [[h["mcmc_calls"] for h in p.history] for p in probs]
     steady = rounds[1:] or rounds
     gpu_s = statistics.mean(r["gpu_ms"] for r in steady) / 1e3
     batched = {
@@ -717,28 +719,35 @@ def run_batched(args):
     torch.cuda.empty_cache()
     # host-driven arm: the same problems (same targets and seeds) one after
     # another, same rounds
-    ssr_h = []
+    ssr_h, calls_h = [], []
     per_round = [0.0] * args.rounds
     for k, (tgt, L, q, N) in enumerate(targets):
-        res = infer(tgt, L, q, N, args.rounds, sweeps=args.chosen_sweeps, sweeps_first=args.first_sweeps,
-                    newtonsteps=1024, seed=2000 + 1000 + k, log=lambda *a: None, reseed='none',
-                    device_resident=True)
+        kw = (dict(equiltime='auto', nsteps=8 * L, min_equil=64, max_equil=args.equil) if args.equil else
+              dict(sweeps=args.chosen_sweeps, sweeps_first=args.first_sweeps))
+        res = infer(tgt, L, q, N, args.rounds, newtonsteps=1024, seed=2000 + 1000 + k, log=lambda *a: None,
+                    reseed='none', device_resident=True, **kw)
         for r, h in enumerate(res["history"]):
             per_round[r] += h["round_s"]
         ssr_h.append([h["ssr"] for h in res["history"]])
+        calls_h.append([h["equil_calls"] for h in res["history"]])
         torch.cuda.empty_cache()
     host_s = statistics.mean(per_round[1:] or per_round)
     same = all(a == b for a, b in zip(ssr_b, ssr_h))
+    same_calls = all(a == b for a, b in zip(calls_b, calls_h)) if args.equil else None
     print(json.dumps({
         "metric": "s per quasi-Newton round of a batch of independent problems, one graph launch vs host loop",
         "unit": "s/round", "value": gpu_s, "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"batched {args.problems} problems, L~U[50,300], q in {{4,8,21}}, "
-                               f"walkers logU[2^14,2^17], {args.chosen_sweeps} sweeps/round after a "
-                               f"{args.first_sweeps}-sweep first round, l1z 2e-4", "rounds": args.rounds,
+                               f"walkers logU[2^14,2^17], " +
+                               (f"equilibration test in the graph (64 to {args.equil} calls of 8L steps)"
+                                if args.equil else f"{args.chosen_sweeps} sweeps/round after a "
+                                f"{args.first_sweeps}-sweep first round") + ", l1z 2e-4", "rounds": args.rounds,
                    "shapes": shapes},
         "batched": batched, "host_loop": {"s_per_round": host_s, "first_round_s": per_round[0]},
         "speedup_host_over_batched": host_s / gpu_s, "identical_ssr_histories": same,
+        "identical_equilibration_calls": same_calls,
+        "equilibration_calls_batched": calls_b[:8] if args.equil else None,
         "tuned_plans_sample": plans, "target_build_s": t_targets}))
 
 
@@ -1118,6 +1127,8 @@ def main():
     ap.add_argument("--shape", default="", help="L,q,N: one shape for --mode kernels")
     ap.add_argument("--hidden", type=int, default=512, help="MADE hidden units (--mode learned / made)")
     ap.add_argument("--made-epochs", type=int, default=48, help="MADE training epochs (--mode learned)")
+    ap.add_argument("--equil", type=int, default=0,
+                    help="--mode batched: equilibrate inside the graph, at most this many sampler calls")
     ap.add_argument("--made-every", type=int, default=4, help="sweeps per proposal step (--mode learned)")
     args = ap.parse_args()
     rank, world, _ = env_rank()
