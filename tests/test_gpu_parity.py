@@ -382,9 +382,11 @@ def test_reg_other_vs_oracle(cuda, kind, entry, params, q):
 
 
 @pytest.mark.parametrize("L,q,N", [(10, 5, 512), (48, 4, 16384), (37, 21, 1000), (93, 4, 3000), (64, 8, 640),
-                                   (232, 21, 4096), (50, 32, 300), (13, 7, 130)])
+                                   (232, 21, 4096), (50, 32, 300), (13, 7, 130), (99, 4, 20000), (128, 8, 9000)])
 def test_bicounts_tensorcore_bitexact(cuda, L, q, N):
-    """FP8 one-hot GEMM counts on tcgen05 equal the integer histogram exactly."""
+    """FP8 one-hot GEMM counts on tcgen05 equal the integer histogram exactly
+    (one chunk, or up to 19 chunks summed with atomics; partial last K
+    step)."""
     seqs = _seqs(L, q, N, 50 + q)
     mem = oracle.pack_seqs(seqs)
     out = empty((L * (L - 1) // 2, q * q), np.uint32)
