@@ -7,7 +7,7 @@
 // floor(128/q) sites of block I and 256 columns = those of floor(256/q)
 // sites of block J; K runs over the chunk, 128 sequences per step.
 //
-// Warp roles.  Eight producer warps stage the step's sequence words
+// Warp roles.  Sixteen producer warps stage the step's sequence words
 // ([word][seq], double-buffered) and write the one-hot tiles A (128 x 128 B)
 // and B (256 x 128 B) as FP8 e4m3 (1.0 = 0x38) straight into shared memory
 // in the K-major 128-byte-swizzled layout the MMA reads, into a ring of 4
@@ -30,8 +30,9 @@ constexpr uint32_t TC_B_BYTES = TC_N * 128;   // 32 KB
 constexpr uint32_t TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;
 constexpr uint32_t TC_MAX_WORDS = 26;         // sequence words staged per K step (rows + columns), q >= 4
 constexpr uint32_t TC_STAGES = 4;
-constexpr uint32_t TC_PRODUCERS = 256;        // warps 0-7: one-hot producers, then the epilogue
-constexpr uint32_t TC_THREADS = TC_PRODUCERS + 32;  // warp 8: TMEM allocation and the MMA-issuing thread
+constexpr uint32_t TC_PRODUCERS = 512;        // warps 0-15: one-hot producers, then the epilogue
+constexpr uint32_t TC_MMA_WARP = TC_PRODUCERS / 32;
+constexpr uint32_t TC_THREADS = TC_PRODUCERS + 32;  // warp 16: TMEM allocation and the MMA-issuing thread
 constexpr uint32_t TC_WORDS_BYTES = TC_MAX_WORDS * TC_KSTEP * 4;
 constexpr uint32_t TC_SMEM = 1024 /*align slack*/ + TC_STAGES * TC_STAGE_BYTES + 2 * TC_WORDS_BYTES + 128;
 constexpr uint32_t TC_WPT = (TC_MAX_WORDS * TC_KSTEP + TC_PRODUCERS - 1) / TC_PRODUCERS;  // staged words per producer
@@ -98,7 +99,7 @@ __device__ __forceinline__ void tile_coords(uint32_t t, const TcGeom &g, uint32_
 }
 
 // true on every producer thread if pred is true on any (named barrier 1
-// over the 256 producer threads; also orders their shared-memory accesses)
+// over the producer threads; also orders their shared-memory accesses)
 __device__ __forceinline__ bool producers_any(bool pred) {
     uint32_t r;
     asm volatile(
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_counts_tc(const uint32_t *__r
         *abort_flag = 0;
         fence_mbar_init();
     }
-    if (warp == 8) {
+    if (warp == TC_MMA_WARP) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
                      "r"(TC_N));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_counts_tc(const uint32_t *__r
     const uint32_t nend = min(nseq, nbeg + g.chunk);
     const uint32_t nk = (nend - nbeg + TC_KSTEP - 1) / TC_KSTEP;
 
-    if (warp == 8) {
+    if (warp == TC_MMA_WARP) {
         // ------------------------------------------------------ MMA thread
         if (lane == 0) {
             uint32_t ks = 0;
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_counts_tc(const uint32_t *__r
         __syncwarp();
     } else {
         // ------------------------------------------------------- producers
-        // Staged word idx = tid + 256 j of a step is seqw[idx]: word row
+        // Staged word idx = tid + 512 j of a step is seqw[idx]: word row
         // idx / 128, sequence k0 + idx % 128.  The loads of step ks + 1 are
         // issued into registers before step ks is generated and stored to
         // shared memory at the start of step ks + 1, so their latency is
@@ -256,12 +257,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_counts_tc(const uint32_t *__r
                     wrow = nwr + gs / 4 - wc0;
                     byte = gs & 3;
                 }
-                // residues of site for sequences grp*16 .. +15, packed 4 per word
-                const uint4 *src = reinterpret_cast<const uint4 *>(seqw + wrow * TC_KSTEP + grp * 16);
+                // residues of site for the step's sequences 32 v + 4 grp + k
+                // (v, k < 4), which go to K positions 16 grp + 4 v + k of
+                // both operands (a K order shared by A and B leaves the
+                // product unchanged; the 8 lanes of a quarter warp read 128
+                // contiguous bytes)
+                const uint32_t *src = seqw + wrow * TC_KSTEP + 4 * grp;
                 uint32_t r[4];
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
-                    uint4 x = src[v];
+                    uint4 x = *reinterpret_cast<const uint4 *>(src + 32 * v);
                     // byte `byte` of each of the 4 words, packed in sequence order
                     uint32_t lo = __byte_perm(x.x, x.y, byte | ((byte + 4) << 4));
                     uint32_t hi = __byte_perm(x.z, x.w, byte | ((byte + 4) << 4));
@@ -306,15 +311,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_counts_tc(const uint32_t *__r
         }
         tc_fence_after();
         if (got && ok && nk > 0 && !*abort_flag) {
-            // warp w reads TMEM lanes 32*(w%4).. (rows), columns [128*(w/4), +128)
+            // warp w reads TMEM lanes 32*(w%4).. (rows), columns [64*(w/4), +64)
             const uint32_t r = 32 * (warp & 3) + lane;
             const uint32_t si = r / q, a = r - si * q;
             const bool rvalid = r < nsr * q;
             const uint32_t gi = i0 + si;
-            const uint32_t cbeg = 128 * (warp >> 2), cend = nsc * q;
+            const uint32_t cbeg = 64 * (warp >> 2), cend = nsc * q;
             uint32_t sj = cbeg / q, b = cbeg - sj * q;  // column (site, residue), advanced with c
 #pragma unroll 1
-            for (uint32_t c0 = cbeg; c0 < cbeg + 128; c0 += 16) {
+            for (uint32_t c0 = cbeg; c0 < cbeg + 64; c0 += 16) {
                 uint32_t v[16];
                 tmem_ld16(tmem + ((32 * (warp & 3)) << 16) + c0, v);
 #pragma unroll
@@ -339,7 +344,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_counts_tc(const uint32_t *__r
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 8) {
+    if (warp == TC_MMA_WARP) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_N));
     }
