@@ -521,8 +521,9 @@ class MCMCGPU:
     # ------------------------------------------------------------ statistics
     # alphabet sizes for which the tcgen05 one-hot GEMM counts beat the
     # shared-memory histogram when nothing was tuned (measured on B200 at
-    # 2^18 walkers against the lanes-over-pairs histogram: 1.4x at q=4-6,
-    # slower from q=8 on and at 2^14 walkers); both give identical integers.
+    # 2^18 walkers against the lanes-over-pairs histogram: 2.5x at q=4, 2.2x
+    # at q=5, 1.8x at q=6, a tie at q=8 and at 2^14 walkers, slower from
+    # q=12 on); both give identical integers.
     TENSOR_COUNT_Q = range(4, 7)
     # the same for the weighted bimarginals (three byte-plane integer GEMMs
     # against the shared-memory fixed-point histogram, identical results):
