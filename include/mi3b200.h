@@ -256,7 +256,9 @@ int mi3_bicounts(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_
  * uint32 counts as mi3_bicounts, computed as FP8 one-hot GEMMs X^T X with
  * tcgen05 MMAs (FP32 accumulation, exact below 2^24 per chunk).  4 <= q <= 32.
  * *status (int32, device, zeroed by the caller) receives
- * MI3_STATUS_TIMEOUT_FULL if a bounded wait for the tensor cores gave up. */
+ * MI3_STATUS_TIMEOUT_FULL if a bounded wait for the tensor cores gave up,
+ * or MI3_STATUS_TIMEOUT_EMPTY if the operand producers' wait for a free
+ * stage did. */
 int mi3_bicounts_tc(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t *bicount,
                     uint32_t L, uint32_t q, int32_t *status, void *stream);
 
