@@ -262,6 +262,13 @@ int mi3_bicounts(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_
 int mi3_bicounts_tc(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t *bicount,
                     uint32_t L, uint32_t q, int32_t *status, void *stream);
 
+/* Launch plan of mi3_bicounts_tc for a shape (host only, no device work):
+ * out4 (nullable) = {output tiles, sequence chunks, sequences per chunk,
+ * sites per row tile}; returns 1, or 0 outside the kernel's range
+ * (L >= 2, 4 <= q <= 32, nseq >= 1).  A chunk holds at most 2^24
+ * sequences, so its FP32 sums of 0/1 products are exact integers. */
+uint32_t mi3_bicounts_tc_plan(uint32_t L, uint32_t q, uint32_t nseq, uint32_t *out4);
+
 /* bicounts_to_bimarg (mcmc.cl:518-528), MCMCGPU.bicounts_to_bimarg
  * (mcmcGPU.py:520-534). */
 int mi3_bicounts_to_bimarg(const uint32_t *bicount, float *bimarg, uint32_t nseq, uint32_t L,

@@ -40,6 +40,7 @@ SIGNATURES = {
     "mi3_rank_corr": (c.c_int, [_vp, _vp, _u32, _vp, _vp, c.c_size_t, _vp]),
     "mi3_equil_decide": (c.c_int, [_vp, _vp, c.c_double, _vp, _vp]),
     "mi3_bicounts": (c.c_int, [_vp, _u32, _u32, _vp, _u32, _u32, _vp]),
+    "mi3_bicounts_tc_plan": (_u32, [_u32, _u32, _u32, _vp]),
     "mi3_bicounts_tc": (c.c_int, [_vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp]),
     "mi3_bicounts_to_bimarg": (c.c_int, [_vp, _vp, _u32, _u32, _u32, _vp]),
     "mi3_weighted_marg_workspace": (c.c_size_t, [_u32, _u32, _u32]),

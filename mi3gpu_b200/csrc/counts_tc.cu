@@ -350,35 +350,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_counts_tc(const uint32_t *__r
     }
 }
 
-}  // namespace mi3
-
-using namespace mi3;
-
-extern "C" int mi3_bicounts_tc(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t *bicount, uint32_t L,
-                               uint32_t q, int32_t *status, void *stream) {
-    if (!seqmem || !bicount || !status) return fail(MI3_ERR_ARG, "mi3_bicounts_tc: null pointer");
-    if (L < 2 || q < 4 || q > 32 || nseq > buflen) return fail(MI3_ERR_ARG, "mi3_bicounts_tc: bad L/q/nseq (4<=q<=32)");
-    cudaStream_t st = as_stream(stream);
-    const uint64_t nbins = npairs_of(L) * q * q;
-    if (nseq == 0) {
-        cudaMemsetAsync(bicount, 0, nbins * 4, st);
-        return check_launch("mi3_bicounts_tc: memset");
-    }
-    TcGeom g;
+// Tile geometry and sequence chunks of a launch (host only).  Returns false
+// when the shape is outside the kernel's range.
+static bool tc_plan(uint32_t L, uint32_t q, uint32_t nseq, TcGeom &g) {
+    if (L < 2 || q < 4 || q > 32 || nseq == 0) return false;
     g.SR = TC_M / q;
     g.SC = TC_N / q;
     g.nrt = (L + g.SR - 1) / g.SR;
     g.nct = (L + g.SC - 1) / g.SC;
     g.ntiles = 0;
     for (uint32_t r = 0; r < g.nrt; ++r) g.ntiles += g.nct - (r * g.SR) / g.SC;
-    if ((g.SR + 3) / 4 + 1 + (g.SC + 3) / 4 + 1 > TC_MAX_WORDS)
-        return fail(MI3_ERR_ARG, "mi3_bicounts_tc: q too small for the staging plan");
+    if ((g.SR + 3) / 4 + 1 + (g.SC + 3) / 4 + 1 > TC_MAX_WORDS) return false;
     // chunks: one CTA per SM (the ring fills the shared memory).  The
     // number of chunks minimises waves x (K steps per chunk + 16, the
     // prologue and the epilogue's 32768 counts in K-step units) over 148
     // SMs, with chunks of at least 8 K steps and at most 2^24 sequences
     // (exact FP32).
-    const uint32_t nks = (nseq + TC_KSTEP - 1) / TC_KSTEP;
+    const uint32_t nks = (uint32_t)(((uint64_t)nseq + TC_KSTEP - 1) / TC_KSTEP);
     const uint32_t max_want = std::min<uint32_t>(4096, std::max<uint32_t>(1, nks / 8));
     uint32_t want = 1;
     uint64_t best = ~0ull;
@@ -391,9 +379,39 @@ extern "C" int mi3_bicounts_tc(const uint32_t *seqmem, uint32_t buflen, uint32_t
         }
     }
     want = std::max<uint32_t>(want, (nks + (1u << 17) - 1) >> 17);
-    const uint32_t chunk = (nks + want - 1) / want * TC_KSTEP;
-    g.chunk = chunk;
-    g.nchunks = (nseq + chunk - 1) / chunk;
+    g.chunk = (nks + want - 1) / want * TC_KSTEP;
+    g.nchunks = (uint32_t)(((uint64_t)nseq + g.chunk - 1) / g.chunk);
+    return true;
+}
+
+}  // namespace mi3
+
+using namespace mi3;
+
+extern "C" uint32_t mi3_bicounts_tc_plan(uint32_t L, uint32_t q, uint32_t nseq, uint32_t *out4) {
+    TcGeom g;
+    if (!tc_plan(L, q, nseq, g)) return 0;
+    if (out4) {
+        out4[0] = g.ntiles;
+        out4[1] = g.nchunks;
+        out4[2] = g.chunk;
+        out4[3] = g.SR;
+    }
+    return 1;
+}
+
+extern "C" int mi3_bicounts_tc(const uint32_t *seqmem, uint32_t buflen, uint32_t nseq, uint32_t *bicount, uint32_t L,
+                               uint32_t q, int32_t *status, void *stream) {
+    if (!seqmem || !bicount || !status) return fail(MI3_ERR_ARG, "mi3_bicounts_tc: null pointer");
+    if (L < 2 || q < 4 || q > 32 || nseq > buflen) return fail(MI3_ERR_ARG, "mi3_bicounts_tc: bad L/q/nseq (4<=q<=32)");
+    cudaStream_t st = as_stream(stream);
+    const uint64_t nbins = npairs_of(L) * q * q;
+    if (nseq == 0) {
+        cudaMemsetAsync(bicount, 0, nbins * 4, st);
+        return check_launch("mi3_bicounts_tc: memset");
+    }
+    TcGeom g;
+    if (!tc_plan(L, q, nseq, g)) return fail(MI3_ERR_ARG, "mi3_bicounts_tc: q too small for the staging plan");
     if (g.nchunks > 1 && cudaMemsetAsync(bicount, 0, nbins * 4, st) != cudaSuccess)
         return check_launch("mi3_bicounts_tc: memset");
     cudaFuncSetAttribute(k_counts_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);

@@ -5,6 +5,7 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 from mi3gpu_b200 import _lib
@@ -105,3 +106,39 @@ def test_metropolis_plans_host_query(L, q, N):
         stage_floats = (m * q * q + 31) // 32 * 32
         smem = 128 * ((16 * st + 4 + 127) // 128) + st * stage_floats * 4 + 256 * 4 + words * nw * 4
         assert smem <= 227 * 1024
+
+
+@pytest.mark.parametrize("L,q,N", [(99, 4, 1 << 18), (48, 4, 1 << 14), (232, 21, 1 << 20), (512, 21, 1 << 19),
+                                   (128, 8, 1 << 18), (150, 12, 1 << 18), (2, 4, 1), (3, 32, 5000),
+                                   (93, 4, 3000), (60, 4, (1 << 24) + 5), (40, 4, 1 << 27), (283, 4, 75776)])
+def test_bicounts_tc_plan_host_query(L, q, N):
+    """The tensor-core count kernel's launch plan is host code: the chunks
+    cover the N sequences in whole 128-sequence K steps, none holds more
+    than 2^24 sequences (FP32 sums of 0/1 products stay exact integers),
+    and the (row tile, column tile) pairs put every site pair i < j in
+    exactly one tile."""
+    out = (ctypes.c_uint32 * 4)()
+    assert _lib.query("mi3_bicounts_tc_plan", L, q, N, out) == 1
+    ntiles, nchunks, chunk, SR = list(out)
+    SC = 256 // q
+    assert SR == 128 // q
+    assert chunk % 128 == 0 and 0 < chunk <= 1 << 24
+    assert (nchunks - 1) * chunk < N <= nchunks * chunk
+    nrt, nct = -(-L // SR), -(-L // SC)
+    tiles = {(r, c) for r in range(nrt) for c in range((r * SR) // SC, nct)}
+    assert len(tiles) == ntiles
+    i, j = np.triu_indices(L, 1)
+    assert all((a, b) in tiles for a, b in set(zip((i // SR).tolist(), (j // SC).tolist())))
+
+
+def test_bicounts_tc_plan_one_wave_at_L99_q4():
+    """L=99, q=4, 2^18 sequences: 6 tiles x 24 chunks of 86 K steps, one
+    wave of 144 CTAs on the 148 SMs."""
+    out = (ctypes.c_uint32 * 4)()
+    assert _lib.query("mi3_bicounts_tc_plan", 99, 4, 1 << 18, out) == 1
+    assert list(out) == [6, 24, 86 * 128, 32]
+
+
+def test_bicounts_tc_plan_rejects_out_of_range():
+    for L, q, N in [(1, 4, 10), (10, 3, 10), (10, 33, 10), (10, 4, 0)]:
+        assert _lib.query("mi3_bicounts_tc_plan", L, q, N, None) == 0
