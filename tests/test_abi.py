@@ -142,3 +142,34 @@ def test_bicounts_tc_plan_one_wave_at_L99_q4():
 def test_bicounts_tc_plan_rejects_out_of_range():
     for L, q, N in [(1, 4, 10), (10, 3, 10), (10, 33, 10), (10, 4, 0)]:
         assert _lib.query("mi3_bicounts_tc_plan", L, q, N, None) == 0
+
+
+# entry points for which null is a valid argument (the default stream, an
+# empty graph handle): they go on to the CUDA runtime, which needs a device
+_NULL_ALLOWED = {"mi3_abi_version", "mi3_capture_begin", "mi3_capture_if_end", "mi3_capture_while_end",
+                 "mi3_graph_destroy", "mi3_stream_destroy"}
+
+
+def _null_args(argtypes):
+    vals = []
+    for a in argtypes:
+        if a in (ctypes.c_void_p, ctypes.c_char_p) or (isinstance(a, type) and issubclass(a, ctypes._Pointer)):
+            vals.append(None)
+        elif a in (ctypes.c_float, ctypes.c_double):
+            vals.append(0.5)
+        else:
+            vals.append(8)
+    return vals
+
+
+@pytest.mark.parametrize("name", sorted(n for n, (rt, _) in _lib.SIGNATURES.items()
+                                        if rt is ctypes.c_int and n not in _NULL_ALLOWED))
+def test_every_entry_point_rejects_null_pointers(name):
+    """Every int-returning entry point checks its pointers on the host and
+    returns MI3_ERR_ARG, with a message naming the call, before any device
+    work (so this runs without a GPU)."""
+    with pytest.raises(_lib.Mi3Error) as e:
+        _lib.call(name, *_null_args(_lib.SIGNATURES[name][1]))
+    assert e.value.code == -1
+    msg = str(e.value).split("): ", 1)[1]  # the library's own message: "<entry point>: <reason>"
+    assert name.startswith(msg.split(":")[0])
