@@ -362,3 +362,72 @@ def test_two_rank_rounds_write_run_directories_once_and_checkpoint_per_rank(tmp_
     for r in res:
         np.testing.assert_array_equal(r["ck_walkers"], r["walkers"])
     assert not np.array_equal(res[0]["walkers"], res[1]["walkers"])
+
+
+def _failing_rank_worker(rank, world, port, out):
+    """iterNewton over two ranks in which rank 1's device fails at its 4th
+    weighted-bimarginal call (a fake of the failing call raising, as a CUDA
+    error surfaces from MCMCGPU); the process group's timeout is short."""
+    import datetime
+    import torch.distributed as dist
+    from mi3gpu_b200 import NewtonSteps, potts
+    from mi3gpu_b200.distributed import RankNode
+    from tests.fake_device import FakeMCMCGPU
+
+    class FailingDevice(FakeMCMCGPU):
+        calls = 0
+
+        def weightedMarg(self, seqbufname='main'):
+            FailingDevice.calls += 1
+            if FailingDevice.calls == 4:
+                raise RuntimeError("injected device failure on rank 1")
+            return super().weightedMarg(seqbufname)
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    L, q, N = 8, 3, 1024
+    n_per = N // world
+    J = potts.synthetic_ground_truth(L, q, seed=5, contact_sigma=0.4)
+    seqs = np.random.default_rng(4).integers(0, q, size=(N, L)).astype('<u1')
+    g = (FailingDevice if rank == 1 else FakeMCMCGPU)(L, q, n_per, seed=2 + rank)
+    node = RankNode(g)
+    node.initMCMC(4 * L)
+    node.initJstep()
+    node.setSeqs('main', seqs[rank * n_per:(rank + 1) * n_per])
+    node.setBuf('J', J)
+    node.calcBicounts('main')
+    f0 = node.collect('bicount') / N
+    target = potts.mutation_pc(f0 * np.exp(np.random.default_rng(3).normal(0, 0.2, f0.shape)), N).astype('<f4')
+    target /= target.sum(axis=1, keepdims=True)
+    node.setBuf('bi target', target)
+    p = NewtonSteps.Param(bimarg=target, gamma0=4e-3, newtonSteps=12, pcdamping=1e-2, fracNeff=0.5,
+                          nwalkers=N, reg='l1z', regarg=(1e-3,), beta=None, distribute_jstep='all')
+    NewtonSteps.iterNewton(p, f0, node, lambda *a: None)
+    out.put(dict(rank=rank, finished=True))
+
+
+def test_two_rank_failure_ends_every_rank_with_an_error():
+    """A rank whose device call fails mid Newton phase raises; the other
+    rank, blocked in the next collective, ends with an error from the
+    process group instead of waiting for good (the reference aborts every
+    MPI rank when one exits, Mi3.py:249-258).  No GPU is involved."""
+    import time
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    t0 = time.time()
+    ps = [ctx.Process(target=_guarded, args=(_failing_rank_worker, r, 2, port, out)) for r in range(2)]
+    for p in ps:
+        p.start()
+    try:
+        res = sorted([out.get(timeout=120) for _ in range(2)], key=lambda r: r["rank"])
+    finally:
+        for p in ps:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert "injected device failure" in res[1].get("error", ""), res
+    assert "error" in res[0] and "finished" not in res[0], res
+    assert all(p.exitcode != 0 for p in ps)
+    assert time.time() - t0 < 120
