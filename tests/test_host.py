@@ -532,3 +532,37 @@ def test_equil_schedule_matches_host_loop(max_equil):
     assert sched == host
     c0, n = sched[-1]
     assert c0 + n >= max_equil and (len(sched) == 1 or sched[-2][0] + sched[-2][1] < max_equil)
+
+
+@pytest.mark.parametrize("device_resident", [False, True])
+@pytest.mark.filterwarnings("ignore::RuntimeWarning")  # numpy on the planted NaN / Inf
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_iterNewton_raises_divergence_on_non_finite_input(bad, device_resident):
+    """A NaN or Inf in the target bimarginals makes dJ, and with it the
+    reweighting weights exp(-E(dJ)), non-finite; the Newton phase stops with
+    the reference's divergence error (NewtonSteps.py:257-260) instead of
+    carrying the bad values into the next round.  (The check is on the
+    weights, as in the reference: a bad J that never reaches dJ is not
+    caught here either, nor a -Inf target, which only zeroes the weights of
+    the sequences it touches; the model bimarginals are recounted from the
+    walkers at the start of the phase.)"""
+    L, q, N = 8, 3, 512
+    rng = np.random.default_rng(7)
+    J = potts.synthetic_ground_truth(L, q, seed=5, contact_sigma=0.4)
+    g = FakeMCMCGPU(L, q, N, seed=2)
+    gpus = GPU_node([g])
+    gpus.initMCMC(4 * L)
+    gpus.initJstep()
+    gpus.setSeqs('main', rng.integers(0, q, size=(N, L)).astype('<u1'))
+    gpus.setBuf('J', J)
+    gpus.calcBicounts('main')
+    f0 = gpus.collect('bicount') / N
+    target = potts.mutation_pc(f0, N).astype('<f4')
+    target /= target.sum(axis=1, keepdims=True)
+    target = target.copy()
+    target[2, 1] = bad
+    gpus.setBuf('bi target', target)
+    p = _param(L, q, N, target, J)
+    p.device_resident = device_resident
+    with pytest.raises(Exception, match="Divergence"):
+        NewtonSteps.iterNewton(p, f0, gpus, lambda *a: None)
