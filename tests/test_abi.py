@@ -173,3 +173,28 @@ def test_every_entry_point_rejects_null_pointers(name):
     assert e.value.code == -1
     msg = str(e.value).split("): ", 1)[1]  # the library's own message: "<entry point>: <reason>"
     assert name.startswith(msg.split(":")[0])
+
+
+_P = 0x100000  # a stand-in device address (never dereferenced: every case fails validation first)
+
+
+def _no_cuda():
+    import torch
+    return not torch.cuda.is_available()
+
+
+@pytest.mark.skipif(not _no_cuda(), reason="host-only validation test; a device would make a launch possible")
+@pytest.mark.parametrize("name,args,code", [
+    ("mi3_init_rng", (_P + 8, 8, 0, 1 << 20, None), -3),
+    ("mi3_unpack_j", (_P, _P + 4, 10, 4, None), -3),
+    ("mi3_unpack_j_tiles", (_P, _P + 4, 10, 4, None), -3),
+    ("mi3_gen_indep", (_P, 64, 64, _P + 8, _P, 10, 4, None), -3),
+    ("mi3_gemm_bf16", (16, 16, 16, _P, 16, 1, _P, 16, 1, _P, 16, 1.0, 0.0, _P + 256, 1 << 30, _P, None), -3),
+    ("mi3_gemm_bf16", (16, 16, 16, _P, 16, 1, _P, 16, 1, _P, 16, 1.0, 0.0, _P, 16, _P, None), -4),
+])
+def test_alignment_and_workspace_rejected_on_the_host(name, args, code):
+    """Misaligned device pointers (MI3_ERR_ALIGN) and short workspaces
+    (MI3_ERR_WORKSPACE) are rejected on the host, before any launch."""
+    with pytest.raises(_lib.Mi3Error) as e:
+        _lib.call(name, *args)
+    assert e.value.code == code
