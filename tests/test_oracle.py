@@ -279,3 +279,23 @@ def test_gauge_change_shifts_every_energy_by_one_constant():
     d = energies(Jg) - energies(J)
     assert abs(d.mean()) > 1.0  # the gauge did move the couplings
     assert np.ptp(d) < 1e-9 * np.abs(d).max()
+
+
+def test_fp64_energies_against_32_digit_sums():
+    """The intent of the reference's Mi3.getEnergiesMultiPrec (Mi3.py:79-90,
+    mpmath at 32 digits): the FP64 oracle that bounds the device energies
+    (1e-5 relative) is itself within 1e-12 of 32-digit sums of the same
+    float32 couplings, at the reference-sized L=232, q=21."""
+    mpmath = pytest.importorskip("mpmath")
+    L, q, n = 232, 21, 6
+    rng = np.random.default_rng(232)
+    J = rng.normal(0, 0.5, size=(L * (L - 1) // 2, q * q)).astype("<f4")
+    seqs = rng.integers(0, q, size=(n, L)).astype("<u1")
+    E = oracle.energies_f64(J, oracle.pack_seqs(seqs), L, q)
+    i, j = np.triu_indices(L, 1)
+    mpmath.mp.dps = 32
+    for k in range(n):
+        s = seqs[k].astype(np.int64)
+        terms = J[np.arange(len(i)), q * s[i] + s[j]]
+        exact = mpmath.fsum(mpmath.mpf(float(t)) for t in terms)
+        assert abs(E[k] - float(exact)) <= 1e-12 * max(1.0, abs(float(exact)))
