@@ -351,9 +351,14 @@ class LearnedSampler:
                       self.seed * 7919 + self.rounds, self.nacc.data_ptr(), s)
             acc = int(self.nacc.item())
         m.check_status()
+        return self._record(acc, N)
+
+    def _record(self, acc, n):
+        """Count one proposal step (acc of n walkers accepted); proposals stop
+        for good once a step's acceptance rate is below min_accept."""
         self.accepted += acc
-        self.proposed += N
-        rate = acc / N
+        self.proposed += n
+        rate = acc / n
         if rate < self.min_accept:
             self.enabled = False
         return rate

@@ -66,3 +66,31 @@ def test_prepare_and_sample_reject_before_launch():
         _lib.call("mi3_made_tc_prepare", L, q, H, G, m.ctypes.data, m.ctypes.data, None, p, p, p, p, p, p, 1 << 30,
                   plan.ctypes.data, None)
     assert e.value.code == -1
+
+
+def test_learned_sampler_hands_over_to_plain_sweeps_below_min_accept():
+    """The interleaving and hand-over of LearnedSampler.sweeps (host logic):
+    one proposal step after every `every`-th sampler call, and none after a
+    step whose acceptance rate fell below min_accept -- the plain sampler
+    carries on alone.  The device work of a proposal step is replaced by
+    scripted acceptance counts."""
+    from mi3gpu_b200.learned import LearnedSampler
+
+    class FakeGpu:
+        calls = 0
+
+        def runMCMC(self):
+            FakeGpu.calls += 1
+
+    N = 1000
+    script = iter([400, 250, 5, 900])  # accepted walkers per proposal step
+    ls = LearnedSampler.__new__(LearnedSampler)
+    ls.gpu, ls.every, ls.min_accept = FakeGpu(), 3, 0.01
+    ls.accepted = ls.proposed = 0
+    ls.enabled = True
+    ls.propose = lambda: ls._record(next(script), N)
+    rates = ls.sweeps(20)
+    assert FakeGpu.calls == 20
+    assert rates == [0.4, 0.25, 0.005]  # the third step (0.5% < 1%) is the last
+    assert not ls.enabled and ls.proposed == 3 * N and ls.accepted == 655
+    assert ls.sweeps(6) == [] and FakeGpu.calls == 26
