@@ -52,3 +52,24 @@ def test_reference_arm_runs_on_rank_0_only():
                env={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert p.returncode == 0, p.stderr[-2000:]
     assert _json_lines(p.stdout) == []
+
+
+def test_clock_summary_parses_nvidia_smi_rows():
+    """The clocks record of the bench line: median SM clock under load, the
+    maximum, and every throttle reason seen Active (rows as nvidia-smi
+    prints them with --format=csv,noheader,nounits)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    cs = bench.ClockSampler(0)
+    assert cs.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+    row = "0, {}, 1965, 812.40, 0x{}, {}, Not Active, Not Active, {}"
+    for text in [row.format(1965, "0000000000000000", "Not Active", "Not Active"),
+                 row.format(1950, "0000000000000004", "Not Active", "Active"),
+                 row.format(1890, "0000000000000004", "Not Active", "Active"),
+                 "0, [N/A], 1965, [N/A], [N/A], [N/A], [N/A], [N/A], [N/A]"]:
+        cs.rows.append([x.strip() for x in text.split(",")])
+    s = cs.summary()
+    assert s["sm_mhz"] == 1950.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 3
+    assert s["reasons"] == ["sw_power_cap"]
+    cs.rows.append([x.strip() for x in row.format(1500, "0000000000000048", "Active", "Not Active").split(",")])
+    assert cs.summary()["reasons"] == ["hw_slowdown", "sw_power_cap"]
