@@ -566,3 +566,42 @@ def test_iterNewton_raises_divergence_on_non_finite_input(bad, device_resident):
     p.device_resident = device_resident
     with pytest.raises(Exception, match="Divergence"):
         NewtonSteps.iterNewton(p, f0, gpus, lambda *a: None)
+
+
+def test_batched_round_positions_and_rewind_follow_updateRngPos():
+    """The batched rounds draw each round's site lists ahead of the graph
+    launch (Problem.round_positions) and, after an in-graph equilibration
+    that stopped early, rewind the stream to the calls actually made
+    (position_state / set_position_state).  Host logic: the sites equal
+    those MCMCGPU.updateRngPos hands to one sampler call after another,
+    across a refill of the 1024-call block, and a rewind followed by fewer
+    calls continues exactly where that many calls end."""
+    from mi3gpu_b200.batched import Problem
+    L, q, nsteps = 5, 3, 8
+
+    def stub(seed):
+        g = FakeMCMCGPU(L, q, 32, seed=seed)
+        g.initMCMC(nsteps, 0, 2 ** 63)
+        p = Problem.__new__(Problem)
+        p.gpu, p.L, p.nsteps = g, L, nsteps
+        return p
+
+    ref = FakeMCMCGPU(L, q, 32, seed=11)
+    ref.initMCMC(nsteps, 0, 2 ** 63)
+
+    def ref_calls(n):
+        out = []
+        for _ in range(n):
+            off = ref.updateRngPos()
+            out.append(ref.bufs['randpos'][off:off + nsteps].copy())
+        return np.concatenate(out)
+
+    p = stub(11)
+    np.testing.assert_array_equal(p.round_positions(1000), ref_calls(1000))
+    st = p.position_state()
+    ahead = p.round_positions(100)  # the longest schedule; call 1025 refills the block
+    p.set_position_state(st)
+    used = p.round_positions(40)  # the calls the equilibration actually made
+    np.testing.assert_array_equal(used, ahead[:40 * nsteps])
+    np.testing.assert_array_equal(used, ref_calls(40))
+    np.testing.assert_array_equal(p.round_positions(70), ref_calls(70))  # 1110 calls in both
