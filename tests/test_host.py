@@ -605,3 +605,26 @@ def test_batched_round_positions_and_rewind_follow_updateRngPos():
     np.testing.assert_array_equal(used, ahead[:40 * nsteps])
     np.testing.assert_array_equal(used, ref_calls(40))
     np.testing.assert_array_equal(p.round_positions(70), ref_calls(70))  # 1110 calls in both
+
+
+def test_untuned_sampler_plan_dispatch():
+    """MCMCGPU.sampler_plan without tuning: the skewed-lane kernel from q=16
+    with at least one CTA of 512 walkers per SM (512 walkers per CTA while
+    L + 31 <= 288, else 256), the row kernel's built-in plan otherwise; an
+    autotuned plan overrides both."""
+    def plan(L, q, N, tuned=None):
+        g = MCMCGPU.__new__(MCMCGPU)
+        g.L, g.q, g.nseq = L, q, {'main': N}
+        if tuned:
+            g.metro_plan = tuned
+        return g.sampler_plan()
+    assert plan(232, 21, 1 << 20) == ('skew', 512)
+    assert plan(257, 21, 1 << 20) == ('skew', 512)
+    assert plan(258, 21, 1 << 20) == ('skew', 256)
+    assert plan(512, 21, 1 << 21) == ('skew', 256)
+    assert plan(546, 21, 1 << 21) == (0, 0, 0)  # L + 31 > 576
+    assert plan(232, 8, 1 << 20) == (0, 0, 0)  # q < 16
+    assert plan(232, 21, 148 * 512 - 32) == (0, 0, 0)  # fewer than one CTA per SM
+    assert plan(232, 21, (1 << 20) + 16) == (0, 0, 0)  # not a multiple of 32
+    assert plan(232, 21, 1 << 20, tuned=[512, 24, 3]) == (512, 24, 3)
+    assert plan(99, 4, 1 << 18, tuned=['skew', 768]) == ('skew', 768)
