@@ -628,3 +628,27 @@ def test_untuned_sampler_plan_dispatch():
     assert plan(232, 21, (1 << 20) + 16) == (0, 0, 0)  # not a multiple of 32
     assert plan(232, 21, 1 << 20, tuned=[512, 24, 3]) == (512, 24, 3)
     assert plan(99, 4, 1 << 18, tuned=['skew', 768]) == ('skew', 768)
+
+
+@pytest.mark.parametrize("L,q,sigma", [(48, 4, 0.5), (60, 21, 0.5), (99, 4, 0.8)])
+def test_synthetic_ground_truth_matches_its_definition(L, q, sigma):
+    """The benchmark workloads' ground truth (fields N(0,1), couplings
+    N(0, 0.05^2) plus N(0, sigma^2) on 3L distinct pairs with j - i >= 4,
+    in the reference's fieldless-even gauge): reproducible from its seed,
+    already in that gauge, and its zero-sum couplings single out exactly
+    3L strong pairs, all at least 4 sites apart."""
+    J = potts.synthetic_ground_truth(L, q, seed=1000 + L, contact_sigma=sigma)
+    assert J.dtype == np.float32 and J.shape == (L * (L - 1) // 2, q * q)
+    np.testing.assert_array_equal(J, potts.synthetic_ground_truth(L, q, seed=1000 + L, contact_sigma=sigma))
+    zeros = np.zeros((L, q))
+    h2, J2 = potts.fieldlessGaugeEven(zeros, J.astype(np.float64))
+    np.testing.assert_allclose(J2, J, atol=1e-5)  # the gauge transform is a no-op on it
+    _, J0 = potts.zeroGauge(zeros, J.astype(np.float64))
+    norm = np.sqrt((J0 ** 2).sum(axis=1))
+    # zero-sum projections: the 3L contacts (norm ~ sigma (q-1)) sit well
+    # above the background (~ 0.05 (q-1)): a gap after the 3L-th largest
+    order = np.argsort(norm)[::-1]
+    assert norm[order[3 * L - 1]] > 1.8 * norm[order[3 * L]]
+    strong = order[:3 * L]
+    i, j = potts.pair_indices(L)
+    assert (j[strong] - i[strong] >= 4).all()
