@@ -35,14 +35,6 @@ def sources():
     return sorted(str(p) for p in CSRC.glob("*.cu"))
 
 
-def needs_rebuild():
-    if not LIB.exists():
-        return True
-    t = LIB.stat().st_mtime
-    deps = list(CSRC.glob("*")) + [ROOT / "include" / "mi3b200.h"]
-    return any(p.stat().st_mtime > t for p in deps)
-
-
 def build_lib(verbose=False, extra=()):
     """Compile each source to an object in parallel, then link the library."""
     from concurrent.futures import ThreadPoolExecutor

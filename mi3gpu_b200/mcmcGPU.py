@@ -183,13 +183,6 @@ class MCMCGPU:
         self.lastevt = evt
         return evt
 
-    def _evtlist(self, evts):
-        if evts is None:
-            return []
-        if isinstance(evts, (list, tuple)):
-            return list(evts)
-        return [evts]
-
     def logProfile(self):
         """Write 'EVT name start end bytes' lines (ns, relative to the first
         profiled command) for completed commands (mcmcGPU.py:224-237)."""
