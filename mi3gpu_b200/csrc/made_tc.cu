@@ -160,22 +160,6 @@ __device__ __forceinline__ void unpack8(const uint4 w, float *f) {
 // then fall in different bank groups.
 __host__ __device__ __forceinline__ uint32_t mt_rsw(uint32_t row) { return (row >> 1) & 3; }
 
-
-
-// four single-column TMEM loads in flight together, one wait
-__device__ __forceinline__ void tmem_ld1x4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, float (&v)[4]) {
-    uint32_t r0, r1, r2, r3;
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r0) : "r"(a0));
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r1) : "r"(a1));
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r2) : "r"(a2));
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r3) : "r"(a3));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    v[0] = __uint_as_float(r0);
-    v[1] = __uint_as_float(r1);
-    v[2] = __uint_as_float(r2);
-    v[3] = __uint_as_float(r3);
-}
-
 __device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
     uint32_t r;
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
@@ -291,20 +275,6 @@ __device__ __forceinline__ float dot16(const unsigned char *row, const float *x)
 #pragma unroll
     for (uint32_t e = 0; e < 16; ++e) s[e & 3] = __fmaf_rn(f[e], x[e], s[e & 3]);
     return (s[0] + s[1]) + (s[2] + s[3]);
-}
-
-// h[k] += row[v0 + k], k < 16, for a swizzled FP32 chunk row
-__device__ __forceinline__ void add16f(const float *chunk, uint32_t rr, uint32_t v0, float *h) {
-    const float *row = chunk + rr * MT_NU;
-    const uint32_t sw = mt_rsw(rr);
-#pragma unroll
-    for (uint32_t gg = 0; gg < 4; ++gg) {
-        const float4 w = *reinterpret_cast<const float4 *>(row + 4 * ((v0 / 4 + gg) ^ sw));
-        h[4 * gg] += w.x;
-        h[4 * gg + 1] += w.y;
-        h[4 * gg + 2] += w.z;
-        h[4 * gg + 3] += w.w;
-    }
 }
 
 // h[k] += row[k], k < 16, for a 16-unit slice of a bf16 row
