@@ -652,3 +652,38 @@ def test_synthetic_ground_truth_matches_its_definition(L, q, sigma):
     strong = order[:3 * L]
     i, j = potts.pair_indices(L)
     assert (j[strong] - i[strong] >= 4).all()
+
+
+def test_profile_log_lines_in_the_reference_format(tmp_path):
+    """MCMCGPU.logProfile (mcmcGPU.py:224-237): completed commands become
+    'EVT name start end bytes' lines in ns relative to the first profiled
+    command, appended to the device's log file; commands still running stay
+    queued for the next call.  CUDA events are replaced by stand-ins with
+    the same query / elapsed_time interface."""
+    from collections import deque
+
+    class Evt:
+        def __init__(self, ms, done=True):
+            self.ms, self.done = ms, done
+
+        def query(self):
+            return self.done
+
+        def elapsed_time(self, other):
+            return other.ms - self.ms
+
+    g = MCMCGPU.__new__(MCMCGPU)
+    g.profile, g.logfn = True, str(tmp_path / "gpu-0.log")
+    t0 = Evt(10.0)
+    g._t0evt = t0
+    running = Evt(10.5, done=False)
+    g.events = deque([(t0, Evt(10.25), "mcmc", None), (Evt(10.25), Evt(10.3), "setBuf J", 4096),
+                      (Evt(10.3), running, "energies", None)])
+    assert g.logProfile() == ["EVT mcmc 0 250000 ", "EVT setBuf J 250000 300000 4096"]
+    assert len(g.events) == 1
+    running.done = True
+    assert g.logProfile() == ["EVT energies 300000 500000 "]
+    assert (tmp_path / "gpu-0.log").read_text().splitlines() == [
+        "EVT mcmc 0 250000 ", "EVT setBuf J 250000 300000 4096", "EVT energies 300000 500000 "]
+    g.profile = False
+    assert g.logProfile() is None
