@@ -28,6 +28,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=None,
                     help="reference checkout (default: $MI3_REFERENCE, else ../reference beside the repository)")
+    ap.add_argument("--out", default=str(HERE / "reference_vectors.npz"), help="output .npz")
     args = ap.parse_args()
     if args.ref is None:
         import os
@@ -110,7 +111,7 @@ def main():
     out["pc_unimarg"] = getUnimarg(ff)
     out["pc_indepF"] = indepF(ff)
 
-    dst = HERE / "reference_vectors.npz"
+    dst = Path(args.out)
     np.savez_compressed(dst, **out)
     print("wrote", dst, dst.stat().st_size, "bytes")
 

@@ -27,6 +27,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=None,
                     help="reference checkout (default: $MI3_REFERENCE, else ../reference beside the repository)")
+    ap.add_argument("--out", default=str(HERE / "hiv_bimarg_pc.npz"), help="output .npz")
     args = ap.parse_args()
     if args.ref is None:
         import os
@@ -39,7 +40,7 @@ def main():
     bim = np.load(src)
     assert bim.shape == (93 * 92 // 2, 16) and bim.dtype == np.float32, (bim.shape, bim.dtype)
     np.savez_compressed(
-        HERE / "hiv_bimarg_pc.npz",
+        Path(args.out),
         bimarg=bim,
         alpha=np.array("ABCD"),
         # recipe of examples/HIV_inference/pbs.sh (the other options are
@@ -50,7 +51,7 @@ def main():
         expect_ssr=np.float64(0.010), expect_ferr=np.float64(0.00856), expect_X=np.float64(-10.118),
         expect_Xo=np.float64(-10.878),
     )
-    print("wrote", HERE / "hiv_bimarg_pc.npz", bim.shape)
+    print("wrote", args.out, bim.shape)
 
 
 if __name__ == "__main__":

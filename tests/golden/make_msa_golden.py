@@ -26,6 +26,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=None,
                     help="reference checkout (default: $MI3_REFERENCE, else ../reference beside the repository)")
+    ap.add_argument("--out", default=str(HERE / "msa_vectors.npz"), help="output .npz")
     args = ap.parse_args()
     if args.ref is None:
         import os
@@ -105,8 +106,8 @@ def main():
     load_case("nuc", b"".join(bytes(b"ACGT"[c] for c in s) + b"\n" for s in nuc), alpha="ACGT")
     load_case("bz2", bz2.compress(body))
 
-    np.savez_compressed(HERE / "msa_vectors.npz", **out)
-    print("wrote", HERE / "msa_vectors.npz", len(out), "arrays")
+    np.savez_compressed(Path(args.out), **out)
+    print("wrote", args.out, len(out), "arrays")
 
 
 if __name__ == "__main__":

@@ -19,6 +19,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=None,
                     help="reference checkout (default: $MI3_REFERENCE, else ../reference beside the repository)")
+    ap.add_argument("--out", default=str(HERE / "validate_vectors.npz"), help="output .npz")
     args = ap.parse_args()
     if args.ref is None:
         import os
@@ -62,7 +63,7 @@ def main():
             out[f"{tag}_msg"] = np.array("")
         except ValueError as e:
             out[f"{tag}_msg"] = np.array(str(e))
-    np.savez_compressed(HERE / "validate_vectors.npz", **out)
+    np.savez_compressed(Path(args.out), **out)
     for tag in cases:
         print(tag, repr(str(out[f"{tag}_msg"])))
 

@@ -299,3 +299,40 @@ def test_fp64_energies_against_32_digit_sums():
         terms = J[np.arange(len(i)), q * s[i] + s[j]]
         exact = mpmath.fsum(mpmath.mpf(float(t)) for t in terms)
         assert abs(E[k] - float(exact)) <= 1e-12 * max(1.0, abs(float(exact)))
+
+
+def _reference_checkout():
+    import os
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    cand = Path(os.environ.get("MI3_REFERENCE") or root.parent / "reference")
+    return cand if (cand / "mi3gpu").is_dir() else None
+
+
+@pytest.mark.parametrize("script,fixture", [("make_golden.py", "reference_vectors.npz"),
+                                            ("make_msa_golden.py", "msa_vectors.npz"),
+                                            ("make_validate_golden.py", "validate_vectors.npz"),
+                                            ("make_hiv_fixture.py", "hiv_bimarg_pc.npz")])
+def test_golden_fixtures_regenerate_from_the_reference(tmp_path, script, fixture):
+    """Where the reference checkout is present, each committed fixture is
+    exactly what its committed script makes from the reference's own code
+    (its numpy utilities, seqload, MWC64X source compiled as C++, the HIV
+    example's target).  Skipped elsewhere: every other test reads only the
+    committed .npz files."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    ref = _reference_checkout()
+    if ref is None:
+        pytest.skip("reference checkout not present")
+    root = Path(__file__).resolve().parents[1]
+    if script == "make_golden.py" and not (root / "oracle" / "_ref" / "libmwc64x_ref.so").exists():
+        pytest.skip("oracle/_ref not built")
+    out = tmp_path / fixture
+    p = subprocess.run([sys.executable, str(root / "tests" / "golden" / script), "--ref", str(ref), "--out", str(out)],
+                       capture_output=True, text=True, timeout=600, cwd=root)
+    assert p.returncode == 0, p.stderr[-2000:]
+    a, b = np.load(out), np.load(root / "tests" / "golden" / fixture)
+    assert sorted(a.files) == sorted(b.files)
+    for k in a.files:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
