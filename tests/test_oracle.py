@@ -336,3 +336,63 @@ def test_golden_fixtures_regenerate_from_the_reference(tmp_path, script, fixture
     assert sorted(a.files) == sorted(b.files)
     for k in a.files:
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+def test_oracle_and_reference_cpu_samplers_match_exact_bimarginals():
+    """The oracle's restatement of the metropolis kernel (bit-exact with the
+    B200 samplers in the GPU tests) and the reference's own CPU sampler
+    (extras/mcmcCPUgenThreaded.c, 16 chains) both sample the Boltzmann
+    distribution: at L=8, q=3 all 3^8 states are weighted exactly; 4096
+    oracle walkers after 60 sweeps, and 4096 reference samples, have
+    bimarginals within the finite-sample error sum f(1 - f)/N of the exact
+    ones and of each other.  The reference sampler's step adds the diagonal
+    blocks of its coupling matrix, which it never writes
+    (mcmcCPUgenThreaded.c:75-78, :194); MALLOC_PERTURB_ gives that memory one
+    byte pattern, whose difference in dE is exactly 0, where leftover heap
+    content would bias small models like this one."""
+    import os
+    import subprocess
+    import tempfile
+    from pathlib import Path
+    L, q, N, sweeps = 8, 3, 4096, 60
+    rng = np.random.default_rng(88)
+    J = rng.normal(0, 0.45, size=(L * (L - 1) // 2, q * q)).astype("<f4")
+    i, j = np.triu_indices(L, 1)
+    idx = np.arange(q ** L)
+    S = np.stack([(idx // q ** (L - 1 - k)) % q for k in range(L)], axis=1)
+    E = sum(J[p].astype(np.float64)[S[:, i[p]] * q + S[:, j[p]]] for p in range(len(i)))
+    w = np.exp(-(E - E.min()))
+    w /= w.sum()
+    f = np.stack([np.bincount(S[:, a] * q + S[:, b], weights=w, minlength=q * q) for a, b in zip(i, j)])
+
+    def bimarg(seqs):
+        return np.stack([np.bincount(seqs[:, a] * q + seqs[:, b], minlength=q * q) / len(seqs)
+                         for a, b in zip(i, j)])
+
+    mem = oracle.pack_seqs(rng.integers(0, q, size=(N, L)).astype("<u1"))
+    st = oracle.init_rng(N, 0, 2 ** 63 // (2 * N))
+    pos = rng.integers(0, L, size=sweeps * L).astype("<u4")
+    oracle.metropolis(J, st, pos, 0, sweeps * L, mem, L, q)
+    f_or = bimarg(oracle.unpack_seqs(mem, L).astype(np.int64))
+    exp_or = float(np.sum(f * (1 - f)) / N)
+    assert np.sum((f_or - f) ** 2) < 1.5 * exp_or
+
+    exe = oracle.ref_cpu_binary()
+    if exe is None:
+        pytest.skip("reference CPU sampler not built (oracle/_ref)")
+    alpha, burn, keep = "ABC", 4, 256
+    env = dict(os.environ, MALLOC_PERTURB_="165")
+    outs = []
+    with tempfile.TemporaryDirectory() as td:
+        jf = Path(td) / "J.dat"
+        J.tofile(jf)
+        for _ in range(16):
+            start = "".join(alpha[k] for k in rng.integers(0, q, size=L))
+            r = subprocess.run([str(exe), str(jf), str(10 * L), str(burn + keep), alpha, start], check=True,
+                               capture_output=True, text=True, env=env)
+            outs.append(np.array([[alpha.index(c) for c in ln] for ln in r.stdout.split()[burn:]]))
+    seqs_ref = np.concatenate(outs)
+    f_ref = bimarg(seqs_ref)
+    exp_ref = float(np.sum(f * (1 - f)) / len(seqs_ref))
+    assert np.sum((f_ref - f) ** 2) < 3.0 * exp_ref  # samples 10 sweeps apart within a chain
+    assert np.sum((f_or - f_ref) ** 2) < 3.0 * exp_ref + 1.5 * exp_or
